@@ -1,0 +1,396 @@
+"""Benchmark: items placed per second, 240x123x100 tray, 24 orientations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (config 3 of the benchmark set): a 240x123x100 int32 tray, 350 seeded
+synthetic items of largest extent 20-50 voxels (superellipsoids, tori, U/L
+hooks; psacking_b200.workloads), all 24 orientations, interlocking-free
+placement, greedy in descending volume order.  One step = one whole packing
+run of the 350 items into an empty tray.
+
+ours      value: the device-resident loop (psb_pack_staged) with the items
+          already staged in HBM, timed with CUDA events on the engine's
+          stream, L2 flushed (256 MiB write) before every step.
+          e2e:   BinPacker.pack_voxels on host numpy arrays through the same
+          C ABI, host->device item upload and device->host tray readback
+          inside the timed region.
+reference the reference's CPU implementation of the path, restated by the
+          oracle (oracle/psb_oracle.py; the reference's own CPU path needs
+          FFTW3, absent on this image), on all host cores; each step is one
+          item (24 orientations, interlocking-free) searched and placed on a
+          tray that already holds the first item.
+Multi-GPU (torchrun): every rank packs its own independent tray of its own
+item stream (no data-path collective); value = items placed on all ranks /
+max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "items placed/s at 240x123x100, 24 orientations"
+UNIT = "items/s"
+N_ITEMS = 350
+TRAY = (240, 123, 100)
+N_ORIENT = 24
+
+
+class PsbResult(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_int32), ("y", ctypes.c_int32), ("z", ctypes.c_int32), ("found", ctypes.c_int32),
+                ("score", ctypes.c_double), ("orientation", ctypes.c_int32), ("diag", ctypes.c_uint32),
+                ("n_candidates", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+def load_lib():
+    lib = ctypes.CDLL(str(ROOT / "psacking_b200" / "libpsb200.so"))
+    lib.psb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    return lib
+
+
+def check(lib, st):
+    if st != 0:
+        buf = ctypes.create_string_buffer(2048)
+        lib.psb_last_error(buf, 2048)
+        raise RuntimeError(f"psb error {st}: {buf.value.decode()}")
+
+
+def parse_profile(lib):
+    buf = ctypes.create_string_buffer(1 << 16)
+    check(lib, lib.psb_profile_report(buf, 1 << 16))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, n, ms = line.split()
+        out[name] = (int(n), float(ms))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(rank):
+    from psacking_b200 import workloads
+    return workloads.config3_items(seed=1 + 1000 * rank, n=N_ITEMS)
+
+
+def sorted_items(items):
+    vols = [int(np.sum(i > 0)) for i in items]
+    return [np.ascontiguousarray(items[i].astype(np.int32)) for i in np.argsort(vols)[::-1]]
+
+
+def algorithmic_bytes(seq, maps, F):
+    """Bytes the two dominant kernels must move, summed over the run, from the
+    item shapes (every item is searched once in all orientations that fit).
+      k_xpass per orientation: read both tray half spectra (2*Fx*Fy*Hz*8 B),
+        read the item's z,y-transformed columns (ex*Fy*Hz*8), write the two
+        products for the valid planes (2*Xv*Fy*Hz*8).
+      k_plane per orientation: read both products (2*Xv*Fy*Hz*8), write the
+        proximity field and free bits of the valid box (Xv*Yv*Zv*4 + bits)."""
+    from psacking_b200.rotations import apply_map
+    Fx, Fy, Fz = F
+    Hz = Fz // 2 + 1
+    xb = pb = 0
+    nor = 0
+    for it in seq:
+        idx = np.argwhere(it > 0)
+        for row in maps:
+            o = apply_map(it, row)
+            if any(o.shape[a] > TRAY[a] for a in range(3)):
+                continue
+            oi = np.argwhere(o > 0)
+            hi = oi.max(axis=0)
+            Xv, Yv, Zv = (TRAY[a] - hi[a] for a in range(3))
+            xb += 2 * Fx * Fy * Hz * 8 + o.shape[0] * Fy * Hz * 8 + 2 * Xv * Fy * Hz * 8
+            pb += 2 * Xv * Fy * Hz * 8 + Xv * Yv * Zv * 4 + Xv * TRAY[1] * ((TRAY[2] + 31) // 32) * 4
+            nor += 1
+    return {"k_xpass": xb, "k_plane": pb, "orientations": nor}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import psacking_b200  # noqa: F401  (fails loudly without the extension)
+    from psacking_b200 import BinPacker
+    from psacking_b200.rotations import orientation_maps
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = load_lib()
+    items = workload(rank)
+    seq = sorted_items(items)
+    maps = orientation_maps(N_ORIENT)
+    tray0 = np.zeros(TRAY, np.int32)
+
+    t = ctypes.c_void_p()
+    check(lib, lib.psb_tray_create(*TRAY, ctypes.byref(t)))
+    ptrs = (ctypes.POINTER(ctypes.c_int32) * len(seq))(*[s.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) for s in seq])
+    dims = np.array([s.shape for s in seq], np.int32).ravel()
+    check(lib, lib.psb_pack_stage(t, ptrs, dims.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(seq)))
+    stream_p = ctypes.c_void_p()
+    check(lib, lib.psb_tray_stream(t, ctypes.byref(stream_p)))
+    stream = torch.cuda.ExternalStream(stream_p.value, device=dev)
+    res = (PsbResult * len(seq))()
+    maps_c = np.ascontiguousarray(maps, np.int32)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def one_step(timed):
+        check(lib, lib.psb_tray_set(t, tray0.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), None))
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        check(lib, lib.psb_pack_staged(t, maps_c.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), N_ORIENT, 1, 0,
+                                       res, None))
+        b.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return a.elapsed_time(b)
+
+    for _ in range(args.warmup):
+        one_step(False)
+    placed_first = [(r.found, r.x, r.y, r.z, r.orientation) for r in res]
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    lib.psb_profile_enable(1)
+    ms = [one_step(True) for _ in range(args.steps)]
+    prof = parse_profile(lib)
+    lib.psb_profile_enable(0)
+    clk = clocks.stop()
+    placed = sum(1 for r in res if r.found)
+    diag = 0
+    for r in res:
+        diag |= r.diag
+    same = placed_first == [(r.found, r.x, r.y, r.z, r.orientation) for r in res]
+    total_ms = sum(ms)
+    Fdims = (ctypes.c_int * 3)()
+    check(lib, lib.psb_tray_fft_dims(t, Fdims))
+    F = tuple(Fdims)
+
+    # e2e through the public API: host numpy in, host numpy out
+    packer = BinPacker(TRAY, num_orientations=N_ORIENT, interlocking_free=True)
+    e2e_ms = []
+    for i in range(max(1, min(args.steps, 2)) + 1):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = packer.pack_voxels(items)
+        b.record()
+        torch.cuda.synchronize()
+        barrier()
+        if i > 0:  # first call is a warm-up of the public path
+            e2e_ms.append(a.elapsed_time(b))
+    e2e_placed = r.num_placed
+    h2d = sum(s.nbytes for s in seq) + sum(int(np.count_nonzero(s)) * 16 for s in seq) + tray0.nbytes
+    d2h = tray0.nbytes + len(seq) * 40
+    check(lib, lib.psb_tray_destroy(t))
+
+    # max over ranks
+    if world > 1:
+        vec = torch.tensor([total_ms, statistics.mean(e2e_ms)], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(vec, op=torch.distributed.ReduceOp.MAX)
+        cnt = torch.tensor([placed, e2e_placed], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(cnt, op=torch.distributed.ReduceOp.SUM)
+        total_ms, e2e_mean = float(vec[0]), float(vec[1])
+        placed_all, e2e_placed_all = float(cnt[0]), float(cnt[1])
+    else:
+        e2e_mean = statistics.mean(e2e_ms)
+        placed_all, e2e_placed_all = placed, e2e_placed
+    if rank != 0:
+        return None
+    value = placed_all * args.steps / (total_ms / 1e3)
+    e2e_value = e2e_placed_all / (e2e_mean / 1e3)
+
+    # roofline of the dominant kernel
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    ab = algorithmic_bytes(seq, maps, F)
+    dom = max((k for k in prof if k in ("k_xpass", "k_plane")), key=lambda k: prof[k][1], default=None)
+    top = max(prof, key=lambda k: prof[k][1]) if prof else None
+    roof = None
+    if dom:
+        n_l, ms_l = prof[dom]
+        per_launch_bytes = ab[dom] / (n_l / args.steps)
+        achieved = per_launch_bytes / (ms_l / n_l / 1e3) / 1e9
+        traffic = None
+        tf = ROOT / "profiles" / f"{dom}_traffic.json"
+        if tf.exists():
+            traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+        roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": int(per_launch_bytes), "avg_launch_ms": ms_l / n_l}
+    launches = sum(v[0] for v in prof.values())
+    share = {k: round(v[1] / max(1e-9, sum(x[1] for x in prof.values())), 4) for k, v in prof.items()}
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FFT), i64/f64 (exact tie guard)",
+        "data": "synthetic (seeded config-3 shapes; Thingi10K unavailable)",
+        "config": {"workload": "config3: 240x123x100 tray, 350 items (extent 20-50), 24 orientations, "
+                               "interlocking-free, K=1 (no lookahead yet)",
+                   "items_per_step": len(seq), "items_placed_per_step": placed, "orientations_per_step": ab["orientations"],
+                   "l2": "256 MiB buffer written before every step", "parallelism": f"replicas x{world} (independent trays)",
+                   "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag},
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_mean, 3),
+                "placements_match_value_leg": e2e_placed == placed},
+        "gpu_launches": int(launches // args.steps * args.steps),
+        "kernel_share": share, "top_kernel": top,
+        "roofline": roof,
+        "clocks": clk,
+    }
+    return out
+
+
+def cpu_sample_setup():
+    """The bounded CPU sample: the tray after the first item of the workload is
+    placed, and the second item (24 orientations, interlocking-free)."""
+    from oracle import psb_oracle as O
+    items = sorted_items(workload(0))
+    tray = np.zeros(TRAY, np.int32)
+    tray, _ = O.pack_voxels([items[0]], TRAY, N_ORIENT, True, False)
+    return items[1], tray
+
+
+def time_cpu_sample(item, tray):
+    from oracle import psb_oracle as O
+    t0 = time.perf_counter()
+    tray2, pl = O.pack_voxels([item], TRAY, N_ORIENT, True, False, initial_tray=tray)
+    dt = time.perf_counter() - t0
+    return dt, sum(1 for p in pl if p["success"])
+
+
+def run_reference(args):
+    item, tray = cpu_sample_setup()
+    for _ in range(args.warmup):
+        time_cpu_sample(item, tray)
+    tot, placed = 0.0, 0
+    for _ in range(args.steps):
+        dt, n = time_cpu_sample(item, tray)
+        tot += dt
+        placed += n
+    v = placed / tot
+    cores = os.cpu_count()
+    cb = {"value": round(v, 5), "unit": UNIT, "cores": cores, "kind": "port",
+          "sample": "1 item (2nd of the config-3 stream) searched in 24 orientations with the interlocking "
+                    "flood fill and placed, tray holding the 1st item; FP64 FFTs on all host cores"}
+    return {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * tot / args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/i64",
+            "data": "synthetic", "config": {"workload": "config3 sample (see cpu_baseline.sample)"},
+            "cpu_baseline": cb, "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    out = run_ours(args, rank, world, local_rank)
+    if rank == 0 and out is not None:
+        if world == 1 and not args.no_cpu_baseline:
+            item, tray = cpu_sample_setup()
+            dt, n = time_cpu_sample(item, tray)
+            out["cpu_baseline"] = {"value": round(n / dt, 5), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                   "sample": "1 item (2nd of the config-3 stream), 24 orientations, "
+                                             "interlocking flood fill, placed; oracle FP64 FFTs on all host cores"}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,175 @@
+/*
+ * psb200.h — C ABI of the B200 placement-search engine for spectral 3D packing.
+ *
+ * Every entry point takes plain host pointers and sizes, returns an int status
+ * (PSB_OK == 0) and never throws.  On failure psb_last_error() gives a message.
+ * Voxel grids are int32, row-major, element (i,j,k) at [(i*ny + j)*nz + k]
+ * (the reference's FlatVoxelGrid layout, spectral_packing/types.h:24-38).
+ *
+ * Each function below names the reference symbol it replaces.  The pybind11
+ * module psacking_b200._core binds them under the reference's Python names
+ * (spectral_packing/bindings.cpp:654-930).
+ */
+#ifndef PSB200_H
+#define PSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PSB_OK            0
+#define PSB_ERR_ARG       1  /* bad shape, size or pointer                     */
+#define PSB_ERR_CUDA      2  /* a CUDA runtime call failed (message has it)    */
+#define PSB_ERR_STATE     3  /* context missing / not initialised             */
+#define PSB_ERR_OVERLAP   4  /* place_in_tray: item intersects tray contents   */
+#define PSB_ERR_LIMIT     5  /* a device-side iteration or capacity limit hit  */
+#define PSB_ERR_NODEVICE  6  /* no CUDA device visible                         */
+
+/* ---- search modes -------------------------------------------------------
+ * PSB_MODE_SCAN : the single-call CPU-scored search, packing.cpp:590-642.
+ *   score = prox + 1e8*pow(k/nz, 3); ties -> lowest linear index;
+ *   found iff best < 1e9 (constants.h INF).
+ * PSB_MODE_BLOCK: the GPU-context search, fft3.cu:147-175 + 527-563 + 1330-1372.
+ *   score = fma((1e8*qz)*qz, qz, prox), qz = k/nz; ties -> lowest 256-block,
+ *   then lowest bit-reversed 8-bit offset inside the block; found iff < 1e29.
+ * PSB_FLAG_INTERLOCK: only positions reachable from the exit faces by the
+ *   Algorithm-3 flood fill count (fft3.cu:234-455, 1377-1459).            */
+#define PSB_MODE_SCAN      0
+#define PSB_MODE_BLOCK     1
+#define PSB_FLAG_INTERLOCK 0x10
+
+/* diagnostic bits in psb_result.diag */
+#define PSB_DIAG_EXACT_RESCORE   0x1  /* FP32 error bound >= 0.5: candidates re-scored exactly */
+#define PSB_DIAG_AMBIGUOUS_COLL  0x2  /* a collision value fell near a rounding boundary      */
+#define PSB_DIAG_FALSE_FREE      0x4  /* exact re-check rejected an FP32 "free" candidate      */
+#define PSB_DIAG_BOUND_EXCEEDED  0x8  /* observed FP32 error exceeded half the error bound     */
+
+typedef struct psb_result {
+    int32_t x, y, z;       /* placement of the item array origin, or -1,-1,-1      */
+    int32_t found;         /* 1 when a valid placement exists                       */
+    double  score;         /* reference score of the placement (0.0 when not found) */
+    int32_t orientation;   /* index into the orientation list, -1 when not found    */
+    uint32_t diag;         /* PSB_DIAG_* bits                                       */
+    int32_t n_candidates;  /* candidates examined by the exact tie guard             */
+    int32_t reserved;
+} psb_result;
+
+typedef struct psb_tray psb_tray;   /* a device-resident tray (GPUTrayContext) */
+
+/* ---- library ------------------------------------------------------------ */
+const char* psb_version(void);
+/* Copies the calling thread's last error message into buf (NUL-terminated). */
+int psb_last_error(char* buf, size_t len);
+/* Number of visible CUDA devices (0 without a GPU; never an error). */
+int psb_device_count(int* n);
+
+/* ---- stateless reference entry points ---------------------------------- */
+
+/* dft_conv3 (fft3.cu:643-715 / packing.cpp:162-213): linear 3-D convolution of
+ * two same-shape grids, truncated to that shape, rounded to int32. */
+int psb_dft_conv3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, int32_t* out);
+
+/* dft_corr3 (packing.cpp:215-229): out[t] = sum_x b[x] * a[t+x], a zero outside. */
+int psb_dft_corr3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, int32_t* out);
+
+/* collision_grid (packing.cpp:241-252, binding bindings.cpp:360-372): the item
+ * is zero-padded to the tray shape; out = dft_corr3(tray, item) with positions
+ * where the item would leave the tray raised to at least 1. */
+int psb_collision_grid(const int32_t* tray, int nx, int ny, int nz,
+                       const int32_t* item, int ex, int ey, int ez, int32_t* out);
+
+/* calculate_distance (fft3.cu:944-1004): L1 distance to voxels equal to 1;
+ * nx+ny+nz+10 everywhere when there is none. */
+int psb_calculate_distance(const int32_t* grid, int nx, int ny, int nz, int32_t* out);
+
+/* interlocking_free_positions (bindings.cpp:561-648 + fft3.cu:348-402):
+ * 1 where the object can be placed and slid out of the tray, else 0. */
+int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
+                                    const int32_t* obj, int ex, int ey, int ez,
+                                    int32_t* out);
+
+/* fft_search_placement (packing.cpp:590-642, binding bindings.cpp:182-203):
+ * distance field from the tray, then a PSB_MODE_SCAN search. */
+int psb_fft_search_placement(const int32_t* item, int ex, int ey, int ez,
+                             const int32_t* tray, int nx, int ny, int nz,
+                             psb_result* out);
+
+/* place_in_tray (packing.cpp:773-788, binding bindings.cpp:259-276): out_tray
+ * receives a copy of tray with item voxels (>0) written as item_id at pos.
+ * PSB_ERR_OVERLAP when an item voxel meets an occupied voxel; overlap_ijk
+ * (may be NULL) then gets the first such tray cell in row-major order. */
+int psb_place_in_tray(const int32_t* item, int ex, int ey, int ez,
+                      const int32_t* tray, int nx, int ny, int nz,
+                      int px, int py, int pz, int32_t item_id,
+                      int32_t* out_tray, int32_t* overlap_ijk);
+
+/* ---- device-resident tray (GPUTrayContext, fft3.cu:1040-1502) ----------- */
+
+int psb_tray_create(int nx, int ny, int nz, psb_tray** out);
+int psb_tray_destroy(psb_tray* t);
+int psb_tray_dims(const psb_tray* t, int* nx, int* ny, int* nz);
+
+/* gpu_tray_context_init (fft3.cu:1106-1175): upload the tray and its distance
+ * field and build both spectra.  phi == NULL computes the distance field on
+ * the device from the tray. */
+int psb_tray_set(psb_tray* t, const int32_t* tray, const int32_t* phi);
+
+/* Copy the device tray / distance field back to the host. */
+int psb_tray_get(psb_tray* t, int32_t* tray, int32_t* phi);
+
+/* fft_search_batch / fft_search_batch_interlocking_free / gpu_tray_search
+ * (fft3.cu:1506-1632): search n orientation arrays against the tray.
+ * items[o] points at an (dims[3o],dims[3o+1],dims[3o+2]) grid.  Orientations
+ * larger than the tray are skipped.  per_orient (may be NULL) receives each
+ * orientation's own best; out receives the best over orientations (strict <,
+ * first wins) with out->orientation its index. */
+int psb_tray_search(psb_tray* t, const int32_t* const* items, const int32_t* dims,
+                    int n, int mode_flags, psb_result* out, psb_result* per_orient);
+
+/* Device-side place (packing.cpp:773-788) on the resident tray, followed by the
+ * spectrum update (and the distance-field update when a voxel equal to 1 was
+ * written).  Rejects overlaps with PSB_ERR_OVERLAP and leaves the tray intact. */
+int psb_tray_place(psb_tray* t, const int32_t* item, int ex, int ey, int ez,
+                   int px, int py, int pz, int32_t item_id);
+
+/* ---- device-resident greedy packing loop (BinPacker.pack_voxels,
+ *      spectral_packer/packer.py:366-544) ------------------------------------
+ * items are already in packing order.  Orientations are generated on the
+ * device from each item by the signed axis permutations in orient_maps
+ * (n_orient entries of 6 ints: src_axis[3], flip[3]), which the caller derives
+ * from its orientation function.  Mode selection follows packer.py:
+ * interlock != 0 -> batch interlocking-free search (PSB_MODE_BLOCK);
+ * n_orient > 1   -> per-orientation cached search (PSB_MODE_BLOCK);
+ * otherwise      -> fft_search_placement (PSB_MODE_SCAN).
+ * out_placements gets one psb_result per item (orientation = index into the
+ * orientation list).  Item k is written with id_offset + (number placed
+ * before it) + 1.  The final tray is copied to final_tray when not NULL. */
+int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items,
+             const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
+             psb_result* out_placements, int32_t* final_tray);
+
+/* psb_pack split in two: stage the items of a run on the device once (their
+ * voxel lists and bounds are computed here), then run the greedy loop over the
+ * staged items.  psb_pack == psb_pack_stage + psb_pack_staged. */
+int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items);
+int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
+                    psb_result* out_placements, int32_t* final_tray);
+
+/* ---- tracing (the reference's SCOPED_TIMER, spectral_packing/timing.h:11-31,
+ *      as CUDA events around every kernel launch; off by default) ---------- */
+int psb_profile_enable(int on);          /* clears previous records            */
+/* "name launches total_ms" lines, one per kernel, after synchronising. */
+int psb_profile_report(char* buf, size_t len);
+/* FFT grid of a tray (F[0..2] >= nx, ny, nz; 2^a 3^b 5^c 7^d). */
+int psb_tray_fft_dims(const psb_tray* t, int* F);
+/* The CUDA stream (cudaStream_t) a tray's kernels run on. */
+int psb_tray_stream(psb_tray* t, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSB200_H */

@@ -1,0 +1,67 @@
+"""psacking_b200 — B200-native placement search for spectral 3D packing.
+
+A drop-in for the hot path of Vrroom/psacking: the module `_core` exposes the
+reference's `spectral_packer._core` functions (spectral_packing/bindings.cpp:
+654-930) on hand-written sm_100a kernels behind the C ABI in include/psb200.h;
+`BinPacker` mirrors spectral_packer.packer.BinPacker.
+
+The extension is required: importing this package without the built
+libpsb200.so / _core module raises ImportError (run psacking_b200.build).
+"""
+from __future__ import annotations
+
+try:
+    from . import _core
+except ImportError as e:  # fail loudly: there is no CPU fallback
+    raise ImportError(
+        "psacking_b200._core is not built (python -m psacking_b200.build): " + str(e)) from e
+
+from ._core import (  # noqa: E402
+    HEIGHT_PENALTY,
+    VOXEL_RESOLUTION,
+    calculate_distance,
+    collision_grid,
+    dft_conv3,
+    dft_corr3,
+    fft_search_batch,
+    fft_search_batch_interlocking_free,
+    fft_search_placement,
+    fft_search_placement_with_cache,
+    get_bounds,
+    gpu_tray_cleanup,
+    gpu_tray_init,
+    gpu_tray_is_initialized,
+    gpu_tray_search,
+    interlocking_free_positions,
+    make_tight,
+    place_in_tray,
+)
+from .packer import BinPacker, PackingResult, PlacementInfo  # noqa: E402
+from .rotations import (  # noqa: E402
+    get_24_orientations,
+    get_orientations,
+    orientation_maps,
+    rotate_90_x,
+    rotate_90_y,
+    rotate_90_z,
+)
+from .vox import save_vox  # noqa: E402
+
+__version__ = _core.__version__
+
+
+def voxelize_stl(path, resolution: int = VOXEL_RESOLUTION):
+    """The reference's mesh voxelizer (bindings.cpp:285-302) is upstream of the
+    placement search and not part of this engine."""
+    raise NotImplementedError("voxelize_stl: mesh voxelization is outside this engine")
+
+
+__all__ = [
+    "BinPacker", "PackingResult", "PlacementInfo", "HEIGHT_PENALTY", "VOXEL_RESOLUTION",
+    "calculate_distance", "collision_grid", "dft_conv3", "dft_corr3", "fft_search_batch",
+    "fft_search_batch_interlocking_free", "fft_search_placement", "fft_search_placement_with_cache",
+    "get_bounds", "gpu_tray_cleanup", "gpu_tray_init", "gpu_tray_is_initialized", "gpu_tray_search",
+    "interlocking_free_positions", "make_tight", "place_in_tray", "save_vox", "voxelize_stl",
+    "get_orientations", "get_24_orientations", "orientation_maps", "rotate_90_x", "rotate_90_y",
+    "rotate_90_z",
+]

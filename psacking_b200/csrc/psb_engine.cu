@@ -1,0 +1,1372 @@
+// psb_engine.cu — host side of the B200 placement-search engine and its C ABI.
+//
+// A psb_tray is the device-resident tray context (the reference's
+// GPUTrayContext, spectral_packing/fft3.cu:1040-1460): tray, distance field,
+// their half spectra, and per-orientation work buffers so that every
+// orientation of a batch is searched by the same kernel launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/psb200.h"
+#include "psb_kernels2.cuh"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(PSB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                 \
+    } while (0)
+
+#define CKL()                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(PSB_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                 \
+    } while (0)
+
+#define TRY(x)                 \
+    do {                       \
+        int r_ = (x);          \
+        if (r_ != PSB_OK) return r_; \
+    } while (0)
+
+constexpr double kP = 100000000.0;  // constants.h:7
+constexpr int kMaxSmem = 227 * 1024;
+constexpr int kCandCap = 1 << 18;
+
+int ensure_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(PSB_ERR_NODEVICE, "no CUDA device visible (%s)", cudaGetErrorString(e));
+    }
+    return PSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-launch CUDA-event profiler (psb_profile_*): off by default
+// ---------------------------------------------------------------------------
+struct ProfRec {
+    const char* name;
+    cudaEvent_t a, b;
+};
+struct Profiler {
+    bool on = false;
+    std::vector<ProfRec> recs;
+    std::vector<cudaEvent_t> pool;
+    std::mutex mu;
+    cudaEvent_t get() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+};
+Profiler g_prof;
+
+struct ProfScope {
+    int idx = -1;
+    cudaStream_t st;
+    ProfScope(const char* name, cudaStream_t s) : st(s) {
+        if (!g_prof.on) return;
+        std::lock_guard<std::mutex> lk(g_prof.mu);
+        ProfRec r{name, g_prof.get(), g_prof.get()};
+        cudaEventRecord(r.a, st);
+        g_prof.recs.push_back(r);
+        idx = (int)g_prof.recs.size() - 1;
+    }
+    ~ProfScope() {
+        if (idx < 0) return;
+        std::lock_guard<std::mutex> lk(g_prof.mu);
+        cudaEventRecord(g_prof.recs[idx].b, st);
+    }
+};
+#define PSB_CAT2(a, b) a##b
+#define PSB_CAT(a, b) PSB_CAT2(a, b)
+#define PROF(name, stream) ProfScope PSB_CAT(prof_, __LINE__)(name, stream)
+
+// ---------------------------------------------------------------------------
+// FFT plans: lengths with factors 2,3,5,7 up to PSB_MAX_FFT
+// ---------------------------------------------------------------------------
+bool factorize(int n, AxisPlan* p) {
+    p->n = n;
+    p->nstages = 0;
+    int m = n;
+    auto push = [&](int r) {
+        if (p->nstages >= PSB_MAX_STAGES) return false;
+        p->radix[p->nstages++] = r;
+        m /= r;
+        return true;
+    };
+    while (m % 8 == 0) if (!push(8)) return false;
+    while (m % 4 == 0) if (!push(4)) return false;
+    while (m % 2 == 0) if (!push(2)) return false;
+    while (m % 3 == 0) if (!push(3)) return false;
+    while (m % 5 == 0) if (!push(5)) return false;
+    while (m % 7 == 0) if (!push(7)) return false;
+    return m == 1;
+}
+
+int fft_len(int n) {
+    for (int m = std::max(n, 1); m <= PSB_MAX_FFT; ++m) {
+        AxisPlan p;
+        if (factorize(m, &p)) return m;
+    }
+    return -1;
+}
+
+struct Plan1D {
+    AxisPlan p;
+    float2* tw = nullptr;
+};
+
+std::mutex g_plan_mu;
+std::map<std::pair<int, int>, Plan1D> g_plans;  // (device, n) -> plan
+
+int get_plan(int n, Plan1D* out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_plans.find({dev, n});
+    if (it != g_plans.end()) { *out = it->second; return PSB_OK; }
+    Plan1D pl;
+    if (!factorize(n, &pl.p)) return fail(PSB_ERR_ARG, "FFT length %d is not 7-smooth", n);
+    std::vector<float2> tw(n);
+    for (int i = 0; i < n; ++i) {
+        double a = -2.0 * M_PI * (double)i / (double)n;
+        tw[i] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    CK(cudaMalloc(&pl.tw, sizeof(float2) * n));
+    CK(cudaMemcpy(pl.tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+    g_plans[{dev, n}] = pl;
+    *out = pl;
+    return PSB_OK;
+}
+
+int set_smem_attrs() {
+    static bool done[64] = {false};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 64 && done[dev]) return PSB_OK;
+    CK(cudaFuncSetAttribute(k_rfft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    CK(cudaFuncSetAttribute(k_irfft_z_int, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    CK(cudaFuncSetAttribute(k_fft_mid<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    CK(cudaFuncSetAttribute(k_fft_mid<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    CK(cudaFuncSetAttribute(k_xpass, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    CK(cudaFuncSetAttribute(k_plane, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    CK(cudaFuncSetAttribute(k_dist_axis, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    if (dev < 64) done[dev] = true;
+    return PSB_OK;
+}
+
+template <class T>
+int dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc((void**)p, sizeof(T) * n));
+    return PSB_OK;
+}
+
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+int grid1d(size_t n, int block = 256) {
+    size_t g = (n + block - 1) / block;
+    return (int)std::max<size_t>(1, std::min<size_t>(g, 148 * 32));
+}
+
+// ---------------------------------------------------------------------------
+// real 3-D transforms on an (n0,n1,n2) grid with FFT dims (F0,F1,F2)
+// ---------------------------------------------------------------------------
+struct Grid3 {
+    int n[3];
+    int F[3];
+    int H;  // F2/2 + 1
+    Plan1D p[3];
+};
+
+int make_grid3(int nx, int ny, int nz, bool linear, Grid3* g) {
+    g->n[0] = nx; g->n[1] = ny; g->n[2] = nz;
+    for (int a = 0; a < 3; ++a) {
+        int want = linear ? 2 * g->n[a] - 1 : g->n[a];
+        g->F[a] = fft_len(want);
+        if (g->F[a] < 0)
+            return fail(PSB_ERR_ARG, "axis %d of length %d needs an FFT longer than %d", a, g->n[a], PSB_MAX_FFT);
+        TRY(get_plan(g->F[a], &g->p[a]));
+    }
+    g->H = g->F[2] / 2 + 1;
+    return PSB_OK;
+}
+
+size_t smem_rz(int N) { return sizeof(float2) * (N + 2 * PSB_PAIRS * N); }
+size_t smem_mid(int N) { return sizeof(float2) * (N + 2 * PSB_TILE * N); }
+
+// forward: src grid -> spectrum [F0][F1][H].  w1: [n0][n1][H], w2: [n0][F1][H]
+int forward3(const Grid3& g, const RzDesc& rz_in, float2* w1, float2* w2, float2* spec, RzDesc* d_rz,
+             MidDesc* d_mid, cudaStream_t st) {
+    RzDesc rz = rz_in;
+    rz.out = w1;
+    CK(cudaMemcpyAsync(d_rz, &rz, sizeof(rz), cudaMemcpyHostToDevice, st));
+    int npairs = (g.n[0] * g.n[1] + 1) / 2;
+    {
+        PROF("k_rfft_z", st);
+        k_rfft_z<<<dim3((npairs + PSB_PAIRS - 1) / PSB_PAIRS, 1), PSB_THREADS, smem_rz(g.F[2]), st>>>(
+            d_rz, nullptr, g.p[2].p, g.p[2].tw);
+    }
+    CKL();
+    MidDesc m[2];
+    // y: [n0][n1->F1][H]
+    m[0] = MidDesc{w1, w2, g.n[0], g.H, g.n[1], g.F[1], (long long)g.n[1] * g.H, (long long)g.F[1] * g.H, g.H, g.H, -1, 0};
+    // x: [1][n0->F0][F1*H]
+    m[1] = MidDesc{w2, spec, 1, g.F[1] * g.H, g.n[0], g.F[0], 0, 0, g.F[1] * g.H, g.F[1] * g.H, -1, 0};
+    CK(cudaMemcpyAsync(d_mid, m, sizeof(m), cudaMemcpyHostToDevice, st));
+    {
+        PROF("k_fft_mid_fwd", st);
+        k_fft_mid<-1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.n[0], 1), PSB_THREADS, smem_mid(g.F[1]), st>>>(
+            d_mid, nullptr, g.p[1].p, g.p[1].tw);
+    }
+    CKL();
+    {
+        PROF("k_fft_mid_fwd", st);
+        k_fft_mid<-1><<<dim3((g.F[1] * g.H + PSB_TILE - 1) / PSB_TILE, 1, 1), PSB_THREADS, smem_mid(g.F[0]), st>>>(
+            d_mid + 1, nullptr, g.p[0].p, g.p[0].tw);
+    }
+    CKL();
+    return PSB_OK;
+}
+
+// inverse: spectrum [F0][F1][H] -> int32 grid (rounded, scaled by 1/(F0 F1 F2))
+int inverse3_int(const Grid3& g, float2* spec, float2* w1, float2* w2, int32_t* out, MidDesc* d_mid,
+                 cudaStream_t st) {
+    MidDesc m[2];
+    // x: [1][F0 -> n0][F1*H]   (spec -> w2 [n0][F1][H])
+    m[0] = MidDesc{spec, w2, 1, g.F[1] * g.H, g.F[0], g.n[0], 0, 0, g.F[1] * g.H, g.F[1] * g.H, -1, 0};
+    // y: [n0][F1 -> n1][H]     (w2 -> w1 [n0][n1][H])
+    m[1] = MidDesc{w2, w1, g.n[0], g.H, g.F[1], g.n[1], (long long)g.F[1] * g.H, (long long)g.n[1] * g.H, g.H, g.H, -1, 0};
+    CK(cudaMemcpyAsync(d_mid, m, sizeof(m), cudaMemcpyHostToDevice, st));
+    {
+        PROF("k_fft_mid_inv", st);
+        k_fft_mid<1><<<dim3((g.F[1] * g.H + PSB_TILE - 1) / PSB_TILE, 1, 1), PSB_THREADS, smem_mid(g.F[0]), st>>>(
+            d_mid, nullptr, g.p[0].p, g.p[0].tw);
+    }
+    CKL();
+    {
+        PROF("k_fft_mid_inv", st);
+        k_fft_mid<1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.n[0], 1), PSB_THREADS, smem_mid(g.F[1]), st>>>(
+            d_mid + 1, nullptr, g.p[1].p, g.p[1].tw);
+    }
+    CKL();
+    int nlines = g.n[0] * g.n[1];
+    float scale = (float)(1.0 / ((double)g.F[0] * g.F[1] * g.F[2]));
+    {
+        PROF("k_irfft_z_int", st);
+        k_irfft_z_int<<<((nlines + 1) / 2 + PSB_PAIRS - 1) / PSB_PAIRS, PSB_THREADS, smem_rz(g.F[2]), st>>>(
+            w1, out, nlines, g.n[2], scale, g.p[2].p, g.p[2].tw);
+    }
+    CKL();
+    return PSB_OK;
+}
+
+int distance_on_device(const int32_t* d_grid, int32_t* d_out, int nx, int ny, int nz, cudaStream_t st) {
+    size_t V = (size_t)nx * ny * nz;
+    int far = nx + ny + nz + 10;  // fft3.cu:948
+    {
+        PROF("k_dist_init", st);
+        k_dist_init<<<grid1d(V), 256, 0, st>>>(d_grid, d_out, V, far);
+    }
+    CKL();
+    for (int axis = 0; axis < 3; ++axis) {
+        int L = axis == 0 ? nx : (axis == 1 ? ny : nz);
+        long long nlines = axis == 0 ? (long long)ny * nz : (axis == 1 ? (long long)nx * nz : (long long)nx * ny);
+        if (L <= 1) continue;
+        long long W = std::min<long long>(256, (96 * 1024) / (4LL * L));
+        if (W >= 1) {
+            long long blocks = (nlines + W - 1) / W;
+            {
+                PROF("k_dist_axis", st);
+                k_dist_axis<<<(unsigned)blocks, 256, (size_t)W * L * 4, st>>>(d_out, axis, nx, ny, nz, (int)W);
+            }
+        } else {
+            {
+                PROF("k_dist_axis_global", st);
+                k_dist_axis_global<<<(unsigned)((nlines + 255) / 256), 256, 0, st>>>(d_out, axis, nx, ny, nz);
+            }
+        }
+        CKL();
+    }
+    return PSB_OK;
+}
+
+int check_grid_args(const void* p, int nx, int ny, int nz, const char* what) {
+    if (!p) return fail(PSB_ERR_ARG, "%s: null pointer", what);
+    if (nx <= 0 || ny <= 0 || nz <= 0) return fail(PSB_ERR_ARG, "%s: dims must be positive, got (%d,%d,%d)", what, nx, ny, nz);
+    return PSB_OK;
+}
+
+bool has_negative(const int32_t* a, size_t n) {
+    for (size_t i = 0; i < n; ++i) if (a[i] < 0) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// host-side item analysis
+// ---------------------------------------------------------------------------
+struct ItemInfo {
+    int dims[3];
+    int lo[3], hi[3];          // bounds of voxels > 0; hi = -1 when none
+    long long sum = 0;         // sum of values
+    double sumsq = 0.0;
+    std::vector<int4> vox;     // nonzero voxels (x, y, z, value)
+};
+
+void analyse_item(const int32_t* a, int ex, int ey, int ez, ItemInfo* info) {
+    info->dims[0] = ex; info->dims[1] = ey; info->dims[2] = ez;
+    for (int k = 0; k < 3; ++k) { info->lo[k] = INT32_MAX; info->hi[k] = -1; }
+    info->sum = 0;
+    info->sumsq = 0.0;
+    info->vox.clear();
+    for (int i = 0; i < ex; ++i)
+        for (int j = 0; j < ey; ++j)
+            for (int k = 0; k < ez; ++k) {
+                int v = a[((size_t)i * ey + j) * ez + k];
+                if (v == 0) continue;
+                info->vox.push_back(make_int4(i, j, k, v));
+                info->sum += v;
+                info->sumsq += (double)v * v;
+                if (v > 0) {
+                    int c[3] = {i, j, k};
+                    for (int q = 0; q < 3; ++q) {
+                        info->lo[q] = std::min(info->lo[q], c[q]);
+                        info->hi[q] = std::max(info->hi[q], c[q]);
+                    }
+                }
+            }
+}
+
+double ulp32(double v) {
+    if (v < 1.0) return 1.19209290e-07;
+    int e;
+    std::frexp(v, &e);  // v = m * 2^e, m in [0.5,1)
+    return std::ldexp(1.0, e - 24);
+}
+
+}  // namespace
+
+// ===========================================================================
+// psb_tray: the device-resident tray context
+// ===========================================================================
+struct psb_tray {
+    int dev = 0;
+    int nx = 0, ny = 0, nz = 0;
+    size_t V = 0;
+    Grid3 g;
+    int nzw = 0;
+    cudaStream_t st = nullptr;
+    bool ready = false;
+
+    int32_t* d_tray = nullptr;
+    int32_t* d_phi = nullptr;
+    float2* d_Socc = nullptr;
+    float2* d_Sphi = nullptr;
+    float2* d_w1 = nullptr;
+    float2* d_w2 = nullptr;
+    double* d_pen = nullptr;
+    RzDesc* d_rz = nullptr;
+    MidDesc* d_mid = nullptr;
+    unsigned long long* d_stats = nullptr;
+    unsigned int* d_err = nullptr;
+    unsigned long long* d_first = nullptr;
+
+    int phi_mean = 0;
+    double phi_norm = 0.0;
+    int phi_maxabs = 0;
+
+    // per-orientation slots
+    int cap = 0;
+    float2 *d_Ai = nullptr, *d_Bi = nullptr, *d_Pc = nullptr, *d_Pd = nullptr;
+    float* d_Dq = nullptr;
+    uint32_t *d_free = nullptr, *d_reach = nullptr;
+    int *d_cnt = nullptr, *d_off = nullptr, *d_rz2 = nullptr, *d_rline = nullptr, *d_par = nullptr, *d_rflag = nullptr,
+        *d_total = nullptr;
+    int *d_cand = nullptr, *d_ncand = nullptr;
+    double* d_cscore = nullptr;
+    unsigned long long *d_smin = nullptr, *d_smin2 = nullptr, *d_best = nullptr, *d_bestkey = nullptr;
+    unsigned int* d_diag = nullptr;
+    OrientDesc* d_od = nullptr;
+    RzDesc* d_rzs = nullptr;
+    MidDesc* d_mids = nullptr;
+    ResultDev* d_res = nullptr;
+    long long sAi = 0, sBi = 0, sP = 0, sD = 0, sBits = 0, sLine = 0, sRun = 0;
+
+    // items of a packing run, staged once (psb_pack_stage)
+    std::vector<ItemInfo> staged;
+    std::vector<size_t> staged_off, staged_voff;
+    int32_t* d_stage = nullptr;
+    int4* d_stage_vox = nullptr;
+    size_t stage_cap = 0, stage_vcap = 0;
+
+    // item staging
+    int32_t* d_items = nullptr;
+    size_t items_cap = 0;
+    int4* d_vox = nullptr;
+    size_t vox_cap = 0;
+
+    ~psb_tray() { release(); }
+
+    void release_slots() {
+        dfree(d_Ai); dfree(d_Bi); dfree(d_Pc); dfree(d_Pd); dfree(d_Dq); dfree(d_free); dfree(d_reach);
+        dfree(d_cnt); dfree(d_off); dfree(d_rz2); dfree(d_rline); dfree(d_par); dfree(d_rflag); dfree(d_total);
+        dfree(d_cand); dfree(d_ncand); dfree(d_cscore); dfree(d_smin); dfree(d_smin2); dfree(d_best);
+        dfree(d_bestkey); dfree(d_diag); dfree(d_od); dfree(d_rzs); dfree(d_mids); dfree(d_res);
+        cap = 0;
+    }
+    void release() {
+        if (dev >= 0) cudaSetDevice(dev);
+        release_slots();
+        dfree(d_tray); dfree(d_phi); dfree(d_Socc); dfree(d_Sphi); dfree(d_w1); dfree(d_w2); dfree(d_pen);
+        dfree(d_rz); dfree(d_mid); dfree(d_stats); dfree(d_err); dfree(d_first); dfree(d_items); dfree(d_vox); dfree(d_stage); dfree(d_stage_vox);
+        if (st) cudaStreamDestroy(st);
+        st = nullptr;
+    }
+
+    int init(int x, int y, int z) {
+        TRY(ensure_device());
+        CK(cudaGetDevice(&dev));
+        TRY(set_smem_attrs());
+        nx = x; ny = y; nz = z;
+        V = (size_t)nx * ny * nz;
+        TRY(make_grid3(nx, ny, nz, false, &g));
+        nzw = (nz + 31) / 32;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        size_t S = (size_t)g.F[0] * g.F[1] * g.H;
+        TRY(dalloc(&d_tray, V)); TRY(dalloc(&d_phi, V));
+        TRY(dalloc(&d_Socc, S)); TRY(dalloc(&d_Sphi, S));
+        TRY(dalloc(&d_w1, (size_t)nx * ny * g.H)); TRY(dalloc(&d_w2, (size_t)nx * g.F[1] * g.H));
+        TRY(dalloc(&d_pen, nz)); TRY(dalloc(&d_rz, 4)); TRY(dalloc(&d_mid, 4)); TRY(dalloc(&d_stats, 4));
+        TRY(dalloc(&d_err, 1)); TRY(dalloc(&d_first, 1));
+        CK(cudaMemset(d_err, 0, sizeof(unsigned int)));
+        // SCAN-mode penalty table with the host libm pow (packing.cpp:630-631)
+        std::vector<double> pen(nz);
+        for (int k = 0; k < nz; ++k) pen[k] = kP * std::pow((k + 0.0) / (nz + 0.0), 3.0);
+        CK(cudaMemcpy(d_pen, pen.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+        return PSB_OK;
+    }
+
+    int ensure_slots(int n) {
+        if (n <= cap) return PSB_OK;
+        release_slots();
+        int c = std::max(n, 1);
+        sAi = (long long)nx * ny * g.H;
+        sBi = (long long)nx * g.F[1] * g.H;
+        sP = (long long)nx * g.F[1] * g.H;
+        sD = (long long)V;
+        sBits = (long long)nx * ny * nzw;
+        sLine = (long long)nx * ny;
+        sRun = (long long)nx * ny * ((nz + 1) / 2);
+        TRY(dalloc(&d_Ai, sAi * c)); TRY(dalloc(&d_Bi, sBi * c));
+        TRY(dalloc(&d_Pc, sP * c)); TRY(dalloc(&d_Pd, sP * c));
+        TRY(dalloc(&d_Dq, sD * c));
+        TRY(dalloc(&d_free, sBits * c)); TRY(dalloc(&d_reach, sBits * c));
+        TRY(dalloc(&d_cnt, sLine * c)); TRY(dalloc(&d_off, sLine * c));
+        TRY(dalloc(&d_rz2, sRun * c)); TRY(dalloc(&d_rline, sRun * c)); TRY(dalloc(&d_par, sRun * c));
+        TRY(dalloc(&d_rflag, sRun * c)); TRY(dalloc(&d_total, c));
+        TRY(dalloc(&d_cand, (size_t)kCandCap * c)); TRY(dalloc(&d_ncand, c));
+        TRY(dalloc(&d_cscore, (size_t)kCandCap * c));
+        TRY(dalloc(&d_smin, c)); TRY(dalloc(&d_smin2, c)); TRY(dalloc(&d_best, c)); TRY(dalloc(&d_bestkey, c));
+        TRY(dalloc(&d_diag, c)); TRY(dalloc(&d_od, c)); TRY(dalloc(&d_rzs, c)); TRY(dalloc(&d_mids, c));
+        TRY(dalloc(&d_res, c));
+        cap = c;
+        return PSB_OK;
+    }
+
+    int ensure_staging(size_t n_items, size_t n_vox) {
+        if (n_items > items_cap) {
+            dfree(d_items);
+            items_cap = std::max(n_items, (size_t)1 << 16);
+            TRY(dalloc(&d_items, items_cap));
+        }
+        if (n_vox > vox_cap) {
+            dfree(d_vox);
+            vox_cap = std::max(n_vox, (size_t)1 << 14);
+            TRY(dalloc(&d_vox, vox_cap));
+        }
+        return PSB_OK;
+    }
+
+    // occupancy spectrum from the device tray
+    int rebuild_occ() {
+        RzDesc rz{SRC_GRID_OCC, d_tray, nx, ny, nz, 0, -1, nullptr};
+        return forward3(g, rz, d_w1, d_w2, d_Socc, d_rz, d_mid, st);
+    }
+
+    // distance spectrum (mean-subtracted) from the device distance field
+    int rebuild_phi_spectrum() {
+        CK(cudaMemsetAsync(d_stats, 0, sizeof(unsigned long long) * 4, st));
+        {
+            PROF("k_stats", st);
+            k_stats<<<grid1d(V), 256, 0, st>>>(d_phi, V, 0, d_stats);
+        }
+        CKL();
+        unsigned long long h[4];
+        CK(cudaMemcpyAsync(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        long long sum = (long long)h[0];
+        phi_mean = (int)std::llround((double)sum / (double)V);
+        CK(cudaMemsetAsync(d_stats, 0, sizeof(unsigned long long) * 4, st));
+        {
+            PROF("k_stats", st);
+            k_stats<<<grid1d(V), 256, 0, st>>>(d_phi, V, phi_mean, d_stats);
+        }
+        CKL();
+        CK(cudaMemcpyAsync(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        phi_norm = std::sqrt((double)(long long)h[1]);
+        phi_maxabs = (int)(unsigned int)(h[2] & 0xffffffffULL);
+        RzDesc rz{SRC_GRID_SUB, d_phi, nx, ny, nz, phi_mean, -1, nullptr};
+        return forward3(g, rz, d_w1, d_w2, d_Sphi, d_rz, d_mid, st);
+    }
+
+    int set(const int32_t* tray, const int32_t* phi) {
+        CK(cudaSetDevice(dev));
+        if (has_negative(tray, V)) return fail(PSB_ERR_ARG, "tray holds negative values; item ids must be >= 0");
+        CK(cudaMemcpyAsync(d_tray, tray, sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
+        if (phi) {
+            CK(cudaMemcpyAsync(d_phi, phi, sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
+        } else {
+            TRY(distance_on_device(d_tray, d_phi, nx, ny, nz, st));
+        }
+        TRY(rebuild_occ());
+        TRY(rebuild_phi_spectrum());
+        CK(cudaStreamSynchronize(st));
+        ready = true;
+        return PSB_OK;
+    }
+
+    // Fill an OrientDesc from an item's analysis and a signed permutation.
+    void describe(const ItemInfo& info, const int* src_axis, const int* flip, const int32_t* d_item,
+                  const int4* d_vx, OrientDesc* od) const {
+        int n[3] = {nx, ny, nz};
+        for (int a = 0; a < 3; ++a) {
+            od->src_axis[a] = src_axis[a];
+            od->flip[a] = flip[a];
+            od->b[a] = info.dims[a];
+            od->e[a] = info.dims[src_axis[a]];
+        }
+        bool empty = info.hi[0] < 0;
+        od->skip = 0;
+        for (int a = 0; a < 3; ++a) {
+            int s = src_axis[a];
+            od->hi[a] = empty ? -1 : (flip[a] ? od->e[a] - 1 - info.lo[s] : info.hi[s]);
+            if (od->e[a] > n[a]) od->skip = 1;
+            // t + hi <= n - 1 ; an empty item (reference hi = -INF) leaves every t valid
+            od->valid[a] = empty ? n[a] : std::max(0, n[a] - od->hi[a]);
+        }
+        od->sumI = info.sum;
+        od->base = (double)phi_mean * (double)info.sum;
+        long long sabs = 0;  // |D'| <= sum|I| * max|phi - m|
+        for (const int4& q : info.vox) sabs += std::llabs((long long)q.w);
+        double maxD = (double)sabs * (double)phi_maxabs;
+        const double eps = 1.1920928955078125e-07;
+        od->delta = 4.0 * eps * std::sqrt(info.sumsq) * phi_norm + 0.5 * ulp32(maxD) + 1e-3;
+        od->exact = (od->delta >= 0.4 || maxD >= 8388608.0) ? 1 : 0;
+        od->item = d_item;
+        od->vox = d_vx;
+        od->nvox = (int)info.vox.size();
+        od->pad = 0;
+    }
+
+    ScoreParams score_params(int mode) const {
+        ScoreParams sp;
+        sp.nx = nx; sp.ny = ny; sp.nz = nz;
+        sp.mode = mode;
+        sp.pen = d_pen;
+        sp.scale = (float)(1.0 / ((double)g.F[0] * g.F[1] * g.F[2]));
+        sp.nzw = nzw;
+        return sp;
+    }
+
+    // Search the n orientations described in ods (device item data already
+    // uploaded).  res receives each orientation's result.
+    int search(const std::vector<OrientDesc>& ods, int mode, bool interlock, std::vector<ResultDev>* res) {
+        const int n = (int)ods.size();
+        TRY(ensure_slots(n));
+        CK(cudaMemcpyAsync(d_od, ods.data(), sizeof(OrientDesc) * n, cudaMemcpyHostToDevice, st));
+        int exmax = 1, eymax = 1;
+        for (auto& o : ods) if (!o.skip) { exmax = std::max(exmax, o.e[0]); eymax = std::max(eymax, o.e[1]); }
+        // item z pass
+        std::vector<RzDesc> rz(n);
+        std::vector<MidDesc> md(n);
+        int maxpairs = 1;
+        for (int o = 0; o < n; ++o) {
+            rz[o] = RzDesc{SRC_ITEM, nullptr, 0, 0, 0, 0, o, d_Ai + (size_t)o * sAi};
+            md[o] = MidDesc{d_Ai + (size_t)o * sAi, d_Bi + (size_t)o * sBi, 0, g.H, 0, g.F[1],
+                            (long long)ods[o].e[1] * g.H, (long long)g.F[1] * g.H, g.H, g.H, o, 0};
+            if (!ods[o].skip) maxpairs = std::max(maxpairs, (ods[o].e[0] * ods[o].e[1] + 1) / 2);
+        }
+        CK(cudaMemcpyAsync(d_rzs, rz.data(), sizeof(RzDesc) * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_mids, md.data(), sizeof(MidDesc) * n, cudaMemcpyHostToDevice, st));
+        {
+            PROF("k_rfft_z", st);
+            k_rfft_z<<<dim3((maxpairs + PSB_PAIRS - 1) / PSB_PAIRS, n), PSB_THREADS, smem_rz(g.F[2]), st>>>(
+                d_rzs, d_od, g.p[2].p, g.p[2].tw);
+        }
+        CKL();
+        {
+            PROF("k_fft_mid_fwd", st);
+            k_fft_mid<-1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, exmax, n), PSB_THREADS, smem_mid(g.F[1]), st>>>(
+                d_mids, d_od, g.p[1].p, g.p[1].tw);
+        }
+        CKL();
+        SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
+        size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
+        {
+            PROF("k_xpass", st);
+            k_xpass<<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], n), PSB_THREADS, smx, st>>>(
+                d_od, sb, d_Socc, d_Sphi, g.F[1], g.H, g.p[0].p, g.p[0].tw);
+        }
+        CKL();
+        CK(cudaMemsetAsync(d_smin, 0xff, sizeof(unsigned long long) * n, st));
+        CK(cudaMemsetAsync(d_smin2, 0xff, sizeof(unsigned long long) * n, st));
+        CK(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long) * n, st));
+        CK(cudaMemsetAsync(d_bestkey, 0xff, sizeof(unsigned long long) * n, st));
+        CK(cudaMemsetAsync(d_diag, 0, sizeof(unsigned int) * n, st));
+        CK(cudaMemsetAsync(d_ncand, 0, sizeof(int) * n, st));
+        CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
+        ScoreParams sp = score_params(mode);
+        PlaneBufs pb{d_free, d_Dq, d_smin, d_diag, sBits, sD};
+        int wsz = std::max(PSB_TILE * g.F[1], PSB_PAIRS * g.F[2]);
+        size_t smp = sizeof(float2) * ((size_t)g.F[1] + g.F[2] + (size_t)ny * g.H + 2 * (size_t)wsz) +
+                     sizeof(uint32_t) * (size_t)ny * nzw;
+        if (smp > (size_t)kMaxSmem) return fail(PSB_ERR_ARG, "tray too large for the plane kernel (%zu B smem)", smp);
+        {
+            PROF("k_plane", st);
+            k_plane<<<dim3(nx, n), PSB_THREADS, smp, st>>>(d_od, sb, pb, sp, g.F[1], g.F[2], g.p[1].p, g.p[2].p,
+                                                            g.p[1].tw, g.p[2].tw);
+        }
+        CKL();
+        const uint32_t* ok = d_free;
+        unsigned long long* smin = d_smin;
+        if (interlock) {
+            FloodBufs fb{d_free, d_reach, sBits, d_cnt, d_off, sLine, d_rz2, d_rline, d_par, d_rflag, sRun, d_total, d_err};
+            int lines = nx * ny;
+            dim3 gl((lines + 255) / 256, n);
+            {
+                PROF("k_ff_count", st);
+                k_ff_count<<<gl, 256, 0, st>>>(d_od, fb, sp);
+            }
+            CKL();
+            {
+                PROF("k_ff_scan", st);
+                k_ff_scan<<<n, 1024, 0, st>>>(d_od, fb, lines);
+            }
+            CKL();
+            {
+                PROF("k_ff_emit", st);
+                k_ff_emit<<<gl, 256, 0, st>>>(d_od, fb, sp);
+            }
+            CKL();
+            {
+                PROF("k_ff_union", st);
+                k_ff_union<<<gl, 256, 0, st>>>(d_od, fb, sp);
+            }
+            CKL();
+            {
+                PROF("k_ff_seed", st);
+                k_ff_seed<<<dim3(296, n), 256, 0, st>>>(d_od, fb);
+            }
+            CKL();
+            {
+                PROF("k_ff_reach", st);
+                k_ff_reach<<<gl, 256, 0, st>>>(d_od, fb, sp);
+            }
+            CKL();
+            ok = d_reach;
+            smin = d_smin2;
+            SelectBufs s0{ok, sBits, d_Dq, sD, smin, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, kCandCap};
+            {
+                PROF("k_select_min", st);
+                k_select_min<<<dim3(nx, n), 256, 0, st>>>(d_od, s0, sp);
+            }
+            CKL();
+        }
+        SelectBufs sel{ok, sBits, d_Dq, sD, smin, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, kCandCap};
+        {
+            PROF("k_collect", st);
+            k_collect<<<dim3(nx, n), 256, 0, st>>>(d_od, sel, sp);
+        }
+        CKL();
+        {
+            PROF("k_rescore", st);
+            k_rescore<<<dim3(148, n), 256, 0, st>>>(d_od, sel, sp, d_tray, d_phi);
+        }
+        CKL();
+        {
+            PROF("k_tiebreak", st);
+            k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_od, sel, sp);
+        }
+        CKL();
+        {
+            PROF("k_finalize", st);
+            k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_od, sel, sp, d_res, n);
+        }
+        CKL();
+        res->resize(n);
+        unsigned int herr = 0;
+        CK(cudaMemcpyAsync(res->data(), d_res, sizeof(ResultDev) * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&herr, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr) return fail(PSB_ERR_LIMIT, "flood fill union-find hit its iteration limit");
+        for (int o = 0; o < n; ++o)
+            if ((*res)[o].diag & 0x100u)
+                return fail(PSB_ERR_LIMIT, "orientation %d: %d tie-guard candidates exceed the capacity %d", o,
+                            (*res)[o].ncand, kCandCap);
+        return PSB_OK;
+    }
+
+    // device placement of an item described by od (slot 0 of d_od is overwritten)
+    int place(const OrientDesc& od, int px, int py, int pz, int32_t id, int32_t* overlap_ijk) {
+        TRY(ensure_slots(1));
+        CK(cudaMemcpyAsync(d_od, &od, sizeof(OrientDesc), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(d_first, 0xff, sizeof(unsigned long long), st));
+        int blocks = std::max(1, std::min(1024, (od.nvox + 255) / 256));
+        k_place_check<<<blocks, 256, 0, st>>>(d_od, d_tray, nx, ny, nz, px, py, pz, d_first);
+        CKL();
+        unsigned long long first = 0;
+        CK(cudaMemcpyAsync(&first, d_first, sizeof(first), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (first != 0xffffffffffffffffULL) {
+            int k = (int)(first % nz), j = (int)((first / nz) % ny), i = (int)(first / ((size_t)ny * nz));
+            if (overlap_ijk) { overlap_ijk[0] = i; overlap_ijk[1] = j; overlap_ijk[2] = k; }
+            return fail(PSB_ERR_OVERLAP,
+                        "(place_in_tray): Item to be placed intersects with contents of tray at position (%d, %d, %d)",
+                        i, j, k);
+        }
+        k_place_write<<<blocks, 256, 0, st>>>(d_od, d_tray, nx, ny, nz, px, py, pz, id);
+        CKL();
+        TRY(rebuild_occ());
+        if (id == 1 && od.nvox > 0) {  // only voxels equal to 1 are distance sources (fft3.cu:948)
+            TRY(distance_on_device(d_tray, d_phi, nx, ny, nz, st));
+            TRY(rebuild_phi_spectrum());
+        }
+        CK(cudaStreamSynchronize(st));
+        return PSB_OK;
+    }
+};
+
+namespace {
+
+const int kIdentity[3] = {0, 1, 2};
+const int kNoFlip[3] = {0, 0, 0};
+
+void to_result(const ResultDev& r, int orient, psb_result* out) {
+    out->x = r.found ? r.x : -1;
+    out->y = r.found ? r.y : -1;
+    out->z = r.found ? r.z : -1;
+    out->found = r.found;
+    out->score = r.found ? r.score : 0.0;
+    out->orientation = r.found ? orient : -1;
+    out->diag = r.diag;
+    out->n_candidates = r.ncand;
+    out->reserved = 0;
+}
+
+// Upload a set of explicit orientation arrays and describe them.
+int stage_arrays(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n, std::vector<OrientDesc>* ods) {
+    std::vector<ItemInfo> infos(n);
+    size_t tot = 0, totv = 0;
+    for (int o = 0; o < n; ++o) {
+        int ex = dims[3 * o], ey = dims[3 * o + 1], ez = dims[3 * o + 2];
+        if (!items[o] || ex <= 0 || ey <= 0 || ez <= 0)
+            return fail(PSB_ERR_ARG, "orientation %d: bad array (dims %d,%d,%d)", o, ex, ey, ez);
+        size_t m = (size_t)ex * ey * ez;
+        if (has_negative(items[o], m)) return fail(PSB_ERR_ARG, "orientation %d holds negative values", o);
+        analyse_item(items[o], ex, ey, ez, &infos[o]);
+        tot += m;
+        totv += infos[o].vox.size();
+    }
+    TRY(t->ensure_staging(tot, totv));
+    size_t off = 0, offv = 0;
+    ods->resize(n);
+    for (int o = 0; o < n; ++o) {
+        size_t m = (size_t)infos[o].dims[0] * infos[o].dims[1] * infos[o].dims[2];
+        CK(cudaMemcpyAsync(t->d_items + off, items[o], sizeof(int32_t) * m, cudaMemcpyHostToDevice, t->st));
+        if (!infos[o].vox.empty())
+            CK(cudaMemcpyAsync(t->d_vox + offv, infos[o].vox.data(), sizeof(int4) * infos[o].vox.size(),
+                               cudaMemcpyHostToDevice, t->st));
+        t->describe(infos[o], kIdentity, kNoFlip, t->d_items + off, t->d_vox + offv, &(*ods)[o]);
+        off += m;
+        offv += infos[o].vox.size();
+    }
+    CK(cudaStreamSynchronize(t->st));  // host vectors die at return
+    return PSB_OK;
+}
+
+// cached contexts for the stateless entry points, keyed by dims
+std::mutex g_util_mu;
+std::map<std::tuple<int, int, int, int>, std::unique_ptr<psb_tray>> g_util;
+
+int util_tray(int nx, int ny, int nz, psb_tray** out) {
+    TRY(ensure_device());
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_util_mu);
+    auto key = std::make_tuple(dev, nx, ny, nz);
+    auto it = g_util.find(key);
+    if (it != g_util.end()) { *out = it->second.get(); return PSB_OK; }
+    if (g_util.size() >= 4) g_util.clear();
+    std::unique_ptr<psb_tray> t(new psb_tray());
+    TRY(t->init(nx, ny, nz));
+    *out = t.get();
+    g_util[key] = std::move(t);
+    return PSB_OK;
+}
+
+// scratch arena for the stateless transforms
+struct Arena {
+    void* p = nullptr;
+    size_t n = 0;
+    int dev = -1;
+};
+thread_local Arena g_arena;
+
+int arena(size_t bytes, void** out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (g_arena.n < bytes || g_arena.dev != dev) {
+        if (g_arena.p && g_arena.dev == dev) cudaFree(g_arena.p);
+        g_arena.p = nullptr;
+        CK(cudaMalloc(&g_arena.p, bytes));
+        g_arena.n = bytes;
+        g_arena.dev = dev;
+    }
+    *out = g_arena.p;
+    return PSB_OK;
+}
+
+// corr (conj_b=1): out[t] = sum_x b[x] a[t+x] ; conv (conj_b=0): linear conv
+int linear_transform_product(const int32_t* a, const int32_t* b, int nx, int ny, int nz, int conj_b, int32_t* out) {
+    TRY(ensure_device());
+    TRY(set_smem_attrs());
+    Grid3 g;
+    TRY(make_grid3(nx, ny, nz, true, &g));
+    size_t V = (size_t)nx * ny * nz;
+    size_t S = (size_t)g.F[0] * g.F[1] * g.H;
+    size_t w1 = (size_t)nx * ny * g.H, w2 = (size_t)nx * g.F[1] * g.H;
+    size_t bytes = sizeof(float2) * (2 * S + w1 + w2) + sizeof(int32_t) * 2 * V + 4096;
+    void* base = nullptr;
+    TRY(arena(bytes, &base));
+    char* p = (char*)base;
+    auto take = [&](size_t n) { char* r = p; p += (n + 255) / 256 * 256; return r; };
+    float2* Sa = (float2*)take(sizeof(float2) * S);
+    float2* Sb = (float2*)take(sizeof(float2) * S);
+    float2* W1 = (float2*)take(sizeof(float2) * w1);
+    float2* W2 = (float2*)take(sizeof(float2) * w2);
+    int32_t* da = (int32_t*)take(sizeof(int32_t) * V);
+    int32_t* db = (int32_t*)take(sizeof(int32_t) * V);
+    RzDesc* d_rz = (RzDesc*)take(sizeof(RzDesc) * 2);
+    MidDesc* d_mid = (MidDesc*)take(sizeof(MidDesc) * 2);
+    cudaStream_t st = 0;
+    CK(cudaMemcpyAsync(da, a, sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(db, b, sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
+    RzDesc ra{SRC_GRID_RAW, da, nx, ny, nz, 0, -1, nullptr};
+    RzDesc rb{SRC_GRID_RAW, db, nx, ny, nz, 0, -1, nullptr};
+    TRY(forward3(g, ra, W1, W2, Sa, d_rz, d_mid, st));
+    CK(cudaStreamSynchronize(st));
+    TRY(forward3(g, rb, W1, W2, Sb, d_rz + 1, d_mid, st));
+    {
+        PROF("k_spec_mul", st);
+        k_spec_mul<<<grid1d(S), 256, 0, st>>>(Sa, Sb, Sa, S, conj_b);
+    }
+    CKL();
+    CK(cudaStreamSynchronize(st));
+    TRY(inverse3_int(g, Sa, W1, W2, da, d_mid, st));
+    CK(cudaMemcpyAsync(out, da, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return PSB_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* psb_version(void) { return "psacking_b200 0.1.0 (sm_100a)"; }
+
+int psb_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return PSB_ERR_ARG;
+    snprintf(buf, len, "%s", g_err.c_str());
+    return PSB_OK;
+}
+
+int psb_device_count(int* n) {
+    if (!n) return fail(PSB_ERR_ARG, "null pointer");
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) { cudaGetLastError(); c = 0; }
+    *n = c;
+    return PSB_OK;
+}
+
+int psb_dft_conv3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, int32_t* out) {
+    TRY(check_grid_args(a, nx, ny, nz, "dft_conv3"));
+    TRY(check_grid_args(b, nx, ny, nz, "dft_conv3"));
+    if (!out) return fail(PSB_ERR_ARG, "dft_conv3: null output");
+    return linear_transform_product(a, b, nx, ny, nz, 0, out);
+}
+
+int psb_dft_corr3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, int32_t* out) {
+    TRY(check_grid_args(a, nx, ny, nz, "dft_corr3"));
+    TRY(check_grid_args(b, nx, ny, nz, "dft_corr3"));
+    if (!out) return fail(PSB_ERR_ARG, "dft_corr3: null output");
+    return linear_transform_product(a, b, nx, ny, nz, 1, out);
+}
+
+int psb_collision_grid(const int32_t* tray, int nx, int ny, int nz, const int32_t* item, int ex, int ey, int ez,
+                       int32_t* out) {
+    TRY(check_grid_args(tray, nx, ny, nz, "collision_grid"));
+    TRY(check_grid_args(item, ex, ey, ez, "collision_grid"));
+    if (ex > nx || ey > ny || ez > nz)
+        return fail(PSB_ERR_ARG, "collision_grid: item (%d,%d,%d) larger than tray (%d,%d,%d)", ex, ey, ez, nx, ny, nz);
+    size_t V = (size_t)nx * ny * nz;
+    std::vector<int32_t> padded(V, 0);
+    ItemInfo info;
+    for (int i = 0; i < ex; ++i)
+        for (int j = 0; j < ey; ++j)
+            memcpy(&padded[((size_t)i * ny + j) * nz], &item[((size_t)i * ey + j) * ez], sizeof(int32_t) * ez);
+    analyse_item(item, ex, ey, ez, &info);
+    TRY(linear_transform_product(tray, padded.data(), nx, ny, nz, 1, out));
+    // bounds of the padded item (voxelGrid.cpp:279-299); empty -> -INF
+    int hx = info.hi[0] < 0 ? -1000000000 : info.hi[0];
+    int hy = info.hi[0] < 0 ? -1000000000 : info.hi[1];
+    int hz = info.hi[0] < 0 ? -1000000000 : info.hi[2];
+    void* base = nullptr;
+    TRY(arena(sizeof(int32_t) * V + 256, &base));
+    int32_t* d = (int32_t*)base;
+    CK(cudaMemcpy(d, out, sizeof(int32_t) * V, cudaMemcpyHostToDevice));
+    k_oob_raise<<<grid1d(V), 256>>>(d, nx, ny, nz, hx, hy, hz);
+    CKL();
+    CK(cudaMemcpy(out, d, sizeof(int32_t) * V, cudaMemcpyDeviceToHost));
+    return PSB_OK;
+}
+
+int psb_calculate_distance(const int32_t* grid, int nx, int ny, int nz, int32_t* out) {
+    TRY(check_grid_args(grid, nx, ny, nz, "calculate_distance"));
+    if (!out) return fail(PSB_ERR_ARG, "calculate_distance: null output");
+    TRY(ensure_device());
+    TRY(set_smem_attrs());
+    size_t V = (size_t)nx * ny * nz;
+    void* base = nullptr;
+    TRY(arena(sizeof(int32_t) * 2 * V + 512, &base));
+    int32_t* dg = (int32_t*)base;
+    int32_t* dd = dg + ((V + 63) / 64) * 64;
+    CK(cudaMemcpy(dg, grid, sizeof(int32_t) * V, cudaMemcpyHostToDevice));
+    TRY(distance_on_device(dg, dd, nx, ny, nz, 0));
+    CK(cudaMemcpy(out, dd, sizeof(int32_t) * V, cudaMemcpyDeviceToHost));
+    return PSB_OK;
+}
+
+int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz, const int32_t* obj, int ex, int ey,
+                                    int ez, int32_t* out) {
+    TRY(check_grid_args(tray, nx, ny, nz, "interlocking_free_positions"));
+    TRY(check_grid_args(obj, ex, ey, ez, "interlocking_free_positions"));
+    if (ex > nx || ey > ny || ez > nz)
+        return fail(PSB_ERR_ARG, "interlocking_free_positions: object larger than tray");
+    // obj_max from voxels != 0, 0 when none (bindings.cpp:585-597)
+    int om[3] = {0, 0, 0};
+    for (int i = 0; i < ex; ++i)
+        for (int j = 0; j < ey; ++j)
+            for (int k = 0; k < ez; ++k)
+                if (obj[((size_t)i * ey + j) * ez + k] != 0) {
+                    om[0] = std::max(om[0], i); om[1] = std::max(om[1], j); om[2] = std::max(om[2], k);
+                }
+    size_t V = (size_t)nx * ny * nz;
+    std::vector<int32_t> coll(V);
+    TRY(psb_collision_grid(tray, nx, ny, nz, obj, ex, ey, ez, coll.data()));
+    psb_tray* t = nullptr;
+    TRY(util_tray(nx, ny, nz, &t));
+    TRY(t->ensure_slots(1));
+    OrientDesc od;
+    memset(&od, 0, sizeof(od));
+    int n[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+        od.e[a] = n[a];
+        od.hi[a] = om[a];
+        od.valid[a] = std::max(0, n[a] - om[a]);
+    }
+    int32_t* dcoll = (int32_t*)t->d_Dq;  // slot 0 proximity buffer reused as int32 scratch
+    CK(cudaMemcpyAsync(dcoll, coll.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, t->st));
+    CK(cudaMemcpyAsync(t->d_od, &od, sizeof(od), cudaMemcpyHostToDevice, t->st));
+    k_bits_from_coll<<<grid1d((size_t)nx * ny), 256, 0, t->st>>>(dcoll, t->d_free, nx, ny, nz, t->nzw, od.valid[0],
+                                                                   od.valid[1], od.valid[2]);
+    CKL();
+    CK(cudaMemsetAsync(t->d_err, 0, sizeof(unsigned int), t->st));
+    ScoreParams sp = t->score_params(1);
+    FloodBufs fb{t->d_free, t->d_reach, t->sBits, t->d_cnt, t->d_off, t->sLine, t->d_rz2, t->d_rline, t->d_par,
+                 t->d_rflag, t->sRun, t->d_total, t->d_err};
+    int lines = nx * ny;
+    dim3 gl((lines + 255) / 256, 1);
+    {
+        PROF("k_ff_count", t->st);
+        k_ff_count<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+    }
+    {
+        PROF("k_ff_scan", t->st);
+        k_ff_scan<<<1, 1024, 0, t->st>>>(t->d_od, fb, lines);
+    }
+    {
+        PROF("k_ff_emit", t->st);
+        k_ff_emit<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+    }
+    {
+        PROF("k_ff_union", t->st);
+        k_ff_union<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+    }
+    {
+        PROF("k_ff_seed", t->st);
+        k_ff_seed<<<dim3(296, 1), 256, 0, t->st>>>(t->d_od, fb);
+    }
+    {
+        PROF("k_ff_reach", t->st);
+        k_ff_reach<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+    }
+    k_bits_to_mask<<<grid1d(V), 256, 0, t->st>>>(t->d_reach, dcoll, nx, ny, nz, t->nzw);
+    CKL();
+    unsigned int herr = 0;
+    CK(cudaMemcpyAsync(out, dcoll, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, t->st));
+    CK(cudaMemcpyAsync(&herr, t->d_err, sizeof(herr), cudaMemcpyDeviceToHost, t->st));
+    CK(cudaStreamSynchronize(t->st));
+    if (herr) return fail(PSB_ERR_LIMIT, "flood fill union-find hit its iteration limit");
+    return PSB_OK;
+}
+
+int psb_fft_search_placement(const int32_t* item, int ex, int ey, int ez, const int32_t* tray, int nx, int ny, int nz,
+                             psb_result* out) {
+    TRY(check_grid_args(item, ex, ey, ez, "fft_search_placement"));
+    TRY(check_grid_args(tray, nx, ny, nz, "fft_search_placement"));
+    if (!out) return fail(PSB_ERR_ARG, "fft_search_placement: null result");
+    psb_result none{-1, -1, -1, 0, 0.0, -1, 0, 0, 0};
+    *out = none;
+    if (ex > nx || ey > ny || ez > nz) return PSB_OK;  // bindings.cpp:189-194
+    psb_tray* t = nullptr;
+    TRY(util_tray(nx, ny, nz, &t));
+    TRY(t->set(tray, nullptr));
+    const int32_t* items[1] = {item};
+    int32_t dims[3] = {ex, ey, ez};
+    return psb_tray_search(t, items, dims, 1, PSB_MODE_SCAN, out, nullptr);
+}
+
+int psb_place_in_tray(const int32_t* item, int ex, int ey, int ez, const int32_t* tray, int nx, int ny, int nz, int px,
+                      int py, int pz, int32_t item_id, int32_t* out_tray, int32_t* overlap_ijk) {
+    TRY(check_grid_args(item, ex, ey, ez, "place_in_tray"));
+    TRY(check_grid_args(tray, nx, ny, nz, "place_in_tray"));
+    if (!out_tray) return fail(PSB_ERR_ARG, "place_in_tray: null output");
+    TRY(ensure_device());
+    size_t V = (size_t)nx * ny * nz;
+    if (out_tray != tray) memcpy(out_tray, tray, sizeof(int32_t) * V);
+    // the clipped box of tray cells the item covers
+    int i0 = std::max(px, 0), j0 = std::max(py, 0), k0 = std::max(pz, 0);
+    int i1 = std::min(nx, px + ex), j1 = std::min(ny, py + ey), k1 = std::min(nz, pz + ez);
+    if (i0 >= i1 || j0 >= j1 || k0 >= k1) return PSB_OK;
+    int bx = i1 - i0, by = j1 - j0, bz = k1 - k0;
+    size_t B = (size_t)bx * by * bz;
+    std::vector<int32_t> box(B);
+    for (int i = 0; i < bx; ++i)
+        for (int j = 0; j < by; ++j)
+            memcpy(&box[((size_t)i * by + j) * bz], &tray[((size_t)(i0 + i) * ny + (j0 + j)) * nz + k0],
+                   sizeof(int32_t) * bz);
+    ItemInfo info;
+    analyse_item(item, ex, ey, ez, &info);
+    size_t I = (size_t)ex * ey * ez;
+    void* base = nullptr;
+    size_t need = sizeof(int32_t) * (B + I) + sizeof(int4) * (info.vox.size() + 1) + sizeof(OrientDesc) + 2048;
+    TRY(arena(need, &base));
+    char* p = (char*)base;
+    auto take = [&](size_t n) { char* r = p; p += (n + 255) / 256 * 256; return r; };
+    int32_t* dbox = (int32_t*)take(sizeof(int32_t) * B);
+    int32_t* ditem = (int32_t*)take(sizeof(int32_t) * I);
+    int4* dvox = (int4*)take(sizeof(int4) * (info.vox.size() + 1));
+    OrientDesc* dod = (OrientDesc*)take(sizeof(OrientDesc));
+    unsigned long long* dfirst = (unsigned long long*)take(sizeof(unsigned long long));
+    OrientDesc od;
+    memset(&od, 0, sizeof(od));
+    for (int a = 0; a < 3; ++a) { od.src_axis[a] = a; od.flip[a] = 0; od.e[a] = info.dims[a]; od.b[a] = info.dims[a]; }
+    od.item = ditem;
+    od.vox = dvox;
+    od.nvox = (int)info.vox.size();
+    CK(cudaMemcpy(dbox, box.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ditem, item, sizeof(int32_t) * I, cudaMemcpyHostToDevice));
+    if (!info.vox.empty()) CK(cudaMemcpy(dvox, info.vox.data(), sizeof(int4) * info.vox.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dod, &od, sizeof(od), cudaMemcpyHostToDevice));
+    CK(cudaMemset(dfirst, 0xff, sizeof(unsigned long long)));
+    int blocks = std::max(1, std::min(1024, (od.nvox + 255) / 256));
+    // the box is a small tray: position relative to the box origin
+    k_place_check<<<blocks, 256>>>(dod, dbox, bx, by, bz, px - i0, py - j0, pz - k0, dfirst);
+    CKL();
+    unsigned long long first = 0;
+    CK(cudaMemcpy(&first, dfirst, sizeof(first), cudaMemcpyDeviceToHost));
+    if (first != 0xffffffffffffffffULL) {
+        int k = (int)(first % bz), j = (int)((first / bz) % by), i = (int)(first / ((size_t)by * bz));
+        i += i0; j += j0; k += k0;
+        // row-major order of the box agrees with the tray's row-major order
+        if (overlap_ijk) { overlap_ijk[0] = i; overlap_ijk[1] = j; overlap_ijk[2] = k; }
+        if (out_tray != tray) memcpy(out_tray, tray, sizeof(int32_t) * V);
+        return fail(PSB_ERR_OVERLAP,
+                    "(place_in_tray): Item to be placed intersects with contents of tray at position (%d, %d, %d)", i,
+                    j, k);
+    }
+    k_place_write<<<blocks, 256>>>(dod, dbox, bx, by, bz, px - i0, py - j0, pz - k0, item_id);
+    CKL();
+    CK(cudaMemcpy(box.data(), dbox, sizeof(int32_t) * B, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < bx; ++i)
+        for (int j = 0; j < by; ++j)
+            memcpy(&out_tray[((size_t)(i0 + i) * ny + (j0 + j)) * nz + k0], &box[((size_t)i * by + j) * bz],
+                   sizeof(int32_t) * bz);
+    return PSB_OK;
+}
+
+int psb_tray_create(int nx, int ny, int nz, psb_tray** out) {
+    if (!out) return fail(PSB_ERR_ARG, "null output");
+    *out = nullptr;
+    if (nx <= 0 || ny <= 0 || nz <= 0) return fail(PSB_ERR_ARG, "tray dims must be positive");
+    std::unique_ptr<psb_tray> t(new psb_tray());
+    TRY(t->init(nx, ny, nz));
+    *out = t.release();
+    return PSB_OK;
+}
+
+int psb_tray_destroy(psb_tray* t) {
+    delete t;
+    return PSB_OK;
+}
+
+int psb_tray_dims(const psb_tray* t, int* nx, int* ny, int* nz) {
+    if (!t || !nx || !ny || !nz) return fail(PSB_ERR_ARG, "null pointer");
+    *nx = t->nx; *ny = t->ny; *nz = t->nz;
+    return PSB_OK;
+}
+
+int psb_tray_set(psb_tray* t, const int32_t* tray, const int32_t* phi) {
+    if (!t || !tray) return fail(PSB_ERR_ARG, "null pointer");
+    return t->set(tray, phi);
+}
+
+int psb_tray_get(psb_tray* t, int32_t* tray, int32_t* phi) {
+    if (!t) return fail(PSB_ERR_ARG, "null tray");
+    CK(cudaSetDevice(t->dev));
+    if (tray) CK(cudaMemcpyAsync(tray, t->d_tray, sizeof(int32_t) * t->V, cudaMemcpyDeviceToHost, t->st));
+    if (phi) CK(cudaMemcpyAsync(phi, t->d_phi, sizeof(int32_t) * t->V, cudaMemcpyDeviceToHost, t->st));
+    CK(cudaStreamSynchronize(t->st));
+    return PSB_OK;
+}
+
+int psb_tray_search(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n, int mode_flags,
+                    psb_result* out, psb_result* per_orient) {
+    if (!t || !items || !dims || !out || n < 0) return fail(PSB_ERR_ARG, "null pointer");
+    if (!t->ready) return fail(PSB_ERR_STATE, "GPU tray context not initialized. Call gpu_tray_init() first.");
+    CK(cudaSetDevice(t->dev));
+    psb_result none{-1, -1, -1, 0, 0.0, -1, 0, 0, 0};
+    *out = none;
+    if (n == 0) return PSB_OK;
+    std::vector<OrientDesc> ods;
+    TRY(stage_arrays(t, items, dims, n, &ods));
+    std::vector<ResultDev> res;
+    int mode = mode_flags & 0xf;
+    TRY(t->search(ods, mode, (mode_flags & PSB_FLAG_INTERLOCK) != 0, &res));
+    double best = 1e300;
+    for (int o = 0; o < n; ++o) {
+        psb_result r;
+        to_result(res[o], o, &r);
+        if (ods[o].skip) r.diag |= 0x200u;
+        if (per_orient) per_orient[o] = r;
+        if (r.found && r.score < best) { best = r.score; *out = r; }  // strict <: first best wins
+    }
+    return PSB_OK;
+}
+
+int psb_tray_place(psb_tray* t, const int32_t* item, int ex, int ey, int ez, int px, int py, int pz, int32_t item_id) {
+    if (!t || !item) return fail(PSB_ERR_ARG, "null pointer");
+    if (!t->ready) return fail(PSB_ERR_STATE, "tray not initialised");
+    CK(cudaSetDevice(t->dev));
+    const int32_t* items[1] = {item};
+    int32_t dims[3] = {ex, ey, ez};
+    std::vector<OrientDesc> ods;
+    TRY(stage_arrays(t, items, dims, 1, &ods));
+    return t->place(ods[0], px, py, pz, item_id, nullptr);
+}
+
+int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items) {
+    if (!t || (!items && n_items > 0) || !dims || n_items < 0) return fail(PSB_ERR_ARG, "null pointer");
+    CK(cudaSetDevice(t->dev));
+    t->staged.clear();
+    t->staged_off.clear();
+    t->staged_voff.clear();
+    size_t tot = 0, totv = 0;
+    t->staged.resize(n_items);
+    for (int it = 0; it < n_items; ++it) {
+        int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
+        if (!items[it] || ex <= 0 || ey <= 0 || ez <= 0) return fail(PSB_ERR_ARG, "item %d: bad array", it);
+        size_t m = (size_t)ex * ey * ez;
+        if (has_negative(items[it], m)) return fail(PSB_ERR_ARG, "item %d holds negative values", it);
+        analyse_item(items[it], ex, ey, ez, &t->staged[it]);
+        t->staged_off.push_back(tot);
+        t->staged_voff.push_back(totv);
+        tot += m;
+        totv += t->staged[it].vox.size();
+    }
+    if (tot > t->stage_cap) {
+        dfree(t->d_stage);
+        t->stage_cap = tot;
+        TRY(dalloc(&t->d_stage, tot));
+    }
+    if (totv > t->stage_vcap) {
+        dfree(t->d_stage_vox);
+        t->stage_vcap = totv;
+        TRY(dalloc(&t->d_stage_vox, totv));
+    }
+    for (int it = 0; it < n_items; ++it) {
+        const ItemInfo& inf = t->staged[it];
+        size_t m = (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
+        CK(cudaMemcpyAsync(t->d_stage + t->staged_off[it], items[it], sizeof(int32_t) * m, cudaMemcpyHostToDevice,
+                           t->st));
+        if (!inf.vox.empty())
+            CK(cudaMemcpyAsync(t->d_stage_vox + t->staged_voff[it], inf.vox.data(), sizeof(int4) * inf.vox.size(),
+                               cudaMemcpyHostToDevice, t->st));
+    }
+    CK(cudaStreamSynchronize(t->st));
+    return PSB_OK;
+}
+
+int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
+                    psb_result* out_placements, int32_t* final_tray) {
+    if (!t || !orient_maps || n_orient <= 0 || !out_placements)
+        return fail(PSB_ERR_ARG, "null pointer or bad orientation count");
+    if (!t->ready) return fail(PSB_ERR_STATE, "tray not initialised");
+    CK(cudaSetDevice(t->dev));
+    for (int o = 0; o < n_orient; ++o) {
+        const int32_t* m = orient_maps + 6 * o;
+        int seen = 0;
+        for (int a = 0; a < 3; ++a) {
+            if (m[a] < 0 || m[a] > 2) return fail(PSB_ERR_ARG, "orientation %d: bad axis map", o);
+            seen |= 1 << m[a];
+        }
+        if (seen != 7) return fail(PSB_ERR_ARG, "orientation %d: axis map is not a permutation", o);
+    }
+    const int mode = (interlock || n_orient > 1) ? PSB_MODE_BLOCK : PSB_MODE_SCAN;
+    int placed = 0;
+    std::vector<OrientDesc> ods(n_orient);
+    std::vector<ResultDev> res;
+    for (int it = 0; it < (int)t->staged.size(); ++it) {
+        const ItemInfo& info = t->staged[it];
+        const int32_t* d_item = t->d_stage + t->staged_off[it];
+        const int4* d_vx = t->d_stage_vox + t->staged_voff[it];
+        for (int o = 0; o < n_orient; ++o)
+            t->describe(info, orient_maps + 6 * o, orient_maps + 6 * o + 3, d_item, d_vx, &ods[o]);
+        TRY(t->search(ods, mode, interlock != 0, &res));
+        psb_result best{-1, -1, -1, 0, 0.0, -1, 0, 0, 0};
+        double bs = 1e300;
+        unsigned int diag = 0;
+        int ncand = 0;
+        for (int o = 0; o < n_orient; ++o) {
+            diag |= res[o].diag;
+            ncand += res[o].ncand;
+            if (ods[o].skip) continue;
+            psb_result r;
+            to_result(res[o], o, &r);
+            if (r.found && r.score < bs) { bs = r.score; best = r; }  // strict <: first best wins
+        }
+        best.diag = diag;
+        best.n_candidates = ncand;
+        if (best.found) {
+            int32_t id = id_offset + placed + 1;
+            TRY(t->place(ods[best.orientation], best.x, best.y, best.z, id, nullptr));
+            ++placed;
+        }
+        out_placements[it] = best;
+    }
+    if (final_tray) TRY(psb_tray_get(t, final_tray, nullptr));
+    return PSB_OK;
+}
+
+int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items, const int32_t* orient_maps,
+             int n_orient, int interlock, int32_t id_offset, psb_result* out_placements, int32_t* final_tray) {
+    TRY(psb_pack_stage(t, items, dims, n_items));
+    return psb_pack_staged(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray);
+}
+
+int psb_profile_enable(int on) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    for (auto& r : g_prof.recs) { g_prof.pool.push_back(r.a); g_prof.pool.push_back(r.b); }
+    g_prof.recs.clear();
+    g_prof.on = on != 0;
+    return PSB_OK;
+}
+
+int psb_profile_report(char* buf, size_t len) {
+    if (!buf || len == 0) return fail(PSB_ERR_ARG, "null buffer");
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    std::map<std::string, std::pair<int, double>> agg;
+    for (auto& r : g_prof.recs) {
+        cudaEventSynchronize(r.b);
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) { cudaGetLastError(); continue; }
+        auto& e = agg[r.name];
+        e.first += 1;
+        e.second += ms;
+    }
+    std::string out;
+    for (auto& kv : agg) {
+        char line[256];
+        snprintf(line, sizeof(line), "%s %d %.6f\n", kv.first.c_str(), kv.second.first, kv.second.second);
+        out += line;
+    }
+    snprintf(buf, len, "%s", out.c_str());
+    return out.size() + 1 > len ? fail(PSB_ERR_ARG, "report truncated") : PSB_OK;
+}
+
+int psb_tray_fft_dims(const psb_tray* t, int* F) {
+    if (!t || !F) return fail(PSB_ERR_ARG, "null pointer");
+    F[0] = t->g.F[0]; F[1] = t->g.F[1]; F[2] = t->g.F[2];
+    return PSB_OK;
+}
+
+int psb_tray_stream(psb_tray* t, void** stream) {
+    if (!t || !stream) return fail(PSB_ERR_ARG, "null pointer");
+    *stream = (void*)t->st;
+    return PSB_OK;
+}
+
+}  // extern "C"

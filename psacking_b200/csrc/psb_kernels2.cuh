@@ -1,0 +1,547 @@
+// psb_kernels2.cuh — selection, exact tie guard, flood fill, distance field
+// and placement kernels.
+#pragma once
+#include "psb_kernels.cuh"
+
+#define PSB_UF_LIMIT (1 << 22)     // bound on union-find retries / path steps
+
+// ---------------------------------------------------------------------------
+// candidate selection and the exact tie guard
+// ---------------------------------------------------------------------------
+struct SelectBufs {
+    const uint32_t* okbits;        // free bits or reach bits, per orientation stride sBits
+    long long sBits;
+    const float* Dq;               // per orientation stride sD
+    long long sD;
+    unsigned long long* smin;      // approx min key per orientation
+    int* cand;                     // per orientation stride cap
+    int* ncand;                    // per orientation
+    double* cscore;                // per orientation stride cap
+    unsigned long long* best;      // exact best score key per orientation
+    unsigned long long* bestkey;   // tie key per orientation
+    unsigned int* diag;
+    int cap;
+};
+
+__device__ __forceinline__ bool okbit(const uint32_t* bits, const ScoreParams& sp, int x, int y, int z) {
+    return (bits[((size_t)x * sp.ny + y) * sp.nzw + (z >> 5)] >> (z & 31)) & 1u;
+}
+
+// min of the approximate score over cells with an ok bit (interlock mode:
+// the reach mask is only known after the flood fill).  grid: (nx, n_orient)
+__global__ void k_select_min(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    const int o = blockIdx.y, x = blockIdx.x;
+    const OrientDesc& od = orients[o];
+    if (od.skip || x >= od.valid[0]) return;
+    const int Yv = od.valid[1], Zv = od.valid[2];
+    const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits;
+    const float* Dq = sb.Dq + (size_t)o * sb.sD;
+    double m = 1e300;
+    for (int idx = threadIdx.x; idx < Yv * Zv; idx += blockDim.x) {
+        int y = idx / Zv, z = idx - y * Zv;
+        if (!okbit(bits, sp, x, y, z)) continue;
+        size_t t = ((size_t)x * sp.ny + y) * sp.nz + z;
+        m = fmin(m, ref_score(sp, od.base + (double)Dq[t], z));
+    }
+    for (int off = 16; off > 0; off >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0 && m < 1e299) atomicMin(&sb.smin[o], ord_key(m));
+}
+
+// collect every ok cell whose approximate score is within the window of the
+// approximate minimum.  grid: (nx, n_orient)
+__global__ void k_collect(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    const int o = blockIdx.y, x = blockIdx.x;
+    const OrientDesc& od = orients[o];
+    if (od.skip || x >= od.valid[0]) return;
+    const unsigned long long mk = sb.smin[o];
+    if (mk == 0xffffffffffffffffULL) return;
+    const double smin = ord_val(mk);
+    const double win = 2.0 * od.delta + 8.0 * (fabs(smin) + 1.0) * 2.220446049250313e-16;
+    const double lim = smin + win;
+    const int Yv = od.valid[1], Zv = od.valid[2];
+    const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits;
+    const float* Dq = sb.Dq + (size_t)o * sb.sD;
+    int* cand = sb.cand + (size_t)o * sb.cap;
+    for (int idx = threadIdx.x; idx < Yv * Zv; idx += blockDim.x) {
+        int y = idx / Zv, z = idx - y * Zv;
+        if (!okbit(bits, sp, x, y, z)) continue;
+        size_t t = ((size_t)x * sp.ny + y) * sp.nz + z;
+        double s = ref_score(sp, od.base + (double)Dq[t], z);
+        if (s <= lim) {
+            int slot = atomicAdd(&sb.ncand[o], 1);
+            if (slot < sb.cap) cand[slot] = (int)t;
+        }
+    }
+}
+
+// exact score of every candidate.  Regime (a): the FP32 value rounds to the
+// exact integer.  Regime (b): direct integer sums over the item's voxels
+// (proximity and collision), the FP64 guard.  One warp per candidate.
+// grid: (blocks, n_orient)
+__global__ void k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp,
+                          const int32_t* __restrict__ tray, const int32_t* __restrict__ phi) {
+    const int o = blockIdx.y;
+    const OrientDesc& od = orients[o];
+    if (od.skip) return;
+    const int n = min(sb.ncand[o], sb.cap);
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int* cand = sb.cand + (size_t)o * sb.cap;
+    double* cs = sb.cscore + (size_t)o * sb.cap;
+    const float* Dq = sb.Dq + (size_t)o * sb.sD;
+    for (int c = warp; c < n; c += nwarps) {
+        const int t = cand[c];
+        const int z = t % sp.nz;
+        const int y = (t / sp.nz) % sp.ny;
+        const int x = t / (sp.nz * sp.ny);
+        double D;
+        bool valid = true;
+        if (!od.exact) {
+            D = od.base + (double)rintf(Dq[t]);
+        } else {
+            long long acc = 0, coll = 0;
+            for (int v = lane; v < od.nvox; v += 32) {
+                int4 q = od.vox[v];
+                int oc[3];
+                orient_voxel(od, q.x, q.y, q.z, oc);
+                size_t g = ((size_t)(x + oc[0]) * sp.ny + (y + oc[1])) * sp.nz + (z + oc[2]);
+                acc += (long long)q.w * phi[g];
+                coll += (long long)q.w * (tray[g] != 0);
+            }
+            for (int off = 16; off > 0; off >>= 1) {
+                acc += __shfl_xor_sync(0xffffffffu, acc, off);
+                coll += __shfl_xor_sync(0xffffffffu, coll, off);
+            }
+            D = (double)acc;
+            if (coll != 0) valid = false;
+            double err = fabs(D - (od.base + (double)Dq[t]));
+            if (lane == 0) {
+                if (!valid) atomicOr(&sb.diag[o], 4u);
+                if (err > od.delta) atomicOr(&sb.diag[o], 8u);
+            }
+        }
+        if (lane == 0) {
+            double s = valid ? ref_score(sp, D, z) : 1e300;
+            cs[c] = s;
+            if (valid) atomicMin(&sb.best[o], ord_key(s));
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned int tie_key(int mode, int idx) {
+    if (mode == 0) return (unsigned int)idx;
+    return ((unsigned int)idx & ~255u) | (__brev((unsigned int)idx & 255u) >> 24);
+}
+__device__ __forceinline__ int untie_key(int mode, unsigned int key) {
+    if (mode == 0) return (int)key;
+    return (int)((key & ~255u) | (__brev(key & 255u) >> 24));
+}
+
+__global__ void k_tiebreak(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    const int o = blockIdx.y;
+    if (orients[o].skip) return;
+    const int n = min(sb.ncand[o], sb.cap);
+    const unsigned long long b = sb.best[o];
+    const int* cand = sb.cand + (size_t)o * sb.cap;
+    const double* cs = sb.cscore + (size_t)o * sb.cap;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        if (cs[c] < 1e299 && ord_key(cs[c]) == b) atomicMin(&sb.bestkey[o], (unsigned long long)tie_key(sp.mode, cand[c]));
+    }
+}
+
+struct ResultDev {
+    int x, y, z, found;
+    double score;
+    int ncand;
+    unsigned int diag;
+};
+
+__global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, ResultDev* out,
+                           int n) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    ResultDev r;
+    r.x = r.y = r.z = -1;
+    r.found = 0;
+    r.score = 0.0;
+    r.ncand = sb.ncand[o];
+    r.diag = sb.diag[o] | (orients[o].exact ? 1u : 0u);
+    if (sb.ncand[o] > sb.cap) r.diag |= 0x100u;
+    if (!orients[o].skip && sb.best[o] != 0xffffffffffffffffULL) {
+        double s = ord_val(sb.best[o]);
+        double cut = sp.mode == 0 ? 1000000000.0 : 1e29;
+        if (s < cut) {
+            int idx = untie_key(sp.mode, (unsigned int)sb.bestkey[o]);
+            r.z = idx % sp.nz;
+            r.y = (idx / sp.nz) % sp.ny;
+            r.x = idx / (sp.nz * sp.ny);
+            r.found = 1;
+            r.score = s;
+        }
+    }
+    out[o] = r;
+}
+
+// ---------------------------------------------------------------------------
+// flood fill (Algorithm 3) by union-find over z-runs of free cells
+// ---------------------------------------------------------------------------
+struct FloodBufs {
+    const uint32_t* freebits;      // stride sBits
+    uint32_t* reach;               // stride sBits
+    long long sBits;
+    int* cnt;                      // per line run count, stride sLine
+    int* off;                      // exclusive offsets, stride sLine
+    long long sLine;
+    int* rz;                       // run z0 | z1 << 16, stride sRun
+    int* rline;
+    int* parent;
+    int* rflag;
+    long long sRun;
+    int* total;                    // runs per orientation
+    unsigned int* err;             // device error word (limit hit)
+};
+
+__device__ __forceinline__ int run_find(int* parent, int x, unsigned int* err) {
+    int it = 0;
+    int p = __ldcg(&parent[x]);
+    while (p != x) {
+        int gp = __ldcg(&parent[p]);
+        if (gp != p) __stcg(&parent[x], gp);   // path halving; gp is an ancestor
+        x = p;
+        p = gp;
+        if (++it > PSB_UF_LIMIT) { atomicOr(err, 1u); return x; }
+    }
+    return x;
+}
+
+__device__ __forceinline__ void run_unite(int* parent, int a, int b, unsigned int* err) {
+    for (int it = 0; it < PSB_UF_LIMIT; ++it) {
+        a = run_find(parent, a, err);
+        b = run_find(parent, b, err);
+        if (a == b) return;
+        if (a > b) { int t = a; a = b; b = t; }
+        int old = atomicCAS(&parent[b], b, a);   // link the larger root under the smaller
+        if (old == b) return;
+        b = old;
+    }
+    atomicOr(err, 1u);
+}
+
+__device__ __forceinline__ bool fbit(const uint32_t* line, int z) { return (line[z >> 5] >> (z & 31)) & 1u; }
+
+// grid: (ceil(nx*ny/256), n_orient)
+__global__ void k_ff_count(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    const int o = blockIdx.y;
+    const OrientDesc& od = orients[o];
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= sp.nx * sp.ny) return;
+    int c = 0;
+    if (!od.skip) {
+        int x = line / sp.ny, y = line - x * sp.ny;
+        if (x < od.valid[0] && y < od.valid[1]) {
+            const uint32_t* w = fb.freebits + (size_t)o * fb.sBits + (size_t)line * sp.nzw;
+            uint32_t prevtop = 0;
+            for (int i = 0; i < sp.nzw; ++i) {
+                uint32_t cur = w[i];
+                c += __popc(cur & ~((cur << 1) | prevtop));
+                prevtop = cur >> 31;
+            }
+        }
+    }
+    fb.cnt[(size_t)o * fb.sLine + line] = c;
+}
+
+// exclusive scan of run counts, one CTA (1024 threads) per orientation
+__global__ void __launch_bounds__(1024) k_ff_scan(const OrientDesc* __restrict__ orients, FloodBufs fb, int nlines) {
+    const int o = blockIdx.x;
+    if (orients[o].skip) return;
+    __shared__ int part[1024];
+    const int tid = threadIdx.x;
+    const int per = (nlines + 1023) / 1024;
+    const int b0 = tid * per, b1 = min(nlines, b0 + per);
+    const int* cnt = fb.cnt + (size_t)o * fb.sLine;
+    int* off = fb.off + (size_t)o * fb.sLine;
+    int s = 0;
+    for (int i = b0; i < b1; ++i) s += cnt[i];
+    part[tid] = s;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+        int v = tid >= d ? part[tid - d] : 0;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    int run = part[tid] - s;
+    for (int i = b0; i < b1; ++i) { off[i] = run; run += cnt[i]; }
+    if (tid == 1023) fb.total[o] = part[1023];
+}
+
+// grid: (ceil(nx*ny/256), n_orient)
+__global__ void k_ff_emit(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    const int o = blockIdx.y;
+    const OrientDesc& od = orients[o];
+    if (od.skip) return;
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= sp.nx * sp.ny) return;
+    int x = line / sp.ny, y = line - x * sp.ny;
+    const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
+    if (x >= Xv || y >= Yv) return;
+    const uint32_t* w = fb.freebits + (size_t)o * fb.sBits + (size_t)line * sp.nzw;
+    int r = fb.off[(size_t)o * fb.sLine + line];
+    const bool side = (x == 0) || (y == 0) || (od.hi[0] >= 0 && x == Xv - 1) || (od.hi[1] >= 0 && y == Yv - 1);
+    int* rz = fb.rz + (size_t)o * fb.sRun;
+    int* rl = fb.rline + (size_t)o * fb.sRun;
+    int* par = fb.parent + (size_t)o * fb.sRun;
+    int* fl = fb.rflag + (size_t)o * fb.sRun;
+    int z = 0;
+    while (z < Zv) {
+        if (!fbit(w, z)) { ++z; continue; }
+        int z0 = z;
+        while (z < Zv && fbit(w, z)) ++z;
+        int z1 = z - 1;
+        bool seed = side || z0 == 0 || (od.hi[2] >= 0 && z1 == Zv - 1);
+        rz[r] = z0 | (z1 << 16);
+        rl[r] = line;
+        par[r] = r;
+        fl[r] = seed ? 1 : 0;
+        ++r;
+    }
+}
+
+// grid: (ceil(nx*ny/256), n_orient)
+__global__ void k_ff_union(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    const int o = blockIdx.y;
+    const OrientDesc& od = orients[o];
+    if (od.skip) return;
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= sp.nx * sp.ny) return;
+    int x = line / sp.ny, y = line - x * sp.ny;
+    if (x >= od.valid[0] || y >= od.valid[1]) return;
+    const int* cnt = fb.cnt + (size_t)o * fb.sLine;
+    const int* off = fb.off + (size_t)o * fb.sLine;
+    const int* rz = fb.rz + (size_t)o * fb.sRun;
+    int* par = fb.parent + (size_t)o * fb.sRun;
+    const int cL = cnt[line], oL = off[line];
+    if (cL == 0) return;
+    for (int nb = 0; nb < 2; ++nb) {
+        int nl;
+        if (nb == 0) { if (x == 0) continue; nl = line - sp.ny; }
+        else { if (y == 0) continue; nl = line - 1; }
+        const int cN = cnt[nl], oN = off[nl];
+        int i = 0, j = 0;
+        while (i < cL && j < cN) {
+            int a = rz[oL + i], b = rz[oN + j];
+            int a0 = a & 0xffff, a1 = a >> 16, b0 = b & 0xffff, b1 = b >> 16;
+            if (a0 <= b1 && b0 <= a1) run_unite(par, oL + i, oN + j, fb.err);
+            if (a1 < b1) ++i; else ++j;
+        }
+    }
+}
+
+// grid: (ceil(maxruns/256), n_orient)
+__global__ void k_ff_seed(const OrientDesc* __restrict__ orients, FloodBufs fb) {
+    const int o = blockIdx.y;
+    if (orients[o].skip) return;
+    const int n = fb.total[o];
+    int* par = fb.parent + (size_t)o * fb.sRun;
+    int* fl = fb.rflag + (size_t)o * fb.sRun;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        if (fl[r] & 1) {
+            int root = run_find(par, r, fb.err);
+            atomicOr(&fl[root], 2);
+        }
+    }
+}
+
+// grid: (ceil(nx*ny/256), n_orient)
+__global__ void k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    const int o = blockIdx.y;
+    const OrientDesc& od = orients[o];
+    if (od.skip) return;
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= sp.nx * sp.ny) return;
+    int x = line / sp.ny, y = line - x * sp.ny;
+    uint32_t* w = fb.reach + (size_t)o * fb.sBits + (size_t)line * sp.nzw;
+    for (int i = 0; i < sp.nzw; ++i) w[i] = 0u;
+    if (x >= od.valid[0] || y >= od.valid[1]) return;
+    const int cL = fb.cnt[(size_t)o * fb.sLine + line], oL = fb.off[(size_t)o * fb.sLine + line];
+    const int* rz = fb.rz + (size_t)o * fb.sRun;
+    int* par = fb.parent + (size_t)o * fb.sRun;
+    const int* fl = fb.rflag + (size_t)o * fb.sRun;
+    for (int i = 0; i < cL; ++i) {
+        int root = run_find(par, oL + i, fb.err);
+        if (!(__ldcg(&fl[root]) & 2)) continue;
+        int a = rz[oL + i];
+        for (int z = a & 0xffff; z <= (a >> 16); ++z) w[z >> 5] |= 1u << (z & 31);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// distance field: exact L1 distance to voxels equal to 1 (fft3.cu:887-1004)
+// ---------------------------------------------------------------------------
+__global__ void k_dist_init(const int32_t* __restrict__ g, int32_t* __restrict__ d, size_t V, int far) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < V; i += (size_t)gridDim.x * blockDim.x)
+        d[i] = g[i] == 1 ? 0 : far;
+}
+
+// One axis: forward then backward min(d, d_nbr + 1) along lines of length L.
+// Lines are staged in shared memory (W lines per CTA) so both the load and
+// the store are coalesced; element p of line l sits at base(l) + p*stride.
+//   axis x: lines l = y*nz+z,        base = l,                 stride = ny*nz
+//   axis y: lines l = x*nz+z,        base = x*ny*nz + z,       stride = nz
+//   axis z: lines l = x*ny+y,        base = l*nz,              stride = 1
+__global__ void k_dist_axis(int32_t* __restrict__ d, int axis, int nx, int ny, int nz, int W) {
+    extern __shared__ int32_t sd[];
+    const int L = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    const long long nlines = axis == 0 ? (long long)ny * nz : (axis == 1 ? (long long)nx * nz : (long long)nx * ny);
+    const long long l0 = (long long)blockIdx.x * W;
+    if (l0 >= nlines) return;
+    const int w = (int)min((long long)W, nlines - l0);
+    const size_t stride = axis == 0 ? (size_t)ny * nz : (axis == 1 ? (size_t)nz : 1);
+    auto base = [&](long long l) -> size_t {
+        if (axis == 0) return (size_t)l;
+        if (axis == 1) return (size_t)(l / nz) * ny * nz + (size_t)(l % nz);
+        return (size_t)l * nz;
+    };
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    if (axis == 2) {
+        for (int idx = tid; idx < w * L; idx += nthr) {
+            int li = idx / L, p = idx - li * L;
+            sd[li * L + p] = d[base(l0 + li) + p];
+        }
+    } else {
+        for (int idx = tid; idx < w * L; idx += nthr) {
+            int p = idx / w, li = idx - p * w;
+            sd[li * L + p] = d[base(l0 + li) + (size_t)p * stride];
+        }
+    }
+    __syncthreads();
+    for (int li = tid; li < w; li += nthr) {
+        int32_t* s = sd + li * L;
+        for (int p = L - 2; p >= 0; --p) s[p] = min(s[p], s[p + 1] + 1);
+        for (int p = 1; p < L; ++p) s[p] = min(s[p], s[p - 1] + 1);
+    }
+    __syncthreads();
+    if (axis == 2) {
+        for (int idx = tid; idx < w * L; idx += nthr) {
+            int li = idx / L, p = idx - li * L;
+            d[base(l0 + li) + p] = sd[li * L + p];
+        }
+    } else {
+        for (int idx = tid; idx < w * L; idx += nthr) {
+            int p = idx / w, li = idx - p * w;
+            d[base(l0 + li) + (size_t)p * stride] = sd[li * L + p];
+        }
+    }
+}
+
+// fallback for very long lines: sequential in global memory, one thread per line
+__global__ void k_dist_axis_global(int32_t* __restrict__ d, int axis, int nx, int ny, int nz) {
+    const int L = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    const long long nlines = axis == 0 ? (long long)ny * nz : (axis == 1 ? (long long)nx * nz : (long long)nx * ny);
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlines) return;
+    size_t stride = axis == 0 ? (size_t)ny * nz : (axis == 1 ? (size_t)nz : 1);
+    size_t b = axis == 0 ? (size_t)l : (axis == 1 ? (size_t)(l / nz) * ny * nz + (size_t)(l % nz) : (size_t)l * nz);
+    for (int p = L - 2; p >= 0; --p) d[b + p * stride] = min(d[b + p * stride], d[b + (p + 1) * stride] + 1);
+    for (int p = 1; p < L; ++p) d[b + p * stride] = min(d[b + p * stride], d[b + (p - 1) * stride] + 1);
+}
+
+// sum and sum of squares (around a shift) for the distance spectrum's mean
+// subtraction; also the max absolute deviation.
+__global__ void k_stats(const int32_t* __restrict__ v, size_t n, int shift, unsigned long long* out) {
+    long long s = 0, s2 = 0;
+    int mx = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        long long d = (long long)v[i] - shift;
+        s += d;
+        s2 += d * d;
+        mx = max(mx, (int)(d < 0 ? -d : d));
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, off);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&out[0], (unsigned long long)s);
+        atomicAdd(&out[1], (unsigned long long)s2);
+        atomicMax((unsigned int*)&out[2], (unsigned int)mx);
+    }
+}
+
+// any negative value?
+__global__ void k_any_negative(const int32_t* __restrict__ v, size_t n, unsigned int* flag) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (v[i] < 0) { atomicOr(flag, 1u); return; }
+}
+
+// ---------------------------------------------------------------------------
+// placement (packing.cpp:773-788)
+// ---------------------------------------------------------------------------
+// first tray cell (row-major) where an item voxel > 0 meets a tray voxel > 0
+__global__ void k_place_check(const OrientDesc* __restrict__ od_p, const int32_t* __restrict__ tray, int nx, int ny,
+                              int nz, int px, int py, int pz, unsigned long long* first) {
+    const OrientDesc od = *od_p;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < od.nvox; v += gridDim.x * blockDim.x) {
+        int4 q = od.vox[v];
+        if (q.w <= 0) continue;
+        int oc[3];
+        orient_voxel(od, q.x, q.y, q.z, oc);
+        int i = px + oc[0], j = py + oc[1], k = pz + oc[2];
+        if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) continue;
+        size_t t = ((size_t)i * ny + j) * nz + k;
+        if (tray[t] > 0) atomicMin(first, (unsigned long long)t);
+    }
+}
+
+__global__ void k_place_write(const OrientDesc* __restrict__ od_p, int32_t* __restrict__ tray, int nx, int ny, int nz,
+                              int px, int py, int pz, int32_t id) {
+    const OrientDesc od = *od_p;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < od.nvox; v += gridDim.x * blockDim.x) {
+        int4 q = od.vox[v];
+        if (q.w <= 0) continue;
+        int oc[3];
+        orient_voxel(od, q.x, q.y, q.z, oc);
+        int i = px + oc[0], j = py + oc[1], k = pz + oc[2];
+        if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) continue;
+        size_t t = ((size_t)i * ny + j) * nz + k;
+        if (tray[t] == 0) tray[t] = id;
+    }
+}
+
+// collision_grid post-pass: out-of-tray positions raised to max(c, 1)
+__global__ void k_oob_raise(int32_t* __restrict__ c, int nx, int ny, int nz, int hx, int hy, int hz) {
+    size_t V = (size_t)nx * ny * nz;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < V; t += (size_t)gridDim.x * blockDim.x) {
+        int k = (int)(t % nz), j = (int)((t / nz) % ny), i = (int)(t / ((size_t)ny * nz));
+        bool in = ((long long)i + hx <= nx - 1) && ((long long)j + hy <= ny - 1) && ((long long)k + hz <= nz - 1);
+        if (!in) c[t] = max(c[t], 1);
+    }
+}
+
+// labels for interlocking_free_positions: free = collision 0 and in bounds
+__global__ void k_bits_from_coll(const int32_t* __restrict__ c, uint32_t* __restrict__ bits, int nx, int ny, int nz,
+                                 int nzw, int Xv, int Yv, int Zv) {
+    size_t nl = (size_t)nx * ny;
+    for (size_t line = blockIdx.x * (size_t)blockDim.x + threadIdx.x; line < nl;
+         line += (size_t)gridDim.x * blockDim.x) {
+        int x = (int)(line / ny), y = (int)(line % ny);
+        uint32_t* w = bits + line * nzw;
+        for (int i = 0; i < nzw; ++i) w[i] = 0u;
+        if (x >= Xv || y >= Yv) continue;
+        for (int z = 0; z < Zv; ++z)
+            if (c[line * nz + z] == 0) w[z >> 5] |= 1u << (z & 31);
+    }
+}
+
+__global__ void k_bits_to_mask(const uint32_t* __restrict__ bits, int32_t* __restrict__ out, int nx, int ny, int nz,
+                               int nzw) {
+    size_t V = (size_t)nx * ny * nz;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < V; t += (size_t)gridDim.x * blockDim.x) {
+        size_t line = t / nz;
+        int z = (int)(t % nz);
+        out[t] = (bits[line * nzw + (z >> 5)] >> (z & 31)) & 1u;
+    }
+}

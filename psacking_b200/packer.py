@@ -1,0 +1,235 @@
+"""BinPacker: the greedy packing loop over the B200 engine.
+
+Mirrors spectral_packer.packer (BinPacker / PackingResult / PlacementInfo,
+spectral_packer/packer.py:33-608): same constructor checks, item order
+(np.argsort(volumes)[::-1]), orientation loop with strict `<` across
+orientations, item ids id_offset + k, and statistics.
+
+Two engines produce identical results:
+  engine="native" (default) one C-ABI call (psb_pack) runs the whole loop with
+                  the tray, its spectra and its distance field resident on the
+                  GPU; orientations are gathered on the device.
+  engine="calls"  the reference's call pattern, one _core call per
+                  orientation (packer.py:447-528), for drop-in comparisons.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+from . import _core
+from .rotations import get_orientations, make_contiguous, orientation_maps
+
+
+@dataclass
+class PlacementInfo:
+    """One item's outcome (packer.py:33-60)."""
+    item_index: int
+    position: Optional[Tuple[int, int, int]]
+    score: Optional[float]
+    success: bool
+    volume: int = 0
+    orientation_index: int = 0
+
+
+@dataclass
+class PackingResult:
+    """Results of a packing run (packer.py:86-165)."""
+    tray: np.ndarray
+    placements: List[PlacementInfo] = field(default_factory=list)
+    num_placed: int = 0
+    num_failed: int = 0
+    density: float = 0.0
+    total_volume: int = 0
+    bounding_box: Optional[Tuple[Tuple[int, int, int], Tuple[int, int, int]]] = None
+    mesh_placements: Optional[list] = None
+    diagnostics: Optional[dict] = None
+
+    def get_item_mask(self, item_id: int) -> np.ndarray:
+        return self.tray == item_id
+
+    def save_vox(self, path: Union[str, Path]) -> None:
+        from .vox import save_vox
+        save_vox(self.tray, str(path))
+
+    def summary(self) -> str:
+        lines = [
+            "Packing Result Summary",
+            "=" * 40,
+            f"Items placed:    {self.num_placed}",
+            f"Items failed:    {self.num_failed}",
+            f"Success rate:    {self.num_placed / max(1, self.num_placed + self.num_failed):.1%}",
+            f"Packing density: {self.density:.1%}",
+            f"Total volume:    {self.total_volume} voxels",
+            f"Tray size:       {self.tray.shape}",
+        ]
+        if self.bounding_box:
+            lo, hi = self.bounding_box
+            lines.append(f"Bounding box:    {lo} to {hi}")
+        return "\n".join(lines)
+
+
+class BinPacker:
+    """Greedy spectral packer (packer.py:168-251).
+
+    height_penalty is stored but, as in the reference, the search always uses
+    1e8 (packer.py:248 vs spectral_packing/constants.h:7)."""
+
+    def __init__(self, tray_size: Tuple[int, int, int], voxel_resolution: int = 128,
+                 height_penalty: float = 1e8, num_orientations: int = 1,
+                 interlocking_free: bool = False, engine: str = "native"):
+        if len(tray_size) != 3:
+            raise ValueError(f"tray_size must be a 3-tuple, got {len(tray_size)} elements")
+        if any(s <= 0 for s in tray_size):
+            raise ValueError(f"tray_size dimensions must be positive, got {tray_size}")
+        if voxel_resolution <= 0:
+            raise ValueError(f"voxel_resolution must be positive, got {voxel_resolution}")
+        if num_orientations not in (1, 4, 6, 24):
+            raise ValueError(f"num_orientations must be 1, 4, 6, or 24, got {num_orientations}")
+        if engine not in ("native", "calls"):
+            raise ValueError("engine must be 'native' or 'calls'")
+        self.tray_size = tuple(int(s) for s in tray_size)
+        self.voxel_resolution = voxel_resolution
+        self.height_penalty = height_penalty
+        self.num_orientations = num_orientations
+        self.interlocking_free = interlocking_free
+        self.engine = engine
+
+    # ------------------------------------------------------------------ files
+    def pack_files(self, paths: Sequence[Union[str, Path]], sort_by_volume: bool = True,
+                   validate_meshes: bool = True, repair_meshes: bool = True) -> PackingResult:
+        raise NotImplementedError(
+            "mesh voxelization is outside this engine; voxelize items first and call pack_voxels")
+
+    # ------------------------------------------------------------------ voxels
+    def _prepare(self, items, sort_by_volume, initial_tray):
+        if len(items) == 0:
+            raise ValueError("items list cannot be empty")
+        processed, volumes = [], []
+        for i, item in enumerate(items):
+            if not isinstance(item, np.ndarray):
+                raise ValueError(f"Item {i} is not a numpy array")
+            if item.ndim != 3:
+                raise ValueError(f"Item {i} must be 3D, got {item.ndim}D")
+            it = item.astype(np.int32)
+            processed.append(it)
+            volumes.append(int(np.sum(it > 0)))
+        if sort_by_volume:
+            order = list(np.argsort(volumes)[::-1])
+        else:
+            order = list(range(len(items)))
+        if initial_tray is not None:
+            if initial_tray.shape != self.tray_size:
+                raise ValueError(f"initial_tray shape {initial_tray.shape} does not match "
+                                 f"tray_size {self.tray_size}")
+            tray = initial_tray.astype(np.int32).copy()
+            id_offset = int(np.max(tray))
+        else:
+            tray = np.zeros(self.tray_size, dtype=np.int32)
+            id_offset = 0
+        return processed, volumes, order, tray, id_offset
+
+    def pack_voxels(self, items: Sequence[np.ndarray], sort_by_volume: bool = True,
+                    initial_tray: Optional[np.ndarray] = None) -> PackingResult:
+        processed, volumes, order, tray, id_offset = self._prepare(items, sort_by_volume, initial_tray)
+        if self.engine == "native":
+            return self._pack_native(processed, volumes, order, tray, id_offset, len(items))
+        return self._pack_calls(processed, volumes, order, tray, id_offset, len(items))
+
+    def _pack_native(self, processed, volumes, order, tray, id_offset, n_items):
+        maps = orientation_maps(self.num_orientations)
+        seq = [np.ascontiguousarray(processed[i]) for i in order]
+        final, res = _core.pack_native(seq, tray, maps, bool(self.interlocking_free), int(id_offset))
+        placements = []
+        diag_or, ncand = 0, 0
+        for k, orig in enumerate(order):
+            pos, found, score, orient, diag, nc = res[k]
+            diag_or |= int(diag)
+            ncand += int(nc)
+            if found:
+                placements.append(PlacementInfo(int(orig), tuple(int(v) for v in pos), float(score), True,
+                                                volumes[orig], int(orient)))
+            else:
+                placements.append(PlacementInfo(int(orig), None, None, False, volumes[orig], 0))
+        return self._finish(final, placements, n_items, {"diag": diag_or, "candidates": ncand})
+
+    def _pack_calls(self, processed, volumes, order, tray, id_offset, n_items):
+        # a fresh run never inherits a cached tray context (the reference's
+        # generation counter restarts at 0 every run, bindings.cpp:209/236)
+        _core.gpu_tray_cleanup()
+        generation = 0
+        placements = []
+        num_placed = 0
+        for orig in order:
+            item = processed[orig]
+            best_pos, best_score, best_o, best_item, found_any = None, float("inf"), 0, item, False
+            orients = get_orientations(item, self.num_orientations)
+            if self.num_orientations > 1 or self.interlocking_free:
+                tray_distance = _core.calculate_distance(tray)
+            if self.interlocking_free:
+                valid, vidx = [], []
+                for o, r in enumerate(orients):
+                    r = make_contiguous(r.astype(np.int32))
+                    if not any(r.shape[a] > self.tray_size[a] for a in range(3)):
+                        valid.append(r)
+                        vidx.append(o)
+                if valid:
+                    pos, found, score, bo = _core.fft_search_batch_interlocking_free(
+                        valid, tray, tray_distance, generation)
+                    if found and bo >= 0:
+                        best_pos, best_score, best_o, best_item, found_any = pos, score, vidx[bo], valid[bo], True
+            else:
+                for o, r in enumerate(orients):
+                    r = make_contiguous(r.astype(np.int32))
+                    if any(r.shape[a] > self.tray_size[a] for a in range(3)):
+                        continue
+                    if self.num_orientations > 1:
+                        pos, found, score = _core.fft_search_placement_with_cache(r, tray, tray_distance, generation)
+                    else:
+                        pos, found, score = _core.fft_search_placement(r, tray)
+                    if found and score < best_score:
+                        best_pos, best_score, best_o, best_item, found_any = pos, score, o, r, True
+            if found_any:
+                tray = _core.place_in_tray(best_item, tray, best_pos, id_offset + num_placed + 1)
+                generation += 1
+                num_placed += 1
+                placements.append(PlacementInfo(int(orig), tuple(best_pos), float(best_score), True,
+                                                volumes[orig], best_o))
+            else:
+                placements.append(PlacementInfo(int(orig), None, None, False, volumes[orig], 0))
+        return self._finish(tray, placements, n_items, None)
+
+    def _finish(self, tray, placements, n_items, diag):
+        placements.sort(key=lambda p: p.item_index)
+        num_placed = sum(1 for p in placements if p.success)
+        density, total, bbox = self._calculate_stats(tray)
+        return PackingResult(tray=tray, placements=placements, num_placed=num_placed,
+                             num_failed=n_items - num_placed, density=density, total_volume=total,
+                             bounding_box=bbox, diagnostics=diag)
+
+    def pack_single(self, item: np.ndarray, tray: Optional[np.ndarray] = None):
+        """packer.py:546-580."""
+        if tray is None:
+            tray = np.zeros(self.tray_size, dtype=np.int32)
+        pos, found, score = _core.fft_search_placement(item.astype(np.int32), tray)
+        if found:
+            return tuple(pos), True, score
+        return None, False, 0.0
+
+    def _calculate_stats(self, tray: np.ndarray):
+        """packer.py:582-601: density = occupied / bounding-box volume."""
+        occupied = int(np.sum(tray > 0))
+        if occupied == 0:
+            return 0.0, 0, None
+        idx = np.argwhere(tray > 0)
+        lo = tuple(idx.min(axis=0).tolist())
+        hi = tuple(idx.max(axis=0).tolist())
+        vol = int(np.prod([b - a + 1 for a, b in zip(lo, hi)]))
+        return (float(occupied / vol) if vol > 0 else 0.0), occupied, (lo, hi)
+
+    def __repr__(self) -> str:
+        return (f"BinPacker(tray_size={self.tray_size}, voxel_resolution={self.voxel_resolution}, "
+                f"num_orientations={self.num_orientations})")

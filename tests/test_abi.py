@@ -1,0 +1,77 @@
+"""The C-ABI library loads and exports every symbol include/psb200.h declares;
+the pybind11 module exposes the reference module's names; without a GPU every
+compute call fails loudly (no CPU fallback)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "psb200.h"
+LIB = ROOT / "psacking_b200" / "libpsb200.so"
+
+REFERENCE_EXPORTS = [  # spectral_packing/bindings.cpp:681-924
+    "fft_search_placement", "fft_search_placement_with_cache", "place_in_tray", "dft_conv3",
+    "dft_corr3", "calculate_distance", "collision_grid", "make_tight", "get_bounds",
+    "gpu_tray_init", "gpu_tray_cleanup", "gpu_tray_is_initialized", "gpu_tray_search",
+    "fft_search_batch", "fft_search_batch_interlocking_free", "interlocking_free_positions",
+]
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(psb_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "psb_tray_search" in syms and "psb_pack" in syms and len(syms) >= 18
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(LIB))
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    lib.psb_version.restype = ctypes.c_char_p
+    assert b"sm_100a" in lib.psb_version()
+    n = ctypes.c_int(-1)
+    assert lib.psb_device_count(ctypes.byref(n)) == 0 and n.value >= 0
+
+
+def test_core_module_mirrors_reference(core):
+    for name in REFERENCE_EXPORTS:
+        assert callable(getattr(core, name)), name
+    assert core.VOXEL_RESOLUTION == 128
+    assert core.HEIGHT_PENALTY == 1e8
+    assert core.__version__ == "0.1.0"
+    import psacking_b200 as p
+    for name in REFERENCE_EXPORTS + ["save_vox", "voxelize_stl", "BinPacker"]:
+        assert hasattr(p, name), name
+
+
+def test_wrong_dimensions_raise(core):
+    # bindings.cpp:75-78 / tests/test_bindings.py:276-284
+    with pytest.raises(RuntimeError, match="3-dimensional"):
+        core.fft_search_placement(np.ones((3, 3), np.int32), np.zeros((5, 5, 5), np.int32))
+
+
+def test_host_utilities(core):
+    from oracle import psb_oracle as O
+    g = np.zeros((5, 5, 5), np.int32)
+    g[1:3, 0:2, 1:4] = 1
+    assert core.get_bounds(g) == ((1, 0, 1), (2, 1, 3))
+    assert core.make_tight(g).shape == (2, 2, 3)
+    assert core.get_bounds(np.zeros((2, 2, 2), np.int32)) == O.bounds(np.zeros((2, 2, 2)))
+    with pytest.raises(ValueError):
+        core.make_tight(np.zeros((2, 2, 2), np.int32))
+
+
+def test_no_gpu_fails_loudly(core):
+    if core.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    with pytest.raises(RuntimeError, match="CUDA"):
+        core.calculate_distance(np.zeros((4, 4, 4), np.int32))
+    with pytest.raises(RuntimeError):
+        core.fft_search_placement(np.ones((2, 2, 2), np.int32), np.zeros((6, 6, 6), np.int32))

@@ -1,0 +1,258 @@
+"""GPU parity: the CUDA path against the CPU oracle and the golden fixture.
+
+Every comparison is exact: positions, found flags and scores (doubles) must be
+bit-identical to the oracle, which is the reference's algorithm in exact
+arithmetic.  Run on a B200 with `pytest -m gpu`."""
+import ctypes
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import psb_oracle as O
+from tests.golden_io import load_records, same_output
+
+pytestmark = pytest.mark.gpu
+
+HERE = Path(__file__).resolve().parent
+SCAN, BLOCK, INTERLOCK = 0, 1, 0x10
+DIAG_FALSE_FREE, DIAG_BOUND = 0x4, 0x8
+
+
+# --------------------------------------------------------------------------
+# golden replay through the drop-in module
+# --------------------------------------------------------------------------
+RECORDS = load_records()
+
+
+def _replay(core, r):
+    a = r["args"]
+    fn = r["fn"]
+    if fn == "fft_search_batch":
+        core.gpu_tray_cleanup()
+        return core.fft_search_batch(list(a[0]), a[1], a[2], 1)
+    if fn == "fft_search_placement_with_cache":
+        core.gpu_tray_cleanup()
+        return core.fft_search_placement_with_cache(a[0], a[1], a[2], 1)
+    if fn == "place_in_tray":
+        return core.place_in_tray(a[0], a[1], a[2], a[3])
+    if fn == "pack_voxels":
+        from psacking_b200 import BinPacker
+        items, tray_size, n_orient, interlock, sort = a
+        outs = []
+        for engine in ("native", "calls"):
+            res = BinPacker(tuple(tray_size), num_orientations=n_orient, interlocking_free=interlock,
+                            engine=engine).pack_voxels(list(items), sort_by_volume=sort)
+            outs.append((res.tray, [(p.position, p.success, p.orientation_index, p.score) for p in res.placements]))
+        assert same_output(outs[0], outs[1])
+        return outs[0]
+    return getattr(core, fn)(*a)
+
+
+@pytest.mark.parametrize("i", range(len(RECORDS)))
+def test_golden_replay(gpu_core, i):
+    r = RECORDS[i]
+    got = _replay(gpu_core, r)
+    assert same_output(got, r["out"]), (r["test"], r["fn"])
+
+
+# --------------------------------------------------------------------------
+# per-orientation search parity on random trays
+# --------------------------------------------------------------------------
+def random_tray(rng, shape, fill, with_first_item=True):
+    tray = np.zeros(shape, np.int32)
+    n = int(fill * np.prod(shape) / 30) + 1
+    for b in range(n):
+        e = [int(rng.integers(1, max(2, s // 4) + 1)) for s in shape]
+        o = [int(rng.integers(0, s - ee + 1)) for s, ee in zip(shape, e)]
+        tray[o[0]:o[0] + e[0], o[1]:o[1] + e[1], o[2]:o[2] + e[2]] = 1 + (b if not with_first_item else b + 1) % 7
+    return tray
+
+
+def random_item(rng, maxe):
+    e = [int(rng.integers(1, m + 1)) for m in maxe]
+    it = (rng.random(e) < 0.7).astype(np.int32)
+    if it.sum() == 0:
+        it[tuple(np.array(e) - 1)] = 1
+    return it
+
+
+def check_search(core, tray, items, flags, phi=None):
+    if phi is None:
+        phi = O.calculate_distance(tray)
+    core.gpu_tray_init(tray, phi)
+    d = core.search_detail(items, flags)
+    mode = "scan" if (flags & 0xF) == SCAN else "block"
+    inter = bool(flags & INTERLOCK)
+    best = None
+    for o, it in enumerate(items):
+        pos, found, score, diag, ncand = d["per_orientation"][o]
+        assert not diag & (DIAG_FALSE_FREE | DIAG_BOUND), (o, hex(diag))
+        if any(it.shape[a] > tray.shape[a] for a in range(3)):
+            assert not found
+            continue
+        want = O.search_one(it, tray, phi, mode=mode, interlock=inter)
+        assert (tuple(pos), found) == (tuple(want[0]), want[1]), (o, pos, want)
+        if found:
+            assert score == want[2], (o, score, want[2])
+            if best is None or score < best[1]:
+                best = (o, score, tuple(pos))
+    bpos, bfound, bscore, bo = d["best"]
+    if best is None:
+        assert not bfound
+    else:
+        assert bfound and bo == best[0] and bscore == best[1] and tuple(bpos) == best[2]
+
+
+SHAPES = [(9, 7, 8), (17, 23, 19), (32, 32, 32), (40, 33, 27), (64, 64, 64)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("flags", [SCAN, BLOCK, BLOCK | INTERLOCK])
+def test_search_random(gpu_core, shape, flags):
+    rng = np.random.default_rng(hash((shape, flags)) % 2**32)
+    for trial in range(3):
+        tray = random_tray(rng, shape, [0.0, 0.15, 0.4][trial])
+        items = [random_item(rng, [max(1, s // 3) for s in shape]) for _ in range(4)]
+        check_search(gpu_core, tray, items, flags)
+
+
+def test_search_empty_and_full(gpu_core):
+    tray = np.zeros((20, 20, 20), np.int32)
+    it = np.ones((3, 3, 3), np.int32)
+    check_search(gpu_core, tray, [it], BLOCK)
+    check_search(gpu_core, tray, [it], SCAN)
+    full = np.ones((6, 6, 6), np.int32)
+    check_search(gpu_core, full, [it], BLOCK | INTERLOCK)
+    big = np.ones((25, 3, 3), np.int32)
+    check_search(gpu_core, tray, [big, it], BLOCK)
+
+
+def test_search_config3_scale(gpu_core):
+    """240x123x100 tray (the benchmark's tray), two large items, 24 orientations
+    of one of them, interlocking mask on: exact parity at full size."""
+    from psacking_b200 import workloads
+    from psacking_b200.rotations import get_orientations
+    rng = np.random.default_rng(11)
+    shape = workloads.TRAY3
+    tray = np.zeros(shape, np.int32)
+    tray[0:60, 0:50, 0:40] = 1
+    tray[100:150, 60:123, 0:30] = 2
+    tray[30:200, 20:40, 40:60] = 3
+    items = workloads.config3_items(5, n=2)
+    ors = [np.ascontiguousarray(o) for o in get_orientations(items[0], 24)][::4] + [items[1]]
+    check_search(gpu_core, tray, ors, BLOCK | INTERLOCK)
+    check_search(gpu_core, tray, ors[:2], BLOCK)
+
+
+# --------------------------------------------------------------------------
+# distance, correlation, flood fill at sizes the oracle handles quickly
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1000, 1, 1), (1, 1, 700), (33, 1, 65), (64, 64, 64), (240, 123, 100)])
+def test_distance(gpu_core, shape):
+    rng = np.random.default_rng(sum(shape))
+    g = (rng.random(shape) < 0.001).astype(np.int32)
+    g[rng.random(shape) < 0.01] = 3
+    assert np.array_equal(gpu_core.calculate_distance(g), O.calculate_distance(g))
+    assert np.array_equal(gpu_core.calculate_distance(np.zeros(shape, np.int32)),
+                          O.calculate_distance(np.zeros(shape, np.int32)))
+
+
+@pytest.mark.parametrize("shape", [(5, 6, 7), (16, 16, 16), (31, 20, 9)])
+def test_corr_conv(gpu_core, shape):
+    rng = np.random.default_rng(shape[0])
+    a = rng.integers(0, 6, shape).astype(np.int32)
+    b = rng.integers(0, 3, shape).astype(np.int32)
+    assert np.array_equal(gpu_core.dft_corr3(a, b), O.dft_corr3(a, b))
+    assert np.array_equal(gpu_core.dft_conv3(a, b), O.dft_conv3(a, b))
+    item = (rng.random((3, 4, 2)) < 0.6).astype(np.int32)
+    assert np.array_equal(gpu_core.collision_grid(a, item), O.collision_grid(a, item))
+    tray = (rng.random(shape) < 0.3).astype(np.int32)
+    assert np.array_equal(gpu_core.interlocking_free_positions(tray, item),
+                          O.interlocking_free_positions(tray, item))
+
+
+def test_place_in_tray(gpu_core):
+    tray = np.zeros((6, 5, 4), np.int32)
+    tray[2, 2, 2] = 9
+    it = np.ones((2, 2, 2), np.int32)
+    out = gpu_core.place_in_tray(it, tray, (0, 0, 0), 5)
+    assert np.array_equal(out, O.place_in_tray(it, tray, (0, 0, 0), 5))
+    with pytest.raises(RuntimeError, match=r"position \(2, 2, 2\)"):
+        gpu_core.place_in_tray(it, tray, (1, 1, 1), 5)
+    # clipped at the tray edge like the reference loop
+    out = gpu_core.place_in_tray(it, tray, (5, 4, 3), 7)
+    assert np.array_equal(out, O.place_in_tray(it, tray, (5, 4, 3), 7))
+
+
+# --------------------------------------------------------------------------
+# whole packing runs: identical placements, trays and densities
+# --------------------------------------------------------------------------
+def run_both(items, tray_size, n_orient, interlock):
+    from psacking_b200 import BinPacker
+    out = {}
+    for engine in ("native", "calls"):
+        r = BinPacker(tray_size, num_orientations=n_orient, interlocking_free=interlock,
+                      engine=engine).pack_voxels(items)
+        out[engine] = r
+    want_tray, want_pl = O.pack_voxels(items, tray_size, n_orient, interlock)
+    for engine, r in out.items():
+        assert np.array_equal(r.tray, want_tray), engine
+        for p, w in zip(r.placements, want_pl):
+            assert (p.success, p.position, p.orientation_index) == (w["success"], w["position"],
+                                                                   w["orientation_index"]), engine
+            if p.success:
+                assert p.score == w["score"]
+        assert r.density == O.density(want_tray)
+    return out
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_config1_packing(gpu_core, seed):
+    from psacking_b200 import workloads
+    run_both(workloads.config1_items(seed), workloads.TRAY1, 1, False)
+
+
+def test_config2_prefix_packing(gpu_core):
+    from psacking_b200 import workloads
+    items = workloads.config2_items(100)[:6]
+    run_both(items, workloads.TRAY2, 24, False)
+
+
+def test_config3_prefix_packing(gpu_core):
+    from psacking_b200 import workloads
+    items = workloads.config3_items(100)[:3]
+    run_both(items, workloads.TRAY3, 24, True)
+
+
+def test_small_interlock_packing(gpu_core):
+    from psacking_b200 import workloads
+    items = workloads.config1_items(7)[:12]
+    run_both(items, (40, 40, 12), 4, True)
+    run_both(items, (40, 40, 12), 6, False)
+
+
+# --------------------------------------------------------------------------
+# the score expression of the reference as nvcc evaluates it
+# --------------------------------------------------------------------------
+def test_reference_score_expression_is_fused(tmp_path):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    so = tmp_path / "probe.so"
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
+                    "-o", str(so), str(HERE / "probes" / "score_probe.cu")], check=True)
+    lib = ctypes.CDLL(str(so))
+    rng = np.random.default_rng(0)
+    n = 4096
+    prox = rng.integers(0, 3_000_000, n).astype(np.int32)
+    nz = 100
+    k = rng.integers(0, nz, n).astype(np.int32)
+    out = np.zeros(n, np.float64)
+    P = ctypes.POINTER
+    rc = lib.run_score_probe(prox.ctypes.data_as(P(ctypes.c_int)), k.ctypes.data_as(P(ctypes.c_int)),
+                             ctypes.c_int(nz), ctypes.c_double(1e8), out.ctypes.data_as(P(ctypes.c_double)),
+                             ctypes.c_int(n))
+    assert rc == 0
+    fused = np.array([O.score_block(int(p), int(kk), nz) for p, kk in zip(prox, k)])
+    assert np.array_equal(out, fused)

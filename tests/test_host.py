@@ -1,0 +1,66 @@
+"""Host-side logic: orientation order, packer argument checks, .vox layout, workloads."""
+import numpy as np
+import pytest
+
+from oracle import psb_oracle as O
+from psacking_b200 import BinPacker, workloads
+from psacking_b200.rotations import apply_map, get_orientations, orientation_maps
+from psacking_b200.vox import encode_vox
+
+
+@pytest.mark.parametrize("n", [1, 4, 6, 24])
+def test_orientations_match_reference_order(n):
+    rng = np.random.default_rng(n)
+    it = rng.integers(0, 4, (2, 3, 5))
+    mine = get_orientations(it, n)
+    ref = O.orientations(it, n)
+    assert len(mine) == n
+    assert all(np.array_equal(a, b) for a, b in zip(mine, ref))
+    maps = orientation_maps(n)
+    assert all(np.array_equal(apply_map(it, maps[k]), ref[k]) for k in range(n))
+
+
+def test_24_orientations_distinct():
+    it = np.arange(2 * 3 * 4).reshape(2, 3, 4)
+    ors = get_orientations(it, 24)
+    keys = {(o.shape, o.tobytes()) for o in ors}
+    assert len(keys) == 24
+
+
+def test_packer_validation():
+    with pytest.raises(ValueError):
+        BinPacker((10, 10))
+    with pytest.raises(ValueError):
+        BinPacker((10, -1, 10))
+    with pytest.raises(ValueError):
+        BinPacker((10, 10, 10), voxel_resolution=0)
+    with pytest.raises(ValueError):
+        BinPacker((10, 10, 10), num_orientations=5)
+    p = BinPacker((10, 10, 10))
+    with pytest.raises(ValueError, match="empty"):
+        p.pack_voxels([])
+    with pytest.raises(ValueError):
+        p.pack_voxels([np.ones((2, 2))])
+    assert "BinPacker(tray_size=(10, 10, 10)" in repr(p)
+
+
+def test_vox_layout():
+    g = np.zeros((2, 1, 3), np.int32)
+    g[1, 0, 2] = 7
+    b = encode_vox(g)
+    assert np.frombuffer(b[:12], "<i4").tolist() == [2, 1, 3]
+    body = np.frombuffer(b[12:12 + 6], np.uint8)
+    # x from high to low, z from high to low: first byte is (1,0,2)
+    assert body[0] == 123 + 7 % 5 and (body[1:] == 255).all()
+    assert len(b) == 12 + 6 + 768
+
+
+def test_workloads_deterministic_and_in_range():
+    a = workloads.config1_items(3)
+    b = workloads.config1_items(3)
+    assert len(a) == 20 and all(np.array_equal(x, y) for x, y in zip(a, b))
+    assert all(max(i.shape) <= 16 for i in a)
+    c3 = workloads.config3_items(0, n=30)
+    assert all(20 <= max(i.shape) <= 50 for i in c3)
+    c2 = workloads.config2_items(0, n=10)
+    assert all(max(i.shape) <= 40 for i in c2)
