@@ -40,7 +40,7 @@ int fail(int code, const char* fmt, ...) {
 #define CK(call)                                                                                   \
     do {                                                                                           \
         cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess)                                                                     \
+        if (e_ != cudaSuccess && (cudaGetLastError(), true))                                       \
             return fail(PSB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
                         __LINE__);                                                                 \
     } while (0)
@@ -60,7 +60,6 @@ int fail(int code, const char* fmt, ...) {
     } while (0)
 
 constexpr double kP = 100000000.0;  // constants.h:7
-constexpr int kMaxSmem = 227 * 1024;
 constexpr int kCandCap = 1 << 18;
 
 int ensure_device() {
@@ -173,18 +172,30 @@ int get_plan(int n, Plan1D* out) {
     return PSB_OK;
 }
 
+int g_smem_optin = 0;  // max dynamic shared memory per block of the current device
+
+template <class K>
+int set_max_dyn_smem(K func) {
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, func));
+    int dyn = g_smem_optin - (int)fa.sharedSizeBytes;
+    CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    return PSB_OK;
+}
+
 int set_smem_attrs() {
     static bool done[64] = {false};
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 64 && done[dev]) return PSB_OK;
-    CK(cudaFuncSetAttribute(k_rfft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
-    CK(cudaFuncSetAttribute(k_irfft_z_int, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
-    CK(cudaFuncSetAttribute(k_fft_mid<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
-    CK(cudaFuncSetAttribute(k_fft_mid<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
-    CK(cudaFuncSetAttribute(k_xpass, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
-    CK(cudaFuncSetAttribute(k_plane, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
-    CK(cudaFuncSetAttribute(k_dist_axis, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+    CK(cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    TRY(set_max_dyn_smem(k_rfft_z));
+    TRY(set_max_dyn_smem(k_irfft_z_int));
+    TRY(set_max_dyn_smem(k_fft_mid<-1>));
+    TRY(set_max_dyn_smem(k_fft_mid<1>));
+    TRY(set_max_dyn_smem(k_xpass));
+    TRY(set_max_dyn_smem(k_plane));
+    TRY(set_max_dyn_smem(k_dist_axis));
     if (dev < 64) done[dev] = true;
     return PSB_OK;
 }
@@ -670,7 +681,7 @@ struct psb_tray {
         int wsz = std::max(PSB_TILE * g.F[1], PSB_PAIRS * g.F[2]);
         size_t smp = sizeof(float2) * ((size_t)g.F[1] + g.F[2] + (size_t)ny * g.H + 2 * (size_t)wsz) +
                      sizeof(uint32_t) * (size_t)ny * nzw;
-        if (smp > (size_t)kMaxSmem) return fail(PSB_ERR_ARG, "tray too large for the plane kernel (%zu B smem)", smp);
+        if (smp + 64 > (size_t)g_smem_optin) return fail(PSB_ERR_ARG, "tray too large for the plane kernel (%zu B smem)", smp);
         {
             PROF("k_plane", st);
             k_plane<<<dim3(nx, n), PSB_THREADS, smp, st>>>(d_od, sb, pb, sp, g.F[1], g.F[2], g.p[1].p, g.p[2].p,
