@@ -128,9 +128,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload(rank):
+def workload(rank, n_items=N_ITEMS):
     from psacking_b200 import workloads
-    return workloads.config3_items(seed=1 + 1000 * rank, n=N_ITEMS)
+    return workloads.config3_items(seed=1 + 1000 * rank, n=n_items)
 
 
 def sorted_items(items):
@@ -175,7 +175,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     lib = load_lib()
-    items = workload(rank)
+    items = workload(rank, args.items)
     seq = sorted_items(items)
     maps = orientation_maps(N_ORIENT)
     tray0 = np.zeros(TRAY, np.int32)
@@ -234,7 +234,7 @@ def run_ours(args, rank, world, local_rank):
     # e2e through the public API: host numpy in, host numpy out
     packer = BinPacker(TRAY, num_orientations=N_ORIENT, interlocking_free=True)
     e2e_ms = []
-    for i in range(max(1, min(args.steps, 2)) + 1):
+    for i in range(0 if args.value_only else max(1, min(args.steps, 2)) + 1):
         flush.fill_(1)
         torch.cuda.synchronize()
         barrier()
@@ -247,7 +247,9 @@ def run_ours(args, rank, world, local_rank):
         barrier()
         if i > 0:  # first call is a warm-up of the public path
             e2e_ms.append(a.elapsed_time(b))
-    e2e_placed = r.num_placed
+    if args.value_only:
+        e2e_ms, r = [total_ms / args.steps], None
+    e2e_placed = r.num_placed if r is not None else placed
     h2d = sum(s.nbytes for s in seq) + sum(int(np.count_nonzero(s)) * 16 for s in seq) + tray0.nbytes
     d2h = tray0.nbytes + len(seq) * 40
     check(lib, lib.psb_tray_destroy(t))
@@ -298,7 +300,7 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FFT), i64/f64 (exact tie guard)",
         "data": "synthetic (seeded config-3 shapes; Thingi10K unavailable)",
-        "config": {"workload": "config3: 240x123x100 tray, 350 items (extent 20-50), 24 orientations, "
+        "config": {"workload": f"config3: 240x123x100 tray, {args.items} items (extent 20-50), 24 orientations, "
                                "interlocking-free, K=1 (no lookahead yet)",
                    "items_per_step": len(seq), "items_placed_per_step": placed, "orientations_per_step": ab["orientations"],
                    "l2": "256 MiB buffer written before every step", "parallelism": f"replicas x{world} (independent trays)",
@@ -361,6 +363,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--items", type=int, default=N_ITEMS, help="profiling only: shorter item stream")
+    ap.add_argument("--value-only", action="store_true", help="profiling only: skip the e2e leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -159,6 +159,11 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
 int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                     psb_result* out_placements, int32_t* final_tray);
 
+/* Kernel variant switch (default on): FFT lengths 64, 100, 125, 128, 240 use
+ * the specialised two-pass kernels; off forces the generic mixed-radix path
+ * (used by the tests to check both). */
+int psb_set_fast_fft(int on);
+
 /* ---- tracing (the reference's SCOPED_TIMER, spectral_packing/timing.h:11-31,
  *      as CUDA events around every kernel launch; off by default) ---------- */
 int psb_profile_enable(int on);          /* clears previous records            */

@@ -420,6 +420,8 @@ PYBIND11_MODULE(_core, m) {
           py::arg("interlock"), py::arg("id_offset"));
     m.def("search_detail", &py_search_detail, py::arg("orientations"), py::arg("flags"));
     m.def("device_count", &py_device_count);
+    m.def("set_fast_fft", [](bool on) { psb_set_fast_fft(on ? 1 : 0); }, py::arg("on"),
+          "Use the specialised two-pass FFT kernels where a plan exists (default) or force the generic path.");
     m.attr("VOXEL_RESOLUTION") = 128;
     m.attr("HEIGHT_PENALTY") = 100000000.0;
     m.attr("__version__") = "0.1.0";

@@ -19,6 +19,7 @@
 
 #include "../../include/psb200.h"
 #include "psb_kernels2.cuh"
+#include "psb_kernels3.cuh"
 
 namespace {
 
@@ -173,6 +174,53 @@ int get_plan(int n, Plan1D* out) {
 }
 
 int g_smem_optin = 0;  // max dynamic shared memory per block of the current device
+bool g_fast_fft = true;  // specialised two-pass kernels where a plan exists
+
+using XpassFn = void (*)(const OrientDesc*, SearchBufs, const float2*, const float2*, int, const float2*);
+using PlaneFn = void (*)(const OrientDesc*, SearchBufs, PlaneBufs, ScoreParams, const float2*, const float2*);
+
+XpassFn xpass2_for(int n) {
+    switch (n) {
+        case 64: return k_xpass2<64>;
+        case 100: return k_xpass2<100>;
+        case 125: return k_xpass2<125>;
+        case 128: return k_xpass2<128>;
+        case 240: return k_xpass2<240>;
+        default: return nullptr;
+    }
+}
+
+#define PSB_PLANE_ROW(NY)                      \
+    case NY:                                   \
+        switch (nz) {                          \
+            case 64: return k_plane2<NY, 64>;   \
+            case 100: return k_plane2<NY, 100>; \
+            case 125: return k_plane2<NY, 125>; \
+            case 128: return k_plane2<NY, 128>; \
+            default: return nullptr;           \
+        }
+PlaneFn plane2_for(int ny, int nz) {
+    switch (ny) {
+        PSB_PLANE_ROW(64)
+        PSB_PLANE_ROW(100)
+        PSB_PLANE_ROW(125)
+        PSB_PLANE_ROW(128)
+        default: return nullptr;
+    }
+}
+#undef PSB_PLANE_ROW
+
+// register-DFT twiddles W_R^i for R <= 32 (offset R*(R-1)/2)
+int init_register_twiddles() {
+    std::vector<float2> t(PSB_TWR_SIZE);
+    for (int R = 1; R <= 32; ++R)
+        for (int i = 0; i < R; ++i) {
+            double a = -2.0 * M_PI * (double)i / (double)R;
+            t[R * (R - 1) / 2 + i] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+    CK(cudaMemcpyToSymbol(c_twr, t.data(), sizeof(float2) * PSB_TWR_SIZE));
+    return PSB_OK;
+}
 
 template <class K>
 int set_max_dyn_smem(K func) {
@@ -196,6 +244,10 @@ int set_smem_attrs() {
     TRY(set_max_dyn_smem(k_xpass));
     TRY(set_max_dyn_smem(k_plane));
     TRY(set_max_dyn_smem(k_dist_axis));
+    for (int n : {64, 100, 125, 128, 240}) TRY(set_max_dyn_smem(xpass2_for(n)));
+    for (int a : {64, 100, 125, 128})
+        for (int b : {64, 100, 125, 128}) TRY(set_max_dyn_smem(plane2_for(a, b)));
+    TRY(init_register_twiddles());
     if (dev < 64) done[dev] = true;
     return PSB_OK;
 }
@@ -662,9 +714,15 @@ struct psb_tray {
         }
         CKL();
         SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
-        size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
-        {
+        XpassFn xf = g_fast_fft ? xpass2_for(g.F[0]) : nullptr;
+        if (xf && xpass2_smem(g.F[0]) + 64 <= (size_t)g_smem_optin) {
             PROF("k_xpass", st);
+            int ncols = g.F[1] * g.H;
+            xf<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
+                d_od, sb, d_Socc, d_Sphi, ncols, g.p[0].tw);
+        } else {
+            PROF("k_xpass", st);
+            size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
             k_xpass<<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], n), PSB_THREADS, smx, st>>>(
                 d_od, sb, d_Socc, d_Sphi, g.F[1], g.H, g.p[0].p, g.p[0].tw);
         }
@@ -678,11 +736,17 @@ struct psb_tray {
         CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
         ScoreParams sp = score_params(mode);
         PlaneBufs pb{d_free, d_Dq, d_smin, d_diag, sBits, sD};
-        int wsz = std::max(PSB_TILE * g.F[1], PSB_PAIRS * g.F[2]);
-        size_t smp = sizeof(float2) * ((size_t)g.F[1] + g.F[2] + (size_t)ny * g.H + 2 * (size_t)wsz) +
-                     sizeof(uint32_t) * (size_t)ny * nzw;
-        if (smp + 64 > (size_t)g_smem_optin) return fail(PSB_ERR_ARG, "tray too large for the plane kernel (%zu B smem)", smp);
-        {
+        PlaneFn pf = g_fast_fft ? plane2_for(g.F[1], g.F[2]) : nullptr;
+        size_t sm2 = plane2_smem(g.F[1], g.F[2], ny, nzw) + 64;
+        if (pf && sm2 <= (size_t)g_smem_optin) {
+            PROF("k_plane", st);
+            pf<<<dim3(nx, n), 256, sm2, st>>>(d_od, sb, pb, sp, g.p[1].tw, g.p[2].tw);
+        } else {
+            int wsz = std::max(PSB_TILE * g.F[1], PSB_PAIRS * g.F[2]);
+            size_t smp = sizeof(float2) * ((size_t)g.F[1] + g.F[2] + (size_t)ny * g.H + 2 * (size_t)wsz) +
+                         sizeof(uint32_t) * (size_t)ny * nzw;
+            if (smp + 64 > (size_t)g_smem_optin)
+                return fail(PSB_ERR_ARG, "tray too large for the plane kernel (%zu B smem)", smp);
             PROF("k_plane", st);
             k_plane<<<dim3(nx, n), PSB_THREADS, smp, st>>>(d_od, sb, pb, sp, g.F[1], g.F[2], g.p[1].p, g.p[2].p,
                                                             g.p[1].tw, g.p[2].tw);
@@ -1336,6 +1400,11 @@ int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int 
              int n_orient, int interlock, int32_t id_offset, psb_result* out_placements, int32_t* final_tray) {
     TRY(psb_pack_stage(t, items, dims, n_items));
     return psb_pack_staged(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray);
+}
+
+int psb_set_fast_fft(int on) {
+    g_fast_fft = on != 0;
+    return PSB_OK;
 }
 
 int psb_profile_enable(int on) {

@@ -1,0 +1,184 @@
+// psb_kernels3.cuh — the search's two hot kernels specialised for FFT
+// lengths with two-pass radix plans (Plan2 in psb_fft2.cuh).  Same inputs,
+// outputs and semantics as k_xpass / k_plane in psb_kernels.cuh, which remain
+// the path for other lengths.
+#pragma once
+#include "psb_fft2.cuh"
+#include "psb_kernels.cuh"
+
+#define PSB_XCOLS 16   // spectrum columns (ky*Hz + kz) per CTA in k_xpass2
+
+// Fused x pass over a tile of PSB_XCOLS consecutive columns c = ky*Hz + kz
+// (contiguous in memory, so every row access of the tile is one 128-byte
+// segment): item forward along x (pass 1 reads global), products with the
+// tray's two spectra fused into the last forward pass, inverse along x for
+// both products (last pass writes global rows x < Xv).
+// grid: (ceil(Fy*Hz / PSB_XCOLS), n_orient), block 256
+template <int N>
+__global__ void __launch_bounds__(256)
+k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __restrict__ Socc,
+         const float2* __restrict__ Sphi, int ncols, const float2* __restrict__ g_tw) {
+    constexpr int C = PSB_XCOLS;
+    constexpr int R0 = Plan2<N>::R0, R1 = Plan2<N>::R1;
+    extern __shared__ float2 sm[];
+    const int o = blockIdx.y;
+    const OrientDesc& od = orients[o];
+    if (od.skip || od.valid[0] <= 0) return;
+    const int c0 = blockIdx.x * C;
+    const int nl = min(C, ncols - c0);
+    float2* tw = sm;
+    float2* A = tw + N;
+    float2* Bc = A + N * C;
+    float2* Bd = Bc + N * C;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    load_twiddles(tw, g_tw, N, tid, nthr);
+    __syncthreads();
+    const int ex = od.e[0], Xv = od.valid[0];
+    const float2* Bi = sb.Bi + (size_t)o * sb.sB + c0;
+    float2* Pc = sb.Pc + (size_t)o * sb.sP + c0;
+    float2* Pd = sb.Pd + (size_t)o * sb.sP + c0;
+    const float2* So = Socc + c0;
+    const float2* Sp = Sphi + c0;
+    tpass<N, R0, 1, -1, C, false>(
+        [&](int c, int n) { return n < ex ? Bi[(size_t)n * ncols + c] : make_float2(0.f, 0.f); },
+        [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
+    __syncthreads();
+    tpass<N, R1, R0, -1, C, false>(
+        [&](int c, int n) { return A[n * C + c]; },
+        [&](int c, int k, float2 v) {
+            size_t g = (size_t)k * ncols + c;
+            Bc[k * C + c] = c_cmul(v, So[g]);
+            Bd[k * C + c] = c_cmul(v, Sp[g]);
+        },
+        nl, tw, tid, nthr);
+    __syncthreads();
+    tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return Bc[n * C + c]; },
+                                 [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
+    __syncthreads();
+    tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
+                                  [&](int c, int x, float2 v) {
+                                      if (x < Xv) Pc[(size_t)x * ncols + c] = v;
+                                  },
+                                  nl, tw, tid, nthr);
+    __syncthreads();
+    tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return Bd[n * C + c]; },
+                                 [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
+    __syncthreads();
+    tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
+                                  [&](int c, int x, float2 v) {
+                                      if (x < Xv) Pd[(size_t)x * ncols + c] = v;
+                                  },
+                                  nl, tw, tid, nthr);
+}
+
+constexpr size_t xpass2_smem(int N) { return sizeof(float2) * ((size_t)N + 3 * (size_t)N * PSB_XCOLS); }
+
+// shared memory of k_plane2: twiddles, work buffer A, the y-inverted plane Q
+// (ny rows) and the plane's free bits
+inline size_t plane2_smem(int NY, int NZ, int ny, int nzw) {
+    const size_t HZ = NZ / 2 + 1;
+    const size_t a = std::max((size_t)NY * HZ, (size_t)((ny + 1) / 2) * NZ);
+    return sizeof(float2) * (NY + NZ + a + (size_t)ny * HZ) + sizeof(uint32_t) * (size_t)ny * nzw;
+}
+
+// Per (x-plane, orientation): inverse along y then C2R along z (two rows per
+// complex transform) for the collision field, then the proximity field.
+// grid: (nx, n_orient), block 256
+template <int NY, int NZ>
+__global__ void __launch_bounds__(256)
+k_plane2(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, ScoreParams sp,
+         const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
+    constexpr int HZ = NZ / 2 + 1;
+    constexpr int RY0 = Plan2<NY>::R0, RY1 = Plan2<NY>::R1;
+    constexpr int RZ0 = Plan2<NZ>::R0, RZ1 = Plan2<NZ>::R1;
+    extern __shared__ float2 sm[];
+    const int o = blockIdx.y;
+    const OrientDesc& od = orients[o];
+    if (od.skip) return;
+    const int x = blockIdx.x;
+    const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
+    if (x >= Xv || Yv <= 0 || Zv <= 0) return;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int ny = sp.ny, nzw = sp.nzw;
+    const int npairs = (Yv + 1) / 2;
+    float2* twy = sm;
+    float2* twz = twy + NY;
+    float2* A = twz + NZ;
+    const size_t asz = max((size_t)NY * HZ, (size_t)((ny + 1) / 2) * NZ);
+    float2* Q = A + asz;
+    uint32_t* bits = (uint32_t*)(Q + (size_t)ny * HZ);
+    load_twiddles(twy, g_twy, NY, tid, nthr);
+    load_twiddles(twz, g_twz, NZ, tid, nthr);
+    for (int i = tid; i < Yv * nzw; i += nthr) bits[i] = 0u;
+    __syncthreads();
+    const float scale = sp.scale;
+    double local_min = 1e300;
+    unsigned int diag = 0;
+    float* Dq = pb.Dq + (size_t)o * pb.sD;
+    const double base = od.base;
+    for (int field = 0; field < 2; ++field) {
+        const float2* P = (field == 0 ? sb.Pc : sb.Pd) + (size_t)o * sb.sP + (size_t)x * NY * HZ;
+        tpass<NY, RY0, 1, 1, HZ, false>([&](int c, int n) { return P[(size_t)n * HZ + c]; },
+                                        [&](int c, int n, float2 v) { A[n * HZ + c] = v; }, HZ, twy, tid, nthr);
+        __syncthreads();
+        tpass<NY, RY1, RY0, 1, HZ, false>([&](int c, int n) { return A[n * HZ + c]; },
+                                          [&](int c, int y, float2 v) {
+                                              if (y < Yv) Q[y * HZ + c] = v;
+                                          },
+                                          HZ, twy, tid, nthr);
+        __syncthreads();
+        tpass<NZ, RZ0, 1, 1, 1, true>(
+            [&](int p, int k) {
+                const int ya = 2 * p, yb = ya + 1;
+                const bool hb = yb < Yv;
+                if (k < HZ) {
+                    float2 xa = Q[ya * HZ + k];
+                    float2 xb = hb ? Q[yb * HZ + k] : make_float2(0.f, 0.f);
+                    return make_float2(xa.x - xb.y, xa.y + xb.x);
+                }
+                float2 xa = Q[ya * HZ + (NZ - k)];
+                float2 xb = hb ? Q[yb * HZ + (NZ - k)] : make_float2(0.f, 0.f);
+                return make_float2(xa.x + xb.y, xb.x - xa.y);
+            },
+            [&](int p, int n, float2 v) { A[p * NZ + n] = v; }, npairs, twz, tid, nthr);
+        __syncthreads();
+        tpass<NZ, RZ1, RZ0, 1, 1, true>(
+            [&](int p, int n) { return A[p * NZ + n]; },
+            [&](int p, int z, float2 v) {
+                if (z >= Zv) return;
+#pragma unroll
+                for (int half = 0; half < 2; ++half) {
+                    const int y = 2 * p + half;
+                    if (y >= Yv) break;
+                    const float val = (half ? v.y : v.x) * scale;
+                    if (field == 0) {
+                        const float rv = rintf(val);
+                        if (rv == 0.f) atomicOr(&bits[y * nzw + (z >> 5)], 1u << (z & 31));
+                        if (fabsf(val - rv) > 0.25f) diag |= 2u;
+                    } else {
+                        const size_t t = ((size_t)x * ny + y) * sp.nz + z;
+                        Dq[t] = val;
+                        if ((bits[y * nzw + (z >> 5)] >> (z & 31)) & 1u)
+                            local_min = fmin(local_min, ref_score(sp, base + (double)val, z));
+                    }
+                }
+            },
+            npairs, twz, tid, nthr);
+        __syncthreads();
+    }
+    uint32_t* fb = pb.freebits + (size_t)o * pb.sBits + (size_t)x * ny * nzw;
+    for (int i = tid; i < Yv * nzw; i += nthr) fb[i] = bits[i];
+    __shared__ double red[8];
+    for (int off = 16; off > 0; off >>= 1) local_min = fmin(local_min, __shfl_xor_sync(0xffffffffu, local_min, off));
+    unsigned int dg = __reduce_or_sync(0xffffffffu, diag);
+    if ((tid & 31) == 0) {
+        red[tid >> 5] = local_min;
+        if (dg) atomicOr(&pb.diag[o], dg);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double m = red[0];
+        for (int w = 1; w < nthr / 32; ++w) m = fmin(m, red[w]);
+        if (m < 1e299) atomicMin(&pb.smin[o], ord_key(m));
+    }
+}

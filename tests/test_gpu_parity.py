@@ -130,7 +130,14 @@ def test_search_empty_and_full(gpu_core):
     check_search(gpu_core, tray, [big, it], BLOCK)
 
 
-def test_search_config3_scale(gpu_core):
+@pytest.fixture(params=["fast", "generic"])
+def fft_variant(request, gpu_core):
+    gpu_core.set_fast_fft(request.param == "fast")
+    yield request.param
+    gpu_core.set_fast_fft(True)
+
+
+def test_search_config3_scale(gpu_core, fft_variant):
     """240x123x100 tray (the benchmark's tray), two large items, 24 orientations
     of one of them, interlocking mask on: exact parity at full size."""
     from psacking_b200 import workloads
@@ -210,18 +217,18 @@ def run_both(items, tray_size, n_orient, interlock):
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
-def test_config1_packing(gpu_core, seed):
+def test_config1_packing(gpu_core, seed, fft_variant):
     from psacking_b200 import workloads
     run_both(workloads.config1_items(seed), workloads.TRAY1, 1, False)
 
 
-def test_config2_prefix_packing(gpu_core):
+def test_config2_prefix_packing(gpu_core, fft_variant):
     from psacking_b200 import workloads
     items = workloads.config2_items(100)[:6]
     run_both(items, workloads.TRAY2, 24, False)
 
 
-def test_config3_prefix_packing(gpu_core):
+def test_config3_prefix_packing(gpu_core, fft_variant):
     from psacking_b200 import workloads
     items = workloads.config3_items(100)[:3]
     run_both(items, workloads.TRAY3, 24, True)
