@@ -51,7 +51,7 @@ N_ORIENT = 24
 class PsbResult(ctypes.Structure):
     _fields_ = [("x", ctypes.c_int32), ("y", ctypes.c_int32), ("z", ctypes.c_int32), ("found", ctypes.c_int32),
                 ("score", ctypes.c_double), ("orientation", ctypes.c_int32), ("diag", ctypes.c_uint32),
-                ("n_candidates", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("n_candidates", ctypes.c_int32), ("err_ratio", ctypes.c_float)]
 
 
 def load_lib():
@@ -225,6 +225,8 @@ def run_ours(args, rank, world, local_rank):
     diag = 0
     for r in res:
         diag |= r.diag
+    cands = [r.n_candidates for r in res]
+    err_ratio = max(r.err_ratio for r in res)
     same = placed_first == [(r.found, r.x, r.y, r.z, r.orientation) for r in res]
     total_ms = sum(ms)
     Fdims = (ctypes.c_int * 3)()
@@ -304,7 +306,10 @@ def run_ours(args, rank, world, local_rank):
                                "interlocking-free, K=1 (no lookahead yet)",
                    "items_per_step": len(seq), "items_placed_per_step": placed, "orientations_per_step": ab["orientations"],
                    "l2": "256 MiB buffer written before every step", "parallelism": f"replicas x{world} (independent trays)",
-                   "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag},
+                   "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag,
+                   "tie_guard": {"candidates_per_item_mean": round(statistics.mean(cands), 1),
+                                 "candidates_per_item_max": max(cands),
+                                 "max_fp32_error_over_bound": round(err_ratio, 4)}},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_mean, 3),
                 "placements_match_value_leg": e2e_placed == placed},

@@ -55,7 +55,7 @@ typedef struct psb_result {
     int32_t orientation;   /* index into the orientation list, -1 when not found    */
     uint32_t diag;         /* PSB_DIAG_* bits                                       */
     int32_t n_candidates;  /* candidates examined by the exact tie guard             */
-    int32_t reserved;
+    float   err_ratio;     /* largest |FP32 - exact| / bound among re-scored candidates */
 } psb_result;
 
 typedef struct psb_tray psb_tray;   /* a device-resident tray (GPUTrayContext) */

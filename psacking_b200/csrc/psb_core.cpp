@@ -354,7 +354,7 @@ py::tuple py_pack_native(py::list items, py::handle initial_tray, py::array_t<in
     py::list pl;
     for (auto& r : res)
         pl.append(py::make_tuple(py::make_tuple(r.x, r.y, r.z), (bool)r.found, r.score, r.orientation, r.diag,
-                                 r.n_candidates));
+                                 r.n_candidates, r.err_ratio));
     return py::make_tuple(out, pl);
 }
 
@@ -377,7 +377,8 @@ py::dict py_search_detail(py::list orientations, int flags) {
     check(st);
     py::list pl;
     for (auto& r : per)
-        pl.append(py::make_tuple(py::make_tuple(r.x, r.y, r.z), (bool)r.found, r.score, r.diag, r.n_candidates));
+        pl.append(py::make_tuple(py::make_tuple(r.x, r.y, r.z), (bool)r.found, r.score, r.diag, r.n_candidates,
+                                 r.err_ratio));
     py::dict d;
     d["best"] = py::make_tuple(py::make_tuple(best.x, best.y, best.z), (bool)best.found, best.score, best.orientation);
     d["per_orientation"] = pl;

@@ -488,6 +488,7 @@ struct psb_tray {
     double* d_cscore = nullptr;
     unsigned long long *d_smin = nullptr, *d_smin2 = nullptr, *d_best = nullptr, *d_bestkey = nullptr;
     unsigned int* d_diag = nullptr;
+    unsigned int* d_errmax = nullptr;
     OrientDesc* d_od = nullptr;
     RzDesc* d_rzs = nullptr;
     MidDesc* d_mids = nullptr;
@@ -513,7 +514,7 @@ struct psb_tray {
         dfree(d_Ai); dfree(d_Bi); dfree(d_Pc); dfree(d_Pd); dfree(d_Dq); dfree(d_free); dfree(d_reach);
         dfree(d_cnt); dfree(d_off); dfree(d_rz2); dfree(d_rline); dfree(d_par); dfree(d_rflag); dfree(d_total);
         dfree(d_cand); dfree(d_ncand); dfree(d_cscore); dfree(d_smin); dfree(d_smin2); dfree(d_best);
-        dfree(d_bestkey); dfree(d_diag); dfree(d_od); dfree(d_rzs); dfree(d_mids); dfree(d_res);
+        dfree(d_bestkey); dfree(d_diag); dfree(d_errmax); dfree(d_od); dfree(d_rzs); dfree(d_mids); dfree(d_res);
         cap = 0;
     }
     void release() {
@@ -538,13 +539,21 @@ struct psb_tray {
         TRY(dalloc(&d_tray, V)); TRY(dalloc(&d_phi, V));
         TRY(dalloc(&d_Socc, S)); TRY(dalloc(&d_Sphi, S));
         TRY(dalloc(&d_w1, (size_t)nx * ny * g.H)); TRY(dalloc(&d_w2, (size_t)nx * g.F[1] * g.H));
-        TRY(dalloc(&d_pen, nz)); TRY(dalloc(&d_rz, 4)); TRY(dalloc(&d_mid, 4)); TRY(dalloc(&d_stats, 4));
+        TRY(dalloc(&d_pen, 3 * (size_t)nz)); TRY(dalloc(&d_rz, 4)); TRY(dalloc(&d_mid, 4)); TRY(dalloc(&d_stats, 4));
         TRY(dalloc(&d_err, 1)); TRY(dalloc(&d_first, 1));
         CK(cudaMemset(d_err, 0, sizeof(unsigned int)));
         // SCAN-mode penalty table with the host libm pow (packing.cpp:630-631)
-        std::vector<double> pen(nz);
-        for (int k = 0; k < nz; ++k) pen[k] = kP * std::pow((k + 0.0) / (nz + 0.0), 3.0);
-        CK(cudaMemcpy(d_pen, pen.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+        // BLOCK-mode factors (fft3.cu:172-173): qz = k/nz, qa = (P*qz)*qz, both
+        // single IEEE operations, identical on host and device
+        std::vector<double> pen(3 * (size_t)nz);
+        for (int k = 0; k < nz; ++k) {
+            pen[k] = kP * std::pow((k + 0.0) / (nz + 0.0), 3.0);
+            volatile double qz = (double)k / (double)nz;
+            volatile double qa = (kP * qz) * qz;
+            pen[nz + k] = qa;
+            pen[2 * nz + k] = qz;
+        }
+        CK(cudaMemcpy(d_pen, pen.data(), sizeof(double) * 3 * nz, cudaMemcpyHostToDevice));
         return PSB_OK;
     }
 
@@ -569,7 +578,7 @@ struct psb_tray {
         TRY(dalloc(&d_cand, (size_t)kCandCap * c)); TRY(dalloc(&d_ncand, c));
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c));
         TRY(dalloc(&d_smin, c)); TRY(dalloc(&d_smin2, c)); TRY(dalloc(&d_best, c)); TRY(dalloc(&d_bestkey, c));
-        TRY(dalloc(&d_diag, c)); TRY(dalloc(&d_od, c)); TRY(dalloc(&d_rzs, c)); TRY(dalloc(&d_mids, c));
+        TRY(dalloc(&d_diag, c)); TRY(dalloc(&d_errmax, c)); TRY(dalloc(&d_od, c)); TRY(dalloc(&d_rzs, c)); TRY(dalloc(&d_mids, c));
         TRY(dalloc(&d_res, c));
         cap = c;
         return PSB_OK;
@@ -676,6 +685,8 @@ struct psb_tray {
         sp.nx = nx; sp.ny = ny; sp.nz = nz;
         sp.mode = mode;
         sp.pen = d_pen;
+        sp.qa = d_pen + nz;
+        sp.qz = d_pen + 2 * nz;
         sp.scale = (float)(1.0 / ((double)g.F[0] * g.F[1] * g.F[2]));
         sp.nzw = nzw;
         return sp;
@@ -732,6 +743,7 @@ struct psb_tray {
         CK(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_bestkey, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_diag, 0, sizeof(unsigned int) * n, st));
+        CK(cudaMemsetAsync(d_errmax, 0, sizeof(unsigned int) * n, st));
         CK(cudaMemsetAsync(d_ncand, 0, sizeof(int) * n, st));
         CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
         ScoreParams sp = score_params(mode);
@@ -790,14 +802,14 @@ struct psb_tray {
             CKL();
             ok = d_reach;
             smin = d_smin2;
-            SelectBufs s0{ok, sBits, d_Dq, sD, smin, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, kCandCap};
+            SelectBufs s0{ok, sBits, d_Dq, sD, smin, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, d_errmax, kCandCap};
             {
                 PROF("k_select_min", st);
                 k_select_min<<<dim3(nx, n), 256, 0, st>>>(d_od, s0, sp);
             }
             CKL();
         }
-        SelectBufs sel{ok, sBits, d_Dq, sD, smin, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, kCandCap};
+        SelectBufs sel{ok, sBits, d_Dq, sD, smin, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, d_errmax, kCandCap};
         {
             PROF("k_collect", st);
             k_collect<<<dim3(nx, n), 256, 0, st>>>(d_od, sel, sp);
@@ -875,7 +887,7 @@ void to_result(const ResultDev& r, int orient, psb_result* out) {
     out->orientation = r.found ? orient : -1;
     out->diag = r.diag;
     out->n_candidates = r.ncand;
-    out->reserved = 0;
+    out->err_ratio = r.err_ratio;
 }
 
 // Upload a set of explicit orientation arrays and describe them.
@@ -1153,7 +1165,7 @@ int psb_fft_search_placement(const int32_t* item, int ex, int ey, int ez, const 
     TRY(check_grid_args(item, ex, ey, ez, "fft_search_placement"));
     TRY(check_grid_args(tray, nx, ny, nz, "fft_search_placement"));
     if (!out) return fail(PSB_ERR_ARG, "fft_search_placement: null result");
-    psb_result none{-1, -1, -1, 0, 0.0, -1, 0, 0, 0};
+    psb_result none{-1, -1, -1, 0, 0.0, -1, 0, 0, 0.f};
     *out = none;
     if (ex > nx || ey > ny || ez > nz) return PSB_OK;  // bindings.cpp:189-194
     psb_tray* t = nullptr;
@@ -1273,7 +1285,7 @@ int psb_tray_search(psb_tray* t, const int32_t* const* items, const int32_t* dim
     if (!t || !items || !dims || !out || n < 0) return fail(PSB_ERR_ARG, "null pointer");
     if (!t->ready) return fail(PSB_ERR_STATE, "GPU tray context not initialized. Call gpu_tray_init() first.");
     CK(cudaSetDevice(t->dev));
-    psb_result none{-1, -1, -1, 0, 0.0, -1, 0, 0, 0};
+    psb_result none{-1, -1, -1, 0, 0.0, -1, 0, 0, 0.f};
     *out = none;
     if (n == 0) return PSB_OK;
     std::vector<OrientDesc> ods;
@@ -1371,13 +1383,15 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
         for (int o = 0; o < n_orient; ++o)
             t->describe(info, orient_maps + 6 * o, orient_maps + 6 * o + 3, d_item, d_vx, &ods[o]);
         TRY(t->search(ods, mode, interlock != 0, &res));
-        psb_result best{-1, -1, -1, 0, 0.0, -1, 0, 0, 0};
+        psb_result best{-1, -1, -1, 0, 0.0, -1, 0, 0, 0.f};
         double bs = 1e300;
         unsigned int diag = 0;
         int ncand = 0;
+        float errr = 0.f;
         for (int o = 0; o < n_orient; ++o) {
             diag |= res[o].diag;
             ncand += res[o].ncand;
+            errr = std::max(errr, res[o].err_ratio);
             if (ods[o].skip) continue;
             psb_result r;
             to_result(res[o], o, &r);
@@ -1385,6 +1399,7 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
         }
         best.diag = diag;
         best.n_candidates = ncand;
+        best.err_ratio = errr;
         if (best.found) {
             int32_t id = id_offset + placed + 1;
             TRY(t->place(ods[best.orientation], best.x, best.y, best.z, id, nullptr));

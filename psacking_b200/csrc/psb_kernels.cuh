@@ -324,18 +324,18 @@ struct ScoreParams {
     int nx, ny, nz;
     int mode;                 // PSB_MODE_SCAN / PSB_MODE_BLOCK
     const double* pen;        // SCAN: P*pow(k/nz,3) per k (host libm)
+    const double* qa;         // BLOCK: (P*qz)*qz per k, qz = k/nz (IEEE, host)
+    const double* qz;         // BLOCK: qz per k
     float scale;              // 1/(Fx*Fy*Fz)
     int nzw;                  // 32-bit words per (x,y) line of bit masks
 };
 
-// score of the reference for proximity value D at height k
+// score of the reference for proximity value D at height k:
+//   SCAN  packing.cpp:630-631  prox + P*pow(k/nz,3)          (plain add)
+//   BLOCK fft3.cu:172-173      prox + P*qz*qz*qz, the last multiply-add fused
 __device__ __forceinline__ double ref_score(const ScoreParams& sp, double D, int k) {
-    if (sp.mode == 0) {
-        return __dadd_rn(D, sp.pen[k]);
-    }
-    double qz = __ddiv_rn((double)k, (double)sp.nz);
-    double a = __dmul_rn(__dmul_rn(100000000.0, qz), qz);
-    return __fma_rn(a, qz, D);
+    if (sp.mode == 0) return __dadd_rn(D, __ldg(&sp.pen[k]));
+    return __fma_rn(__ldg(&sp.qa[k]), __ldg(&sp.qz[k]), D);
 }
 
 struct PlaneBufs {

@@ -20,6 +20,7 @@ struct SelectBufs {
     unsigned long long* best;      // exact best score key per orientation
     unsigned long long* bestkey;   // tie key per orientation
     unsigned int* diag;
+    unsigned int* errmax;          // max |D~ - D| / delta seen by the exact re-check (float bits)
     int cap;
 };
 
@@ -119,6 +120,7 @@ __global__ void k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb,
             if (lane == 0) {
                 if (!valid) atomicOr(&sb.diag[o], 4u);
                 if (err > od.delta) atomicOr(&sb.diag[o], 8u);
+                atomicMax(&sb.errmax[o], __float_as_uint((float)(err / od.delta)));
             }
         }
         if (lane == 0) {
@@ -155,6 +157,8 @@ struct ResultDev {
     double score;
     int ncand;
     unsigned int diag;
+    float err_ratio;
+    int pad;
 };
 
 __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, ResultDev* out,
@@ -166,6 +170,8 @@ __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb
     r.found = 0;
     r.score = 0.0;
     r.ncand = sb.ncand[o];
+    r.err_ratio = __uint_as_float(sb.errmax[o]);
+    r.pad = 0;
     r.diag = sb.diag[o] | (orients[o].exact ? 1u : 0u);
     if (sb.ncand[o] > sb.cap) r.diag |= 0x100u;
     if (!orients[o].skip && sb.best[o] != 0xffffffffffffffffULL) {

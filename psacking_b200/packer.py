@@ -144,17 +144,19 @@ class BinPacker:
         seq = [np.ascontiguousarray(processed[i]) for i in order]
         final, res = _core.pack_native(seq, tray, maps, bool(self.interlocking_free), int(id_offset))
         placements = []
-        diag_or, ncand = 0, 0
+        diag_or, ncand, err = 0, 0, 0.0
         for k, orig in enumerate(order):
-            pos, found, score, orient, diag, nc = res[k]
+            pos, found, score, orient, diag, nc, er = res[k]
             diag_or |= int(diag)
             ncand += int(nc)
+            err = max(err, float(er))
             if found:
                 placements.append(PlacementInfo(int(orig), tuple(int(v) for v in pos), float(score), True,
                                                 volumes[orig], int(orient)))
             else:
                 placements.append(PlacementInfo(int(orig), None, None, False, volumes[orig], 0))
-        return self._finish(final, placements, n_items, {"diag": diag_or, "candidates": ncand})
+        return self._finish(final, placements, n_items,
+                            {"diag": diag_or, "candidates": ncand, "max_err_ratio": err})
 
     def _pack_calls(self, processed, volumes, order, tray, id_offset, n_items):
         # a fresh run never inherits a cached tray context (the reference's

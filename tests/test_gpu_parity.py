@@ -88,7 +88,8 @@ def check_search(core, tray, items, flags, phi=None):
     inter = bool(flags & INTERLOCK)
     best = None
     for o, it in enumerate(items):
-        pos, found, score, diag, ncand = d["per_orientation"][o]
+        pos, found, score, diag, ncand, err_ratio = d["per_orientation"][o]
+        assert err_ratio <= 1.0
         assert not diag & (DIAG_FALSE_FREE | DIAG_BOUND), (o, hex(diag))
         if any(it.shape[a] > tray.shape[a] for a in range(3)):
             assert not found
