@@ -76,6 +76,27 @@ int psb_dft_conv3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, in
 /* dft_corr3 (packing.cpp:215-229): out[t] = sum_x b[x] * a[t+x], a zero outside. */
 int psb_dft_corr3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, int32_t* out);
 
+/* dft_corr3 for callers that cannot allocate device memory.  No counterpart
+ * in the reference.  Some callers own every byte of device memory themselves
+ * (a framework's caching allocator, a fixed memory budget) or must not call
+ * cudaMalloc/cudaFree because those calls synchronise the device and are not
+ * stream-ordered (latency-critical loops, code that will later be captured).
+ * This variant computes exactly what psb_dft_corr3 computes, but:
+ *   - d_a, d_b and d_out are DEVICE pointers to (nx,ny,nz) int32 grids that
+ *     the caller provides; work is queued on `stream` (a cudaStream_t, NULL
+ *     for the default stream) and the call returns without synchronising;
+ *   - its scratch is a fixed 3 MiB array in the library's device code, held
+ *     by every GPU that loads the library until the process exits;
+ *   - every axis must be <= 32 voxels; larger grids return PSB_ERR_LIMIT;
+ *   - it calls no cudaMalloc/cudaFree or other allocating routine.
+ * The first call on each device looks up the array's device address (make it
+ * before any stream capture).  All calls share the one array: calls that
+ * overlap on the GPU (different streams, or different host threads) race and
+ * must be serialised by the caller; calls queued on one stream are safe.
+ * Nothing in the array needs to start at zero: each call writes all it reads. */
+int psb_dft_corr3_noalloc(const int32_t* d_a, const int32_t* d_b, int nx, int ny, int nz,
+                          int32_t* d_out, void* stream);
+
 /* collision_grid (packing.cpp:241-252, binding bindings.cpp:360-372): the item
  * is zero-padded to the tray shape; out = dft_corr3(tray, item) with positions
  * where the item would leave the tray raised to at least 1. */

@@ -1042,6 +1042,100 @@ int psb_dft_corr3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, in
     return linear_transform_product(a, b, nx, ny, nz, 1, out);
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// dft_corr3 for callers that cannot allocate device memory
+// ---------------------------------------------------------------------------
+// Everything psb_dft_corr3 would allocate (two spectra, two transform work
+// buffers, the twiddle tables and the launch descriptors) lives in this fixed
+// array instead.  It is created when the library's device code is loaded on a
+// GPU and stays there until the process exits, on every GPU that loads it.
+namespace {
+constexpr int kNoAllocMaxSide = 32;                         // every axis <= 32 voxels
+constexpr size_t kNoAllocScratchBytes = (size_t)3 << 20;   // 3 MiB per GPU
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {nullptr};  // device address of the array, per device
+}  // namespace
+
+extern "C" {
+
+int psb_dft_corr3_noalloc(const int32_t* d_a, const int32_t* d_b, int nx, int ny, int nz, int32_t* d_out,
+                          void* stream) {
+    if (!d_a || !d_b || !d_out) return fail(PSB_ERR_ARG, "dft_corr3_noalloc: null device pointer");
+    if (nx <= 0 || ny <= 0 || nz <= 0)
+        return fail(PSB_ERR_ARG, "dft_corr3_noalloc: dims must be positive, got (%d,%d,%d)", nx, ny, nz);
+    if (nx > kNoAllocMaxSide || ny > kNoAllocMaxSide || nz > kNoAllocMaxSide)
+        return fail(PSB_ERR_LIMIT,
+                    "dft_corr3_noalloc: grid (%d,%d,%d) exceeds the fixed scratch limit of %d voxels per axis; "
+                    "use psb_dft_corr3", nx, ny, nz, kNoAllocMaxSide);
+    TRY(ensure_device());
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(PSB_ERR_ARG, "dft_corr3_noalloc: device index %d out of range", dev);
+    void* scratch = nullptr;
+    {
+        // once per device, with that device current: the array's device address
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_noalloc_ptr[dev] = p;
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    Grid3 g;
+    g.n[0] = nx; g.n[1] = ny; g.n[2] = nz;
+    for (int a = 0; a < 3; ++a) {
+        g.F[a] = fft_len(2 * g.n[a] - 1);
+        if (g.F[a] < 0 || !factorize(g.F[a], &g.p[a].p))
+            return fail(PSB_ERR_ARG, "dft_corr3_noalloc: no FFT length for axis %d", a);
+    }
+    g.H = g.F[2] / 2 + 1;
+    const size_t S = (size_t)g.F[0] * g.F[1] * g.H;
+    const size_t w1 = (size_t)nx * ny * g.H, w2 = (size_t)nx * g.F[1] * g.H;
+    char* p = (char*)scratch;
+    size_t used = 0;
+    auto take = [&](size_t n) {
+        char* r = p + used;
+        used += (n + 255) / 256 * 256;
+        return r;
+    };
+    float2* tw[3];
+    for (int a = 0; a < 3; ++a) tw[a] = (float2*)take(sizeof(float2) * g.F[a]);
+    RzDesc* d_rz = (RzDesc*)take(sizeof(RzDesc) * 2);
+    MidDesc* d_mid = (MidDesc*)take(sizeof(MidDesc) * 2);
+    float2* Sa = (float2*)take(sizeof(float2) * S);
+    float2* Sb = (float2*)take(sizeof(float2) * S);
+    float2* W1 = (float2*)take(sizeof(float2) * w1);
+    float2* W2 = (float2*)take(sizeof(float2) * w2);
+    if (used > kNoAllocScratchBytes)
+        return fail(PSB_ERR_LIMIT, "dft_corr3_noalloc: grid (%d,%d,%d) needs %zu B of scratch, the fixed array has %zu B",
+                    nx, ny, nz, used, kNoAllocScratchBytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    // twiddle tables into the array (every byte the transforms read is
+    // written first in stream order, so nothing needs clearing)
+    for (int a = 0; a < 3; ++a) {
+        std::vector<float2> t(g.F[a]);
+        for (int i = 0; i < g.F[a]; ++i) {
+            double ang = -2.0 * M_PI * (double)i / (double)g.F[a];
+            t[i] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+        CK(cudaMemcpyAsync(tw[a], t.data(), sizeof(float2) * g.F[a], cudaMemcpyHostToDevice, st));
+        g.p[a].tw = tw[a];
+    }
+    RzDesc ra{SRC_GRID_RAW, d_a, nx, ny, nz, 0, -1, nullptr};
+    RzDesc rb{SRC_GRID_RAW, d_b, nx, ny, nz, 0, -1, nullptr};
+    TRY(forward3(g, ra, W1, W2, Sa, d_rz, d_mid, st));
+    TRY(forward3(g, rb, W1, W2, Sb, d_rz + 1, d_mid, st));
+    k_spec_mul<<<grid1d(S), 256, 0, st>>>(Sa, Sb, Sa, S, 1);
+    CKL();
+    TRY(inverse3_int(g, Sa, W1, W2, d_out, d_mid, st));
+    return PSB_OK;
+}
+
 int psb_collision_grid(const int32_t* tray, int nx, int ny, int nz, const int32_t* item, int ex, int ey, int ez,
                        int32_t* out) {
     TRY(check_grid_args(tray, nx, ny, nz, "collision_grid"));
