@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -137,12 +138,23 @@ bool factorize(int n, AxisPlan* p) {
     return m == 1;
 }
 
-int fft_len(int n) {
+int fft_len_smooth(int n) {
     for (int m = std::max(n, 1); m <= PSB_MAX_FFT; ++m) {
         AxisPlan p;
         if (factorize(m, &p)) return m;
     }
     return -1;
+}
+
+// Smallest 7-smooth length >= n, or the smallest length >= n with a
+// specialised two-pass plan when that is at most 6% longer (e.g. 123 -> 128
+// rather than 125: radices 16 x 8 instead of 25 x 5, fewer registers).
+int fft_len(int n) {
+    int s = fft_len_smooth(n);
+    if (s < 0) return s;
+    for (int m = s; m <= PSB_MAX_FFT && m <= s + s / 16; ++m)
+        if (fast_len(m)) return m;
+    return s;
 }
 
 struct Plan1D {
@@ -473,6 +485,8 @@ struct psb_tray {
     unsigned int* d_err = nullptr;
     unsigned long long* d_first = nullptr;
 
+    int subbatch = 0;        // orientations per x-pass/plane-pass launch pair (0: all)
+
     int phi_mean = 0;
     double phi_norm = 0.0;
     int phi_maxabs = 0;
@@ -534,6 +548,7 @@ struct psb_tray {
         V = (size_t)nx * ny * nz;
         TRY(make_grid3(nx, ny, nz, false, &g));
         nzw = (nz + 31) / 32;
+        if (const char* e = getenv("PSB_SUBBATCH")) subbatch = atoi(e);
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         size_t S = (size_t)g.F[0] * g.F[1] * g.H;
         TRY(dalloc(&d_tray, V)); TRY(dalloc(&d_phi, V));
@@ -725,19 +740,6 @@ struct psb_tray {
         }
         CKL();
         SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
-        XpassFn xf = g_fast_fft ? xpass2_for(g.F[0]) : nullptr;
-        if (xf && xpass2_smem(g.F[0]) + 64 <= (size_t)g_smem_optin) {
-            PROF("k_xpass", st);
-            int ncols = g.F[1] * g.H;
-            xf<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
-                d_od, sb, d_Socc, d_Sphi, ncols, g.p[0].tw);
-        } else {
-            PROF("k_xpass", st);
-            size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
-            k_xpass<<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], n), PSB_THREADS, smx, st>>>(
-                d_od, sb, d_Socc, d_Sphi, g.F[1], g.H, g.p[0].p, g.p[0].tw);
-        }
-        CKL();
         CK(cudaMemsetAsync(d_smin, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_smin2, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long) * n, st));
@@ -748,22 +750,46 @@ struct psb_tray {
         CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
         ScoreParams sp = score_params(mode);
         PlaneBufs pb{d_free, d_Dq, d_smin, d_diag, sBits, sD};
+        XpassFn xf = g_fast_fft ? xpass2_for(g.F[0]) : nullptr;
+        if (xf && xpass2_smem(g.F[0]) + 64 > (size_t)g_smem_optin) xf = nullptr;
         PlaneFn pf = g_fast_fft ? plane2_for(g.F[1], g.F[2]) : nullptr;
-        size_t sm2 = plane2_smem(g.F[1], g.F[2], ny, nzw) + 64;
-        if (pf && sm2 <= (size_t)g_smem_optin) {
-            PROF("k_plane", st);
-            pf<<<dim3(nx, n), 256, sm2, st>>>(d_od, sb, pb, sp, g.p[1].tw, g.p[2].tw);
-        } else {
-            int wsz = std::max(PSB_TILE * g.F[1], PSB_PAIRS * g.F[2]);
-            size_t smp = sizeof(float2) * ((size_t)g.F[1] + g.F[2] + (size_t)ny * g.H + 2 * (size_t)wsz) +
-                         sizeof(uint32_t) * (size_t)ny * nzw;
-            if (smp + 64 > (size_t)g_smem_optin)
-                return fail(PSB_ERR_ARG, "tray too large for the plane kernel (%zu B smem)", smp);
-            PROF("k_plane", st);
-            k_plane<<<dim3(nx, n), PSB_THREADS, smp, st>>>(d_od, sb, pb, sp, g.F[1], g.F[2], g.p[1].p, g.p[2].p,
-                                                            g.p[1].tw, g.p[2].tw);
+        const size_t sm2 = plane2_smem(g.F[1], g.F[2], ny, nzw) + 64;
+        if (pf && sm2 > (size_t)g_smem_optin) pf = nullptr;
+        const int wsz = std::max(PSB_TILE * g.F[1], PSB_PAIRS * g.F[2]);
+        const size_t smp = sizeof(float2) * ((size_t)g.F[1] + g.F[2] + (size_t)ny * g.H + 2 * (size_t)wsz) +
+                           sizeof(uint32_t) * (size_t)ny * nzw;
+        if (!pf && smp + 64 > (size_t)g_smem_optin)
+            return fail(PSB_ERR_ARG, "tray too large for the plane kernel (%zu B smem)", smp);
+        // x pass then plane pass per sub-batch of orientations, so a
+        // sub-batch's products can still be in L2 when the plane pass reads them
+        const int sub = subbatch > 0 ? std::min(subbatch, n) : n;
+        for (int o0 = 0; o0 < n; o0 += sub) {
+            const int m = std::min(sub, n - o0);
+            SearchBufs sbo{d_Bi + (size_t)o0 * sBi, d_Pc + (size_t)o0 * sP, d_Pd + (size_t)o0 * sP, sBi, sP};
+            PlaneBufs pbo{d_free + (size_t)o0 * sBits, d_Dq + (size_t)o0 * sD, d_smin + o0, d_diag + o0, sBits, sD};
+            const OrientDesc* odo = d_od + o0;
+            if (xf) {
+                PROF("k_xpass", st);
+                int ncols = g.F[1] * g.H;
+                xf<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, m), 256, xpass2_smem(g.F[0]), st>>>(
+                    odo, sbo, d_Socc, d_Sphi, ncols, g.p[0].tw);
+            } else {
+                PROF("k_xpass", st);
+                size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
+                k_xpass<<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], m), PSB_THREADS, smx, st>>>(
+                    odo, sbo, d_Socc, d_Sphi, g.F[1], g.H, g.p[0].p, g.p[0].tw);
+            }
+            CKL();
+            if (pf) {
+                PROF("k_plane", st);
+                pf<<<dim3(nx, m), PSB_PLANE_THREADS, sm2, st>>>(odo, sbo, pbo, sp, g.p[1].tw, g.p[2].tw);
+            } else {
+                PROF("k_plane", st);
+                k_plane<<<dim3(nx, m), PSB_THREADS, smp, st>>>(odo, sbo, pbo, sp, g.F[1], g.F[2], g.p[1].p,
+                                                                g.p[2].p, g.p[1].tw, g.p[2].tw);
+            }
+            CKL();
         }
-        CKL();
         const uint32_t* ok = d_free;
         unsigned long long* smin = d_smin;
         if (interlock) {

@@ -28,8 +28,7 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
     const int nl = min(C, ncols - c0);
     float2* tw = sm;
     float2* A = tw + N;
-    float2* Bc = A + N * C;
-    float2* Bd = Bc + N * C;
+    float2* X = A + N * C;
     const int tid = threadIdx.x, nthr = blockDim.x;
     load_twiddles(tw, g_tw, N, tid, nthr);
     __syncthreads();
@@ -43,16 +42,11 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
         [&](int c, int n) { return n < ex ? Bi[(size_t)n * ncols + c] : make_float2(0.f, 0.f); },
         [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
     __syncthreads();
-    tpass<N, R1, R0, -1, C, false>(
-        [&](int c, int n) { return A[n * C + c]; },
-        [&](int c, int k, float2 v) {
-            size_t g = (size_t)k * ncols + c;
-            Bc[k * C + c] = c_cmul(v, So[g]);
-            Bd[k * C + c] = c_cmul(v, Sp[g]);
-        },
-        nl, tw, tid, nthr);
+    tpass<N, R1, R0, -1, C, false>([&](int c, int n) { return A[n * C + c]; },
+                                   [&](int c, int k, float2 v) { X[k * C + c] = v; }, nl, tw, tid, nthr);
     __syncthreads();
-    tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return Bc[n * C + c]; },
+    // products conj(I^) * S formed as the inverse's first pass loads them
+    tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return c_cmul(X[n * C + c], So[(size_t)n * ncols + c]); },
                                  [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
     __syncthreads();
     tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
@@ -61,7 +55,7 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
                                   },
                                   nl, tw, tid, nthr);
     __syncthreads();
-    tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return Bd[n * C + c]; },
+    tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return c_cmul(X[n * C + c], Sp[(size_t)n * ncols + c]); },
                                  [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
     __syncthreads();
     tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
@@ -71,7 +65,7 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
                                   nl, tw, tid, nthr);
 }
 
-constexpr size_t xpass2_smem(int N) { return sizeof(float2) * ((size_t)N + 3 * (size_t)N * PSB_XCOLS); }
+constexpr size_t xpass2_smem(int N) { return sizeof(float2) * ((size_t)N + 2 * (size_t)N * PSB_XCOLS); }
 
 // shared memory of k_plane2: twiddles, work buffer A, the y-inverted plane Q
 // (ny rows) and the plane's free bits
@@ -83,9 +77,10 @@ inline size_t plane2_smem(int NY, int NZ, int ny, int nzw) {
 
 // Per (x-plane, orientation): inverse along y then C2R along z (two rows per
 // complex transform) for the collision field, then the proximity field.
-// grid: (nx, n_orient), block 256
+// grid: (nx, n_orient), block PSB_PLANE_THREADS
+#define PSB_PLANE_THREADS 512
 template <int NY, int NZ>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(PSB_PLANE_THREADS, 2)
 k_plane2(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, ScoreParams sp,
          const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
     constexpr int HZ = NZ / 2 + 1;
@@ -168,7 +163,7 @@ k_plane2(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     }
     uint32_t* fb = pb.freebits + (size_t)o * pb.sBits + (size_t)x * ny * nzw;
     for (int i = tid; i < Yv * nzw; i += nthr) fb[i] = bits[i];
-    __shared__ double red[8];
+    __shared__ double red[PSB_PLANE_THREADS / 32];
     for (int off = 16; off > 0; off >>= 1) local_min = fmin(local_min, __shfl_xor_sync(0xffffffffu, local_min, off));
     unsigned int dg = __reduce_or_sync(0xffffffffu, diag);
     if ((tid & 31) == 0) {
