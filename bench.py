@@ -130,7 +130,8 @@ class ClockSampler:
 
 def workload(rank, n_items=N_ITEMS):
     from psacking_b200 import workloads
-    return workloads.config3_items(seed=1 + 1000 * rank, n=n_items)
+    from psacking_b200.shard import stream_seed
+    return workloads.config3_items(seed=stream_seed(rank), n=n_items)
 
 
 def sorted_items(items):
@@ -257,16 +258,9 @@ def run_ours(args, rank, world, local_rank):
     check(lib, lib.psb_tray_destroy(t))
 
     # max over ranks
-    if world > 1:
-        vec = torch.tensor([total_ms, statistics.mean(e2e_ms)], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(vec, op=torch.distributed.ReduceOp.MAX)
-        cnt = torch.tensor([placed, e2e_placed], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(cnt, op=torch.distributed.ReduceOp.SUM)
-        total_ms, e2e_mean = float(vec[0]), float(vec[1])
-        placed_all, e2e_placed_all = float(cnt[0]), float(cnt[1])
-    else:
-        e2e_mean = statistics.mean(e2e_ms)
-        placed_all, e2e_placed_all = placed, e2e_placed
+    from psacking_b200.shard import reduce_run
+    total_ms, placed_all = reduce_run(total_ms, placed, device=dev)
+    e2e_mean, e2e_placed_all = reduce_run(statistics.mean(e2e_ms), e2e_placed, device=dev)
     if rank != 0:
         return None
     value = placed_all * args.steps / (total_ms / 1e3)

@@ -180,7 +180,7 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
 int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                     psb_result* out_placements, int32_t* final_tray);
 
-/* Kernel variant switch (default on): FFT lengths 64, 100, 125, 128, 240 use
+/* Kernel variant switch (default on): FFT lengths 64, 100, 128, 240 use
  * the specialised two-pass kernels; off forces the generic mixed-radix path
  * (used by the tests to check both). */
 int psb_set_fast_fft(int on);

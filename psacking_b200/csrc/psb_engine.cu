@@ -195,7 +195,6 @@ XpassFn xpass2_for(int n) {
     switch (n) {
         case 64: return k_xpass2<64>;
         case 100: return k_xpass2<100>;
-        case 125: return k_xpass2<125>;
         case 128: return k_xpass2<128>;
         case 240: return k_xpass2<240>;
         default: return nullptr;
@@ -207,7 +206,6 @@ XpassFn xpass2_for(int n) {
         switch (nz) {                          \
             case 64: return k_plane2<NY, 64>;   \
             case 100: return k_plane2<NY, 100>; \
-            case 125: return k_plane2<NY, 125>; \
             case 128: return k_plane2<NY, 128>; \
             default: return nullptr;           \
         }
@@ -215,7 +213,6 @@ PlaneFn plane2_for(int ny, int nz) {
     switch (ny) {
         PSB_PLANE_ROW(64)
         PSB_PLANE_ROW(100)
-        PSB_PLANE_ROW(125)
         PSB_PLANE_ROW(128)
         default: return nullptr;
     }
@@ -256,9 +253,9 @@ int set_smem_attrs() {
     TRY(set_max_dyn_smem(k_xpass));
     TRY(set_max_dyn_smem(k_plane));
     TRY(set_max_dyn_smem(k_dist_axis));
-    for (int n : {64, 100, 125, 128, 240}) TRY(set_max_dyn_smem(xpass2_for(n)));
-    for (int a : {64, 100, 125, 128})
-        for (int b : {64, 100, 125, 128}) TRY(set_max_dyn_smem(plane2_for(a, b)));
+    for (int n : {64, 100, 128, 240}) TRY(set_max_dyn_smem(xpass2_for(n)));
+    for (int a : {64, 100, 128})
+        for (int b : {64, 100, 128}) TRY(set_max_dyn_smem(plane2_for(a, b)));
     TRY(init_register_twiddles());
     if (dev < 64) done[dev] = true;
     return PSB_OK;

@@ -1,7 +1,7 @@
 // psb_fft2.cuh — compile-time-sized FFT passes with large register radices.
 //
 // A length-N transform is split into two or three Stockham passes of radix
-// R (e.g. 240 = 16 x 15, 125 = 25 x 5, 100 = 10 x 10).  Each butterfly of
+// R (e.g. 240 = 16 x 15, 128 = 16 x 8, 100 = 10 x 10).  Each butterfly of
 // radix R is a register DFT (itself a compile-time split into the small
 // kernels of psb_fft.cuh), so a 240-point line costs one shared-memory round
 // trip instead of four.  The first pass may read straight from global memory
@@ -66,12 +66,11 @@ template <int DIR> struct RDFT<8, DIR> { static __device__ __forceinline__ void 
 template <int N> struct Plan2;
 template <> struct Plan2<64> { static constexpr int R0 = 8, R1 = 8; };
 template <> struct Plan2<100> { static constexpr int R0 = 10, R1 = 10; };
-template <> struct Plan2<125> { static constexpr int R0 = 25, R1 = 5; };
 template <> struct Plan2<128> { static constexpr int R0 = 16, R1 = 8; };
 template <> struct Plan2<240> { static constexpr int R0 = 16, R1 = 15; };
 
 __host__ __device__ constexpr bool fast_len(int n) {
-    return n == 64 || n == 100 || n == 125 || n == 128 || n == 240;
+    return n == 64 || n == 100 || n == 128 || n == 240;
 }
 
 // One Stockham pass of radix R over `nl` lines.  Butterfly b maps to
