@@ -341,14 +341,23 @@ py::tuple py_pack_native(py::list items, py::handle initial_tray, py::array_t<in
     auto out = new_grid(tr.n);
     int st;
     {
+        // the packing context (about 90 MB per orientation slot) is kept for
+        // the next run with the same tray shape instead of being rebuilt
         py::gil_scoped_release nogil;
-        psb_tray* t = nullptr;
-        st = psb_tray_create(tr.n[0], tr.n[1], tr.n[2], &t);
-        if (st == PSB_OK) st = psb_tray_set(t, tr.ptr(), nullptr);
+        static psb_tray* pack_ctx = nullptr;
+        if (pack_ctx) {
+            int dx, dy, dz;
+            psb_tray_dims(pack_ctx, &dx, &dy, &dz);
+            if (dx != tr.n[0] || dy != tr.n[1] || dz != tr.n[2]) {
+                psb_tray_destroy(pack_ctx);
+                pack_ctx = nullptr;
+            }
+        }
+        st = pack_ctx ? PSB_OK : psb_tray_create(tr.n[0], tr.n[1], tr.n[2], &pack_ctx);
+        if (st == PSB_OK) st = psb_tray_set(pack_ctx, tr.ptr(), nullptr);
         if (st == PSB_OK)
-            st = psb_pack(t, ptrs.data(), dims.data(), (int)gs.size(), maps.data(), n_orient, interlock ? 1 : 0,
-                          id_offset, res.data(), out.mutable_data());
-        if (t) psb_tray_destroy(t);
+            st = psb_pack(pack_ctx, ptrs.data(), dims.data(), (int)gs.size(), maps.data(), n_orient,
+                          interlock ? 1 : 0, id_offset, res.data(), out.mutable_data());
     }
     check(st);
     py::list pl;

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -21,6 +22,7 @@
 #include "../../include/psb200.h"
 #include "psb_kernels2.cuh"
 #include "psb_kernels3.cuh"
+#include "psb_loop.cuh"
 
 namespace {
 
@@ -306,12 +308,10 @@ int make_grid3(int nx, int ny, int nz, bool linear, Grid3* g) {
 size_t smem_rz(int N) { return sizeof(float2) * (N + 2 * PSB_PAIRS * N); }
 size_t smem_mid(int N) { return sizeof(float2) * (N + 2 * PSB_TILE * N); }
 
-// forward: src grid -> spectrum [F0][F1][H].  w1: [n0][n1][H], w2: [n0][F1][H]
-int forward3(const Grid3& g, const RzDesc& rz_in, float2* w1, float2* w2, float2* spec, RzDesc* d_rz,
-             MidDesc* d_mid, cudaStream_t st) {
-    RzDesc rz = rz_in;
-    rz.out = w1;
-    CK(cudaMemcpyAsync(d_rz, &rz, sizeof(rz), cudaMemcpyHostToDevice, st));
+// forward with descriptors already on the device: d_rz[0] (z pass, out = w1),
+// d_mid[0] (y pass w1 -> w2), d_mid[1] (x pass w2 -> spectrum).  No host copies,
+// so it can be queued inside the asynchronous packing loop.
+int forward3_dev(const Grid3& g, const RzDesc* d_rz, const MidDesc* d_mid, cudaStream_t st) {
     int npairs = (g.n[0] * g.n[1] + 1) / 2;
     {
         PROF("k_rfft_z", st);
@@ -319,12 +319,6 @@ int forward3(const Grid3& g, const RzDesc& rz_in, float2* w1, float2* w2, float2
             d_rz, nullptr, g.p[2].p, g.p[2].tw);
     }
     CKL();
-    MidDesc m[2];
-    // y: [n0][n1->F1][H]
-    m[0] = MidDesc{w1, w2, g.n[0], g.H, g.n[1], g.F[1], (long long)g.n[1] * g.H, (long long)g.F[1] * g.H, g.H, g.H, -1, 0};
-    // x: [1][n0->F0][F1*H]
-    m[1] = MidDesc{w2, spec, 1, g.F[1] * g.H, g.n[0], g.F[0], 0, 0, g.F[1] * g.H, g.F[1] * g.H, -1, 0};
-    CK(cudaMemcpyAsync(d_mid, m, sizeof(m), cudaMemcpyHostToDevice, st));
     {
         PROF("k_fft_mid_fwd", st);
         k_fft_mid<-1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.n[0], 1), PSB_THREADS, smem_mid(g.F[1]), st>>>(
@@ -338,6 +332,27 @@ int forward3(const Grid3& g, const RzDesc& rz_in, float2* w1, float2* w2, float2
     }
     CKL();
     return PSB_OK;
+}
+
+// the two MidDescs of a forward transform (w1 -> w2 -> spec)
+void forward_mids(const Grid3& g, float2* w1, float2* w2, float2* spec, const int* gate, MidDesc* m) {
+    // y: [n0][n1->F1][H]
+    m[0] = MidDesc{w1, w2, g.n[0], g.H, g.n[1], g.F[1], (long long)g.n[1] * g.H, (long long)g.F[1] * g.H, g.H, g.H,
+                   -1, 0, gate};
+    // x: [1][n0->F0][F1*H]
+    m[1] = MidDesc{w2, spec, 1, g.F[1] * g.H, g.n[0], g.F[0], 0, 0, g.F[1] * g.H, g.F[1] * g.H, -1, 0, gate};
+}
+
+// forward: src grid -> spectrum [F0][F1][H].  w1: [n0][n1][H], w2: [n0][F1][H]
+int forward3(const Grid3& g, const RzDesc& rz_in, float2* w1, float2* w2, float2* spec, RzDesc* d_rz,
+             MidDesc* d_mid, cudaStream_t st) {
+    RzDesc rz = rz_in;
+    rz.out = w1;
+    CK(cudaMemcpyAsync(d_rz, &rz, sizeof(rz), cudaMemcpyHostToDevice, st));
+    MidDesc m[2];
+    forward_mids(g, w1, w2, spec, nullptr, m);
+    CK(cudaMemcpyAsync(d_mid, m, sizeof(m), cudaMemcpyHostToDevice, st));
+    return forward3_dev(g, d_rz, d_mid, st);
 }
 
 // inverse: spectrum [F0][F1][H] -> int32 grid (rounded, scaled by 1/(F0 F1 F2))
@@ -372,12 +387,13 @@ int inverse3_int(const Grid3& g, float2* spec, float2* w1, float2* w2, int32_t* 
     return PSB_OK;
 }
 
-int distance_on_device(const int32_t* d_grid, int32_t* d_out, int nx, int ny, int nz, cudaStream_t st) {
+int distance_on_device(const int32_t* d_grid, int32_t* d_out, int nx, int ny, int nz, cudaStream_t st,
+                       const int* gate = nullptr) {
     size_t V = (size_t)nx * ny * nz;
     int far = nx + ny + nz + 10;  // fft3.cu:948
     {
         PROF("k_dist_init", st);
-        k_dist_init<<<grid1d(V), 256, 0, st>>>(d_grid, d_out, V, far);
+        k_dist_init<<<grid1d(V), 256, 0, st>>>(d_grid, d_out, V, far, gate);
     }
     CKL();
     for (int axis = 0; axis < 3; ++axis) {
@@ -389,12 +405,12 @@ int distance_on_device(const int32_t* d_grid, int32_t* d_out, int nx, int ny, in
             long long blocks = (nlines + W - 1) / W;
             {
                 PROF("k_dist_axis", st);
-                k_dist_axis<<<(unsigned)blocks, 256, (size_t)W * L * 4, st>>>(d_out, axis, nx, ny, nz, (int)W);
+                k_dist_axis<<<(unsigned)blocks, 256, (size_t)W * L * 4, st>>>(d_out, axis, nx, ny, nz, (int)W, gate);
             }
         } else {
             {
                 PROF("k_dist_axis_global", st);
-                k_dist_axis_global<<<(unsigned)((nlines + 255) / 256), 256, 0, st>>>(d_out, axis, nx, ny, nz);
+                k_dist_axis_global<<<(unsigned)((nlines + 255) / 256), 256, 0, st>>>(d_out, axis, nx, ny, nz, gate);
             }
         }
         CKL();
@@ -484,6 +500,17 @@ struct psb_tray {
 
     int subbatch = 0;        // orientations per x-pass/plane-pass launch pair (0: all)
 
+    // asynchronous packing loop: device state, distance statistics and the
+    // transform descriptors of the occupancy / distance spectra (uploaded once)
+    LoopState* d_ls = nullptr;
+    PhiStats* d_ps = nullptr;
+    RzDesc* d_rzd = nullptr;    // [0] occ, [1] phi, [2] occ gated, [3] phi gated
+    MidDesc* d_midd = nullptr;  // pairs in the same order
+    OrientDesc* d_od_all = nullptr;
+    size_t od_all_cap = 0;
+    DecisionDev* d_dec = nullptr;
+    size_t dec_cap = 0;
+
     int phi_mean = 0;
     double phi_norm = 0.0;
     int phi_maxabs = 0;
@@ -494,7 +521,7 @@ struct psb_tray {
     float* d_Dq = nullptr;
     uint32_t *d_free = nullptr, *d_reach = nullptr;
     int *d_cnt = nullptr, *d_off = nullptr, *d_rz2 = nullptr, *d_rline = nullptr, *d_par = nullptr, *d_rflag = nullptr,
-        *d_total = nullptr;
+        *d_total = nullptr, *d_blk = nullptr;
     int *d_cand = nullptr, *d_ncand = nullptr;
     double* d_cscore = nullptr;
     unsigned long long *d_smin = nullptr, *d_smin2 = nullptr, *d_best = nullptr, *d_bestkey = nullptr;
@@ -523,7 +550,7 @@ struct psb_tray {
 
     void release_slots() {
         dfree(d_Ai); dfree(d_Bi); dfree(d_Pc); dfree(d_Pd); dfree(d_Dq); dfree(d_free); dfree(d_reach);
-        dfree(d_cnt); dfree(d_off); dfree(d_rz2); dfree(d_rline); dfree(d_par); dfree(d_rflag); dfree(d_total);
+        dfree(d_cnt); dfree(d_off); dfree(d_rz2); dfree(d_rline); dfree(d_par); dfree(d_rflag); dfree(d_total); dfree(d_blk);
         dfree(d_cand); dfree(d_ncand); dfree(d_cscore); dfree(d_smin); dfree(d_smin2); dfree(d_best);
         dfree(d_bestkey); dfree(d_diag); dfree(d_errmax); dfree(d_od); dfree(d_rzs); dfree(d_mids); dfree(d_res);
         cap = 0;
@@ -533,6 +560,7 @@ struct psb_tray {
         release_slots();
         dfree(d_tray); dfree(d_phi); dfree(d_Socc); dfree(d_Sphi); dfree(d_w1); dfree(d_w2); dfree(d_pen);
         dfree(d_rz); dfree(d_mid); dfree(d_stats); dfree(d_err); dfree(d_first); dfree(d_items); dfree(d_vox); dfree(d_stage); dfree(d_stage_vox);
+        dfree(d_ls); dfree(d_ps); dfree(d_rzd); dfree(d_midd); dfree(d_od_all); dfree(d_dec);
         if (st) cudaStreamDestroy(st);
         st = nullptr;
     }
@@ -566,6 +594,23 @@ struct psb_tray {
             pen[2 * nz + k] = qz;
         }
         CK(cudaMemcpy(d_pen, pen.data(), sizeof(double) * 3 * nz, cudaMemcpyHostToDevice));
+        TRY(dalloc(&d_ls, 1)); TRY(dalloc(&d_ps, 1)); TRY(dalloc(&d_rzd, 4)); TRY(dalloc(&d_midd, 8));
+        CK(cudaMemset(d_ls, 0, sizeof(LoopState)));
+        CK(cudaMemset(d_ps, 0, sizeof(PhiStats)));
+        const int* mean_p = (const int*)((const char*)d_ps + offsetof(PhiStats, mean));
+        const int* placed_now = (const int*)((const char*)d_ls + offsetof(LoopState, placed_now));
+        const int* need_phi = (const int*)((const char*)d_ls + offsetof(LoopState, need_phi));
+        RzDesc rz[4] = {RzDesc{SRC_GRID_OCC, d_tray, nx, ny, nz, 0, -1, d_w1, nullptr, nullptr},
+                        RzDesc{SRC_GRID_SUB, d_phi, nx, ny, nz, 0, -1, d_w1, nullptr, mean_p},
+                        RzDesc{SRC_GRID_OCC, d_tray, nx, ny, nz, 0, -1, d_w1, placed_now, nullptr},
+                        RzDesc{SRC_GRID_SUB, d_phi, nx, ny, nz, 0, -1, d_w1, need_phi, mean_p}};
+        MidDesc md[8];
+        forward_mids(g, d_w1, d_w2, d_Socc, nullptr, md + 0);
+        forward_mids(g, d_w1, d_w2, d_Sphi, nullptr, md + 2);
+        forward_mids(g, d_w1, d_w2, d_Socc, placed_now, md + 4);
+        forward_mids(g, d_w1, d_w2, d_Sphi, need_phi, md + 6);
+        CK(cudaMemcpy(d_rzd, rz, sizeof(rz), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_midd, md, sizeof(md), cudaMemcpyHostToDevice));
         return PSB_OK;
     }
 
@@ -587,11 +632,22 @@ struct psb_tray {
         TRY(dalloc(&d_cnt, sLine * c)); TRY(dalloc(&d_off, sLine * c));
         TRY(dalloc(&d_rz2, sRun * c)); TRY(dalloc(&d_rline, sRun * c)); TRY(dalloc(&d_par, sRun * c));
         TRY(dalloc(&d_rflag, sRun * c)); TRY(dalloc(&d_total, c));
+        TRY(dalloc(&d_blk, (size_t)((nx * ny + 255) / 256) * c));
         TRY(dalloc(&d_cand, (size_t)kCandCap * c)); TRY(dalloc(&d_ncand, c));
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c));
         TRY(dalloc(&d_smin, c)); TRY(dalloc(&d_smin2, c)); TRY(dalloc(&d_best, c)); TRY(dalloc(&d_bestkey, c));
         TRY(dalloc(&d_diag, c)); TRY(dalloc(&d_errmax, c)); TRY(dalloc(&d_od, c)); TRY(dalloc(&d_rzs, c)); TRY(dalloc(&d_mids, c));
         TRY(dalloc(&d_res, c));
+        // item transform descriptors of each slot (orientation-relative)
+        std::vector<RzDesc> rz(c);
+        std::vector<MidDesc> md(c);
+        for (int o = 0; o < c; ++o) {
+            rz[o] = RzDesc{SRC_ITEM, nullptr, 0, 0, 0, 0, o, d_Ai + (size_t)o * sAi, nullptr, nullptr};
+            md[o] = MidDesc{d_Ai + (size_t)o * sAi, d_Bi + (size_t)o * sBi, 0, g.H, 0, g.F[1], 0,
+                            (long long)g.F[1] * g.H, g.H, g.H, o, 0, nullptr};
+        }
+        CK(cudaMemcpy(d_rzs, rz.data(), sizeof(RzDesc) * c, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_mids, md.data(), sizeof(MidDesc) * c, cudaMemcpyHostToDevice));
         cap = c;
         return PSB_OK;
     }
@@ -611,36 +667,52 @@ struct psb_tray {
     }
 
     // occupancy spectrum from the device tray
-    int rebuild_occ() {
-        RzDesc rz{SRC_GRID_OCC, d_tray, nx, ny, nz, 0, -1, nullptr};
-        return forward3(g, rz, d_w1, d_w2, d_Socc, d_rz, d_mid, st);
+    int rebuild_occ() { return forward3_dev(g, d_rzd + 0, d_midd + 0, st); }
+    // ... only when the current item of the asynchronous loop was placed
+    int rebuild_occ_gated() { return forward3_dev(g, d_rzd + 2, d_midd + 4, st); }
+
+    // mean, norm and max deviation of the distance field, on the device
+    int phi_stats(const int* gate) {
+        unsigned long long* raw = (unsigned long long*)((char*)d_ps + offsetof(PhiStats, raw));
+        const int* mean_p = (const int*)((const char*)d_ps + offsetof(PhiStats, mean));
+        CK(cudaMemsetAsync(raw, 0, sizeof(unsigned long long) * 4, st));
+        {
+            PROF("k_stats", st);
+            k_stats_g<<<grid1d(V), 256, 0, st>>>(d_phi, V, nullptr, raw, gate);
+        }
+        CKL();
+        k_phi_mean<<<1, 1, 0, st>>>(d_ps, (unsigned long long)V, gate);
+        CKL();
+        {
+            PROF("k_stats", st);
+            k_stats_g<<<grid1d(V), 256, 0, st>>>(d_phi, V, mean_p, raw, gate);
+        }
+        CKL();
+        k_phi_norm<<<1, 1, 0, st>>>(d_ps, gate);
+        CKL();
+        return PSB_OK;
     }
 
     // distance spectrum (mean-subtracted) from the device distance field
     int rebuild_phi_spectrum() {
-        CK(cudaMemsetAsync(d_stats, 0, sizeof(unsigned long long) * 4, st));
-        {
-            PROF("k_stats", st);
-            k_stats<<<grid1d(V), 256, 0, st>>>(d_phi, V, 0, d_stats);
-        }
-        CKL();
-        unsigned long long h[4];
-        CK(cudaMemcpyAsync(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, st));
+        TRY(phi_stats(nullptr));
+        TRY(forward3_dev(g, d_rzd + 1, d_midd + 2, st));
+        PhiStats h;
+        CK(cudaMemcpyAsync(&h, d_ps, sizeof(h), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        long long sum = (long long)h[0];
-        phi_mean = (int)std::llround((double)sum / (double)V);
-        CK(cudaMemsetAsync(d_stats, 0, sizeof(unsigned long long) * 4, st));
-        {
-            PROF("k_stats", st);
-            k_stats<<<grid1d(V), 256, 0, st>>>(d_phi, V, phi_mean, d_stats);
-        }
-        CKL();
-        CK(cudaMemcpyAsync(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        phi_norm = std::sqrt((double)(long long)h[1]);
-        phi_maxabs = (int)(unsigned int)(h[2] & 0xffffffffULL);
-        RzDesc rz{SRC_GRID_SUB, d_phi, nx, ny, nz, phi_mean, -1, nullptr};
-        return forward3(g, rz, d_w1, d_w2, d_Sphi, d_rz, d_mid, st);
+        phi_mean = h.mean;
+        phi_norm = h.norm;
+        phi_maxabs = h.maxabs;
+        return PSB_OK;
+    }
+
+    // distance field, its statistics and spectrum, only when the current item
+    // of the asynchronous loop wrote voxels equal to 1
+    int rebuild_phi_gated() {
+        const int* need_phi = (const int*)((const char*)d_ls + offsetof(LoopState, need_phi));
+        TRY(distance_on_device(d_tray, d_phi, nx, ny, nz, st, need_phi));
+        TRY(phi_stats(need_phi));
+        return forward3_dev(g, d_rzd + 3, d_midd + 6, st);
     }
 
     int set(const int32_t* tray, const int32_t* phi) {
@@ -684,12 +756,14 @@ struct psb_tray {
         for (const int4& q : info.vox) sabs += std::llabs((long long)q.w);
         double maxD = (double)sabs * (double)phi_maxabs;
         const double eps = 1.1920928955078125e-07;
-        od->delta = 4.0 * eps * std::sqrt(info.sumsq) * phi_norm + 0.5 * ulp32(maxD) + 1e-3;
+        od->delta = 2.0 * eps * std::sqrt(info.sumsq) * phi_norm + 0.5 * ulp32(maxD) + 1e-3;
         od->exact = (od->delta >= 0.4 || maxD >= 8388608.0) ? 1 : 0;
         od->item = d_item;
         od->vox = d_vx;
         od->nvox = (int)info.vox.size();
         od->pad = 0;
+        od->sumsq = info.sumsq;
+        od->sabs = sabs;
     }
 
     ScoreParams score_params(int mode) const {
@@ -704,36 +778,30 @@ struct psb_tray {
         return sp;
     }
 
-    // Search the n orientations described in ods (device item data already
-    // uploaded).  res receives each orientation's result.
-    int search(const std::vector<OrientDesc>& ods, int mode, bool interlock, std::vector<ResultDev>* res) {
+    // Queue the search of the n orientations whose descriptors are at d_odb
+    // (device item data already there); each orientation's result goes to
+    // d_out[o].  ods is the host copy (dims for the launch shapes).  No host
+    // copy or synchronisation happens here.
+    int search_async(const OrientDesc* d_odb, const std::vector<OrientDesc>& ods, int mode, bool interlock,
+                     ResultDev* d_out) {
         const int n = (int)ods.size();
         TRY(ensure_slots(n));
-        CK(cudaMemcpyAsync(d_od, ods.data(), sizeof(OrientDesc) * n, cudaMemcpyHostToDevice, st));
-        int exmax = 1, eymax = 1;
-        for (auto& o : ods) if (!o.skip) { exmax = std::max(exmax, o.e[0]); eymax = std::max(eymax, o.e[1]); }
-        // item z pass
-        std::vector<RzDesc> rz(n);
-        std::vector<MidDesc> md(n);
-        int maxpairs = 1;
-        for (int o = 0; o < n; ++o) {
-            rz[o] = RzDesc{SRC_ITEM, nullptr, 0, 0, 0, 0, o, d_Ai + (size_t)o * sAi};
-            md[o] = MidDesc{d_Ai + (size_t)o * sAi, d_Bi + (size_t)o * sBi, 0, g.H, 0, g.F[1],
-                            (long long)ods[o].e[1] * g.H, (long long)g.F[1] * g.H, g.H, g.H, o, 0};
-            if (!ods[o].skip) maxpairs = std::max(maxpairs, (ods[o].e[0] * ods[o].e[1] + 1) / 2);
-        }
-        CK(cudaMemcpyAsync(d_rzs, rz.data(), sizeof(RzDesc) * n, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_mids, md.data(), sizeof(MidDesc) * n, cudaMemcpyHostToDevice, st));
+        int exmax = 1, maxpairs = 1;
+        for (auto& o : ods)
+            if (!o.skip) {
+                exmax = std::max(exmax, o.e[0]);
+                maxpairs = std::max(maxpairs, (o.e[0] * o.e[1] + 1) / 2);
+            }
         {
             PROF("k_rfft_z", st);
             k_rfft_z<<<dim3((maxpairs + PSB_PAIRS - 1) / PSB_PAIRS, n), PSB_THREADS, smem_rz(g.F[2]), st>>>(
-                d_rzs, d_od, g.p[2].p, g.p[2].tw);
+                d_rzs, d_odb, g.p[2].p, g.p[2].tw);
         }
         CKL();
         {
             PROF("k_fft_mid_fwd", st);
             k_fft_mid<-1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, exmax, n), PSB_THREADS, smem_mid(g.F[1]), st>>>(
-                d_mids, d_od, g.p[1].p, g.p[1].tw);
+                d_mids, d_odb, g.p[1].p, g.p[1].tw);
         }
         CKL();
         SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
@@ -764,7 +832,7 @@ struct psb_tray {
             const int m = std::min(sub, n - o0);
             SearchBufs sbo{d_Bi + (size_t)o0 * sBi, d_Pc + (size_t)o0 * sP, d_Pd + (size_t)o0 * sP, sBi, sP};
             PlaneBufs pbo{d_free + (size_t)o0 * sBits, d_Dq + (size_t)o0 * sD, d_smin + o0, d_diag + o0, sBits, sD};
-            const OrientDesc* odo = d_od + o0;
+            const OrientDesc* odo = d_odb + o0;
             if (xf) {
                 PROF("k_xpass", st);
                 int ncols = g.F[1] * g.H;
@@ -788,71 +856,73 @@ struct psb_tray {
             CKL();
         }
         const uint32_t* ok = d_free;
-        unsigned long long* smin = d_smin;
         if (interlock) {
             FloodBufs fb{d_free, d_reach, sBits, d_cnt, d_off, sLine, d_rz2, d_rline, d_par, d_rflag, sRun, d_total, d_err};
             int lines = nx * ny;
-            dim3 gl((lines + 255) / 256, n);
+            const int nblk = (lines + 255) / 256;
+            dim3 gl(nblk, n);
             {
                 PROF("k_ff_count", st);
-                k_ff_count<<<gl, 256, 0, st>>>(d_od, fb, sp);
+                k_ff_count<<<gl, 256, 0, st>>>(d_odb, fb, sp, d_blk, nblk);
             }
             CKL();
             {
                 PROF("k_ff_scan", st);
-                k_ff_scan<<<n, 1024, 0, st>>>(d_od, fb, lines);
+                k_ff_scan<<<n, 32, 0, st>>>(d_odb, fb, d_blk, nblk);
             }
             CKL();
             {
                 PROF("k_ff_emit", st);
-                k_ff_emit<<<gl, 256, 0, st>>>(d_od, fb, sp);
+                k_ff_emit<<<gl, 256, 0, st>>>(d_odb, fb, sp, d_blk, nblk);
             }
             CKL();
             {
                 PROF("k_ff_union", st);
-                k_ff_union<<<gl, 256, 0, st>>>(d_od, fb, sp);
+                k_ff_union<<<gl, 256, 0, st>>>(d_odb, fb, sp);
             }
             CKL();
             {
                 PROF("k_ff_seed", st);
-                k_ff_seed<<<dim3(296, n), 256, 0, st>>>(d_od, fb);
+                k_ff_seed<<<dim3(296, n), 256, 0, st>>>(d_odb, fb);
             }
             CKL();
             {
                 PROF("k_ff_reach", st);
-                k_ff_reach<<<gl, 256, 0, st>>>(d_od, fb, sp);
+                k_ff_reach<<<gl, 256, 0, st>>>(d_odb, fb, sp);
             }
             CKL();
             ok = d_reach;
-            smin = d_smin2;
-            SelectBufs s0{ok, sBits, d_Dq, sD, smin, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, d_errmax, kCandCap};
-            {
-                PROF("k_select_min", st);
-                k_select_min<<<dim3(nx, n), 256, 0, st>>>(d_od, s0, sp);
-            }
-            CKL();
         }
-        SelectBufs sel{ok, sBits, d_Dq, sD, smin, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, d_errmax, kCandCap};
+        SelectBufs sel{ok, sBits, d_Dq, sD, d_smin2, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, d_errmax, kCandCap};
         {
             PROF("k_collect", st);
-            k_collect<<<dim3(nx, n), 256, 0, st>>>(d_od, sel, sp);
+            k_collect_plane<<<dim3(nx, n), 256, 0, st>>>(d_odb, sel, sp);
         }
         CKL();
         {
             PROF("k_rescore", st);
-            k_rescore<<<dim3(148, n), 256, 0, st>>>(d_od, sel, sp, d_tray, d_phi);
+            k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_tray, d_phi);
         }
         CKL();
         {
             PROF("k_tiebreak", st);
-            k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_od, sel, sp);
+            k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp);
         }
         CKL();
         {
             PROF("k_finalize", st);
-            k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_od, sel, sp, d_res, n);
+            k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_odb, sel, sp, d_out, n);
         }
         CKL();
+        return PSB_OK;
+    }
+
+    // Synchronous search (the drop-in entry points): upload, queue, wait, check.
+    int search(const std::vector<OrientDesc>& ods, int mode, bool interlock, std::vector<ResultDev>* res) {
+        const int n = (int)ods.size();
+        TRY(ensure_slots(n));
+        CK(cudaMemcpyAsync(d_od, ods.data(), sizeof(OrientDesc) * n, cudaMemcpyHostToDevice, st));
+        TRY(search_async(d_od, ods, mode, interlock, d_res));
         res->resize(n);
         unsigned int herr = 0;
         CK(cudaMemcpyAsync(res->data(), d_res, sizeof(ResultDev) * n, cudaMemcpyDeviceToHost, st));
@@ -1242,18 +1312,19 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
     FloodBufs fb{t->d_free, t->d_reach, t->sBits, t->d_cnt, t->d_off, t->sLine, t->d_rz2, t->d_rline, t->d_par,
                  t->d_rflag, t->sRun, t->d_total, t->d_err};
     int lines = nx * ny;
-    dim3 gl((lines + 255) / 256, 1);
+    const int nblk = (lines + 255) / 256;
+    dim3 gl(nblk, 1);
     {
         PROF("k_ff_count", t->st);
-        k_ff_count<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+        k_ff_count<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp, t->d_blk, nblk);
     }
     {
         PROF("k_ff_scan", t->st);
-        k_ff_scan<<<1, 1024, 0, t->st>>>(t->d_od, fb, lines);
+        k_ff_scan<<<1, 32, 0, t->st>>>(t->d_od, fb, t->d_blk, nblk);
     }
     {
         PROF("k_ff_emit", t->st);
-        k_ff_emit<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+        k_ff_emit<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp, t->d_blk, nblk);
     }
     {
         PROF("k_ff_union", t->st);
@@ -1490,40 +1561,98 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
         if (seen != 7) return fail(PSB_ERR_ARG, "orientation %d: axis map is not a permutation", o);
     }
     const int mode = (interlock || n_orient > 1) ? PSB_MODE_BLOCK : PSB_MODE_SCAN;
-    int placed = 0;
-    std::vector<OrientDesc> ods(n_orient);
-    std::vector<ResultDev> res;
-    for (int it = 0; it < (int)t->staged.size(); ++it) {
-        const ItemInfo& info = t->staged[it];
-        const int32_t* d_item = t->d_stage + t->staged_off[it];
-        const int4* d_vx = t->d_stage_vox + t->staged_voff[it];
-        for (int o = 0; o < n_orient; ++o)
-            t->describe(info, orient_maps + 6 * o, orient_maps + 6 * o + 3, d_item, d_vx, &ods[o]);
-        TRY(t->search(ods, mode, interlock != 0, &res));
-        psb_result best{-1, -1, -1, 0, 0.0, -1, 0, 0, 0.f};
-        double bs = 1e300;
-        unsigned int diag = 0;
-        int ncand = 0;
-        float errr = 0.f;
-        for (int o = 0; o < n_orient; ++o) {
-            diag |= res[o].diag;
-            ncand += res[o].ncand;
-            errr = std::max(errr, res[o].err_ratio);
-            if (ods[o].skip) continue;
-            psb_result r;
-            to_result(res[o], o, &r);
-            if (r.found && r.score < bs) { bs = r.score; best = r; }  // strict <: first best wins
-        }
-        best.diag = diag;
-        best.n_candidates = ncand;
-        best.err_ratio = errr;
-        if (best.found) {
-            int32_t id = id_offset + placed + 1;
-            TRY(t->place(ods[best.orientation], best.x, best.y, best.z, id, nullptr));
-            ++placed;
-        }
-        out_placements[it] = best;
+    const int n_items = (int)t->staged.size();
+    if (n_items == 0) {
+        if (final_tray) TRY(psb_tray_get(t, final_tray, nullptr));
+        return PSB_OK;
     }
+    TRY(t->ensure_slots(n_orient));
+    // every orientation of every item, described once (bounds, maps, sizes);
+    // the error bounds are filled on the device by k_prep from the current
+    // distance statistics
+    std::vector<OrientDesc> all((size_t)n_items * n_orient);
+    for (int it = 0; it < n_items; ++it)
+        for (int o = 0; o < n_orient; ++o)
+            t->describe(t->staged[it], orient_maps + 6 * o, orient_maps + 6 * o + 3,
+                        t->d_stage + t->staged_off[it], t->d_stage_vox + t->staged_voff[it],
+                        &all[(size_t)it * n_orient + o]);
+    if (all.size() > t->od_all_cap) {
+        dfree(t->d_od_all);
+        t->od_all_cap = all.size();
+        TRY(dalloc(&t->d_od_all, t->od_all_cap));
+    }
+    if ((size_t)n_items > t->dec_cap) {
+        dfree(t->d_dec);
+        t->dec_cap = n_items;
+        TRY(dalloc(&t->d_dec, t->dec_cap));
+    }
+    CK(cudaMemcpyAsync(t->d_od_all, all.data(), sizeof(OrientDesc) * all.size(), cudaMemcpyHostToDevice, t->st));
+    LoopState ls0;
+    memset(&ls0, 0, sizeof(ls0));
+    ls0.id_offset = id_offset;
+    CK(cudaMemcpyAsync(t->d_ls, &ls0, sizeof(ls0), cudaMemcpyHostToDevice, t->st));
+    CK(cudaStreamSynchronize(t->st));
+    // While no item is placed yet and ids start at 1, the next placement writes
+    // distance sources (voxels == 1); the host waits on those few items and
+    // queues the gated distance rebuild.  After that ids are >= 2, the
+    // distance field is final and the rest of the run is queued without waits.
+    bool first_pending = (id_offset == 0);
+    std::vector<OrientDesc> host_ods(n_orient);
+    for (int it = 0; it < n_items; ++it) {
+        OrientDesc* d_odb = t->d_od_all + (size_t)it * n_orient;
+        for (int o = 0; o < n_orient; ++o) host_ods[o] = all[(size_t)it * n_orient + o];
+        k_prep<<<(n_orient + 63) / 64, 64, 0, t->st>>>(d_odb, n_orient, t->d_ps);
+        CKL();
+        TRY(t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res));
+        k_decide<<<1, 32, 0, t->st>>>(d_odb, t->d_res, n_orient, t->d_ls, t->d_dec + it, t->d_err);
+        CKL();
+        {
+            PROF("k_place_check", t->st);
+            k_place_check_g<<<64, 256, 0, t->st>>>(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
+        }
+        CKL();
+        {
+            PROF("k_place_write", t->st);
+            k_place_write_g<<<64, 256, 0, t->st>>>(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
+        }
+        CKL();
+        k_place_done<<<1, 32, 0, t->st>>>(d_odb, t->d_ls, t->d_dec + it);
+        CKL();
+        TRY(t->rebuild_occ_gated());
+        if (first_pending) {
+            TRY(t->rebuild_phi_gated());
+            LoopState h;
+            CK(cudaMemcpyAsync(&h, t->d_ls, sizeof(h), cudaMemcpyDeviceToHost, t->st));
+            CK(cudaStreamSynchronize(t->st));
+            if (h.placed > 0) first_pending = false;
+        }
+    }
+    std::vector<DecisionDev> dec(n_items);
+    LoopState h;
+    CK(cudaMemcpyAsync(dec.data(), t->d_dec, sizeof(DecisionDev) * n_items, cudaMemcpyDeviceToHost, t->st));
+    CK(cudaMemcpyAsync(&h, t->d_ls, sizeof(h), cudaMemcpyDeviceToHost, t->st));
+    CK(cudaStreamSynchronize(t->st));
+    for (int it = 0; it < n_items; ++it) {
+        psb_result r;
+        r.x = dec[it].x; r.y = dec[it].y; r.z = dec[it].z;
+        r.found = dec[it].found;
+        r.score = dec[it].score;
+        r.orientation = dec[it].orientation;
+        r.diag = dec[it].diag;
+        r.n_candidates = dec[it].ncand;
+        r.err_ratio = dec[it].err_ratio;
+        out_placements[it] = r;
+    }
+    if (h.err & 1u) return fail(PSB_ERR_LIMIT, "flood fill union-find hit its iteration limit");
+    if (h.err & 2u) return fail(PSB_ERR_LIMIT, "tie-guard candidates exceeded the capacity %d", kCandCap);
+    if (h.err & 4u)
+        return fail(PSB_ERR_OVERLAP, "(place_in_tray): a searched position overlapped the tray on exact re-check");
+    // host copies of the distance statistics for later synchronous searches
+    PhiStats ps;
+    CK(cudaMemcpy(&ps, t->d_ps, sizeof(ps), cudaMemcpyDeviceToHost));
+    t->phi_mean = ps.mean;
+    t->phi_norm = ps.norm;
+    t->phi_maxabs = ps.maxabs;
     if (final_tray) TRY(psb_tray_get(t, final_tray, nullptr));
     return PSB_OK;
 }

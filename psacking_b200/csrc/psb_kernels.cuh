@@ -35,6 +35,8 @@ struct OrientDesc {
     const int4* vox;          // device voxel list of the base item (x,y,z,value)
     int nvox;
     int pad;
+    double sumsq;             // sum of squared item values
+    long long sabs;           // sum of |item values|
 };
 
 __device__ __forceinline__ int orient_src_index(const OrientDesc& d, int i0, int i1, int i2) {
@@ -65,6 +67,8 @@ struct RzDesc {
     int sub;                  // SRC_GRID_SUB: value - sub
     int orient;               // SRC_ITEM: index into OrientDesc array
     float2* out;              // [n0*n1][Hz]
+    const int* gate;          // when set, the transform runs only if *gate != 0
+    const int* subp;          // SRC_GRID_SUB: device-side shift (overrides sub)
 };
 
 // real lines -> half spectra along z.  Two real lines are packed into one
@@ -75,8 +79,10 @@ k_rfft_z(const RzDesc* __restrict__ descs, const OrientDesc* __restrict__ orient
          AxisPlan plan, const float2* __restrict__ g_tw) {
     extern __shared__ float2 sm[];
     const RzDesc d = descs[blockIdx.y];
+    if (d.gate && !*d.gate) return;
     const int N = plan.n, Hz = N / 2 + 1;
     int n0 = d.n0, n1 = d.n1, n2 = d.n2;
+    const int sub = d.subp ? *d.subp : d.sub;
     OrientDesc od;
     if (d.kind == SRC_ITEM) {
         od = orients[d.orient];
@@ -109,7 +115,7 @@ k_rfft_z(const RzDesc* __restrict__ descs, const OrientDesc* __restrict__ orient
                 int ra = d.grid[(size_t)la * n2 + z];
                 int rb = lb < nlines ? d.grid[(size_t)lb * n2 + z] : 0;
                 if (d.kind == SRC_GRID_OCC) { ra = ra != 0; rb = rb != 0; }
-                else if (d.kind == SRC_GRID_SUB) { ra -= d.sub; rb = lb < nlines ? rb - d.sub : 0; }
+                else if (d.kind == SRC_GRID_SUB) { ra -= sub; rb = lb < nlines ? rb - sub : 0; }
                 va = (float)ra;
                 vb = (float)rb;
             }
@@ -185,6 +191,7 @@ struct MidDesc {
     int in_sl, out_sl;
     int orient;               // >= 0: take A/Lin from the orientation (item y pass)
     int pad;
+    const int* gate;          // when set, the transform runs only if *gate != 0
 };
 
 // grid: (ceil(Cmax / PSB_TILE), Amax, nbatch)
@@ -194,11 +201,13 @@ k_fft_mid(const MidDesc* __restrict__ descs, const OrientDesc* __restrict__ orie
           const float2* __restrict__ g_tw) {
     extern __shared__ float2 sm[];
     MidDesc d = descs[blockIdx.z];
+    if (d.gate && !*d.gate) return;
     if (d.orient >= 0) {
         const OrientDesc& od = orients[d.orient];
         if (od.skip) return;
         d.A = od.e[0];
         d.Lin = od.e[1];
+        d.in_sa = (long long)od.e[1] * d.C;  // item partials are [ex][ey][C]
     }
     const int a = blockIdx.y;
     const int c0 = blockIdx.x * PSB_TILE;

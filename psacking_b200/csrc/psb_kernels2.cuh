@@ -28,9 +28,16 @@ __device__ __forceinline__ bool okbit(const uint32_t* bits, const ScoreParams& s
     return (bits[((size_t)x * sp.ny + y) * sp.nzw + (z >> 5)] >> (z & 31)) & 1u;
 }
 
-// min of the approximate score over cells with an ok bit (interlock mode:
-// the reach mask is only known after the flood fill).  grid: (nx, n_orient)
-__global__ void k_select_min(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+// Candidate collection, one CTA per (x plane, orientation).  Pass 1: the
+// minimum approximate score over the plane's ok cells (free or reachable).
+// Pass 2: every ok cell within the window of that plane minimum becomes a
+// candidate, its approximate score kept in cscore.  The orientation minimum
+// smin is the minimum of the plane minima.  A cell within the window of smin
+// is within the (slightly wider) window of its own plane's minimum, so the
+// list holds every cell the exact guard must see; k_rescore drops the others.
+// Replaces compute_scores_kernel + argmin_reduction_kernel (fft3.cu:147-215,
+// 527-563).  grid: (nx, n_orient)
+__global__ void k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
     const int o = blockIdx.y, x = blockIdx.x;
     const OrientDesc& od = orients[o];
     if (od.skip || x >= od.valid[0]) return;
@@ -44,25 +51,22 @@ __global__ void k_select_min(const OrientDesc* __restrict__ orients, SelectBufs 
         size_t t = ((size_t)x * sp.ny + y) * sp.nz + z;
         m = fmin(m, ref_score(sp, od.base + (double)Dq[t], z));
     }
+    __shared__ double red[32];
     for (int off = 16; off > 0; off >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, off));
-    if ((threadIdx.x & 31) == 0 && m < 1e299) atomicMin(&sb.smin[o], ord_key(m));
-}
-
-// collect every ok cell whose approximate score is within the window of the
-// approximate minimum.  grid: (nx, n_orient)
-__global__ void k_collect(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
-    const int o = blockIdx.y, x = blockIdx.x;
-    const OrientDesc& od = orients[o];
-    if (od.skip || x >= od.valid[0]) return;
-    const unsigned long long mk = sb.smin[o];
-    if (mk == 0xffffffffffffffffULL) return;
-    const double smin = ord_val(mk);
-    const double win = 2.0 * od.delta + 8.0 * (fabs(smin) + 1.0) * 2.220446049250313e-16;
-    const double lim = smin + win;
-    const int Yv = od.valid[1], Zv = od.valid[2];
-    const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits;
-    const float* Dq = sb.Dq + (size_t)o * sb.sD;
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmin(b, red[w]);
+        red[0] = b;
+        if (b < 1e299) atomicMin(&sb.smin[o], ord_key(b));
+    }
+    __syncthreads();
+    const double pm = red[0];
+    if (pm >= 1e299) return;
+    const double lim = pm + 2.0 * od.delta + 1e-4 + 8.0 * (fabs(pm) + 1.0) * 2.220446049250313e-16;
     int* cand = sb.cand + (size_t)o * sb.cap;
+    double* cs = sb.cscore + (size_t)o * sb.cap;
     for (int idx = threadIdx.x; idx < Yv * Zv; idx += blockDim.x) {
         int y = idx / Zv, z = idx - y * Zv;
         if (!okbit(bits, sp, x, y, z)) continue;
@@ -70,7 +74,10 @@ __global__ void k_collect(const OrientDesc* __restrict__ orients, SelectBufs sb,
         double s = ref_score(sp, od.base + (double)Dq[t], z);
         if (s <= lim) {
             int slot = atomicAdd(&sb.ncand[o], 1);
-            if (slot < sb.cap) cand[slot] = (int)t;
+            if (slot < sb.cap) {
+                cand[slot] = (int)t;
+                cs[slot] = s;
+            }
         }
     }
 }
@@ -79,55 +86,72 @@ __global__ void k_collect(const OrientDesc* __restrict__ orients, SelectBufs sb,
 // exact integer.  Regime (b): direct integer sums over the item's voxels
 // (proximity and collision), the FP64 guard.  One warp per candidate.
 // grid: (blocks, n_orient)
-__global__ void k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp,
-                          const int32_t* __restrict__ tray, const int32_t* __restrict__ phi) {
+__global__ void __launch_bounds__(256)
+k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ tray,
+          const int32_t* __restrict__ phi) {
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
     const int n = min(sb.ncand[o], sb.cap);
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int* cand = sb.cand + (size_t)o * sb.cap;
     double* cs = sb.cscore + (size_t)o * sb.cap;
     const float* Dq = sb.Dq + (size_t)o * sb.sD;
-    for (int c = warp; c < n; c += nwarps) {
+    const double smin = ord_val(sb.smin[o]);
+    const double glim = smin + 2.0 * od.delta + 8.0 * (fabs(smin) + 1.0) * 2.220446049250313e-16;
+    if (!od.exact) {
+        // regime (a): the FP32 value rounds to the exact integer; one thread per candidate
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+            if (cs[c] > glim) { cs[c] = 1e300; continue; }
+            const int t = cand[c];
+            const double s = ref_score(sp, od.base + (double)rintf(Dq[t]), t % sp.nz);
+            cs[c] = s;
+            atomicMin(&sb.best[o], ord_key(s));
+        }
+        return;
+    }
+    // regime (b): one CTA per candidate sums the item's voxels exactly
+    __shared__ long long red_acc[8], red_coll[8];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int c = blockIdx.x; c < n; c += gridDim.x) {
+        if (cs[c] > glim) {  // outside the orientation's window: provably not the minimum
+            if (tid == 0) cs[c] = 1e300;
+            continue;
+        }
         const int t = cand[c];
         const int z = t % sp.nz;
         const int y = (t / sp.nz) % sp.ny;
         const int x = t / (sp.nz * sp.ny);
-        double D;
-        bool valid = true;
-        if (!od.exact) {
-            D = od.base + (double)rintf(Dq[t]);
-        } else {
-            long long acc = 0, coll = 0;
-            for (int v = lane; v < od.nvox; v += 32) {
-                int4 q = od.vox[v];
-                int oc[3];
-                orient_voxel(od, q.x, q.y, q.z, oc);
-                size_t g = ((size_t)(x + oc[0]) * sp.ny + (y + oc[1])) * sp.nz + (z + oc[2]);
-                acc += (long long)q.w * phi[g];
-                coll += (long long)q.w * (tray[g] != 0);
-            }
-            for (int off = 16; off > 0; off >>= 1) {
-                acc += __shfl_xor_sync(0xffffffffu, acc, off);
-                coll += __shfl_xor_sync(0xffffffffu, coll, off);
-            }
-            D = (double)acc;
-            if (coll != 0) valid = false;
-            double err = fabs(D - (od.base + (double)Dq[t]));
-            if (lane == 0) {
-                if (!valid) atomicOr(&sb.diag[o], 4u);
-                if (err > od.delta) atomicOr(&sb.diag[o], 8u);
-                atomicMax(&sb.errmax[o], __float_as_uint((float)(err / od.delta)));
-            }
+        long long acc = 0, coll = 0;
+        const int nv = od.nvox;
+#pragma unroll 4
+        for (int v = tid; v < nv; v += 256) {
+            const int4 q = __ldg(&od.vox[v]);
+            int oc[3];
+            orient_voxel(od, q.x, q.y, q.z, oc);
+            const size_t g = ((size_t)(x + oc[0]) * sp.ny + (y + oc[1])) * sp.nz + (z + oc[2]);
+            acc += (long long)q.w * __ldg(&phi[g]);
+            coll += (long long)q.w * (__ldg(&tray[g]) != 0);
         }
-        if (lane == 0) {
-            double s = valid ? ref_score(sp, D, z) : 1e300;
+        for (int off = 16; off > 0; off >>= 1) {
+            acc += __shfl_xor_sync(0xffffffffu, acc, off);
+            coll += __shfl_xor_sync(0xffffffffu, coll, off);
+        }
+        if (lane == 0) { red_acc[wid] = acc; red_coll[wid] = coll; }
+        __syncthreads();
+        if (tid == 0) {
+            long long A = 0, Cc = 0;
+            for (int w = 0; w < 8; ++w) { A += red_acc[w]; Cc += red_coll[w]; }
+            const double D = (double)A;
+            const bool valid = Cc == 0;
+            const double err = fabs(D - (od.base + (double)Dq[t]));
+            if (!valid) atomicOr(&sb.diag[o], 4u);
+            if (err > od.delta) atomicOr(&sb.diag[o], 8u);
+            atomicMax(&sb.errmax[o], __float_as_uint((float)(err / od.delta)));
+            const double s = valid ? ref_score(sp, D, z) : 1e300;
             cs[c] = s;
             if (valid) atomicMin(&sb.best[o], ord_key(s));
         }
+        __syncthreads();
     }
 }
 
@@ -236,82 +260,123 @@ __device__ __forceinline__ void run_unite(int* parent, int a, int b, unsigned in
 
 __device__ __forceinline__ bool fbit(const uint32_t* line, int z) { return (line[z >> 5] >> (z & 31)) & 1u; }
 
-// grid: (ceil(nx*ny/256), n_orient)
-__global__ void k_ff_count(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+// run starts of a line's free bits (bit z set where a run begins), word by word
+__device__ __forceinline__ uint32_t run_starts(const uint32_t* w, int i, uint32_t prevtop) {
+    const uint32_t cur = w[i];
+    return cur & ~((cur << 1) | prevtop);
+}
+
+// Per line: its number of z-runs.  Per 256-line block: the block's total
+// (blk[o][b]).  grid: (ceil(nx*ny/256), n_orient), block 256
+__global__ void __launch_bounds__(256)
+k_ff_count(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, int* __restrict__ blk, int nblk) {
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     const int line = blockIdx.x * blockDim.x + threadIdx.x;
-    if (line >= sp.nx * sp.ny) return;
     int c = 0;
-    if (!od.skip) {
+    if (!od.skip && line < sp.nx * sp.ny) {
         int x = line / sp.ny, y = line - x * sp.ny;
         if (x < od.valid[0] && y < od.valid[1]) {
             const uint32_t* w = fb.freebits + (size_t)o * fb.sBits + (size_t)line * sp.nzw;
             uint32_t prevtop = 0;
             for (int i = 0; i < sp.nzw; ++i) {
-                uint32_t cur = w[i];
-                c += __popc(cur & ~((cur << 1) | prevtop));
-                prevtop = cur >> 31;
+                c += __popc(run_starts(w, i, prevtop));
+                prevtop = w[i] >> 31;
             }
         }
     }
-    fb.cnt[(size_t)o * fb.sLine + line] = c;
+    if (line < sp.nx * sp.ny) fb.cnt[(size_t)o * fb.sLine + line] = c;
+    c = __reduce_add_sync(0xffffffffu, c);
+    __shared__ int ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int i = 0; i < 8; ++i) t += ws[i];
+        blk[(size_t)o * nblk + blockIdx.x] = t;
+    }
 }
 
-// exclusive scan of run counts, one CTA (1024 threads) per orientation
-__global__ void __launch_bounds__(1024) k_ff_scan(const OrientDesc* __restrict__ orients, FloodBufs fb, int nlines) {
+// Exclusive scan of the block totals of one orientation (one warp per
+// orientation); total runs in fb.total.  grid: (n_orient), block 32
+__global__ void k_ff_scan(const OrientDesc* __restrict__ orients, FloodBufs fb, int* __restrict__ blk, int nblk) {
     const int o = blockIdx.x;
     if (orients[o].skip) return;
-    __shared__ int part[1024];
-    const int tid = threadIdx.x;
-    const int per = (nlines + 1023) / 1024;
-    const int b0 = tid * per, b1 = min(nlines, b0 + per);
-    const int* cnt = fb.cnt + (size_t)o * fb.sLine;
-    int* off = fb.off + (size_t)o * fb.sLine;
-    int s = 0;
-    for (int i = b0; i < b1; ++i) s += cnt[i];
-    part[tid] = s;
-    __syncthreads();
-    for (int d = 1; d < 1024; d <<= 1) {
-        int v = tid >= d ? part[tid - d] : 0;
-        __syncthreads();
-        part[tid] += v;
-        __syncthreads();
+    int* b = blk + (size_t)o * nblk;
+    const int lane = threadIdx.x;
+    int carry = 0;
+    for (int base = 0; base < nblk; base += 32) {
+        const int i = base + lane;
+        const int v = i < nblk ? b[i] : 0;
+        int incl = v;
+        for (int d = 1; d < 32; d <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+        if (i < nblk) b[i] = carry + incl - v;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
     }
-    int run = part[tid] - s;
-    for (int i = b0; i < b1; ++i) { off[i] = run; run += cnt[i]; }
-    if (tid == 1023) fb.total[o] = part[1023];
+    if (lane == 0) fb.total[o] = carry;
 }
 
-// grid: (ceil(nx*ny/256), n_orient)
-__global__ void k_ff_emit(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+// Per line: its offset (block prefix + scan inside the block) and its runs,
+// found by bit scanning (one step per run, not per z).
+// grid: (ceil(nx*ny/256), n_orient), block 256
+__global__ void __launch_bounds__(256)
+k_ff_emit(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, const int* __restrict__ blk, int nblk) {
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
     const int line = blockIdx.x * blockDim.x + threadIdx.x;
-    if (line >= sp.nx * sp.ny) return;
+    const bool inl = line < sp.nx * sp.ny;
+    const int c = inl ? fb.cnt[(size_t)o * fb.sLine + line] : 0;
+    // block-level exclusive scan of c
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = c;
+    for (int d = 1; d < 32; d <<= 1) {
+        int u = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += u;
+    }
+    __shared__ int ws[8];
+    if (lane == 31) ws[wid] = incl;
+    __syncthreads();
+    int wpre = 0;
+    for (int i = 0; i < wid; ++i) wpre += ws[i];
+    int r = blk[(size_t)o * nblk + blockIdx.x] + wpre + incl - c;
+    if (!inl) return;
+    fb.off[(size_t)o * fb.sLine + line] = r;
+    if (c == 0) return;
     int x = line / sp.ny, y = line - x * sp.ny;
     const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
-    if (x >= Xv || y >= Yv) return;
     const uint32_t* w = fb.freebits + (size_t)o * fb.sBits + (size_t)line * sp.nzw;
-    int r = fb.off[(size_t)o * fb.sLine + line];
     const bool side = (x == 0) || (y == 0) || (od.hi[0] >= 0 && x == Xv - 1) || (od.hi[1] >= 0 && y == Yv - 1);
     int* rz = fb.rz + (size_t)o * fb.sRun;
     int* rl = fb.rline + (size_t)o * fb.sRun;
     int* par = fb.parent + (size_t)o * fb.sRun;
     int* fl = fb.rflag + (size_t)o * fb.sRun;
+    // walk runs: start = first set bit at or after z, end = first clear bit after it
     int z = 0;
+    const int nzw = sp.nzw;
     while (z < Zv) {
-        if (!fbit(w, z)) { ++z; continue; }
-        int z0 = z;
-        while (z < Zv && fbit(w, z)) ++z;
-        int z1 = z - 1;
-        bool seed = side || z0 == 0 || (od.hi[2] >= 0 && z1 == Zv - 1);
+        int wi = z >> 5;
+        uint32_t m = w[wi] & (0xffffffffu << (z & 31));
+        while (!m && ++wi < nzw) m = w[wi];
+        if (!m) break;
+        const int z0 = (wi << 5) + __ffs(m) - 1;
+        if (z0 >= Zv) break;
+        // first zero at or after z0
+        int wj = z0 >> 5;
+        uint32_t inv = ~w[wj] & (0xffffffffu << (z0 & 31));
+        while (!inv && ++wj < nzw) inv = ~w[wj];
+        int z1 = inv ? (wj << 5) + __ffs(inv) - 2 : (nzw << 5) - 1;
+        if (z1 >= Zv) z1 = Zv - 1;
+        const bool seed = side || z0 == 0 || (od.hi[2] >= 0 && z1 == Zv - 1);
         rz[r] = z0 | (z1 << 16);
         rl[r] = line;
         par[r] = r;
         fl[r] = seed ? 1 : 0;
         ++r;
+        z = z1 + 1;
     }
 }
 
@@ -386,7 +451,9 @@ __global__ void k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb,
 // ---------------------------------------------------------------------------
 // distance field: exact L1 distance to voxels equal to 1 (fft3.cu:887-1004)
 // ---------------------------------------------------------------------------
-__global__ void k_dist_init(const int32_t* __restrict__ g, int32_t* __restrict__ d, size_t V, int far) {
+__global__ void k_dist_init(const int32_t* __restrict__ g, int32_t* __restrict__ d, size_t V, int far,
+                            const int* gate) {
+    if (gate && !*gate) return;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < V; i += (size_t)gridDim.x * blockDim.x)
         d[i] = g[i] == 1 ? 0 : far;
 }
@@ -397,8 +464,9 @@ __global__ void k_dist_init(const int32_t* __restrict__ g, int32_t* __restrict__
 //   axis x: lines l = y*nz+z,        base = l,                 stride = ny*nz
 //   axis y: lines l = x*nz+z,        base = x*ny*nz + z,       stride = nz
 //   axis z: lines l = x*ny+y,        base = l*nz,              stride = 1
-__global__ void k_dist_axis(int32_t* __restrict__ d, int axis, int nx, int ny, int nz, int W) {
+__global__ void k_dist_axis(int32_t* __restrict__ d, int axis, int nx, int ny, int nz, int W, const int* gate) {
     extern __shared__ int32_t sd[];
+    if (gate && !*gate) return;
     const int L = axis == 0 ? nx : (axis == 1 ? ny : nz);
     const long long nlines = axis == 0 ? (long long)ny * nz : (axis == 1 ? (long long)nx * nz : (long long)nx * ny);
     const long long l0 = (long long)blockIdx.x * W;
@@ -443,7 +511,8 @@ __global__ void k_dist_axis(int32_t* __restrict__ d, int axis, int nx, int ny, i
 }
 
 // fallback for very long lines: sequential in global memory, one thread per line
-__global__ void k_dist_axis_global(int32_t* __restrict__ d, int axis, int nx, int ny, int nz) {
+__global__ void k_dist_axis_global(int32_t* __restrict__ d, int axis, int nx, int ny, int nz, const int* gate) {
+    if (gate && !*gate) return;
     const int L = axis == 0 ? nx : (axis == 1 ? ny : nz);
     const long long nlines = axis == 0 ? (long long)ny * nz : (axis == 1 ? (long long)nx * nz : (long long)nx * ny);
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,0 +1,201 @@
+// psb_loop.cuh — device-side decisions of the greedy packing loop, so the
+// host can queue a whole run without waiting on any item.
+//
+// Per item the stream runs: k_prep (error bounds from the current distance
+// statistics) -> the search -> k_decide (best orientation, strict <, first
+// wins: fft3.cu:1625 / packer.py:500) -> k_place_check / k_place_write /
+// k_place_done (packing.cpp:773-788) -> the occupancy spectrum rebuild, gated
+// on "placed".  Gated kernels read a device flag and return at once when it
+// is 0.
+#pragma once
+#include "psb_kernels2.cuh"
+
+struct PhiStats {
+    unsigned long long raw[4];  // k_stats accumulators (sum, sum of squares, max |.|)
+    int mean;                   // rounded mean of phi
+    int maxabs;                 // max |phi - mean|
+    double norm;                // || phi - mean ||_2
+};
+
+struct LoopState {
+    int placed;       // items placed so far in this run
+    int id_offset;
+    int do_place;     // current item found a position
+    int placed_now;   // current item was written into the tray (gate of the rebuild)
+    int need_phi;     // current item wrote voxels equal to 1 (gate of the distance rebuild)
+    int orient;       // chosen orientation of the current item
+    int px, py, pz;
+    int id;
+    unsigned int err; // 1: union-find limit, 2: candidate overflow, 4: placement overlap
+    unsigned long long first;  // first overlapping tray cell of the current item
+};
+
+// error bound and base of every orientation of one item (psb_tray::describe)
+__global__ void k_prep(OrientDesc* __restrict__ od, int n, const PhiStats* __restrict__ ps) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    OrientDesc& d = od[o];
+    const double maxD = (double)d.sabs * (double)ps->maxabs;
+    double ulp = 1.1920928955078125e-07;
+    if (maxD >= 1.0) {
+        int e;
+        frexp(maxD, &e);
+        ulp = ldexp(1.0, e - 24);
+    }
+    const double eps = 1.1920928955078125e-07;
+    d.delta = 2.0 * eps * sqrt(d.sumsq) * ps->norm + 0.5 * ulp + 1e-3;
+    d.exact = (d.delta >= 0.4 || maxD >= 8388608.0) ? 1 : 0;
+    d.base = (double)ps->mean * (double)d.sumI;
+}
+
+struct DecisionDev {
+    int x, y, z, found;
+    double score;
+    int orientation;
+    unsigned int diag;
+    int ncand;
+    float err_ratio;
+};
+
+// best over orientations (strict <: the first minimum wins), one thread
+__global__ void k_decide(const OrientDesc* __restrict__ od, const ResultDev* __restrict__ res, int n,
+                         LoopState* ls, DecisionDev* out, const unsigned int* uf_err) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int best = -1;
+    double bs = 1e300;
+    unsigned int diag = 0;
+    int ncand = 0;
+    float er = 0.f;
+    for (int o = 0; o < n; ++o) {
+        const ResultDev r = res[o];
+        diag |= r.diag;
+        ncand += r.ncand;
+        er = fmaxf(er, r.err_ratio);
+        if (r.diag & 0x100u) ls->err |= 2u;
+        if (od[o].skip) continue;
+        if (r.found && r.score < bs) {
+            bs = r.score;
+            best = o;
+        }
+    }
+    if (*uf_err) ls->err |= 1u;
+    DecisionDev d;
+    d.diag = diag;
+    d.ncand = ncand;
+    d.err_ratio = er;
+    if (best >= 0) {
+        const ResultDev r = res[best];
+        d.x = r.x; d.y = r.y; d.z = r.z;
+        d.found = 1;
+        d.score = r.score;
+        d.orientation = best;
+        ls->do_place = 1;
+        ls->orient = best;
+        ls->px = r.x; ls->py = r.y; ls->pz = r.z;
+        ls->id = ls->id_offset + ls->placed + 1;
+    } else {
+        d.x = d.y = d.z = -1;
+        d.found = 0;
+        d.score = 0.0;
+        d.orientation = -1;
+        ls->do_place = 0;
+    }
+    ls->placed_now = 0;
+    ls->need_phi = 0;
+    ls->first = 0xffffffffffffffffULL;
+    *out = d;
+}
+
+__global__ void k_place_check_g(const OrientDesc* __restrict__ od_item, LoopState* ls, const int32_t* __restrict__ tray,
+                                int nx, int ny, int nz) {
+    if (!ls->do_place) return;
+    const OrientDesc& od = od_item[ls->orient];
+    const int px = ls->px, py = ls->py, pz = ls->pz;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < od.nvox; v += gridDim.x * blockDim.x) {
+        int4 q = od.vox[v];
+        if (q.w <= 0) continue;
+        int oc[3];
+        orient_voxel(od, q.x, q.y, q.z, oc);
+        int i = px + oc[0], j = py + oc[1], k = pz + oc[2];
+        if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) continue;
+        size_t t = ((size_t)i * ny + j) * nz + k;
+        if (tray[t] > 0) atomicMin(&ls->first, (unsigned long long)t);
+    }
+}
+
+__global__ void k_place_write_g(const OrientDesc* __restrict__ od_item, const LoopState* ls, int32_t* __restrict__ tray,
+                                int nx, int ny, int nz) {
+    if (!ls->do_place || ls->first != 0xffffffffffffffffULL) return;
+    const OrientDesc& od = od_item[ls->orient];
+    const int px = ls->px, py = ls->py, pz = ls->pz, id = ls->id;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < od.nvox; v += gridDim.x * blockDim.x) {
+        int4 q = od.vox[v];
+        if (q.w <= 0) continue;
+        int oc[3];
+        orient_voxel(od, q.x, q.y, q.z, oc);
+        int i = px + oc[0], j = py + oc[1], k = pz + oc[2];
+        if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) continue;
+        size_t t = ((size_t)i * ny + j) * nz + k;
+        if (tray[t] == 0) tray[t] = id;
+    }
+}
+
+// commit: count the placement, set the rebuild gates; an overlap (an FP32
+// "free" cell that the exact check rejects) marks the item unplaced and
+// raises the run's error word
+__global__ void k_place_done(const OrientDesc* __restrict__ od_item, LoopState* ls, DecisionDev* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (!ls->do_place) return;
+    if (ls->first != 0xffffffffffffffffULL) {
+        ls->err |= 4u;
+        out->found = 0;
+        out->x = out->y = out->z = -1;
+        out->orientation = -1;
+        out->score = 0.0;
+        ls->do_place = 0;
+        return;
+    }
+    ls->placed += 1;
+    ls->placed_now = od_item[ls->orient].nvox > 0 ? 1 : 0;
+    ls->need_phi = (ls->id == 1 && od_item[ls->orient].nvox > 0) ? 1 : 0;
+}
+
+// distance statistics on the device: mean after the first k_stats pass,
+// norm and max after the second
+__global__ void k_phi_mean(PhiStats* ps, unsigned long long V, const int* gate) {
+    if (gate && !*gate) return;
+    const long long sum = (long long)ps->raw[0];
+    ps->mean = (int)llround((double)sum / (double)V);
+    ps->raw[0] = ps->raw[1] = ps->raw[2] = ps->raw[3] = 0ULL;
+}
+
+__global__ void k_phi_norm(PhiStats* ps, const int* gate) {
+    if (gate && !*gate) return;
+    ps->norm = sqrt((double)(long long)ps->raw[1]);
+    ps->maxabs = (int)(unsigned int)(ps->raw[2] & 0xffffffffULL);
+}
+
+// k_stats with a device-side shift and a gate
+__global__ void k_stats_g(const int32_t* __restrict__ v, size_t n, const int* shiftp, unsigned long long* out,
+                          const int* gate) {
+    if (gate && !*gate) return;
+    const int shift = shiftp ? *shiftp : 0;
+    long long s = 0, s2 = 0;
+    int mx = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        long long d = (long long)v[i] - shift;
+        s += d;
+        s2 += d * d;
+        mx = max(mx, (int)(d < 0 ? -d : d));
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, off);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&out[0], (unsigned long long)s);
+        atomicAdd(&out[1], (unsigned long long)s2);
+        atomicMax((unsigned int*)&out[2], (unsigned int)mx);
+    }
+}
