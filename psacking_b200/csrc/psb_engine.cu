@@ -221,6 +221,37 @@ PlaneFn plane2_for(int ny, int nz) {
 }
 #undef PSB_PLANE_ROW
 
+using FwdPlaneFn = void (*)(FwdSrc, const OrientDesc*, const float2*, const float2*);
+using XfwdFn = void (*)(const float2*, float2*, int, int, const int*, const float2*);
+
+#define PSB_FWD_ROW(NY)                           \
+    case NY:                                      \
+        switch (nz) {                             \
+            case 64: return k_fwd_plane<NY, 64>;   \
+            case 100: return k_fwd_plane<NY, 100>; \
+            case 128: return k_fwd_plane<NY, 128>; \
+            default: return nullptr;              \
+        }
+FwdPlaneFn fwd_plane_for(int ny, int nz) {
+    switch (ny) {
+        PSB_FWD_ROW(64)
+        PSB_FWD_ROW(100)
+        PSB_FWD_ROW(128)
+        default: return nullptr;
+    }
+}
+#undef PSB_FWD_ROW
+
+XfwdFn xfwd_for(int n) {
+    switch (n) {
+        case 64: return k_xfwd<64>;
+        case 100: return k_xfwd<100>;
+        case 128: return k_xfwd<128>;
+        case 240: return k_xfwd<240>;
+        default: return nullptr;
+    }
+}
+
 // register-DFT twiddles W_R^i for R <= 32 (offset R*(R-1)/2)
 int init_register_twiddles() {
     std::vector<float2> t(PSB_TWR_SIZE);
@@ -257,7 +288,11 @@ int set_smem_attrs() {
     TRY(set_max_dyn_smem(k_dist_axis));
     for (int n : {64, 100, 128, 240}) TRY(set_max_dyn_smem(xpass2_for(n)));
     for (int a : {64, 100, 128})
-        for (int b : {64, 100, 128}) TRY(set_max_dyn_smem(plane2_for(a, b)));
+        for (int b : {64, 100, 128}) {
+            TRY(set_max_dyn_smem(plane2_for(a, b)));
+            TRY(set_max_dyn_smem(fwd_plane_for(a, b)));
+        }
+    for (int n : {64, 100, 128, 240}) TRY(set_max_dyn_smem(xfwd_for(n)));
     TRY(init_register_twiddles());
     if (dev < 64) done[dev] = true;
     return PSB_OK;
@@ -666,10 +701,41 @@ struct psb_tray {
         return PSB_OK;
     }
 
+    // spectrum of the occupancy (phi = false) or of phi - mean (phi = true);
+    // gated: only when *gate != 0 at run time.  Specialised kernels when the
+    // FFT lengths have plans, the generic descriptor path otherwise.
+    int tray_forward(bool phi, const int* gate) {
+        FwdPlaneFn ff = g_fast_fft ? fwd_plane_for(g.F[1], g.F[2]) : nullptr;
+        XfwdFn xf = g_fast_fft ? xfwd_for(g.F[0]) : nullptr;
+        const size_t smf = fwd_plane_smem(g.F[1], g.F[2], ny) + 64;
+        if (ff && xf && smf <= (size_t)g_smem_optin && xfwd_smem(g.F[0]) + 64 <= (size_t)g_smem_optin) {
+            const int* mean_p = (const int*)((const char*)d_ps + offsetof(PhiStats, mean));
+            FwdSrc src{phi ? (int)SRC_GRID_SUB : (int)SRC_GRID_OCC, phi ? d_phi : d_tray, nx, ny, nz, mean_p, gate,
+                       d_w2, 0};
+            {
+                PROF("k_fwd_plane", st);
+                ff<<<dim3(nx, 1), 256, smf, st>>>(src, nullptr, g.p[1].tw, g.p[2].tw);
+            }
+            CKL();
+            {
+                PROF("k_xfwd", st);
+                const int ncols = g.F[1] * g.H;
+                xf<<<(ncols + PSB_XCOLS - 1) / PSB_XCOLS, 256, xfwd_smem(g.F[0]), st>>>(
+                    d_w2, phi ? d_Sphi : d_Socc, nx, ncols, gate, g.p[0].tw);
+            }
+            CKL();
+            return PSB_OK;
+        }
+        const int idx = (phi ? 1 : 0) + (gate ? 2 : 0);
+        return forward3_dev(g, d_rzd + idx, d_midd + 2 * idx, st);
+    }
+
     // occupancy spectrum from the device tray
-    int rebuild_occ() { return forward3_dev(g, d_rzd + 0, d_midd + 0, st); }
+    int rebuild_occ() { return tray_forward(false, nullptr); }
     // ... only when the current item of the asynchronous loop was placed
-    int rebuild_occ_gated() { return forward3_dev(g, d_rzd + 2, d_midd + 4, st); }
+    int rebuild_occ_gated() {
+        return tray_forward(false, (const int*)((const char*)d_ls + offsetof(LoopState, placed_now)));
+    }
 
     // mean, norm and max deviation of the distance field, on the device
     int phi_stats(const int* gate) {
@@ -696,7 +762,7 @@ struct psb_tray {
     // distance spectrum (mean-subtracted) from the device distance field
     int rebuild_phi_spectrum() {
         TRY(phi_stats(nullptr));
-        TRY(forward3_dev(g, d_rzd + 1, d_midd + 2, st));
+        TRY(tray_forward(true, nullptr));
         PhiStats h;
         CK(cudaMemcpyAsync(&h, d_ps, sizeof(h), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -712,7 +778,7 @@ struct psb_tray {
         const int* need_phi = (const int*)((const char*)d_ls + offsetof(LoopState, need_phi));
         TRY(distance_on_device(d_tray, d_phi, nx, ny, nz, st, need_phi));
         TRY(phi_stats(need_phi));
-        return forward3_dev(g, d_rzd + 3, d_midd + 6, st);
+        return tray_forward(true, need_phi);
     }
 
     int set(const int32_t* tray, const int32_t* phi) {
@@ -792,16 +858,27 @@ struct psb_tray {
                 exmax = std::max(exmax, o.e[0]);
                 maxpairs = std::max(maxpairs, (o.e[0] * o.e[1] + 1) / 2);
             }
-        {
-            PROF("k_rfft_z", st);
-            k_rfft_z<<<dim3((maxpairs + PSB_PAIRS - 1) / PSB_PAIRS, n), PSB_THREADS, smem_rz(g.F[2]), st>>>(
-                d_rzs, d_odb, g.p[2].p, g.p[2].tw);
-        }
-        CKL();
-        {
-            PROF("k_fft_mid_fwd", st);
-            k_fft_mid<-1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, exmax, n), PSB_THREADS, smem_mid(g.F[1]), st>>>(
-                d_mids, d_odb, g.p[1].p, g.p[1].tw);
+        int eymax = 1;
+        for (auto& o : ods)
+            if (!o.skip) eymax = std::max(eymax, o.e[1]);
+        FwdPlaneFn ff = g_fast_fft ? fwd_plane_for(g.F[1], g.F[2]) : nullptr;
+        const size_t smf = fwd_plane_smem(g.F[1], g.F[2], eymax) + 64;
+        if (ff && smf <= (size_t)g_smem_optin) {
+            FwdSrc src{SRC_ITEM, nullptr, 0, 0, 0, nullptr, nullptr, d_Bi, sBi};
+            PROF("k_fwd_plane", st);
+            ff<<<dim3(exmax, n), 256, smf, st>>>(src, d_odb, g.p[1].tw, g.p[2].tw);
+        } else {
+            {
+                PROF("k_rfft_z", st);
+                k_rfft_z<<<dim3((maxpairs + PSB_PAIRS - 1) / PSB_PAIRS, n), PSB_THREADS, smem_rz(g.F[2]), st>>>(
+                    d_rzs, d_odb, g.p[2].p, g.p[2].tw);
+            }
+            CKL();
+            {
+                PROF("k_fft_mid_fwd", st);
+                k_fft_mid<-1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, exmax, n), PSB_THREADS, smem_mid(g.F[1]), st>>>(
+                    d_mids, d_odb, g.p[1].p, g.p[1].tw);
+            }
         }
         CKL();
         SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};

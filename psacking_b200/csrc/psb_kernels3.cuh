@@ -177,3 +177,116 @@ k_plane2(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
         if (m < 1e299) atomicMin(&pb.smin[o], ord_key(m));
     }
 }
+
+// ---------------------------------------------------------------------------
+// forward transforms of the item (per orientation) and of the tray's grids
+// ---------------------------------------------------------------------------
+struct FwdSrc {
+    int kind;            // SRC_ITEM (orientation gather) or SRC_GRID_OCC / SRC_GRID_SUB
+    const int32_t* grid; // tray grid (n0, n1, n2)
+    int n0, n1, n2;
+    const int* subp;     // SRC_GRID_SUB: device-side shift
+    const int* gate;     // when set, run only if *gate != 0
+    float2* out;         // [n0][NY][HZ] per batch element
+    long long out_stride;
+};
+
+// One x slab per CTA: each z line (real, zero-padded to NZ) is transformed as
+// a complex line (half the outputs kept), then every kz column is transformed
+// along y.  Writes out[i][ky][kz] for all ky < NY.  Replaces k_rfft_z + the y
+// k_fft_mid of the generic path.  grid: (max slabs, batch), block 256
+template <int NY, int NZ>
+__global__ void __launch_bounds__(256)
+k_fwd_plane(FwdSrc src, const OrientDesc* __restrict__ orients, const float2* __restrict__ g_twy,
+            const float2* __restrict__ g_twz) {
+    constexpr int HZ = NZ / 2 + 1;
+    constexpr int RY0 = Plan2<NY>::R0, RY1 = Plan2<NY>::R1;
+    constexpr int RZ0 = Plan2<NZ>::R0, RZ1 = Plan2<NZ>::R1;
+    extern __shared__ float2 sm[];
+    if (src.gate && !*src.gate) return;
+    const int b = blockIdx.y, i = blockIdx.x;
+    int n0 = src.n0, n1 = src.n1, n2 = src.n2;
+    OrientDesc od;
+    if (src.kind == SRC_ITEM) {
+        od = orients[b];
+        if (od.skip) return;
+        n0 = od.e[0]; n1 = od.e[1]; n2 = od.e[2];
+    }
+    if (i >= n0) return;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int shift = (src.kind == SRC_GRID_SUB && src.subp) ? *src.subp : 0;
+    float2* twy = sm;
+    float2* twz = twy + NY;
+    float2* A = twz + NZ;
+    const int asz = max(n1 * NZ, NY * HZ);
+    float2* Q = A + asz;
+    load_twiddles(twy, g_twy, NY, tid, nthr);
+    load_twiddles(twz, g_twz, NZ, tid, nthr);
+    __syncthreads();
+    // z: complex transform of each real line j < n1
+    tpass<NZ, RZ0, 1, -1, 1, true>(
+        [&](int j, int k) {
+            float v = 0.f;
+            if (k < n2) {
+                if (src.kind == SRC_ITEM) {
+                    v = (float)od.item[orient_src_index(od, i, j, k)];
+                } else {
+                    const int r = src.grid[((size_t)i * n1 + j) * n2 + k];
+                    v = (float)(src.kind == SRC_GRID_OCC ? (r != 0) : (r - shift));
+                }
+            }
+            return make_float2(v, 0.f);
+        },
+        [&](int j, int n, float2 v) { A[j * NZ + n] = v; }, n1, twz, tid, nthr);
+    __syncthreads();
+    tpass<NZ, RZ1, RZ0, -1, 1, true>([&](int j, int n) { return A[j * NZ + n]; },
+                                     [&](int j, int kz, float2 v) {
+                                         if (kz < HZ) Q[j * HZ + kz] = v;
+                                     },
+                                     n1, twz, tid, nthr);
+    __syncthreads();
+    // y: columns kz (rows j >= n1 are zero)
+    tpass<NY, RY0, 1, -1, HZ, false>([&](int c, int n) { return n < n1 ? Q[n * HZ + c] : make_float2(0.f, 0.f); },
+                                     [&](int c, int n, float2 v) { A[n * HZ + c] = v; }, HZ, twy, tid, nthr);
+    __syncthreads();
+    float2* out = src.out + (size_t)b * src.out_stride + (size_t)i * NY * HZ;
+    tpass<NY, RY1, RY0, -1, HZ, false>([&](int c, int n) { return A[n * HZ + c]; },
+                                       [&](int c, int ky, float2 v) { out[(size_t)ky * HZ + c] = v; }, HZ, twy, tid,
+                                       nthr);
+}
+
+inline size_t fwd_plane_smem(int NY, int NZ, int n1) {
+    const size_t HZ = NZ / 2 + 1;
+    const size_t a = std::max((size_t)n1 * NZ, (size_t)NY * HZ);
+    return sizeof(float2) * (NY + NZ + a + (size_t)n1 * HZ);
+}
+
+// x forward of a [n0][ncols] slab stack into the spectrum [N][ncols]
+// (rows >= n0 are zero).  grid: ceil(ncols / PSB_XCOLS), block 256
+template <int N>
+__global__ void __launch_bounds__(256)
+k_xfwd(const float2* __restrict__ in, float2* __restrict__ out, int n0, int ncols, const int* gate,
+       const float2* __restrict__ g_tw) {
+    constexpr int C = PSB_XCOLS;
+    constexpr int R0 = Plan2<N>::R0, R1 = Plan2<N>::R1;
+    extern __shared__ float2 sm[];
+    if (gate && !*gate) return;
+    const int c0 = blockIdx.x * C;
+    const int nl = min(C, ncols - c0);
+    float2* tw = sm;
+    float2* A = tw + N;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    load_twiddles(tw, g_tw, N, tid, nthr);
+    __syncthreads();
+    const float2* src = in + c0;
+    float2* dst = out + c0;
+    tpass<N, R0, 1, -1, C, false>(
+        [&](int c, int n) { return n < n0 ? src[(size_t)n * ncols + c] : make_float2(0.f, 0.f); },
+        [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
+    __syncthreads();
+    tpass<N, R1, R0, -1, C, false>([&](int c, int n) { return A[n * C + c]; },
+                                   [&](int c, int k, float2 v) { dst[(size_t)k * ncols + c] = v; }, nl, tw, tid,
+                                   nthr);
+}
+
+constexpr size_t xfwd_smem(int N) { return sizeof(float2) * ((size_t)N + (size_t)N * PSB_XCOLS); }
