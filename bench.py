@@ -315,6 +315,48 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
+def run_many(args, rank, world, local_rank):
+    """Many-tray form: 64 trays with sides drawn from 64..160, 50-300 config-2
+    style items each, 24 orientations; trays are sharded round robin across
+    ranks and packed concurrently on each GPU (psb_pack_many)."""
+    import torch
+    from psacking_b200 import BinPacker, workloads
+    from psacking_b200.shard import reduce_run, tray_shard
+    torch.cuda.set_device(local_rank)
+    trays = workloads.config5_trays(seed=5, n_trays=args.trays)
+    mine = [trays[i] for i in tray_shard(len(trays), rank, world)]
+    packer = BinPacker((8, 8, 8), num_orientations=N_ORIENT, interlocking_free=False)
+    for _ in range(args.warmup):
+        packer.pack_many(mine[:2], concurrency=args.concurrency)
+    ms, placed, searched = [], 0, 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        res = packer.pack_many(mine, concurrency=args.concurrency)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+        placed += sum(r.num_placed for r in res)
+        searched += sum(len(r.placements) for r in res)
+    total_ms, placed_all = reduce_run(sum(ms), placed, device=torch.device("cuda", local_rank))
+    if rank != 0:
+        return None
+    dens = [r.density for r in res]
+    return {"metric": "items placed/s, 64 trays 64-160 per axis, 24 orientations (many-tray form)",
+            "value": round(placed_all / (total_ms / 1e3), 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32 (FFT), i64/f64 (exact tie guard)",
+            "data": "synthetic (seeded config-5 trays)",
+            "config": {"workload": f"config5: {len(trays)} trays, sides 64..160, 50-300 items each, 24 orientations",
+                       "trays_on_rank0": len(mine), "items_searched_rank0_per_step": searched // args.steps,
+                       "concurrency": args.concurrency, "mean_density_rank0": round(float(np.mean(dens)), 4),
+                       "parallelism": f"trays sharded over {world} GPU(s), {args.concurrency} concurrent streams each"}}
+
+
 def cpu_sample_setup():
     """The bounded CPU sample: the tray after the first item of the workload is
     placed, and the second item (24 orientations, interlocking-free)."""
@@ -364,6 +406,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--items", type=int, default=N_ITEMS, help="profiling only: shorter item stream")
     ap.add_argument("--value-only", action="store_true", help="profiling only: skip the e2e leg")
+    ap.add_argument("--workload", default="config3", choices=["config3", "config5"])
+    ap.add_argument("--trays", type=int, default=64, help="config5: number of trays")
+    ap.add_argument("--concurrency", type=int, default=8, help="config5: trays packed at once per GPU")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -380,9 +425,9 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device("cuda", local_rank))
-    out = run_ours(args, rank, world, local_rank)
+    out = run_many(args, rank, world, local_rank) if args.workload == "config5" else run_ours(args, rank, world, local_rank)
     if rank == 0 and out is not None:
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and args.workload == "config3":
             item, tray = cpu_sample_setup()
             dt, n = time_cpu_sample(item, tray)
             out["cpu_baseline"] = {"value": round(n / dt, 5), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",

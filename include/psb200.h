@@ -185,6 +185,17 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
  * (used by the tests to check both). */
 int psb_set_fast_fft(int on);
 
+/* Many independent trays (the many-tray form of the benchmark set): tray i
+ * has dims tray_dims[3i..3i+2] and items_per_tray[i] items, which follow the
+ * previous trays' items in `items` / `item_dims` and are already in packing
+ * order.  Each tray starts empty and is packed exactly as psb_pack would;
+ * up to `concurrency` trays run at once, each on its own CUDA stream and host
+ * worker thread.  out_placements has one result per item (same order);
+ * final_trays (may be NULL) has one output grid per tray. */
+int psb_pack_many(int n_trays, const int32_t* tray_dims, const int32_t* const* items, const int32_t* item_dims,
+                  const int32_t* items_per_tray, const int32_t* orient_maps, int n_orient, int interlock,
+                  int concurrency, psb_result* out_placements, int32_t* const* final_trays);
+
 /* ---- tracing (the reference's SCOPED_TIMER, spectral_packing/timing.h:11-31,
  *      as CUDA events around every kernel launch; off by default) ---------- */
 int psb_profile_enable(int on);          /* clears previous records            */

@@ -367,6 +367,55 @@ py::tuple py_pack_native(py::list items, py::handle initial_tray, py::array_t<in
     return py::make_tuple(out, pl);
 }
 
+// trays: list of (dims, [items in packing order]) -> list of (final tray, placements)
+py::list py_pack_many(py::list trays, py::array_t<int32_t> orient_maps, bool interlock, int concurrency) {
+    auto maps = py::array_t<int32_t, py::array::c_style | py::array::forcecast>::ensure(orient_maps);
+    if (maps.ndim() != 2 || maps.shape(1) != 6) throw std::runtime_error("orient_maps must be (n, 6) int32");
+    const int n_orient = (int)maps.shape(0);
+    std::vector<Grid> grids;
+    std::vector<const int32_t*> ptrs;
+    std::vector<int32_t> idims, tdims, counts;
+    for (auto tr : trays) {
+        py::tuple tt = tr.cast<py::tuple>();
+        py::tuple d = tt[0].cast<py::tuple>();
+        for (int a = 0; a < 3; ++a) tdims.push_back(d[a].cast<int>());
+        py::list its = tt[1].cast<py::list>();
+        counts.push_back((int)py::len(its));
+        for (auto it : its) grids.push_back(to_grid(it));
+    }
+    for (auto& g : grids) {
+        ptrs.push_back(g.ptr());
+        idims.insert(idims.end(), {g.n[0], g.n[1], g.n[2]});
+    }
+    const int n_trays = (int)counts.size();
+    std::vector<psb_result> res(grids.size());
+    std::vector<py::array_t<int32_t>> outs;
+    std::vector<int32_t*> outp;
+    for (int i = 0; i < n_trays; ++i) {
+        outs.push_back(new_grid(&tdims[3 * i]));
+        outp.push_back(outs.back().mutable_data());
+    }
+    int st;
+    {
+        py::gil_scoped_release nogil;
+        st = psb_pack_many(n_trays, tdims.data(), ptrs.data(), idims.data(), counts.data(), maps.data(), n_orient,
+                           interlock ? 1 : 0, concurrency, res.data(), outp.data());
+    }
+    check(st);
+    py::list out;
+    size_t k = 0;
+    for (int i = 0; i < n_trays; ++i) {
+        py::list pl;
+        for (int j = 0; j < counts[i]; ++j, ++k) {
+            const psb_result& r = res[k];
+            pl.append(py::make_tuple(py::make_tuple(r.x, r.y, r.z), (bool)r.found, r.score, r.orientation, r.diag,
+                                     r.n_candidates, r.err_ratio));
+        }
+        out.append(py::make_tuple(outs[i], pl));
+    }
+    return out;
+}
+
 py::dict py_search_detail(py::list orientations, int flags) {
     if (!py_gpu_tray_is_initialized()) throw std::runtime_error("GPU tray context not initialized");
     auto gs = to_grids(orientations);
@@ -429,6 +478,8 @@ PYBIND11_MODULE(_core, m) {
     m.def("pack_native", &py_pack_native, py::arg("items"), py::arg("initial_tray"), py::arg("orient_maps"),
           py::arg("interlock"), py::arg("id_offset"));
     m.def("search_detail", &py_search_detail, py::arg("orientations"), py::arg("flags"));
+    m.def("pack_many", &py_pack_many, py::arg("trays"), py::arg("orient_maps"), py::arg("interlock"),
+          py::arg("concurrency") = 8);
     m.def("device_count", &py_device_count);
     m.def("set_fast_fft", [](bool on) { psb_set_fast_fft(on ? 1 : 0); }, py::arg("on"),
           "Use the specialised two-pass FFT kernels where a plan exists (default) or force the generic path.");

@@ -18,6 +18,8 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <atomic>
+#include <thread>
 
 #include "../../include/psb200.h"
 #include "psb_kernels2.cuh"
@@ -298,17 +300,27 @@ int set_smem_attrs() {
     return PSB_OK;
 }
 
+// Device allocations.  With a stream they are stream-ordered (the tray's own
+// stream), so creating and freeing trays never synchronises the whole device
+// while other trays are running.
 template <class T>
-int dalloc(T** p, size_t n) {
+int dalloc(T** p, size_t n, cudaStream_t s = nullptr) {
     *p = nullptr;
     if (n == 0) n = 1;
-    CK(cudaMalloc((void**)p, sizeof(T) * n));
+    if (s) {
+        CK(cudaMallocAsync((void**)p, sizeof(T) * n, s));
+    } else {
+        CK(cudaMalloc((void**)p, sizeof(T) * n));
+    }
     return PSB_OK;
 }
 
 template <class T>
-void dfree(T*& p) {
-    if (p) cudaFree(p);
+void dfree(T*& p, cudaStream_t s = nullptr) {
+    if (p) {
+        if (s) cudaFreeAsync(p, s);
+        else cudaFree(p);
+    }
     p = nullptr;
 }
 
@@ -584,19 +596,22 @@ struct psb_tray {
     ~psb_tray() { release(); }
 
     void release_slots() {
-        dfree(d_Ai); dfree(d_Bi); dfree(d_Pc); dfree(d_Pd); dfree(d_Dq); dfree(d_free); dfree(d_reach);
-        dfree(d_cnt); dfree(d_off); dfree(d_rz2); dfree(d_rline); dfree(d_par); dfree(d_rflag); dfree(d_total); dfree(d_blk);
-        dfree(d_cand); dfree(d_ncand); dfree(d_cscore); dfree(d_smin); dfree(d_smin2); dfree(d_best);
-        dfree(d_bestkey); dfree(d_diag); dfree(d_errmax); dfree(d_od); dfree(d_rzs); dfree(d_mids); dfree(d_res);
+        dfree(d_Ai, st); dfree(d_Bi, st); dfree(d_Pc, st); dfree(d_Pd, st); dfree(d_Dq, st); dfree(d_free, st); dfree(d_reach, st);
+        dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
+        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_smin2, st); dfree(d_best, st);
+        dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
     void release() {
         if (dev >= 0) cudaSetDevice(dev);
         release_slots();
-        dfree(d_tray); dfree(d_phi); dfree(d_Socc); dfree(d_Sphi); dfree(d_w1); dfree(d_w2); dfree(d_pen);
-        dfree(d_rz); dfree(d_mid); dfree(d_stats); dfree(d_err); dfree(d_first); dfree(d_items); dfree(d_vox); dfree(d_stage); dfree(d_stage_vox);
-        dfree(d_ls); dfree(d_ps); dfree(d_rzd); dfree(d_midd); dfree(d_od_all); dfree(d_dec);
-        if (st) cudaStreamDestroy(st);
+        dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_pen, st);
+        dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st); dfree(d_stage_vox, st);
+        dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_dec, st);
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
         st = nullptr;
     }
 
@@ -611,11 +626,13 @@ struct psb_tray {
         if (const char* e = getenv("PSB_SUBBATCH")) subbatch = atoi(e);
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         size_t S = (size_t)g.F[0] * g.F[1] * g.H;
-        TRY(dalloc(&d_tray, V)); TRY(dalloc(&d_phi, V));
-        TRY(dalloc(&d_Socc, S)); TRY(dalloc(&d_Sphi, S));
-        TRY(dalloc(&d_w1, (size_t)nx * ny * g.H)); TRY(dalloc(&d_w2, (size_t)nx * g.F[1] * g.H));
-        TRY(dalloc(&d_pen, 3 * (size_t)nz)); TRY(dalloc(&d_rz, 4)); TRY(dalloc(&d_mid, 4)); TRY(dalloc(&d_stats, 4));
-        TRY(dalloc(&d_err, 1)); TRY(dalloc(&d_first, 1));
+        TRY(dalloc(&d_tray, V, st)); TRY(dalloc(&d_phi, V, st));
+        TRY(dalloc(&d_Socc, S, st)); TRY(dalloc(&d_Sphi, S, st));
+        TRY(dalloc(&d_w1, (size_t)nx * ny * g.H, st)); TRY(dalloc(&d_w2, (size_t)nx * g.F[1] * g.H, st));
+        TRY(dalloc(&d_pen, 3 * (size_t)nz, st)); TRY(dalloc(&d_rz, 4, st)); TRY(dalloc(&d_mid, 4, st)); TRY(dalloc(&d_stats, 4, st));
+        TRY(dalloc(&d_err, 1, st)); TRY(dalloc(&d_first, 1, st));
+        TRY(dalloc(&d_ls, 1, st)); TRY(dalloc(&d_ps, 1, st)); TRY(dalloc(&d_rzd, 4, st)); TRY(dalloc(&d_midd, 8, st));
+        CK(cudaStreamSynchronize(st));  // stream-ordered allocations complete before plain copies touch them
         CK(cudaMemset(d_err, 0, sizeof(unsigned int)));
         // SCAN-mode penalty table with the host libm pow (packing.cpp:630-631)
         // BLOCK-mode factors (fft3.cu:172-173): qz = k/nz, qa = (P*qz)*qz, both
@@ -629,7 +646,6 @@ struct psb_tray {
             pen[2 * nz + k] = qz;
         }
         CK(cudaMemcpy(d_pen, pen.data(), sizeof(double) * 3 * nz, cudaMemcpyHostToDevice));
-        TRY(dalloc(&d_ls, 1)); TRY(dalloc(&d_ps, 1)); TRY(dalloc(&d_rzd, 4)); TRY(dalloc(&d_midd, 8));
         CK(cudaMemset(d_ls, 0, sizeof(LoopState)));
         CK(cudaMemset(d_ps, 0, sizeof(PhiStats)));
         const int* mean_p = (const int*)((const char*)d_ps + offsetof(PhiStats, mean));
@@ -660,19 +676,19 @@ struct psb_tray {
         sBits = (long long)nx * ny * nzw;
         sLine = (long long)nx * ny;
         sRun = (long long)nx * ny * ((nz + 1) / 2);
-        TRY(dalloc(&d_Ai, sAi * c)); TRY(dalloc(&d_Bi, sBi * c));
-        TRY(dalloc(&d_Pc, sP * c)); TRY(dalloc(&d_Pd, sP * c));
-        TRY(dalloc(&d_Dq, sD * c));
-        TRY(dalloc(&d_free, sBits * c)); TRY(dalloc(&d_reach, sBits * c));
-        TRY(dalloc(&d_cnt, sLine * c)); TRY(dalloc(&d_off, sLine * c));
-        TRY(dalloc(&d_rz2, sRun * c)); TRY(dalloc(&d_rline, sRun * c)); TRY(dalloc(&d_par, sRun * c));
-        TRY(dalloc(&d_rflag, sRun * c)); TRY(dalloc(&d_total, c));
-        TRY(dalloc(&d_blk, (size_t)((nx * ny + 255) / 256) * c));
-        TRY(dalloc(&d_cand, (size_t)kCandCap * c)); TRY(dalloc(&d_ncand, c));
-        TRY(dalloc(&d_cscore, (size_t)kCandCap * c));
-        TRY(dalloc(&d_smin, c)); TRY(dalloc(&d_smin2, c)); TRY(dalloc(&d_best, c)); TRY(dalloc(&d_bestkey, c));
-        TRY(dalloc(&d_diag, c)); TRY(dalloc(&d_errmax, c)); TRY(dalloc(&d_od, c)); TRY(dalloc(&d_rzs, c)); TRY(dalloc(&d_mids, c));
-        TRY(dalloc(&d_res, c));
+        TRY(dalloc(&d_Ai, sAi * c, st)); TRY(dalloc(&d_Bi, sBi * c, st));
+        TRY(dalloc(&d_Pc, sP * c, st)); TRY(dalloc(&d_Pd, sP * c, st));
+        TRY(dalloc(&d_Dq, sD * c, st));
+        TRY(dalloc(&d_free, sBits * c, st)); TRY(dalloc(&d_reach, sBits * c, st));
+        TRY(dalloc(&d_cnt, sLine * c, st)); TRY(dalloc(&d_off, sLine * c, st));
+        TRY(dalloc(&d_rz2, sRun * c, st)); TRY(dalloc(&d_rline, sRun * c, st)); TRY(dalloc(&d_par, sRun * c, st));
+        TRY(dalloc(&d_rflag, sRun * c, st)); TRY(dalloc(&d_total, c, st));
+        TRY(dalloc(&d_blk, (size_t)((nx * ny + 255) / 256) * c, st));
+        TRY(dalloc(&d_cand, (size_t)kCandCap * c, st)); TRY(dalloc(&d_ncand, c, st));
+        TRY(dalloc(&d_cscore, (size_t)kCandCap * c, st));
+        TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_smin2, c, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
+        TRY(dalloc(&d_diag, c, st)); TRY(dalloc(&d_errmax, c, st)); TRY(dalloc(&d_od, c, st)); TRY(dalloc(&d_rzs, c, st)); TRY(dalloc(&d_mids, c, st));
+        TRY(dalloc(&d_res, c, st));
         // item transform descriptors of each slot (orientation-relative)
         std::vector<RzDesc> rz(c);
         std::vector<MidDesc> md(c);
@@ -681,6 +697,7 @@ struct psb_tray {
             md[o] = MidDesc{d_Ai + (size_t)o * sAi, d_Bi + (size_t)o * sBi, 0, g.H, 0, g.F[1], 0,
                             (long long)g.F[1] * g.H, g.H, g.H, o, 0, nullptr};
         }
+        CK(cudaStreamSynchronize(st));  // stream-ordered allocations complete
         CK(cudaMemcpy(d_rzs, rz.data(), sizeof(RzDesc) * c, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(d_mids, md.data(), sizeof(MidDesc) * c, cudaMemcpyHostToDevice));
         cap = c;
@@ -689,14 +706,14 @@ struct psb_tray {
 
     int ensure_staging(size_t n_items, size_t n_vox) {
         if (n_items > items_cap) {
-            dfree(d_items);
+            dfree(d_items, st);
             items_cap = std::max(n_items, (size_t)1 << 16);
-            TRY(dalloc(&d_items, items_cap));
+            TRY(dalloc(&d_items, items_cap, st));
         }
         if (n_vox > vox_cap) {
-            dfree(d_vox);
+            dfree(d_vox, st);
             vox_cap = std::max(n_vox, (size_t)1 << 14);
-            TRY(dalloc(&d_vox, vox_cap));
+            TRY(dalloc(&d_vox, vox_cap, st));
         }
         return PSB_OK;
     }
@@ -1600,14 +1617,14 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
         totv += t->staged[it].vox.size();
     }
     if (tot > t->stage_cap) {
-        dfree(t->d_stage);
+        dfree(t->d_stage, t->st);
         t->stage_cap = tot;
-        TRY(dalloc(&t->d_stage, tot));
+        TRY(dalloc(&t->d_stage, tot, t->st));
     }
     if (totv > t->stage_vcap) {
-        dfree(t->d_stage_vox);
+        dfree(t->d_stage_vox, t->st);
         t->stage_vcap = totv;
-        TRY(dalloc(&t->d_stage_vox, totv));
+        TRY(dalloc(&t->d_stage_vox, totv, t->st));
     }
     for (int it = 0; it < n_items; ++it) {
         const ItemInfo& inf = t->staged[it];
@@ -1654,14 +1671,14 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
                         t->d_stage + t->staged_off[it], t->d_stage_vox + t->staged_voff[it],
                         &all[(size_t)it * n_orient + o]);
     if (all.size() > t->od_all_cap) {
-        dfree(t->d_od_all);
+        dfree(t->d_od_all, t->st);
         t->od_all_cap = all.size();
-        TRY(dalloc(&t->d_od_all, t->od_all_cap));
+        TRY(dalloc(&t->d_od_all, t->od_all_cap, t->st));
     }
     if ((size_t)n_items > t->dec_cap) {
-        dfree(t->d_dec);
+        dfree(t->d_dec, t->st);
         t->dec_cap = n_items;
-        TRY(dalloc(&t->d_dec, t->dec_cap));
+        TRY(dalloc(&t->d_dec, t->dec_cap, t->st));
     }
     CK(cudaMemcpyAsync(t->d_od_all, all.data(), sizeof(OrientDesc) * all.size(), cudaMemcpyHostToDevice, t->st));
     LoopState ls0;
@@ -1738,6 +1755,53 @@ int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int 
              int n_orient, int interlock, int32_t id_offset, psb_result* out_placements, int32_t* final_tray) {
     TRY(psb_pack_stage(t, items, dims, n_items));
     return psb_pack_staged(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray);
+}
+
+int psb_pack_many(int n_trays, const int32_t* tray_dims, const int32_t* const* items, const int32_t* item_dims,
+                  const int32_t* items_per_tray, const int32_t* orient_maps, int n_orient, int interlock,
+                  int concurrency, psb_result* out_placements, int32_t* const* final_trays) {
+    if (n_trays < 0 || !tray_dims || !items_per_tray || !orient_maps || !out_placements)
+        return fail(PSB_ERR_ARG, "pack_many: null pointer");
+    TRY(ensure_device());
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::vector<size_t> first(n_trays + 1, 0);
+    for (int i = 0; i < n_trays; ++i) {
+        if (items_per_tray[i] < 0) return fail(PSB_ERR_ARG, "pack_many: tray %d has a negative item count", i);
+        first[i + 1] = first[i] + (size_t)items_per_tray[i];
+    }
+    const int workers = std::max(1, std::min(concurrency > 0 ? concurrency : 8, std::max(1, n_trays)));
+    std::atomic<int> next(0);
+    std::vector<int> status(n_trays, PSB_OK);
+    std::vector<std::string> messages(n_trays);
+    auto work = [&]() {
+        cudaSetDevice(dev);
+        for (int i = next.fetch_add(1); i < n_trays; i = next.fetch_add(1)) {
+            const int nx = tray_dims[3 * i], ny = tray_dims[3 * i + 1], nz = tray_dims[3 * i + 2];
+            psb_tray* t = nullptr;
+            int st = psb_tray_create(nx, ny, nz, &t);
+            std::vector<int32_t> empty;
+            if (st == PSB_OK) {
+                empty.assign((size_t)nx * ny * nz, 0);
+                st = psb_tray_set(t, empty.data(), nullptr);
+            }
+            if (st == PSB_OK)
+                st = psb_pack(t, items + first[i], item_dims + 3 * first[i], items_per_tray[i], orient_maps, n_orient,
+                              interlock, 0, out_placements + first[i], final_trays ? final_trays[i] : nullptr);
+            if (st != PSB_OK) {
+                status[i] = st;
+                messages[i] = g_err;
+            }
+            if (t) psb_tray_destroy(t);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; ++w) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    for (int i = 0; i < n_trays; ++i)
+        if (status[i] != PSB_OK) return fail(status[i], "pack_many: tray %d: %s", i, messages[i].c_str());
+    return PSB_OK;
 }
 
 int psb_set_fast_fft(int on) {

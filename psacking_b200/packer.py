@@ -212,6 +212,34 @@ class BinPacker:
                              num_failed=n_items - num_placed, density=density, total_volume=total,
                              bounding_box=bbox, diagnostics=diag)
 
+    def pack_many(self, trays: Sequence[Tuple[Tuple[int, int, int], Sequence[np.ndarray]]],
+                  sort_by_volume: bool = True, concurrency: int = 8) -> List[PackingResult]:
+        """Pack independent trays (each (dims, items), starting empty) with
+        this packer's orientation and interlocking settings.  Equivalent to one
+        BinPacker(dims, ...).pack_voxels(items) per tray; up to `concurrency`
+        trays run at once on separate CUDA streams."""
+        jobs, metas = [], []
+        for dims, items in trays:
+            sub = BinPacker(dims, self.voxel_resolution, self.height_penalty, self.num_orientations,
+                            self.interlocking_free)
+            processed, volumes, order, _, _ = sub._prepare(items, sort_by_volume, None)
+            jobs.append((tuple(int(d) for d in dims), [np.ascontiguousarray(processed[i]) for i in order]))
+            metas.append((sub, volumes, order, len(items)))
+        outs = _core.pack_many(jobs, orientation_maps(self.num_orientations), bool(self.interlocking_free),
+                               int(concurrency))
+        results = []
+        for (sub, volumes, order, n_items), (final, res) in zip(metas, outs):
+            placements = []
+            for k, orig in enumerate(order):
+                pos, found, score, orient = res[k][:4]
+                if found:
+                    placements.append(PlacementInfo(int(orig), tuple(int(v) for v in pos), float(score), True,
+                                                    volumes[orig], int(orient)))
+                else:
+                    placements.append(PlacementInfo(int(orig), None, None, False, volumes[orig], 0))
+            results.append(sub._finish(final, placements, n_items, None))
+        return results
+
     def pack_single(self, item: np.ndarray, tray: Optional[np.ndarray] = None):
         """packer.py:546-580."""
         if tray is None:

@@ -264,3 +264,23 @@ def test_reference_score_expression_is_fused(tmp_path):
     assert rc == 0
     fused = np.array([O.score_block(int(p), int(kk), nz) for p, kk in zip(prox, k)])
     assert np.array_equal(out, fused)
+
+
+# --------------------------------------------------------------------------
+# many independent trays (concurrent streams) == one run per tray
+# --------------------------------------------------------------------------
+def test_pack_many_matches_single_runs(gpu_core):
+    from psacking_b200 import BinPacker, workloads
+    rng = np.random.default_rng(3)
+    trays = []
+    for t in range(5):
+        dims = tuple(int(v) for v in rng.integers(40, 90, 3))
+        trays.append((dims, workloads.config2_items(500 + t, n=int(rng.integers(4, 9)))))
+    for n_orient, inter in [(4, True), (1, False), (24, False)]:
+        p = BinPacker((8, 8, 8), num_orientations=n_orient, interlocking_free=inter)
+        many = p.pack_many(trays, concurrency=3)
+        for (dims, items), r in zip(trays, many):
+            one = BinPacker(dims, num_orientations=n_orient, interlocking_free=inter).pack_voxels(items)
+            assert np.array_equal(r.tray, one.tray)
+            assert [(q.position, q.orientation_index, q.score) for q in r.placements] == \
+                   [(q.position, q.orientation_index, q.score) for q in one.placements]
