@@ -309,6 +309,7 @@ def run_ours(args, rank, world, local_rank):
                 "placements_match_value_leg": e2e_placed == placed},
         "gpu_launches": int(launches // args.steps * args.steps),
         "kernel_share": share, "top_kernel": top,
+        "kernel_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in prof.items()},
         "roofline": roof,
         "clocks": clk,
     }

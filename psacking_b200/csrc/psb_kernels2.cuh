@@ -28,55 +28,112 @@ __device__ __forceinline__ bool okbit(const uint32_t* bits, const ScoreParams& s
     return (bits[((size_t)x * sp.ny + y) * sp.nzw + (z >> 5)] >> (z & 31)) & 1u;
 }
 
-// Candidate collection, one CTA per (x plane, orientation).  Pass 1: the
-// minimum approximate score over the plane's ok cells (free or reachable).
-// Pass 2: every ok cell within the window of that plane minimum becomes a
-// candidate, its approximate score kept in cscore.  The orientation minimum
-// smin is the minimum of the plane minima.  A cell within the window of smin
-// is within the (slightly wider) window of its own plane's minimum, so the
-// list holds every cell the exact guard must see; k_rescore drops the others.
-// Replaces compute_scores_kernel + argmin_reduction_kernel (fft3.cu:147-215,
-// 527-563).  grid: (nx, n_orient)
-__global__ void k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+// ordered encoding of floats for atomicMin on unsigned int
+__device__ __forceinline__ unsigned int ford_key(float v) {
+    unsigned int b = __float_as_uint(v);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ford_val(unsigned int k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+#define PSB_ZWORDS (PSB_MAX_FFT / 32)   // 32-bit words of z per row, at most
+
+// Candidate collection, one CTA per (x plane, orientation), one warp per row
+// y, one lane per z inside each 32-bit word of ok bits.  Pass 1: the minimum
+// approximate score over the plane's ok cells (free or reachable); the score
+// rises with the proximity at fixed z, so it is the minimum over z of the
+// score of the per-z minimum proximity.  Pass 2: every ok cell within the
+// window of that plane minimum becomes a candidate, its approximate score
+// kept in cscore; an FP32 per-z proximity threshold (rounded up, with slack)
+// screens the cells before the double-precision score.  The orientation
+// minimum smin is the minimum of the plane minima.  A cell within the window
+// of smin is within the (slightly wider) window of its own plane's minimum, so
+// the list holds every cell the exact guard must see; k_rescore drops the
+// others.  Replaces compute_scores_kernel + argmin_reduction_kernel
+// (fft3.cu:147-215, 527-563).  grid: (nx, n_orient), 256 threads
+__global__ void __launch_bounds__(256)
+k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
     const int o = blockIdx.y, x = blockIdx.x;
     const OrientDesc& od = orients[o];
     if (od.skip || x >= od.valid[0]) return;
     const int Yv = od.valid[1], Zv = od.valid[2];
-    const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits;
-    const float* Dq = sb.Dq + (size_t)o * sb.sD;
-    double m = 1e300;
-    for (int idx = threadIdx.x; idx < Yv * Zv; idx += blockDim.x) {
-        int y = idx / Zv, z = idx - y * Zv;
-        if (!okbit(bits, sp, x, y, z)) continue;
-        size_t t = ((size_t)x * sp.ny + y) * sp.nz + z;
-        m = fmin(m, ref_score(sp, od.base + (double)Dq[t], z));
-    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int nw = (Zv + 31) >> 5;
+    const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits + (size_t)x * sp.ny * sp.nzw;
+    const float* Dq = sb.Dq + (size_t)o * sb.sD + (size_t)x * sp.ny * sp.nz;
+    const double base = od.base;
+    __shared__ unsigned int zmin[PSB_MAX_FFT];
     __shared__ double red[32];
-    for (int off = 16; off > 0; off >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, off));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double b = red[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmin(b, red[w]);
-        red[0] = b;
-        if (b < 1e299) atomicMin(&sb.smin[o], ord_key(b));
+    for (int z = threadIdx.x; z < Zv; z += blockDim.x) zmin[z] = 0xffffffffu;
+    float m[PSB_ZWORDS];
+#pragma unroll
+    for (int w = 0; w < PSB_ZWORDS; ++w) m[w] = INFINITY;
+    for (int y = warp; y < Yv; y += nwarp) {
+        const uint32_t* brow = bits + (size_t)y * sp.nzw;
+        const float* drow = Dq + (size_t)y * sp.nz;
+#pragma unroll
+        for (int w = 0; w < PSB_ZWORDS; ++w) {
+            if (w < nw) {
+                const int z = w * 32 + lane;
+                if (((brow[w] >> lane) & 1u) && z < Zv) m[w] = fminf(m[w], drow[z]);
+            }
+        }
     }
     __syncthreads();
-    const double pm = red[0];
+#pragma unroll
+    for (int w = 0; w < PSB_ZWORDS; ++w)
+        if (w < nw && m[w] != INFINITY) atomicMin(&zmin[w * 32 + lane], ford_key(m[w]));
+    __syncthreads();
+    double pm = 1e300;
+    for (int z = threadIdx.x; z < Zv; z += blockDim.x)
+        if (zmin[z] != 0xffffffffu) pm = fmin(pm, ref_score(sp, base + (double)ford_val(zmin[z]), z));
+    for (int off = 16; off > 0; off >>= 1) pm = fmin(pm, __shfl_xor_sync(0xffffffffu, pm, off));
+    if (lane == 0) red[warp] = pm;
+    __syncthreads();
+    pm = red[0];
+    for (int w = 1; w < nwarp; ++w) pm = fmin(pm, red[w]);
     if (pm >= 1e299) return;
+    if (threadIdx.x == 0) atomicMin(&sb.smin[o], ord_key(pm));
     const double lim = pm + 2.0 * od.delta + 1e-4 + 8.0 * (fabs(pm) + 1.0) * 2.220446049250313e-16;
+    // score(D) <= lim needs D <= lim - score(0) at that z, up to roundings:
+    // 1.0 of slack, then rounded up to FP32; the exact test follows
+#pragma unroll
+    for (int w = 0; w < PSB_ZWORDS; ++w) {
+        const int z = w * 32 + lane;
+        m[w] = (w < nw && z < Zv) ? __double2float_ru(lim - ref_score(sp, base, z) + 1.0) : -INFINITY;
+    }
     int* cand = sb.cand + (size_t)o * sb.cap;
     double* cs = sb.cscore + (size_t)o * sb.cap;
-    for (int idx = threadIdx.x; idx < Yv * Zv; idx += blockDim.x) {
-        int y = idx / Zv, z = idx - y * Zv;
-        if (!okbit(bits, sp, x, y, z)) continue;
-        size_t t = ((size_t)x * sp.ny + y) * sp.nz + z;
-        double s = ref_score(sp, od.base + (double)Dq[t], z);
-        if (s <= lim) {
-            int slot = atomicAdd(&sb.ncand[o], 1);
-            if (slot < sb.cap) {
-                cand[slot] = (int)t;
-                cs[slot] = s;
+    for (int y = warp; y < Yv; y += nwarp) {
+        const uint32_t* brow = bits + (size_t)y * sp.nzw;
+        const float* drow = Dq + (size_t)y * sp.nz;
+#pragma unroll
+        for (int w = 0; w < PSB_ZWORDS; ++w) {
+            if (w < nw) {
+                const int z = w * 32 + lane;
+                bool take = false;
+                double s = 0.0;
+                if (((brow[w] >> lane) & 1u) && z < Zv) {
+                    const float d = drow[z];
+                    if (d <= m[w]) {
+                        s = ref_score(sp, base + (double)d, z);
+                        take = s <= lim;
+                    }
+                }
+                const unsigned int tk = __ballot_sync(0xffffffffu, take);
+                if (tk) {
+                    int slot0 = 0;
+                    if (lane == 0) slot0 = atomicAdd(&sb.ncand[o], __popc(tk));
+                    slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+                    if (take) {
+                        const int slot = slot0 + __popc(tk & ((1u << lane) - 1u));
+                        if (slot < sb.cap) {
+                            cand[slot] = (int)(((size_t)x * sp.ny + y) * sp.nz + z);
+                            cs[slot] = s;
+                        }
+                    }
+                }
             }
         }
     }

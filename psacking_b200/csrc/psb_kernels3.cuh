@@ -68,11 +68,12 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
 constexpr size_t xpass2_smem(int N) { return sizeof(float2) * ((size_t)N + 2 * (size_t)N * PSB_XCOLS); }
 
 // shared memory of k_plane2: twiddles, work buffer A, the y-inverted plane Q
-// (ny rows) and the plane's free bits
+// (ny rows) and the plane's free mask, one byte per (y, z)
 inline size_t plane2_smem(int NY, int NZ, int ny, int nzw) {
+    (void)nzw;
     const size_t HZ = NZ / 2 + 1;
     const size_t a = std::max((size_t)NY * HZ, (size_t)((ny + 1) / 2) * NZ);
-    return sizeof(float2) * (NY + NZ + a + (size_t)ny * HZ) + sizeof(uint32_t) * (size_t)ny * nzw;
+    return sizeof(float2) * (NY + NZ + a + (size_t)ny * HZ);
 }
 
 // Per (x-plane, orientation): inverse along y then C2R along z (two rows per
@@ -101,16 +102,15 @@ k_plane2(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     float2* A = twz + NZ;
     const size_t asz = max((size_t)NY * HZ, (size_t)((ny + 1) / 2) * NZ);
     float2* Q = A + asz;
-    uint32_t* bits = (uint32_t*)(Q + (size_t)ny * HZ);
+    // free mask of field 0 as bytes [y][z] (NZ per row), over Q: Q is idle from
+    // the first z pass of field 0 until the second y pass of field 1
+    uint8_t* freeb = (uint8_t*)Q;
     load_twiddles(twy, g_twy, NY, tid, nthr);
     load_twiddles(twz, g_twz, NZ, tid, nthr);
-    for (int i = tid; i < Yv * nzw; i += nthr) bits[i] = 0u;
     __syncthreads();
     const float scale = sp.scale;
-    double local_min = 1e300;
     unsigned int diag = 0;
     float* Dq = pb.Dq + (size_t)o * pb.sD;
-    const double base = od.base;
     for (int field = 0; field < 2; ++field) {
         const float2* P = (field == 0 ? sb.Pc : sb.Pd) + (size_t)o * sb.sP + (size_t)x * NY * HZ;
         tpass<NY, RY0, 1, 1, HZ, false>([&](int c, int n) { return P[(size_t)n * HZ + c]; },
@@ -148,34 +148,31 @@ k_plane2(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
                     const float val = (half ? v.y : v.x) * scale;
                     if (field == 0) {
                         const float rv = rintf(val);
-                        if (rv == 0.f) atomicOr(&bits[y * nzw + (z >> 5)], 1u << (z & 31));
+                        freeb[y * NZ + z] = rv == 0.f;  // one writer per (y, z): no atomics
                         if (fabsf(val - rv) > 0.25f) diag |= 2u;
                     } else {
-                        const size_t t = ((size_t)x * ny + y) * sp.nz + z;
-                        Dq[t] = val;
-                        if ((bits[y * nzw + (z >> 5)] >> (z & 31)) & 1u)
-                            local_min = fmin(local_min, ref_score(sp, base + (double)val, z));
+                        Dq[((size_t)x * ny + y) * sp.nz + z] = val;
                     }
                 }
             },
             npairs, twz, tid, nthr);
         __syncthreads();
+        if (field == 0) {
+            // pack the byte mask into the plane's free bits (z < Zv; the rest
+            // zero) before field 1 reuses Q; its first y pass writes only A,
+            // and the barrier after that pass orders these reads first
+            uint32_t* fb = pb.freebits + (size_t)o * pb.sBits + (size_t)x * ny * nzw;
+            for (int i = tid; i < Yv * nzw; i += nthr) {
+                const int y = i / nzw, w = i - y * nzw;
+                uint32_t word = 0u;
+                const int z0 = w * 32, z1 = min(Zv, z0 + 32);
+                for (int z = z0; z < z1; ++z) word |= (uint32_t)freeb[y * NZ + z] << (z - z0);
+                fb[i] = word;
+            }
+        }
     }
-    uint32_t* fb = pb.freebits + (size_t)o * pb.sBits + (size_t)x * ny * nzw;
-    for (int i = tid; i < Yv * nzw; i += nthr) fb[i] = bits[i];
-    __shared__ double red[PSB_PLANE_THREADS / 32];
-    for (int off = 16; off > 0; off >>= 1) local_min = fmin(local_min, __shfl_xor_sync(0xffffffffu, local_min, off));
     unsigned int dg = __reduce_or_sync(0xffffffffu, diag);
-    if ((tid & 31) == 0) {
-        red[tid >> 5] = local_min;
-        if (dg) atomicOr(&pb.diag[o], dg);
-    }
-    __syncthreads();
-    if (tid == 0) {
-        double m = red[0];
-        for (int w = 1; w < nthr / 32; ++w) m = fmin(m, red[w]);
-        if (m < 1e299) atomicMin(&pb.smin[o], ord_key(m));
-    }
+    if ((tid & 31) == 0 && dg) atomicOr(&pb.diag[o], dg);
 }
 
 // ---------------------------------------------------------------------------
