@@ -6,7 +6,7 @@ reference's `spectral_packer._core` functions (spectral_packing/bindings.cpp:
 `BinPacker` mirrors spectral_packer.packer.BinPacker.
 
 The extension is required: importing this package without the built
-libpsb200.so / _core module raises ImportError (run psacking_b200.build).
+libpsb200.so / _core module raises ImportError (run python psacking_b200/build.py).
 """
 from __future__ import annotations
 
@@ -14,7 +14,7 @@ try:
     from . import _core
 except ImportError as e:  # fail loudly: there is no CPU fallback
     raise ImportError(
-        "psacking_b200._core is not built (python -m psacking_b200.build): " + str(e)) from e
+        "psacking_b200._core is not built (python psacking_b200/build.py): " + str(e)) from e
 
 from ._core import (  # noqa: E402
     HEIGHT_PENALTY,

@@ -1,6 +1,6 @@
 """Build the engine in-tree for sm_100a.
 
-    python -m psacking_b200.build          # or __graft_entry__.build()
+    python psacking_b200/build.py          # or __graft_entry__.build()
 
 Produces, next to this file:
   libpsb200.so   the C-ABI library (include/psb200.h), nvcc, sm_100a only
@@ -50,8 +50,7 @@ def _run(cmd):
 
 def build(force: bool = False, verbose: bool = False) -> None:
     nvcc = _nvcc()
-    cu_sources = [CSRC / "psb_engine.cu", CSRC / "psb_kernels.cuh", CSRC / "psb_kernels2.cuh",
-                  CSRC / "psb_fft.cuh", ROOT / "include" / "psb200.h"]
+    cu_sources = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "psb200.h"]
     if force or _stale(LIB, cu_sources):
         cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
                "--expt-relaxed-constexpr",
