@@ -47,6 +47,11 @@ extern "C" {
 #define PSB_DIAG_AMBIGUOUS_COLL  0x2  /* a collision value fell near a rounding boundary      */
 #define PSB_DIAG_FALSE_FREE      0x4  /* exact re-check rejected an FP32 "free" candidate      */
 #define PSB_DIAG_BOUND_EXCEEDED  0x8  /* observed FP32 error exceeded half the error bound     */
+#define PSB_DIAG_CAND_OVERFLOW   0x100 /* tie-guard candidates exceeded the list capacity     */
+#define PSB_DIAG_SKIPPED         0x200 /* orientation larger than the tray, not searched      */
+#define PSB_DIAG_FLOOD_FILL      0x400 /* interlocking search: the winner over the free cells
+                                          had no straight free run to a seed face, so the
+                                          flood fill and a second selection ran             */
 
 typedef struct psb_result {
     int32_t x, y, z;       /* placement of the item array origin, or -1,-1,-1      */
@@ -184,6 +189,11 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
  * the specialised two-pass kernels; off forces the generic mixed-radix path
  * (used by the tests to check both). */
 int psb_set_fast_fft(int on);
+/* Plane-pass kernel for the specialised FFT lengths: 3 (default; warp-owned
+ * line transforms, two block barriers per field) or 2 (every radix pass
+ * spread over the CTA).  Same results; a tuning and comparison switch.
+ * No counterpart in the reference (cuFFT there). */
+int psb_set_plane_variant(int v);
 
 /* Many independent trays (the many-tray form of the benchmark set): tray i
  * has dims tray_dims[3i..3i+2] and items_per_tray[i] items, which follow the
@@ -200,6 +210,9 @@ int psb_pack_many(int n_trays, const int32_t* tray_dims, const int32_t* const* i
  *      as CUDA events around every kernel launch; off by default) ---------- */
 int psb_profile_enable(int on);          /* clears previous records            */
 /* "name launches total_ms" lines, one per kernel, after synchronising. */
+/* Restrict the profiler to the named kernels (comma-separated profiler
+ * names, e.g. "k_plane,k_xpass"); NULL or "" records every kernel. */
+int psb_profile_filter(const char* names);
 int psb_profile_report(char* buf, size_t len);
 /* FFT grid of a tray (F[0..2] >= nx, ny, nz; 2^a 3^b 5^c 7^d). */
 int psb_tray_fft_dims(const psb_tray* t, int* F);

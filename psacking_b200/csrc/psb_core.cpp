@@ -416,7 +416,7 @@ py::list py_pack_many(py::list trays, py::array_t<int32_t> orient_maps, bool int
     return out;
 }
 
-py::dict py_search_detail(py::list orientations, int flags) {
+py::dict py_search_detail(py::list orientations, int flags, bool per_orientation) {
     if (!py_gpu_tray_is_initialized()) throw std::runtime_error("GPU tray context not initialized");
     auto gs = to_grids(orientations);
     std::vector<const int32_t*> ptrs;
@@ -430,15 +430,18 @@ py::dict py_search_detail(py::list orientations, int flags) {
     int st;
     {
         py::gil_scoped_release nogil;
-        st = psb_tray_search(g_ctx, ptrs.data(), dims.data(), (int)gs.size(), flags, &best, per.data());
+        st = psb_tray_search(g_ctx, ptrs.data(), dims.data(), (int)gs.size(), flags, &best,
+                             per_orientation ? per.data() : nullptr);
     }
     check(st);
     py::list pl;
-    for (auto& r : per)
+    if (per_orientation)
+        for (auto& r : per)
         pl.append(py::make_tuple(py::make_tuple(r.x, r.y, r.z), (bool)r.found, r.score, r.diag, r.n_candidates,
                                  r.err_ratio));
     py::dict d;
     d["best"] = py::make_tuple(py::make_tuple(best.x, best.y, best.z), (bool)best.found, best.score, best.orientation);
+    d["best_diag"] = best.diag;
     d["per_orientation"] = pl;
     return d;
 }
@@ -477,12 +480,17 @@ PYBIND11_MODULE(_core, m) {
     // engine extensions (not in the reference module)
     m.def("pack_native", &py_pack_native, py::arg("items"), py::arg("initial_tray"), py::arg("orient_maps"),
           py::arg("interlock"), py::arg("id_offset"));
-    m.def("search_detail", &py_search_detail, py::arg("orientations"), py::arg("flags"));
+    m.def("search_detail", &py_search_detail, py::arg("orientations"), py::arg("flags"),
+          py::arg("per_orientation") = true,
+          "Search the initialised tray.  per_orientation=True: every orientation's own result (interlocking "
+          "searches run the flood fill for all of them); False: only the best (lazy flood fill).");
     m.def("pack_many", &py_pack_many, py::arg("trays"), py::arg("orient_maps"), py::arg("interlock"),
           py::arg("concurrency") = 8);
     m.def("device_count", &py_device_count);
     m.def("set_fast_fft", [](bool on) { psb_set_fast_fft(on ? 1 : 0); }, py::arg("on"),
           "Use the specialised two-pass FFT kernels where a plan exists (default) or force the generic path.");
+    m.def("set_plane_variant", [](int v) { check(psb_set_plane_variant(v)); }, py::arg("variant"),
+          "Plane-pass kernel for the specialised lengths: 3 (warp-owned lines, default) or 2.");
     m.attr("VOXEL_RESOLUTION") = 128;
     m.attr("HEIGHT_PENALTY") = 100000000.0;
     m.attr("__version__") = "0.1.0";

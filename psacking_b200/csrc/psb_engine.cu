@@ -24,6 +24,7 @@
 #include "../../include/psb200.h"
 #include "psb_kernels2.cuh"
 #include "psb_kernels3.cuh"
+#include "psb_kernels4.cuh"
 #include "psb_loop.cuh"
 
 namespace {
@@ -87,6 +88,7 @@ struct ProfRec {
 };
 struct Profiler {
     bool on = false;
+    std::vector<std::string> only;  // when non-empty: record only these kernels
     std::vector<ProfRec> recs;
     std::vector<cudaEvent_t> pool;
     std::mutex mu;
@@ -105,6 +107,9 @@ struct ProfScope {
     ProfScope(const char* name, cudaStream_t s) : st(s) {
         if (!g_prof.on) return;
         std::lock_guard<std::mutex> lk(g_prof.mu);
+        if (!g_prof.only.empty() &&
+            std::find(g_prof.only.begin(), g_prof.only.end(), std::string(name)) == g_prof.only.end())
+            return;
         ProfRec r{name, g_prof.get(), g_prof.get()};
         cudaEventRecord(r.a, st);
         g_prof.recs.push_back(r);
@@ -223,6 +228,27 @@ PlaneFn plane2_for(int ny, int nz) {
 }
 #undef PSB_PLANE_ROW
 
+#define PSB_PLANE3_ROW(NY)                     \
+    case NY:                                   \
+        switch (nz) {                          \
+            case 64: return k_plane3<NY, 64>;   \
+            case 100: return k_plane3<NY, 100>; \
+            case 128: return k_plane3<NY, 128>; \
+            default: return nullptr;           \
+        }
+PlaneFn plane3_for(int ny, int nz) {
+    switch (ny) {
+        PSB_PLANE3_ROW(64)
+        PSB_PLANE3_ROW(100)
+        PSB_PLANE3_ROW(128)
+        default: return nullptr;
+    }
+}
+#undef PSB_PLANE3_ROW
+
+// plane-pass variant: 3 (warp-owned lines, default) or 2 (CTA-wide passes)
+int g_plane_variant = 3;
+
 using FwdPlaneFn = void (*)(FwdSrc, const OrientDesc*, const float2*, const float2*);
 using XfwdFn = void (*)(const float2*, float2*, int, int, const int*, const float2*);
 
@@ -281,6 +307,7 @@ int set_smem_attrs() {
     CK(cudaGetDevice(&dev));
     if (dev < 64 && done[dev]) return PSB_OK;
     CK(cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (const char* e = getenv("PSB_PLANE_VARIANT")) g_plane_variant = atoi(e) == 2 ? 2 : 3;
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
     TRY(set_max_dyn_smem(k_fft_mid<-1>));
@@ -292,6 +319,7 @@ int set_smem_attrs() {
     for (int a : {64, 100, 128})
         for (int b : {64, 100, 128}) {
             TRY(set_max_dyn_smem(plane2_for(a, b)));
+            TRY(set_max_dyn_smem(plane3_for(a, b)));
             TRY(set_max_dyn_smem(fwd_plane_for(a, b)));
         }
     for (int n : {64, 100, 128, 240}) TRY(set_max_dyn_smem(xfwd_for(n)));
@@ -571,7 +599,9 @@ struct psb_tray {
         *d_total = nullptr, *d_blk = nullptr;
     int *d_cand = nullptr, *d_ncand = nullptr;
     double* d_cscore = nullptr;
-    unsigned long long *d_smin = nullptr, *d_smin2 = nullptr, *d_best = nullptr, *d_bestkey = nullptr;
+    unsigned long long *d_smin = nullptr, *d_best = nullptr, *d_bestkey = nullptr;
+    unsigned long long* d_pmin = nullptr;   // per (orientation, x plane) minimum approximate score key
+    int* d_needff = nullptr;                // lazy interlocking search: flood fill needed
     unsigned int* d_diag = nullptr;
     unsigned int* d_errmax = nullptr;
     OrientDesc* d_od = nullptr;
@@ -598,7 +628,7 @@ struct psb_tray {
     void release_slots() {
         dfree(d_Ai, st); dfree(d_Bi, st); dfree(d_Pc, st); dfree(d_Pd, st); dfree(d_Dq, st); dfree(d_free, st); dfree(d_reach, st);
         dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
-        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_smin2, st); dfree(d_best, st);
+        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_best, st);
         dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
@@ -606,7 +636,7 @@ struct psb_tray {
         if (dev >= 0) cudaSetDevice(dev);
         release_slots();
         dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_pen, st);
-        dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st); dfree(d_stage_vox, st);
+        dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st); dfree(d_stage_vox, st);
         dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_dec, st);
         if (st) {
             cudaStreamSynchronize(st);
@@ -630,7 +660,7 @@ struct psb_tray {
         TRY(dalloc(&d_Socc, S, st)); TRY(dalloc(&d_Sphi, S, st));
         TRY(dalloc(&d_w1, (size_t)nx * ny * g.H, st)); TRY(dalloc(&d_w2, (size_t)nx * g.F[1] * g.H, st));
         TRY(dalloc(&d_pen, 3 * (size_t)nz, st)); TRY(dalloc(&d_rz, 4, st)); TRY(dalloc(&d_mid, 4, st)); TRY(dalloc(&d_stats, 4, st));
-        TRY(dalloc(&d_err, 1, st)); TRY(dalloc(&d_first, 1, st));
+        TRY(dalloc(&d_err, 1, st)); TRY(dalloc(&d_first, 1, st)); TRY(dalloc(&d_needff, 1, st));
         TRY(dalloc(&d_ls, 1, st)); TRY(dalloc(&d_ps, 1, st)); TRY(dalloc(&d_rzd, 4, st)); TRY(dalloc(&d_midd, 8, st));
         CK(cudaStreamSynchronize(st));  // stream-ordered allocations complete before plain copies touch them
         CK(cudaMemset(d_err, 0, sizeof(unsigned int)));
@@ -686,7 +716,7 @@ struct psb_tray {
         TRY(dalloc(&d_blk, (size_t)((nx * ny + 255) / 256) * c, st));
         TRY(dalloc(&d_cand, (size_t)kCandCap * c, st)); TRY(dalloc(&d_ncand, c, st));
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c, st));
-        TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_smin2, c, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
+        TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
         TRY(dalloc(&d_diag, c, st)); TRY(dalloc(&d_errmax, c, st)); TRY(dalloc(&d_od, c, st)); TRY(dalloc(&d_rzs, c, st)); TRY(dalloc(&d_mids, c, st));
         TRY(dalloc(&d_res, c, st));
         // item transform descriptors of each slot (orientation-relative)
@@ -865,8 +895,16 @@ struct psb_tray {
     // (device item data already there); each orientation's result goes to
     // d_out[o].  ods is the host copy (dims for the launch shapes).  No host
     // copy or synchronisation happens here.
+    //
+    // Interlocking-free searches run lazily unless every orientation's own
+    // result is wanted (lazy = false): the selection first runs over the free
+    // cells; when the overall winner has a straight free run to a seed face it
+    // is reachable, hence also the winner over the reachable cells, and the
+    // flood fill is skipped (k_line_check).  Otherwise the flood fill and a
+    // second selection over the reachable cells run, gated on the device flag
+    // d_needff, so the host never waits.
     int search_async(const OrientDesc* d_odb, const std::vector<OrientDesc>& ods, int mode, bool interlock,
-                     ResultDev* d_out) {
+                     ResultDev* d_out, bool lazy = true) {
         const int n = (int)ods.size();
         TRY(ensure_slots(n));
         int exmax = 1, maxpairs = 1;
@@ -900,7 +938,6 @@ struct psb_tray {
         CKL();
         SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
         CK(cudaMemsetAsync(d_smin, 0xff, sizeof(unsigned long long) * n, st));
-        CK(cudaMemsetAsync(d_smin2, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_bestkey, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_diag, 0, sizeof(unsigned int) * n, st));
@@ -908,12 +945,25 @@ struct psb_tray {
         CK(cudaMemsetAsync(d_ncand, 0, sizeof(int) * n, st));
         CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
         ScoreParams sp = score_params(mode);
-        PlaneBufs pb{d_free, d_Dq, d_smin, d_diag, sBits, sD};
         XpassFn xf = g_fast_fft ? xpass2_for(g.F[0]) : nullptr;
         if (xf && xpass2_smem(g.F[0]) + 64 > (size_t)g_smem_optin) xf = nullptr;
-        PlaneFn pf = g_fast_fft ? plane2_for(g.F[1], g.F[2]) : nullptr;
-        const size_t sm2 = plane2_smem(g.F[1], g.F[2], ny, nzw) + 64;
-        if (pf && sm2 > (size_t)g_smem_optin) pf = nullptr;
+        PlaneFn pf = nullptr;
+        size_t sm2 = 0;
+        int pthreads = PSB_PLANE_THREADS;
+        bool plane_writes_min = false;  // the plane kernel itself writes the free-cell plane minima
+        if (g_fast_fft && g_plane_variant == 3) {
+            pf = plane3_for(g.F[1], g.F[2]);
+            sm2 = plane3_smem(g.F[1], g.F[2], ny) + 64;
+            pthreads = PSB_PLANE3_THREADS;
+            if (pf && sm2 > (size_t)g_smem_optin) pf = nullptr;
+            plane_writes_min = pf != nullptr;
+        }
+        if (g_fast_fft && !pf) {
+            pf = plane2_for(g.F[1], g.F[2]);
+            sm2 = plane2_smem(g.F[1], g.F[2], ny, nzw) + 64;
+            pthreads = PSB_PLANE_THREADS;
+            if (pf && sm2 > (size_t)g_smem_optin) pf = nullptr;
+        }
         const int wsz = std::max(PSB_TILE * g.F[1], PSB_PAIRS * g.F[2]);
         const size_t smp = sizeof(float2) * ((size_t)g.F[1] + g.F[2] + (size_t)ny * g.H + 2 * (size_t)wsz) +
                            sizeof(uint32_t) * (size_t)ny * nzw;
@@ -925,7 +975,8 @@ struct psb_tray {
         for (int o0 = 0; o0 < n; o0 += sub) {
             const int m = std::min(sub, n - o0);
             SearchBufs sbo{d_Bi + (size_t)o0 * sBi, d_Pc + (size_t)o0 * sP, d_Pd + (size_t)o0 * sP, sBi, sP};
-            PlaneBufs pbo{d_free + (size_t)o0 * sBits, d_Dq + (size_t)o0 * sD, d_smin + o0, d_diag + o0, sBits, sD};
+            PlaneBufs pbo{d_free + (size_t)o0 * sBits, d_Dq + (size_t)o0 * sD, d_smin + o0, d_diag + o0, sBits, sD,
+                          d_pmin + (size_t)o0 * nx, (long long)nx};
             const OrientDesc* odo = d_odb + o0;
             if (xf) {
                 PROF("k_xpass", st);
@@ -941,7 +992,7 @@ struct psb_tray {
             CKL();
             if (pf) {
                 PROF("k_plane", st);
-                pf<<<dim3(nx, m), PSB_PLANE_THREADS, sm2, st>>>(odo, sbo, pbo, sp, g.p[1].tw, g.p[2].tw);
+                pf<<<dim3(nx, m), pthreads, sm2, st>>>(odo, sbo, pbo, sp, g.p[1].tw, g.p[2].tw);
             } else {
                 PROF("k_plane", st);
                 k_plane<<<dim3(nx, m), PSB_THREADS, smp, st>>>(odo, sbo, pbo, sp, g.F[1], g.F[2], g.p[1].p,
@@ -949,9 +1000,35 @@ struct psb_tray {
             }
             CKL();
         }
-        const uint32_t* ok = d_free;
-        if (interlock) {
-            FloodBufs fb{d_free, d_reach, sBits, d_cnt, d_off, sLine, d_rz2, d_rline, d_par, d_rflag, sRun, d_total, d_err};
+        auto select = [&](const uint32_t* ok, const int* gate) -> int {
+            SelectBufs sel{ok,      sBits,   d_Dq,   sD,    d_smin, d_cand, d_ncand,          d_cscore, d_best,
+                           d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate};
+            {
+                PROF("k_collect", st);
+                k_collect_plane<<<dim3(nx, n), 256, 0, st>>>(d_odb, sel, sp);
+            }
+            CKL();
+            {
+                PROF("k_rescore", st);
+                k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_tray, d_phi);
+            }
+            CKL();
+            {
+                PROF("k_tiebreak", st);
+                k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp);
+            }
+            CKL();
+            {
+                PROF("k_finalize", st);
+                k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_odb, sel, sp, d_out, n);
+            }
+            CKL();
+            return PSB_OK;
+        };
+        // flood fill over the free bits, then a selection over the reachable cells
+        auto reach_select = [&](const int* gate) -> int {
+            FloodBufs fb{d_free, d_reach, sBits, d_cnt,  d_off, sLine, d_rz2,
+                         d_rline, d_par, d_rflag, sRun, d_total, d_err, gate};
             int lines = nx * ny;
             const int nblk = (lines + 255) / 256;
             dim3 gl(nblk, n);
@@ -985,38 +1062,49 @@ struct psb_tray {
                 k_ff_reach<<<gl, 256, 0, st>>>(d_odb, fb, sp);
             }
             CKL();
-            ok = d_reach;
+            SelectBufs sel{d_reach,   sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
+                           d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate};
+            k_sel_reset<<<1, 128, 0, st>>>(sel, n);
+            CKL();
+            {
+                PROF("k_plane_min", st);
+                k_plane_min<<<dim3(nx, n), PSB_PMIN_THREADS, 0, st>>>(d_odb, sel, sp);
+            }
+            CKL();
+            return select(d_reach, gate);
+        };
+        // plane minima over the free cells (k_plane3 and the generic k_plane
+        // write them themselves)
+        if (pf && !plane_writes_min && (!interlock || lazy)) {
+            SelectBufs sel{d_free,    sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
+                           d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, nullptr};
+            PROF("k_plane_min", st);
+            k_plane_min<<<dim3(nx, n), PSB_PMIN_THREADS, 0, st>>>(d_odb, sel, sp);
+            CKL();
         }
-        SelectBufs sel{ok, sBits, d_Dq, sD, d_smin2, d_cand, d_ncand, d_cscore, d_best, d_bestkey, d_diag, d_errmax, kCandCap};
-        {
-            PROF("k_collect", st);
-            k_collect_plane<<<dim3(nx, n), 256, 0, st>>>(d_odb, sel, sp);
+        if (!interlock) {
+            TRY(select(d_free, nullptr));
+        } else if (!lazy) {
+            TRY(reach_select(nullptr));
+        } else {
+            TRY(select(d_free, nullptr));
+            {
+                PROF("k_line_check", st);
+                k_line_check<<<1, 192, 0, st>>>(d_odb, d_out, n, d_free, sBits, sp, d_needff);
+            }
+            CKL();
+            TRY(reach_select(d_needff));
         }
-        CKL();
-        {
-            PROF("k_rescore", st);
-            k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_tray, d_phi);
-        }
-        CKL();
-        {
-            PROF("k_tiebreak", st);
-            k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp);
-        }
-        CKL();
-        {
-            PROF("k_finalize", st);
-            k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_odb, sel, sp, d_out, n);
-        }
-        CKL();
         return PSB_OK;
     }
 
     // Synchronous search (the drop-in entry points): upload, queue, wait, check.
-    int search(const std::vector<OrientDesc>& ods, int mode, bool interlock, std::vector<ResultDev>* res) {
+    int search(const std::vector<OrientDesc>& ods, int mode, bool interlock, std::vector<ResultDev>* res,
+               bool lazy = true) {
         const int n = (int)ods.size();
         TRY(ensure_slots(n));
         CK(cudaMemcpyAsync(d_od, ods.data(), sizeof(OrientDesc) * n, cudaMemcpyHostToDevice, st));
-        TRY(search_async(d_od, ods, mode, interlock, d_res));
+        TRY(search_async(d_od, ods, mode, interlock, d_res, lazy));
         res->resize(n);
         unsigned int herr = 0;
         CK(cudaMemcpyAsync(res->data(), d_res, sizeof(ResultDev) * n, cudaMemcpyDeviceToHost, st));
@@ -1404,7 +1492,7 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
     CK(cudaMemsetAsync(t->d_err, 0, sizeof(unsigned int), t->st));
     ScoreParams sp = t->score_params(1);
     FloodBufs fb{t->d_free, t->d_reach, t->sBits, t->d_cnt, t->d_off, t->sLine, t->d_rz2, t->d_rline, t->d_par,
-                 t->d_rflag, t->sRun, t->d_total, t->d_err};
+                 t->d_rflag, t->sRun, t->d_total, t->d_err, nullptr};
     int lines = nx * ny;
     const int nblk = (lines + 255) / 256;
     dim3 gl(nblk, 1);
@@ -1574,7 +1662,8 @@ int psb_tray_search(psb_tray* t, const int32_t* const* items, const int32_t* dim
     TRY(stage_arrays(t, items, dims, n, &ods));
     std::vector<ResultDev> res;
     int mode = mode_flags & 0xf;
-    TRY(t->search(ods, mode, (mode_flags & PSB_FLAG_INTERLOCK) != 0, &res));
+    // every orientation's own result is exact only without the lazy flood fill
+    TRY(t->search(ods, mode, (mode_flags & PSB_FLAG_INTERLOCK) != 0, &res, per_orient == nullptr));
     double best = 1e300;
     for (int o = 0; o < n; ++o) {
         psb_result r;
@@ -1809,11 +1898,34 @@ int psb_set_fast_fft(int on) {
     return PSB_OK;
 }
 
+int psb_set_plane_variant(int v) {
+    if (v != 2 && v != 3) return fail(PSB_ERR_ARG, "plane variant must be 2 or 3");
+    g_plane_variant = v;
+    return PSB_OK;
+}
+
 int psb_profile_enable(int on) {
     std::lock_guard<std::mutex> lk(g_prof.mu);
     for (auto& r : g_prof.recs) { g_prof.pool.push_back(r.a); g_prof.pool.push_back(r.b); }
     g_prof.recs.clear();
     g_prof.on = on != 0;
+    return PSB_OK;
+}
+
+int psb_profile_filter(const char* names) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    g_prof.only.clear();
+    if (!names) return PSB_OK;
+    std::string cur;
+    for (const char* c = names;; ++c) {
+        if (*c == ',' || *c == 0) {
+            if (!cur.empty()) g_prof.only.push_back(cur);
+            cur.clear();
+            if (*c == 0) break;
+        } else {
+            cur += *c;
+        }
+    }
     return PSB_OK;
 }
 

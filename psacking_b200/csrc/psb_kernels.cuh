@@ -353,6 +353,8 @@ struct PlaneBufs {
     unsigned long long* smin; // per orientation approx min score key
     unsigned int* diag;       // per orientation diag bits
     long long sBits, sD;
+    unsigned long long* pmin; // per (orientation, x plane) approx min score key over free cells
+    long long pstride;        // pmin stride per orientation
 };
 
 // Per (x-plane, orientation): inverse along y, C2R along z for the collision
@@ -469,6 +471,7 @@ k_plane(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sco
     if (tid == 0) {
         double m = red[0];
         for (int w = 1; w < nthr / 32; ++w) m = fmin(m, red[w]);
+        pb.pmin[(size_t)o * pb.pstride + x] = m < 1e299 ? ord_key(m) : 0xffffffffffffffffULL;
         if (m < 1e299) atomicMin(&pb.smin[o], ord_key(m));
     }
 }

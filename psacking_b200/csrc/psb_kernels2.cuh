@@ -22,6 +22,9 @@ struct SelectBufs {
     unsigned int* diag;
     unsigned int* errmax;          // max |D~ - D| / delta seen by the exact re-check (float bits)
     int cap;
+    unsigned long long* pmin;      // per (orientation, x plane) approx min key, stride pstride
+    long long pstride;
+    const int* gate;               // when set, the kernels run only if *gate != 0
 };
 
 __device__ __forceinline__ bool okbit(const uint32_t* bits, const ScoreParams& sp, int x, int y, int z) {
@@ -39,65 +42,109 @@ __device__ __forceinline__ float ford_val(unsigned int k) {
 
 #define PSB_ZWORDS (PSB_MAX_FFT / 32)   // 32-bit words of z per row, at most
 
-// Candidate collection, one CTA per (x plane, orientation), one warp per row
-// y, one lane per z inside each 32-bit word of ok bits.  Pass 1: the minimum
-// approximate score over the plane's ok cells (free or reachable); the score
-// rises with the proximity at fixed z, so it is the minimum over z of the
-// score of the per-z minimum proximity.  Pass 2: every ok cell within the
-// window of that plane minimum becomes a candidate, its approximate score
-// kept in cscore; an FP32 per-z proximity threshold (rounded up, with slack)
-// screens the cells before the double-precision score.  The orientation
-// minimum smin is the minimum of the plane minima.  A cell within the window
-// of smin is within the (slightly wider) window of its own plane's minimum, so
-// the list holds every cell the exact guard must see; k_rescore drops the
-// others.  Replaces compute_scores_kernel + argmin_reduction_kernel
-// (fft3.cu:147-215, 527-563).  grid: (nx, n_orient), 256 threads
-__global__ void __launch_bounds__(256)
-k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+// The reference scores every cell and reduces them (compute_scores_kernel +
+// argmin_reduction_kernel, fft3.cu:147-215, 527-563).  Here the minimum is
+// found in two steps.  (1) Per (x plane, orientation) the minimum approximate
+// score over the plane's ok cells (free or reachable) goes to pmin[o][x] and,
+// by atomicMin, to the orientation minimum smin[o]: the score rises with the
+// proximity at fixed z, so the plane minimum is the minimum over z of the
+// score of the per-z minimum proximity.  k_plane2 / k_plane produce these for
+// the free cells while they write the field; k_plane_min produces them for
+// another mask (the reachable cells).  (2) k_collect_plane keeps every ok cell
+// whose approximate score lies within the window smin + 2 delta of the
+// orientation minimum (planes whose minimum is above the window are skipped
+// without reading them); k_rescore scores those candidates exactly.
+
+// (1) for an arbitrary ok mask.  One CTA per (x plane, orientation): thread
+// (g, l) owns z = l (+128, ...) and walks rows y = g, g + 4, ... (4 row
+// groups), so loads are coalesced along z, independent across rows and no
+// atomics are needed; the row groups meet in shared memory.
+// grid: (nx, n_orient), block PSB_PMIN_THREADS
+#define PSB_PMIN_ZL 128
+#define PSB_PMIN_RG 4
+#define PSB_PMIN_THREADS (PSB_PMIN_ZL * PSB_PMIN_RG)
+__global__ void __launch_bounds__(PSB_PMIN_THREADS)
+k_plane_min(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.y, x = blockIdx.x;
     const OrientDesc& od = orients[o];
     if (od.skip || x >= od.valid[0]) return;
     const int Yv = od.valid[1], Zv = od.valid[2];
+    if (Yv <= 0 || Zv <= 0) return;
+    const int l = threadIdx.x % PSB_PMIN_ZL, g = threadIdx.x / PSB_PMIN_ZL;
+    const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits + (size_t)x * sp.ny * sp.nzw;
+    const float* Dq = sb.Dq + (size_t)o * sb.sD + (size_t)x * sp.ny * sp.nz;
+    __shared__ unsigned int part[PSB_PMIN_RG][PSB_PMIN_ZL];
+    __shared__ double red[PSB_PMIN_THREADS / 32];
+    double pm = 1e300;
+    for (int z0 = 0; z0 < Zv; z0 += PSB_PMIN_ZL) {
+        const int z = z0 + l;
+        unsigned int mk = 0xffffffffu;
+        if (z < Zv) {
+            const int wz = z >> 5, bz = z & 31;
+            int y = g;
+#pragma unroll 1
+            for (; y + 3 * PSB_PMIN_RG < Yv; y += 4 * PSB_PMIN_RG) {
+                uint32_t b[4];
+                float d[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int yy = y + u * PSB_PMIN_RG;
+                    b[u] = __ldg(&bits[(size_t)yy * sp.nzw + wz]);
+                    d[u] = __ldg(&Dq[(size_t)yy * sp.nz + z]);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if ((b[u] >> bz) & 1u) mk = min(mk, ford_key(d[u]));
+            }
+            for (; y < Yv; y += PSB_PMIN_RG)
+                if ((__ldg(&bits[(size_t)y * sp.nzw + wz]) >> bz) & 1u)
+                    mk = min(mk, ford_key(__ldg(&Dq[(size_t)y * sp.nz + z])));
+        }
+        part[g][l] = mk;
+        __syncthreads();
+        if (g == 0 && z < Zv) {
+#pragma unroll
+            for (int r = 1; r < PSB_PMIN_RG; ++r) mk = min(mk, part[r][l]);
+            if (mk != 0xffffffffu) pm = fmin(pm, ref_score(sp, od.base + (double)ford_val(mk), z));
+        }
+        __syncthreads();
+    }
+    for (int off = 16; off > 0; off >>= 1) pm = fmin(pm, __shfl_xor_sync(0xffffffffu, pm, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < PSB_PMIN_THREADS / 32; ++w) pm = fmin(pm, red[w]);
+        sb.pmin[(size_t)o * sb.pstride + x] = pm < 1e299 ? ord_key(pm) : 0xffffffffffffffffULL;
+        if (pm < 1e299) atomicMin(&sb.smin[o], ord_key(pm));
+    }
+}
+
+// (2) candidate collection, one CTA per (x plane, orientation), one warp per
+// row y.  An FP32 per-z proximity threshold (rounded up, with slack) screens
+// the cells before the double-precision score.  grid: (nx, n_orient)
+__global__ void __launch_bounds__(256)
+k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    if (sb.gate && !*sb.gate) return;
+    const int o = blockIdx.y, x = blockIdx.x;
+    const OrientDesc& od = orients[o];
+    if (od.skip || x >= od.valid[0]) return;
+    const int Yv = od.valid[1], Zv = od.valid[2];
+    if (Yv <= 0 || Zv <= 0) return;
+    const unsigned long long gk = sb.smin[o];
+    if (gk == 0xffffffffffffffffULL) return;  // no ok cell in any plane
+    const double pm = ord_val(gk);
+    const double lim = pm + 2.0 * od.delta + 1e-4 + 8.0 * (fabs(pm) + 1.0) * 2.220446049250313e-16;
+    const unsigned long long pk = sb.pmin[(size_t)o * sb.pstride + x];
+    if (pk == 0xffffffffffffffffULL || ord_val(pk) > lim) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int nw = (Zv + 31) >> 5;
     const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits + (size_t)x * sp.ny * sp.nzw;
     const float* Dq = sb.Dq + (size_t)o * sb.sD + (size_t)x * sp.ny * sp.nz;
     const double base = od.base;
-    __shared__ unsigned int zmin[PSB_MAX_FFT];
-    __shared__ double red[32];
-    for (int z = threadIdx.x; z < Zv; z += blockDim.x) zmin[z] = 0xffffffffu;
-    float m[PSB_ZWORDS];
-#pragma unroll
-    for (int w = 0; w < PSB_ZWORDS; ++w) m[w] = INFINITY;
-    for (int y = warp; y < Yv; y += nwarp) {
-        const uint32_t* brow = bits + (size_t)y * sp.nzw;
-        const float* drow = Dq + (size_t)y * sp.nz;
-#pragma unroll
-        for (int w = 0; w < PSB_ZWORDS; ++w) {
-            if (w < nw) {
-                const int z = w * 32 + lane;
-                if (((brow[w] >> lane) & 1u) && z < Zv) m[w] = fminf(m[w], drow[z]);
-            }
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int w = 0; w < PSB_ZWORDS; ++w)
-        if (w < nw && m[w] != INFINITY) atomicMin(&zmin[w * 32 + lane], ford_key(m[w]));
-    __syncthreads();
-    double pm = 1e300;
-    for (int z = threadIdx.x; z < Zv; z += blockDim.x)
-        if (zmin[z] != 0xffffffffu) pm = fmin(pm, ref_score(sp, base + (double)ford_val(zmin[z]), z));
-    for (int off = 16; off > 0; off >>= 1) pm = fmin(pm, __shfl_xor_sync(0xffffffffu, pm, off));
-    if (lane == 0) red[warp] = pm;
-    __syncthreads();
-    pm = red[0];
-    for (int w = 1; w < nwarp; ++w) pm = fmin(pm, red[w]);
-    if (pm >= 1e299) return;
-    if (threadIdx.x == 0) atomicMin(&sb.smin[o], ord_key(pm));
-    const double lim = pm + 2.0 * od.delta + 1e-4 + 8.0 * (fabs(pm) + 1.0) * 2.220446049250313e-16;
     // score(D) <= lim needs D <= lim - score(0) at that z, up to roundings:
     // 1.0 of slack, then rounded up to FP32; the exact test follows
+    float m[PSB_ZWORDS];
 #pragma unroll
     for (int w = 0; w < PSB_ZWORDS; ++w) {
         const int z = w * 32 + lane;
@@ -139,6 +186,18 @@ k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScorePara
     }
 }
 
+// per-orientation selection state back to "nothing seen" (the gated second
+// round of the lazy interlocking search)
+__global__ void k_sel_reset(SelectBufs sb, int n) {
+    if (sb.gate && !*sb.gate) return;
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x) {
+        sb.smin[o] = 0xffffffffffffffffULL;
+        sb.best[o] = 0xffffffffffffffffULL;
+        sb.bestkey[o] = 0xffffffffffffffffULL;
+        sb.ncand[o] = 0;
+    }
+}
+
 // exact score of every candidate.  Regime (a): the FP32 value rounds to the
 // exact integer.  Regime (b): direct integer sums over the item's voxels
 // (proximity and collision), the FP64 guard.  One warp per candidate.
@@ -146,6 +205,7 @@ k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScorePara
 __global__ void __launch_bounds__(256)
 k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ tray,
           const int32_t* __restrict__ phi) {
+    if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
@@ -222,6 +282,7 @@ __device__ __forceinline__ int untie_key(int mode, unsigned int key) {
 }
 
 __global__ void k_tiebreak(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.y;
     if (orients[o].skip) return;
     const int n = min(sb.ncand[o], sb.cap);
@@ -244,6 +305,7 @@ struct ResultDev {
 
 __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, ResultDev* out,
                            int n) {
+    if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
     ResultDev r;
@@ -255,6 +317,7 @@ __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb
     r.pad = 0;
     r.diag = sb.diag[o] | (orients[o].exact ? 1u : 0u);
     if (sb.ncand[o] > sb.cap) r.diag |= 0x100u;
+    if (sb.gate) r.diag |= 0x400u;  // the gated second selection (lazy flood fill) ran
     if (!orients[o].skip && sb.best[o] != 0xffffffffffffffffULL) {
         double s = ord_val(sb.best[o]);
         double cut = sp.mode == 0 ? 1000000000.0 : 1e29;
@@ -268,6 +331,83 @@ __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb
         }
     }
     out[o] = r;
+}
+
+// Index of the best found result (smallest score; on equal scores the lowest
+// index, i.e. strict < in index order: fft3.cu:1625, packer.py:500), or -1.
+// Called by one full warp; every lane returns the answer.
+__device__ __forceinline__ int best_result(const OrientDesc* __restrict__ orients, const ResultDev* __restrict__ res,
+                                           int n) {
+    const int lane = threadIdx.x & 31;
+    double bs = 1e300;
+    int bo = -1;
+    for (int o = lane; o < n; o += 32) {
+        if (orients[o].skip || !res[o].found) continue;
+        const double sc = res[o].score;
+        if (sc < bs) {  // o grows along a lane: strict < keeps the first
+            bs = sc;
+            bo = o;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const double os = __shfl_xor_sync(0xffffffffu, bs, off);
+        const int oo = __shfl_xor_sync(0xffffffffu, bo, off);
+        if (oo >= 0 && (bo < 0 || os < bs || (os == bs && oo < bo))) {
+            bs = os;
+            bo = oo;
+        }
+    }
+    return bo;
+}
+
+// Lazy interlocking search.  The best cell over the FREE cells of all
+// orientations (strict < over orientations, the first minimum wins) is also
+// the best over the REACHABLE cells when it is itself reachable, because the
+// reachable cells are a subset of the free ones.  A straight run of free
+// cells from it to a seed face (i = 0, j = 0, k = 0 always; the far faces
+// i = Xv-1, j = Yv-1, k = Zv-1 when the item is non-empty, as k_ff_emit seeds
+// them; fft3.cu:263-293) proves it reachable without the flood fill.
+// need_ff = 0: proven (or nothing is free: then nothing is reachable either);
+// need_ff = 1: the flood fill and a second selection must run.
+// grid: 1, block 192 (one warp per ray)
+__global__ void k_line_check(const OrientDesc* __restrict__ orients, const ResultDev* __restrict__ res, int n,
+                             const uint32_t* __restrict__ freebits, long long sBits, ScoreParams sp, int* need_ff) {
+    __shared__ int s_best, s_clear;
+    if (threadIdx.x < 32) {
+        const int best = best_result(orients, res, n);
+        if (threadIdx.x == 0) {
+            s_best = best;
+            s_clear = 0;
+        }
+    }
+    __syncthreads();
+    const int o = s_best;
+    if (o < 0) {
+        if (threadIdx.x == 0) *need_ff = 0;
+        return;
+    }
+    const OrientDesc& od = orients[o];
+    const int t[3] = {res[o].x, res[o].y, res[o].z};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < 6) {
+        const int a = warp >> 1, dir = (warp & 1) ? 1 : -1;
+        const bool usable = dir < 0 || od.hi[a] >= 0;
+        const int len = dir < 0 ? t[a] : od.valid[a] - 1 - t[a];  // cells between t and the face
+        bool blocked = !usable || len < 0;
+        if (!blocked) {
+            for (int s = 1 + lane; s <= len; s += 32) {
+                int c[3] = {t[0], t[1], t[2]};
+                c[a] += dir * s;
+                const uint32_t w =
+                    freebits[(size_t)o * sBits + ((size_t)c[0] * sp.ny + c[1]) * sp.nzw + (c[2] >> 5)];
+                if (!((w >> (c[2] & 31)) & 1u)) blocked = true;
+            }
+        }
+        blocked = __any_sync(0xffffffffu, blocked);
+        if (!blocked && lane == 0) atomicOr(&s_clear, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *need_ff = s_clear ? 0 : 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -287,6 +427,7 @@ struct FloodBufs {
     long long sRun;
     int* total;                    // runs per orientation
     unsigned int* err;             // device error word (limit hit)
+    const int* gate;               // when set, the kernels run only if *gate != 0
 };
 
 __device__ __forceinline__ int run_find(int* parent, int x, unsigned int* err) {
@@ -327,6 +468,7 @@ __device__ __forceinline__ uint32_t run_starts(const uint32_t* w, int i, uint32_
 // (blk[o][b]).  grid: (ceil(nx*ny/256), n_orient), block 256
 __global__ void __launch_bounds__(256)
 k_ff_count(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, int* __restrict__ blk, int nblk) {
+    if (fb.gate && !*fb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     const int line = blockIdx.x * blockDim.x + threadIdx.x;
@@ -357,6 +499,7 @@ k_ff_count(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp,
 // Exclusive scan of the block totals of one orientation (one warp per
 // orientation); total runs in fb.total.  grid: (n_orient), block 32
 __global__ void k_ff_scan(const OrientDesc* __restrict__ orients, FloodBufs fb, int* __restrict__ blk, int nblk) {
+    if (fb.gate && !*fb.gate) return;
     const int o = blockIdx.x;
     if (orients[o].skip) return;
     int* b = blk + (size_t)o * nblk;
@@ -381,6 +524,7 @@ __global__ void k_ff_scan(const OrientDesc* __restrict__ orients, FloodBufs fb, 
 // grid: (ceil(nx*ny/256), n_orient), block 256
 __global__ void __launch_bounds__(256)
 k_ff_emit(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, const int* __restrict__ blk, int nblk) {
+    if (fb.gate && !*fb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
@@ -439,6 +583,7 @@ k_ff_emit(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, 
 
 // grid: (ceil(nx*ny/256), n_orient)
 __global__ void k_ff_union(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    if (fb.gate && !*fb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
@@ -469,6 +614,7 @@ __global__ void k_ff_union(const OrientDesc* __restrict__ orients, FloodBufs fb,
 
 // grid: (ceil(maxruns/256), n_orient)
 __global__ void k_ff_seed(const OrientDesc* __restrict__ orients, FloodBufs fb) {
+    if (fb.gate && !*fb.gate) return;
     const int o = blockIdx.y;
     if (orients[o].skip) return;
     const int n = fb.total[o];
@@ -484,6 +630,7 @@ __global__ void k_ff_seed(const OrientDesc* __restrict__ orients, FloodBufs fb) 
 
 // grid: (ceil(nx*ny/256), n_orient)
 __global__ void k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    if (fb.gate && !*fb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;

@@ -4,7 +4,7 @@
 // the path for other lengths.
 #pragma once
 #include "psb_fft2.cuh"
-#include "psb_kernels.cuh"
+#include "psb_kernels2.cuh"
 
 #define PSB_XCOLS 16   // spectrum columns (ky*Hz + kz) per CTA in k_xpass2
 
@@ -67,8 +67,9 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
 
 constexpr size_t xpass2_smem(int N) { return sizeof(float2) * ((size_t)N + 2 * (size_t)N * PSB_XCOLS); }
 
-// shared memory of k_plane2: twiddles, work buffer A, the y-inverted plane Q
-// (ny rows) and the plane's free mask, one byte per (y, z)
+// shared memory of k_plane2: twiddles, work buffer A and the y-inverted plane
+// Q (ny rows; it also holds the plane's free mask as one byte per (y, z)
+// while Q is idle)
 inline size_t plane2_smem(int NY, int NZ, int ny, int nzw) {
     (void)nzw;
     const size_t HZ = NZ / 2 + 1;

@@ -57,27 +57,25 @@ struct DecisionDev {
     float err_ratio;
 };
 
-// best over orientations (strict <: the first minimum wins), one thread
+// best over orientations (strict <: the first minimum wins), one warp
 __global__ void k_decide(const OrientDesc* __restrict__ od, const ResultDev* __restrict__ res, int n,
                          LoopState* ls, DecisionDev* out, const unsigned int* uf_err) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int best = -1;
-    double bs = 1e300;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const int best = best_result(od, res, n);
     unsigned int diag = 0;
     int ncand = 0;
     float er = 0.f;
-    for (int o = 0; o < n; ++o) {
-        const ResultDev r = res[o];
+    for (int o = threadIdx.x; o < n; o += 32) {
+        const ResultDev& r = res[o];
         diag |= r.diag;
         ncand += r.ncand;
         er = fmaxf(er, r.err_ratio);
-        if (r.diag & 0x100u) ls->err |= 2u;
-        if (od[o].skip) continue;
-        if (r.found && r.score < bs) {
-            bs = r.score;
-            best = o;
-        }
     }
+    diag = __reduce_or_sync(0xffffffffu, diag);
+    ncand = __reduce_add_sync(0xffffffffu, ncand);
+    for (int off = 16; off > 0; off >>= 1) er = fmaxf(er, __shfl_xor_sync(0xffffffffu, er, off));
+    if (threadIdx.x != 0) return;
+    if (diag & 0x100u) ls->err |= 2u;
     if (*uf_err) ls->err |= 1u;
     DecisionDev d;
     d.diag = diag;

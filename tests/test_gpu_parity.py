@@ -131,11 +131,56 @@ def test_search_empty_and_full(gpu_core):
     check_search(gpu_core, tray, [big, it], BLOCK)
 
 
-@pytest.fixture(params=["fast", "generic"])
+DIAG_FLOOD_FILL = 0x400
+
+
+def caged_tray(hole):
+    """A sealed box (walls of id 2, thickness 2) whose cavity holds the only
+    distance source (a voxel equal to 1): the best free cell for a 5^3 item is
+    inside the cavity.  hole: None (sealed), "offset" (a roof opening away
+    from the source: reachable only by a bent path) or "above" (an opening
+    straight above the best cell)."""
+    tray = np.zeros((40, 40, 100), np.int32)
+    tray[4:24, 4:24, 0:16] = 2
+    tray[6:22, 6:22, 1:14] = 0
+    tray[14, 14, 1] = 1
+    if hole == "offset":
+        tray[16:22, 16:22, 14:16] = 0
+    elif hole == "above":
+        tray[6:22, 6:22, 14:16] = 0
+    return tray
+
+
+@pytest.mark.parametrize("hole", [None, "offset", "above"])
+def test_lazy_interlock_search(gpu_core, hole):
+    """The interlocking search runs the flood fill only when the best free
+    cell has no straight free run to a seed face; the answer is the oracle's
+    either way (sealed cavity: the winner moves outside; bent path: it stays
+    inside; straight path: no flood fill)."""
+    tray = caged_tray(hole)
+    phi = O.calculate_distance(tray)
+    item = np.ones((5, 5, 5), np.int32)
+    ors = [item, np.ones((3, 5, 7), np.int32)]
+    want = O.fft_search_batch(ors, tray, phi, interlock=True)
+    gpu_core.gpu_tray_init(tray, phi)
+    d = gpu_core.search_detail(ors, BLOCK | INTERLOCK, per_orientation=False)
+    pos, found, score, bo = d["best"]
+    assert (tuple(pos), found, score, bo) == (tuple(want[0]), want[1], want[2], want[3])
+    ran = bool(d["best_diag"] & DIAG_FLOOD_FILL)
+    assert ran == (hole != "above"), hex(d["best_diag"])
+    inside = 6 <= pos[0] < 22 and 6 <= pos[1] < 22 and 1 <= pos[2] < 14
+    assert inside == (hole is not None)
+    got = gpu_core.fft_search_batch_interlocking_free(ors, tray, phi, 1)
+    assert (tuple(got[0]), got[1], got[2], got[3]) == (tuple(want[0]), want[1], want[2], want[3])
+
+
+@pytest.fixture(params=["fast", "plane2", "generic"])
 def fft_variant(request, gpu_core):
-    gpu_core.set_fast_fft(request.param == "fast")
+    gpu_core.set_fast_fft(request.param != "generic")
+    gpu_core.set_plane_variant(2 if request.param == "plane2" else 3)
     yield request.param
     gpu_core.set_fast_fft(True)
+    gpu_core.set_plane_variant(3)
 
 
 def test_search_config3_scale(gpu_core, fft_variant):
