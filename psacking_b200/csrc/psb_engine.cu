@@ -228,15 +228,15 @@ PlaneFn plane2_for(int ny, int nz) {
 }
 #undef PSB_PLANE_ROW
 
-#define PSB_PLANE3_ROW(NY)                     \
-    case NY:                                   \
-        switch (nz) {                          \
-            case 64: return k_plane3<NY, 64>;   \
-            case 100: return k_plane3<NY, 100>; \
-            case 128: return k_plane3<NY, 128>; \
-            default: return nullptr;           \
+#define PSB_PLANE3_ROW(NY)                                                                \
+    case NY:                                                                              \
+        switch (nz) {                                                                     \
+            case 64: return field ? k_plane3<NY, 64, 1> : k_plane3<NY, 64, 0>;             \
+            case 100: return field ? k_plane3<NY, 100, 1> : k_plane3<NY, 100, 0>;          \
+            case 128: return field ? k_plane3<NY, 128, 1> : k_plane3<NY, 128, 0>;          \
+            default: return nullptr;                                                      \
         }
-PlaneFn plane3_for(int ny, int nz) {
+PlaneFn plane3_for(int ny, int nz, int field) {
     switch (ny) {
         PSB_PLANE3_ROW(64)
         PSB_PLANE3_ROW(100)
@@ -246,7 +246,9 @@ PlaneFn plane3_for(int ny, int nz) {
 }
 #undef PSB_PLANE3_ROW
 
-// plane-pass variant: 3 (warp-owned lines, default) or 2 (CTA-wide passes)
+// plane-pass variant: 3 (warp-owned lines, collision and proximity in two
+// launches with the flood fill between them, default) or 2 (both fields in
+// one CTA-wide launch, lazy flood fill)
 int g_plane_variant = 3;
 
 using FwdPlaneFn = void (*)(FwdSrc, const OrientDesc*, const float2*, const float2*);
@@ -319,7 +321,8 @@ int set_smem_attrs() {
     for (int a : {64, 100, 128})
         for (int b : {64, 100, 128}) {
             TRY(set_max_dyn_smem(plane2_for(a, b)));
-            TRY(set_max_dyn_smem(plane3_for(a, b)));
+            TRY(set_max_dyn_smem(plane3_for(a, b, 0)));
+            TRY(set_max_dyn_smem(plane3_for(a, b, 1)));
             TRY(set_max_dyn_smem(fwd_plane_for(a, b)));
         }
     for (int n : {64, 100, 128, 240}) TRY(set_max_dyn_smem(xfwd_for(n)));
@@ -602,6 +605,7 @@ struct psb_tray {
     unsigned long long *d_smin = nullptr, *d_best = nullptr, *d_bestkey = nullptr;
     unsigned long long* d_pmin = nullptr;   // per (orientation, x plane) minimum approximate score key
     int* d_needff = nullptr;                // lazy interlocking search: flood fill needed
+    unsigned char* d_okplane = nullptr;     // per (orientation, x plane): holds an ok cell
     unsigned int* d_diag = nullptr;
     unsigned int* d_errmax = nullptr;
     OrientDesc* d_od = nullptr;
@@ -628,7 +632,7 @@ struct psb_tray {
     void release_slots() {
         dfree(d_Ai, st); dfree(d_Bi, st); dfree(d_Pc, st); dfree(d_Pd, st); dfree(d_Dq, st); dfree(d_free, st); dfree(d_reach, st);
         dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
-        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_best, st);
+        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_best, st);
         dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
@@ -716,7 +720,7 @@ struct psb_tray {
         TRY(dalloc(&d_blk, (size_t)((nx * ny + 255) / 256) * c, st));
         TRY(dalloc(&d_cand, (size_t)kCandCap * c, st)); TRY(dalloc(&d_ncand, c, st));
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c, st));
-        TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
+        TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_okplane, (size_t)nx * c, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
         TRY(dalloc(&d_diag, c, st)); TRY(dalloc(&d_errmax, c, st)); TRY(dalloc(&d_od, c, st)); TRY(dalloc(&d_rzs, c, st)); TRY(dalloc(&d_mids, c, st));
         TRY(dalloc(&d_res, c, st));
         // item transform descriptors of each slot (orientation-relative)
@@ -891,6 +895,114 @@ struct psb_tray {
         return sp;
     }
 
+    // Flood fill (Algorithm 3) of every orientation's free bits into its
+    // reach bits.  okplane, when set, receives the planes that hold a
+    // reachable cell; gate, when set, makes every launch conditional.
+    int flood_fill(const OrientDesc* d_odb, int n, const ScoreParams& sp, const int* gate, unsigned char* okplane) {
+        FloodBufs fb{d_free, d_reach, sBits, d_cnt, d_off,   sLine, d_rz2,    d_rline,
+                     d_par,  d_rflag, sRun,  d_total, d_err, gate,  okplane, (long long)nx};
+        const int lines = nx * ny;
+        const int nblk = (lines + 255) / 256;
+        const dim3 gl(nblk, n);
+        {
+            PROF("k_ff_count", st);
+            k_ff_count<<<gl, 256, 0, st>>>(d_odb, fb, sp, d_blk, nblk);
+        }
+        CKL();
+        {
+            PROF("k_ff_scan", st);
+            k_ff_scan<<<n, 32, 0, st>>>(d_odb, fb, d_blk, nblk);
+        }
+        CKL();
+        {
+            PROF("k_ff_emit", st);
+            k_ff_emit<<<gl, 256, 0, st>>>(d_odb, fb, sp, d_blk, nblk);
+        }
+        CKL();
+        {
+            PROF("k_ff_union", st);
+            k_ff_union<<<gl, 256, 0, st>>>(d_odb, fb, sp);
+        }
+        CKL();
+        {
+            PROF("k_ff_seed", st);
+            k_ff_seed<<<dim3(296, n), 256, 0, st>>>(d_odb, fb);
+        }
+        CKL();
+        {
+            PROF("k_ff_reach", st);
+            k_ff_reach<<<gl, 256, 0, st>>>(d_odb, fb, sp);
+        }
+        CKL();
+        return PSB_OK;
+    }
+
+    // The default search for the specialised FFT lengths: collision plane
+    // pass (free bits) -> flood fill (interlocking mode) -> proximity plane
+    // pass only on the planes that hold an ok cell (free, or reachable) ->
+    // selection over the ok cells.  An item that fits nowhere costs no
+    // proximity transform, and every orientation's own result is exact.
+    int search_split(const OrientDesc* d_odb, int n, const ScoreParams& sp, bool interlock, XpassFn xf, PlaneFn p0,
+                     PlaneFn p1, size_t smem, ResultDev* d_out) {
+        SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
+        CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
+        if (xf) {
+            PROF("k_xpass", st);
+            const int ncols = g.F[1] * g.H;
+            xf<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
+                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw);
+        } else {
+            PROF("k_xpass", st);
+            const size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
+            k_xpass<<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], n), PSB_THREADS, smx, st>>>(
+                d_odb, sb, d_Socc, d_Sphi, g.F[1], g.H, g.p[0].p, g.p[0].tw);
+        }
+        CKL();
+        const uint32_t* ok = interlock ? d_reach : d_free;
+        PlaneBufs pb{d_free, d_Dq, d_smin, d_diag, sBits, sD, d_pmin, (long long)nx, ok, d_okplane, interlock ? 0 : 1};
+        {
+            PROF("k_plane_coll", st);
+            p0<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
+        }
+        CKL();
+        if (interlock) TRY(flood_fill(d_odb, n, sp, nullptr, d_okplane));
+        {
+            PROF("k_plane", st);
+            p1<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
+        }
+        CKL();
+        return select_over(d_odb, n, sp, ok, nullptr, d_out);
+    }
+
+    // Selection over the ok cells from the plane minima: candidates in the
+    // window of each orientation's minimum, exact re-score, tie rule, result.
+    int select_over(const OrientDesc* d_odb, int n, const ScoreParams& sp, const uint32_t* ok, const int* gate,
+                    ResultDev* d_out) {
+        SelectBufs sel{ok,        sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
+                       d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate};
+        {
+            PROF("k_collect", st);
+            k_collect_plane<<<dim3(nx, n), 256, 0, st>>>(d_odb, sel, sp);
+        }
+        CKL();
+        {
+            PROF("k_rescore", st);
+            k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_tray, d_phi);
+        }
+        CKL();
+        {
+            PROF("k_tiebreak", st);
+            k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp);
+        }
+        CKL();
+        {
+            PROF("k_finalize", st);
+            k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_odb, sel, sp, d_out, n);
+        }
+        CKL();
+        return PSB_OK;
+    }
+
     // Queue the search of the n orientations whose descriptors are at d_odb
     // (device item data already there); each orientation's result goes to
     // d_out[o].  ods is the host copy (dims for the launch shapes).  No host
@@ -936,7 +1048,6 @@ struct psb_tray {
             }
         }
         CKL();
-        SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
         CK(cudaMemsetAsync(d_smin, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long) * n, st));
         CK(cudaMemsetAsync(d_bestkey, 0xff, sizeof(unsigned long long) * n, st));
@@ -947,21 +1058,17 @@ struct psb_tray {
         ScoreParams sp = score_params(mode);
         XpassFn xf = g_fast_fft ? xpass2_for(g.F[0]) : nullptr;
         if (xf && xpass2_smem(g.F[0]) + 64 > (size_t)g_smem_optin) xf = nullptr;
+        if (g_fast_fft && g_plane_variant == 3) {
+            PlaneFn p0 = plane3_for(g.F[1], g.F[2], 0), p1 = plane3_for(g.F[1], g.F[2], 1);
+            const size_t sm3 = plane3_smem(g.F[1], g.F[2], ny) + 64;
+            if (p0 && p1 && sm3 <= (size_t)g_smem_optin) return search_split(d_odb, n, sp, interlock, xf, p0, p1, sm3, d_out);
+        }
         PlaneFn pf = nullptr;
         size_t sm2 = 0;
-        int pthreads = PSB_PLANE_THREADS;
-        bool plane_writes_min = false;  // the plane kernel itself writes the free-cell plane minima
-        if (g_fast_fft && g_plane_variant == 3) {
-            pf = plane3_for(g.F[1], g.F[2]);
-            sm2 = plane3_smem(g.F[1], g.F[2], ny) + 64;
-            pthreads = PSB_PLANE3_THREADS;
-            if (pf && sm2 > (size_t)g_smem_optin) pf = nullptr;
-            plane_writes_min = pf != nullptr;
-        }
-        if (g_fast_fft && !pf) {
+        const int pthreads = PSB_PLANE_THREADS;
+        if (g_fast_fft) {
             pf = plane2_for(g.F[1], g.F[2]);
             sm2 = plane2_smem(g.F[1], g.F[2], ny, nzw) + 64;
-            pthreads = PSB_PLANE_THREADS;
             if (pf && sm2 > (size_t)g_smem_optin) pf = nullptr;
         }
         const int wsz = std::max(PSB_TILE * g.F[1], PSB_PAIRS * g.F[2]);
@@ -976,7 +1083,7 @@ struct psb_tray {
             const int m = std::min(sub, n - o0);
             SearchBufs sbo{d_Bi + (size_t)o0 * sBi, d_Pc + (size_t)o0 * sP, d_Pd + (size_t)o0 * sP, sBi, sP};
             PlaneBufs pbo{d_free + (size_t)o0 * sBits, d_Dq + (size_t)o0 * sD, d_smin + o0, d_diag + o0, sBits, sD,
-                          d_pmin + (size_t)o0 * nx, (long long)nx};
+                          d_pmin + (size_t)o0 * nx, (long long)nx, nullptr, nullptr, 0};
             const OrientDesc* odo = d_odb + o0;
             if (xf) {
                 PROF("k_xpass", st);
@@ -1001,67 +1108,11 @@ struct psb_tray {
             CKL();
         }
         auto select = [&](const uint32_t* ok, const int* gate) -> int {
-            SelectBufs sel{ok,      sBits,   d_Dq,   sD,    d_smin, d_cand, d_ncand,          d_cscore, d_best,
-                           d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate};
-            {
-                PROF("k_collect", st);
-                k_collect_plane<<<dim3(nx, n), 256, 0, st>>>(d_odb, sel, sp);
-            }
-            CKL();
-            {
-                PROF("k_rescore", st);
-                k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_tray, d_phi);
-            }
-            CKL();
-            {
-                PROF("k_tiebreak", st);
-                k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp);
-            }
-            CKL();
-            {
-                PROF("k_finalize", st);
-                k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_odb, sel, sp, d_out, n);
-            }
-            CKL();
-            return PSB_OK;
+            return select_over(d_odb, n, sp, ok, gate, d_out);
         };
         // flood fill over the free bits, then a selection over the reachable cells
         auto reach_select = [&](const int* gate) -> int {
-            FloodBufs fb{d_free, d_reach, sBits, d_cnt,  d_off, sLine, d_rz2,
-                         d_rline, d_par, d_rflag, sRun, d_total, d_err, gate};
-            int lines = nx * ny;
-            const int nblk = (lines + 255) / 256;
-            dim3 gl(nblk, n);
-            {
-                PROF("k_ff_count", st);
-                k_ff_count<<<gl, 256, 0, st>>>(d_odb, fb, sp, d_blk, nblk);
-            }
-            CKL();
-            {
-                PROF("k_ff_scan", st);
-                k_ff_scan<<<n, 32, 0, st>>>(d_odb, fb, d_blk, nblk);
-            }
-            CKL();
-            {
-                PROF("k_ff_emit", st);
-                k_ff_emit<<<gl, 256, 0, st>>>(d_odb, fb, sp, d_blk, nblk);
-            }
-            CKL();
-            {
-                PROF("k_ff_union", st);
-                k_ff_union<<<gl, 256, 0, st>>>(d_odb, fb, sp);
-            }
-            CKL();
-            {
-                PROF("k_ff_seed", st);
-                k_ff_seed<<<dim3(296, n), 256, 0, st>>>(d_odb, fb);
-            }
-            CKL();
-            {
-                PROF("k_ff_reach", st);
-                k_ff_reach<<<gl, 256, 0, st>>>(d_odb, fb, sp);
-            }
-            CKL();
+            TRY(flood_fill(d_odb, n, sp, gate, nullptr));
             SelectBufs sel{d_reach,   sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
                            d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate};
             k_sel_reset<<<1, 128, 0, st>>>(sel, n);
@@ -1075,7 +1126,7 @@ struct psb_tray {
         };
         // plane minima over the free cells (k_plane3 and the generic k_plane
         // write them themselves)
-        if (pf && !plane_writes_min && (!interlock || lazy)) {
+        if (pf && (!interlock || lazy)) {
             SelectBufs sel{d_free,    sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
                            d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, nullptr};
             PROF("k_plane_min", st);
@@ -1492,7 +1543,7 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
     CK(cudaMemsetAsync(t->d_err, 0, sizeof(unsigned int), t->st));
     ScoreParams sp = t->score_params(1);
     FloodBufs fb{t->d_free, t->d_reach, t->sBits, t->d_cnt, t->d_off, t->sLine, t->d_rz2, t->d_rline, t->d_par,
-                 t->d_rflag, t->sRun, t->d_total, t->d_err, nullptr};
+                 t->d_rflag, t->sRun, t->d_total, t->d_err, nullptr, nullptr, 0};
     int lines = nx * ny;
     const int nblk = (lines + 255) / 256;
     dim3 gl(nblk, 1);

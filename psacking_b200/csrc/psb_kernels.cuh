@@ -353,8 +353,11 @@ struct PlaneBufs {
     unsigned long long* smin; // per orientation approx min score key
     unsigned int* diag;       // per orientation diag bits
     long long sBits, sD;
-    unsigned long long* pmin; // per (orientation, x plane) approx min score key over free cells
-    long long pstride;        // pmin stride per orientation
+    unsigned long long* pmin; // per (orientation, x plane) approx min score key over ok cells
+    long long pstride;        // pmin / okplane stride per orientation
+    const uint32_t* okbits;   // k_plane3 field 1: cells that count (free, or reachable)
+    unsigned char* okplane;   // k_plane3: per (orientation, x plane) "has an ok cell"
+    int set_okplane;          // k_plane3 field 0 sets okplane from the free cells
 };
 
 // Per (x-plane, orientation): inverse along y, C2R along z for the collision

@@ -428,6 +428,8 @@ struct FloodBufs {
     int* total;                    // runs per orientation
     unsigned int* err;             // device error word (limit hit)
     const int* gate;               // when set, the kernels run only if *gate != 0
+    unsigned char* okplane;        // when set, k_ff_reach flags planes holding a reachable cell
+    long long okstride;            // okplane stride per orientation
 };
 
 __device__ __forceinline__ int run_find(int* parent, int x, unsigned int* err) {
@@ -644,12 +646,15 @@ __global__ void k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb,
     const int* rz = fb.rz + (size_t)o * fb.sRun;
     int* par = fb.parent + (size_t)o * fb.sRun;
     const int* fl = fb.rflag + (size_t)o * fb.sRun;
+    bool any = false;
     for (int i = 0; i < cL; ++i) {
         int root = run_find(par, oL + i, fb.err);
         if (!(__ldcg(&fl[root]) & 2)) continue;
         int a = rz[oL + i];
         for (int z = a & 0xffff; z <= (a >> 16); ++z) w[z >> 5] |= 1u << (z & 31);
+        any = true;
     }
+    if (any && fb.okplane) fb.okplane[(size_t)o * fb.okstride + x] = 1;
 }
 
 // ---------------------------------------------------------------------------

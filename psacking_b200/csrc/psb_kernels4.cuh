@@ -54,8 +54,13 @@ inline size_t plane3_smem(int NY, int NZ, int ny) {
     return sizeof(float2) * (NY + NZ + std::max(wy, wz) + q);
 }
 
+// One field of the plane pass.  FIELD 0 (collision): free bits, and when
+// pb.set_okplane the plane's "has a free cell" flag.  FIELD 1 (proximity):
+// runs only for planes whose okplane flag is set (a free cell, or after the
+// flood fill a reachable one); writes the FP32 proximity field and the
+// plane's minimum approximate score over its ok cells (pmin, smin).
 // grid: (nx, n_orient), block PSB_PLANE3_THREADS
-template <int NY, int NZ>
+template <int NY, int NZ, int FIELD>
 __global__ void __launch_bounds__(PSB_PLANE3_THREADS, 2)
 k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, ScoreParams sp,
          const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
@@ -74,6 +79,10 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
     if (x >= Xv || Yv <= 0 || Zv <= 0) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (FIELD == 1 && !pb.okplane[(size_t)o * pb.pstride + x]) {
+        if (tid == 0) pb.pmin[(size_t)o * pb.pstride + x] = 0xffffffffffffffffULL;
+        return;
+    }
     const int ny = sp.ny, nzw = sp.nzw;
     const int npairs = (Yv + 1) / 2;
     float2* twy = sm;
@@ -87,181 +96,182 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     unsigned int diag = 0;
     float* Dq = pb.Dq + (size_t)o * pb.sD + (size_t)x * ny * sp.nz;
     uint32_t* fbits = pb.freebits + (size_t)o * pb.sBits + (size_t)x * ny * nzw;
+    const uint32_t* obits = pb.okbits + (size_t)o * pb.sBits + (size_t)x * ny * nzw;
 
-    // y pass: line (column) c = t*PER + li / L, lane j = lane % L
+    // y pass: line (column) c = t*PER + lane / L, lane j = lane % L
     const int yl = lane / LY::L, yj = lane - yl * LY::L;
     // z pass: line (row pair) p = t*PER + lane / L
     const int zl = lane / LZ::L, zj = lane - zl * LZ::L;
 
-    // per-z minimum proximity of the free cells, per lane: lane zj of line zl
-    // sees z = z0(s, r) + zj in every task, so slot (s, r) always means the
-    // same z; the lines of a warp are folded together by shuffles
-    float zmin[LZ::B2 * LZ::R1];
+    // FIELD 1: per-z minimum proximity of the ok cells, per lane: lane zj of
+    // line zl sees z = z0(s, r) + zj in every task, so slot (s, r) always means
+    // the same z; the lines of a warp are folded together by shuffles
+    float zmin[FIELD == 1 ? LZ::B2 * LZ::R1 : 1];
 #pragma unroll
-    for (int i = 0; i < LZ::B2 * LZ::R1; ++i) zmin[i] = INFINITY;
+    for (int i = 0; i < (FIELD == 1 ? LZ::B2 * LZ::R1 : 1); ++i) zmin[i] = INFINITY;
+    unsigned int anyfree = 0u;
 
+    const float2* P = (FIELD == 0 ? sb.Pc : sb.Pd) + (size_t)o * sb.sP + (size_t)x * NY * HZ;
+    for (int t = warp; t * LY::PER < HZ; t += NWARP) {
+        const int c = t * LY::PER + yl;
+        const bool act = yl < LY::PER && c < HZ;
+        float2* slab = W + (size_t)(t * LY::PER + (act ? yl : 0)) * LY::SLAB;
+        if (act) {
+            float2 v[LY::R0];
 #pragma unroll
-    for (int field = 0; field < 2; ++field) {
-        const float2* P = (field == 0 ? sb.Pc : sb.Pd) + (size_t)o * sb.sP + (size_t)x * NY * HZ;
-        for (int t = warp; t * LY::PER < HZ; t += NWARP) {
-            const int c = t * LY::PER + yl;
-            const bool act = yl < LY::PER && c < HZ;
-            float2* slab = W + (size_t)(t * LY::PER + (act ? yl : 0)) * LY::SLAB;
-            if (act) {
-                float2 v[LY::R0];
+            for (int r = 0; r < LY::R0; ++r) v[r] = P[(size_t)(yj + r * LY::L) * HZ + c];
+            RDFT<LY::R0, 1>::run(v);
 #pragma unroll
-                for (int r = 0; r < LY::R0; ++r) v[r] = P[(size_t)(yj + r * LY::L) * HZ + c];
-                RDFT<LY::R0, 1>::run(v);
-#pragma unroll
-                for (int r = 0; r < LY::R0; ++r) slab[LY::park(yj, r)] = v[r];
-            }
-            __syncwarp();
-            if (act) {
-#pragma unroll
-                for (int s = 0; s < LY::B2; ++s) {
-                    const int j2 = yj + s * LY::L;
-                    float2 u[LY::R1];
-#pragma unroll
-                    for (int r = 0; r < LY::R1; ++r) u[r] = slab[LY::fetch(j2, r)];
-                    if (j2 != 0) {
-#pragma unroll
-                        for (int r = 1; r < LY::R1; ++r) {
-                            float2 w = twy[r * j2];
-                            w.y = -w.y;
-                            u[r] = c_mul(u[r], w);
-                        }
-                    }
-                    RDFT<LY::R1, 1>::run(u);
-#pragma unroll
-                    for (int r = 0; r < LY::R1; ++r) {
-                        const int y = j2 + r * LY::R0;
-                        if (y < Yv) Q[y * HZ + c] = u[r];
-                    }
-                }
-            }
-            __syncwarp();
+            for (int r = 0; r < LY::R0; ++r) slab[LY::park(yj, r)] = v[r];
         }
-        __syncthreads();
-        // z pass: C2R of two rows per complex line (rows 2p, 2p+1)
-        for (int t = warp; t * LZ::PER < npairs; t += NWARP) {
-            const int p = t * LZ::PER + zl;
-            const bool act = zl < LZ::PER && p < npairs;
-            const int ya = 2 * p, yb = ya + 1;
-            const bool hb = yb < Yv;
-            float2* slab = W + (size_t)(warp * LZ::PER + (act ? zl : 0)) * LZ::SLAB;
-            if (act) {
-                float2 v[LZ::R0];
+        __syncwarp();
+        if (act) {
 #pragma unroll
-                for (int r = 0; r < LZ::R0; ++r) {
-                    const int k = zj + r * LZ::L;
-                    if (k < HZ) {
-                        const float2 xa = Q[ya * HZ + k];
-                        const float2 xb = hb ? Q[yb * HZ + k] : make_float2(0.f, 0.f);
-                        v[r] = make_float2(xa.x - xb.y, xa.y + xb.x);
-                    } else {
-                        const float2 xa = Q[ya * HZ + (NZ - k)];
-                        const float2 xb = hb ? Q[yb * HZ + (NZ - k)] : make_float2(0.f, 0.f);
-                        v[r] = make_float2(xa.x + xb.y, xb.x - xa.y);
+            for (int s = 0; s < LY::B2; ++s) {
+                const int j2 = yj + s * LY::L;
+                float2 u[LY::R1];
+#pragma unroll
+                for (int r = 0; r < LY::R1; ++r) u[r] = slab[LY::fetch(j2, r)];
+                if (j2 != 0) {
+#pragma unroll
+                    for (int r = 1; r < LY::R1; ++r) {
+                        float2 w = twy[r * j2];
+                        w.y = -w.y;
+                        u[r] = c_mul(u[r], w);
                     }
                 }
-                RDFT<LZ::R0, 1>::run(v);
+                RDFT<LY::R1, 1>::run(u);
 #pragma unroll
-                for (int r = 0; r < LZ::R0; ++r) slab[LZ::park(zj, r)] = v[r];
+                for (int r = 0; r < LY::R1; ++r) {
+                    const int y = j2 + r * LY::R0;
+                    if (y < Yv) Q[y * HZ + c] = u[r];
+                }
             }
-            __syncwarp();
-            // field 0: free words being assembled; field 1: the free words of
-            // rows ya, yb written by field 0 (this CTA's own global stores,
-            // ordered by the barriers in between)
-            uint32_t wa[NZW], wb[NZW];
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // z pass: C2R of two rows per complex line (rows 2p, 2p+1)
+    for (int t = warp; t * LZ::PER < npairs; t += NWARP) {
+        const int p = t * LZ::PER + zl;
+        const bool act = zl < LZ::PER && p < npairs;
+        const int ya = 2 * p, yb = ya + 1;
+        const bool hb = yb < Yv;
+        float2* slab = W + (size_t)(warp * LZ::PER + (act ? zl : 0)) * LZ::SLAB;
+        if (act) {
+            float2 v[LZ::R0];
+#pragma unroll
+            for (int r = 0; r < LZ::R0; ++r) {
+                const int k = zj + r * LZ::L;
+                if (k < HZ) {
+                    const float2 xa = Q[ya * HZ + k];
+                    const float2 xb = hb ? Q[yb * HZ + k] : make_float2(0.f, 0.f);
+                    v[r] = make_float2(xa.x - xb.y, xa.y + xb.x);
+                } else {
+                    const float2 xa = Q[ya * HZ + (NZ - k)];
+                    const float2 xb = hb ? Q[yb * HZ + (NZ - k)] : make_float2(0.f, 0.f);
+                    v[r] = make_float2(xa.x + xb.y, xb.x - xa.y);
+                }
+            }
+            RDFT<LZ::R0, 1>::run(v);
+#pragma unroll
+            for (int r = 0; r < LZ::R0; ++r) slab[LZ::park(zj, r)] = v[r];
+        }
+        __syncwarp();
+        // FIELD 0: free words being assembled; FIELD 1: the ok words of rows ya, yb
+        uint32_t wa[NZW], wb[NZW];
+#pragma unroll
+        for (int i = 0; i < NZW; ++i) {
+            wa[i] = wb[i] = 0u;
+            if (FIELD == 1 && i < nzw) {
+                if (act) wa[i] = obits[(size_t)ya * nzw + i];
+                if (act && hb) wb[i] = obits[(size_t)yb * nzw + i];
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < LZ::B2; ++s) {
+            const int j2 = zj + s * LZ::L;
+            float2 u[LZ::R1];
+#pragma unroll
+            for (int r = 0; r < LZ::R1; ++r) u[r] = make_float2(0.f, 0.f);
+            if (act) {
+#pragma unroll
+                for (int r = 0; r < LZ::R1; ++r) u[r] = slab[LZ::fetch(j2, r)];
+                if (j2 != 0) {
+#pragma unroll
+                    for (int r = 1; r < LZ::R1; ++r) {
+                        float2 w = twz[r * j2];
+                        w.y = -w.y;
+                        u[r] = c_mul(u[r], w);
+                    }
+                }
+                RDFT<LZ::R1, 1>::run(u);
+            }
+#pragma unroll
+            for (int r = 0; r < LZ::R1; ++r) {
+                // lanes zj = 0..L-1 of this line hold z = z0 + zj, L consecutive cells
+                const int z0 = s * LZ::L + r * LZ::R0;
+                const int z = z0 + zj;
+                const bool zin = act && z < Zv;
+                const float va = u[r].x * scale, vb = u[r].y * scale;
+                const int w0 = z0 >> 5, sh = z0 & 31;  // compile-time: static word index
+                if (FIELD == 0) {
+                    const float ra = rintf(va), rb = rintf(vb);
+                    if (zin && fabsf(va - ra) > 0.25f) diag |= 2u;
+                    if (zin && hb && fabsf(vb - rb) > 0.25f) diag |= 2u;
+                    const unsigned int ba = __ballot_sync(0xffffffffu, zin && ra == 0.f);
+                    const unsigned int bb = __ballot_sync(0xffffffffu, zin && hb && rb == 0.f);
+                    const unsigned int msk = (1u << LZ::L) - 1u;
+                    const unsigned int ca = (ba >> (zl * LZ::L)) & msk;
+                    const unsigned int cb = (bb >> (zl * LZ::L)) & msk;
+                    wa[w0] |= ca << sh;
+                    wb[w0] |= cb << sh;
+                    if (sh + LZ::L > 32 && w0 + 1 < NZW) {
+                        wa[w0 + 1] |= ca >> (32 - sh);
+                        wb[w0 + 1] |= cb >> (32 - sh);
+                    }
+                } else {
+                    if (zin) {
+                        Dq[(size_t)ya * sp.nz + z] = va;
+                        if (hb) Dq[(size_t)yb * sp.nz + z] = vb;
+                    }
+                    uint32_t ca = wa[w0] >> sh, cb = wb[w0] >> sh;
+                    if (sh + LZ::L > 32 && w0 + 1 < NZW) {
+                        ca |= wa[w0 + 1] << (32 - sh);
+                        cb |= wb[w0 + 1] << (32 - sh);
+                    }
+                    float m = INFINITY;
+                    if (zin && ((ca >> zj) & 1u)) m = va;
+                    if (zin && hb && ((cb >> zj) & 1u)) m = fminf(m, vb);
+#pragma unroll
+                    for (int d = LZ::L; d < 32; d <<= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, d));
+                    zmin[s * LZ::R1 + r] = fminf(zmin[s * LZ::R1 + r], m);
+                }
+            }
+        }
+        if (FIELD == 0 && act && zj == 0) {
 #pragma unroll
             for (int i = 0; i < NZW; ++i) {
-                wa[i] = wb[i] = 0u;
-                if (field == 1 && i < nzw) {
-                    if (act) wa[i] = fbits[(size_t)ya * nzw + i];
-                    if (act && hb) wb[i] = fbits[(size_t)yb * nzw + i];
+                if (i < nzw) {
+                    fbits[(size_t)ya * nzw + i] = wa[i];
+                    if (hb) fbits[(size_t)yb * nzw + i] = wb[i];
+                    anyfree |= wa[i] | wb[i];
                 }
             }
-#pragma unroll
-            for (int s = 0; s < LZ::B2; ++s) {
-                const int j2 = zj + s * LZ::L;
-                float2 u[LZ::R1];
-#pragma unroll
-                for (int r = 0; r < LZ::R1; ++r) u[r] = make_float2(0.f, 0.f);
-                if (act) {
-#pragma unroll
-                    for (int r = 0; r < LZ::R1; ++r) u[r] = slab[LZ::fetch(j2, r)];
-                    if (j2 != 0) {
-#pragma unroll
-                        for (int r = 1; r < LZ::R1; ++r) {
-                            float2 w = twz[r * j2];
-                            w.y = -w.y;
-                            u[r] = c_mul(u[r], w);
-                        }
-                    }
-                    RDFT<LZ::R1, 1>::run(u);
-                }
-#pragma unroll
-                for (int r = 0; r < LZ::R1; ++r) {
-                    // lanes zj = 0..L-1 of this line hold z = z0 + zj, L consecutive cells
-                    const int z0 = s * LZ::L + r * LZ::R0;
-                    const int z = z0 + zj;
-                    const bool zin = act && z < Zv;
-                    const float va = u[r].x * scale, vb = u[r].y * scale;
-                    if (field == 0) {
-                        const float ra = rintf(va), rb = rintf(vb);
-                        if (zin && fabsf(va - ra) > 0.25f) diag |= 2u;
-                        if (zin && hb && fabsf(vb - rb) > 0.25f) diag |= 2u;
-                        const unsigned int ba = __ballot_sync(0xffffffffu, zin && ra == 0.f);
-                        const unsigned int bb = __ballot_sync(0xffffffffu, zin && hb && rb == 0.f);
-                        const unsigned int msk = (1u << LZ::L) - 1u;
-                        const unsigned int ca = (ba >> (zl * LZ::L)) & msk;
-                        const unsigned int cb = (bb >> (zl * LZ::L)) & msk;
-                        // z0 is a compile-time constant here: the word index is static
-                        const int w0 = z0 >> 5, sh = z0 & 31;
-                        wa[w0] |= ca << sh;
-                        wb[w0] |= cb << sh;
-                        if (sh + LZ::L > 32 && w0 + 1 < NZW) {
-                            wa[w0 + 1] |= ca >> (32 - sh);
-                            wb[w0 + 1] |= cb >> (32 - sh);
-                        }
-                    } else {
-                        if (zin) {
-                            Dq[(size_t)ya * sp.nz + z] = va;
-                            if (hb) Dq[(size_t)yb * sp.nz + z] = vb;
-                        }
-                        const int w0 = z0 >> 5, sh = z0 & 31;
-                        uint32_t ca = wa[w0] >> sh, cb = wb[w0] >> sh;
-                        if (sh + LZ::L > 32 && w0 + 1 < NZW) {
-                            ca |= wa[w0 + 1] << (32 - sh);
-                            cb |= wb[w0 + 1] << (32 - sh);
-                        }
-                        float m = INFINITY;
-                        if (zin && ((ca >> zj) & 1u)) m = va;
-                        if (zin && hb && ((cb >> zj) & 1u)) m = fminf(m, vb);
-#pragma unroll
-                        for (int d = LZ::L; d < 32; d <<= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, d));
-                        zmin[s * LZ::R1 + r] = fminf(zmin[s * LZ::R1 + r], m);
-                    }
-                }
-            }
-            if (field == 0 && act && zj == 0) {
-#pragma unroll
-                for (int i = 0; i < NZW; ++i) {
-                    if (i < nzw) {
-                        fbits[(size_t)ya * nzw + i] = wa[i];
-                        if (hb) fbits[(size_t)yb * nzw + i] = wb[i];
-                    }
-                }
-            }
-            __syncwarp();
         }
-        __syncthreads();
+        __syncwarp();
     }
-    unsigned int dg = __reduce_or_sync(0xffffffffu, diag);
-    if ((tid & 31) == 0 && dg) atomicOr(&pb.diag[o], dg);
-    // the plane's minimum approximate score over its free cells (the score
-    // rises with the proximity at fixed z): per-warp per-z minima meet in
-    // the now idle plane buffer Q, then one double score per z
+    if (FIELD == 0) {
+        const unsigned int dg = __reduce_or_sync(0xffffffffu, diag);
+        if (lane == 0 && dg) atomicOr(&pb.diag[o], dg);
+        if (pb.set_okplane && __any_sync(0xffffffffu, anyfree != 0u) && lane == 0)
+            pb.okplane[(size_t)o * pb.pstride + x] = 1;
+        return;
+    }
+    // FIELD 1: the plane's minimum approximate score over its ok cells (the
+    // score rises with the proximity at fixed z): per-warp per-z minima meet
+    // in the plane buffer Q (idle once every warp has passed the barrier)
+    __syncthreads();
     float* zw = (float*)Q;   // [NWARP][NZ]
     for (int i = tid; i < NWARP * NZ; i += PSB_PLANE3_THREADS) zw[i] = INFINITY;
     __syncthreads();
@@ -271,7 +281,7 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
 #pragma unroll
             for (int r = 0; r < LZ::R1; ++r) {
                 const int z = s * LZ::L + r * LZ::R0 + zj;
-                zw[warp * NZ + z] = zmin[s * LZ::R1 + r];
+                zw[warp * NZ + z] = zmin[(FIELD == 1) ? s * LZ::R1 + r : 0];
             }
     }
     __syncthreads();

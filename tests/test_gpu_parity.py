@@ -151,23 +151,30 @@ def caged_tray(hole):
     return tray
 
 
+@pytest.mark.parametrize("variant", [3, 2])
 @pytest.mark.parametrize("hole", [None, "offset", "above"])
-def test_lazy_interlock_search(gpu_core, hole):
-    """The interlocking search runs the flood fill only when the best free
-    cell has no straight free run to a seed face; the answer is the oracle's
-    either way (sealed cavity: the winner moves outside; bent path: it stays
-    inside; straight path: no flood fill)."""
+def test_caged_interlock_search(gpu_core, hole, variant):
+    """A cavity whose best free cell is sealed, reachable by a bent path, or
+    by a straight one: the answer is the oracle's (sealed: the winner moves
+    outside; otherwise it stays inside).  Variant 3 (default) always runs the
+    flood fill before the proximity pass; variant 2 runs it lazily, only when
+    the best free cell has no straight free run to a seed face."""
+    gpu_core.set_plane_variant(variant)
     tray = caged_tray(hole)
     phi = O.calculate_distance(tray)
     item = np.ones((5, 5, 5), np.int32)
     ors = [item, np.ones((3, 5, 7), np.int32)]
     want = O.fft_search_batch(ors, tray, phi, interlock=True)
     gpu_core.gpu_tray_init(tray, phi)
-    d = gpu_core.search_detail(ors, BLOCK | INTERLOCK, per_orientation=False)
+    try:
+        d = gpu_core.search_detail(ors, BLOCK | INTERLOCK, per_orientation=False)
+    finally:
+        gpu_core.set_plane_variant(3)
     pos, found, score, bo = d["best"]
     assert (tuple(pos), found, score, bo) == (tuple(want[0]), want[1], want[2], want[3])
-    ran = bool(d["best_diag"] & DIAG_FLOOD_FILL)
-    assert ran == (hole != "above"), hex(d["best_diag"])
+    if variant == 2:
+        ran = bool(d["best_diag"] & DIAG_FLOOD_FILL)
+        assert ran == (hole != "above"), hex(d["best_diag"])
     inside = 6 <= pos[0] < 22 and 6 <= pos[1] < 22 and 1 <= pos[2] < 14
     assert inside == (hole is not None)
     got = gpu_core.fft_search_batch_interlocking_free(ors, tray, phi, 1)
