@@ -140,31 +140,33 @@ def sorted_items(items):
 
 
 def algorithmic_bytes(seq, maps, F):
-    """Bytes the two dominant kernels must move, summed over the run, from the
-    item shapes (every item is searched once in all orientations that fit).
-      k_xpass per orientation: read both tray half spectra (2*Fx*Fy*Hz*8 B),
-        read the item's z,y-transformed columns (ex*Fy*Hz*8), write the two
-        products for the valid planes (2*Xv*Fy*Hz*8).
-      k_plane per orientation: read both products (2*Xv*Fy*Hz*8), write the
-        proximity field and free bits of the valid box (Xv*Yv*Zv*4 + bits)."""
+    """Bytes the two always-running transform kernels must move, summed over
+    the run, from the item shapes (every item is searched once in all
+    orientations that fit).
+      k_xpass_coll per orientation: read the occupancy half spectrum
+        (Fx*Fy*Hz*8 B), read the item's z,y-transformed columns (ex*Fy*Hz*8),
+        write the collision product for the valid planes (Xv*Fy*Hz*8).
+      k_plane_coll per orientation: read that product (Xv*Fy*Hz*8), write the
+        free bits of the valid planes (Xv*ny*ceil(nz/32)*4).
+    The proximity kernels (k_xpass_prox, k_plane_prox) run only on the planes
+    that hold a reachable cell and are reported by time only."""
     from psacking_b200.rotations import apply_map
     Fx, Fy, Fz = F
     Hz = Fz // 2 + 1
     xb = pb = 0
     nor = 0
     for it in seq:
-        idx = np.argwhere(it > 0)
         for row in maps:
             o = apply_map(it, row)
             if any(o.shape[a] > TRAY[a] for a in range(3)):
                 continue
             oi = np.argwhere(o > 0)
             hi = oi.max(axis=0)
-            Xv, Yv, Zv = (TRAY[a] - hi[a] for a in range(3))
-            xb += 2 * Fx * Fy * Hz * 8 + o.shape[0] * Fy * Hz * 8 + 2 * Xv * Fy * Hz * 8
-            pb += 2 * Xv * Fy * Hz * 8 + Xv * Yv * Zv * 4 + Xv * TRAY[1] * ((TRAY[2] + 31) // 32) * 4
+            Xv = TRAY[0] - hi[0]
+            xb += Fx * Fy * Hz * 8 + o.shape[0] * Fy * Hz * 8 + Xv * Fy * Hz * 8
+            pb += Xv * Fy * Hz * 8 + Xv * TRAY[1] * ((TRAY[2] + 31) // 32) * 4
             nor += 1
-    return {"k_xpass": xb, "k_plane": pb, "orientations": nor}
+    return {"k_xpass_coll": xb, "k_plane_coll": pb, "orientations": nor}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -221,7 +223,7 @@ def run_ours(args, rank, world, local_rank):
     # roofline's live durations); the full per-kernel breakdown comes from one
     # extra step after it, so the timed loop is not slowed by ~50 event
     # records per item
-    lib.psb_profile_filter(b"k_plane,k_xpass")
+    lib.psb_profile_filter(b"k_plane_coll,k_xpass_coll")
     lib.psb_profile_enable(1)
     ms = [one_step(True) for _ in range(args.steps)]
     prof_top = parse_profile(lib)
@@ -285,7 +287,8 @@ def run_ours(args, rank, world, local_rank):
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     ab = algorithmic_bytes(seq, maps, F)
-    dom = max((k for k in prof_top if k in ("k_xpass", "k_plane")), key=lambda k: prof_top[k][1], default=None)
+    dom = max((k for k in prof_top if k in ("k_xpass_coll", "k_plane_coll")), key=lambda k: prof_top[k][1],
+              default=None)
     top = max(prof, key=lambda k: prof[k][1]) if prof else None
     roof = None
     if dom:

@@ -197,17 +197,21 @@ int get_plan(int n, Plan1D* out) {
 int g_smem_optin = 0;  // max dynamic shared memory per block of the current device
 bool g_fast_fft = true;  // specialised two-pass kernels where a plan exists
 
-using XpassFn = void (*)(const OrientDesc*, SearchBufs, const float2*, const float2*, int, const float2*);
+using XpassFn = void (*)(const OrientDesc*, SearchBufs, const float2*, const float2*, int, const float2*,
+                         const unsigned char*, long long);
 using PlaneFn = void (*)(const OrientDesc*, SearchBufs, PlaneBufs, ScoreParams, const float2*, const float2*);
 
-XpassFn xpass2_for(int n) {
+// mode 0: both products, 1: collision only, 2: proximity only (gated)
+XpassFn xpass2_for(int n, int mode = 0) {
+#define PSB_XP(N) return mode == 1 ? k_xpass2<N, 1> : (mode == 2 ? k_xpass2<N, 2> : k_xpass2<N, 0>)
     switch (n) {
-        case 64: return k_xpass2<64>;
-        case 100: return k_xpass2<100>;
-        case 128: return k_xpass2<128>;
-        case 240: return k_xpass2<240>;
+        case 64: PSB_XP(64);
+        case 100: PSB_XP(100);
+        case 128: PSB_XP(128);
+        case 240: PSB_XP(240);
         default: return nullptr;
     }
+#undef PSB_XP
 }
 
 #define PSB_PLANE_ROW(NY)                      \
@@ -317,7 +321,8 @@ int set_smem_attrs() {
     TRY(set_max_dyn_smem(k_xpass));
     TRY(set_max_dyn_smem(k_plane));
     TRY(set_max_dyn_smem(k_dist_axis));
-    for (int n : {64, 100, 128, 240}) TRY(set_max_dyn_smem(xpass2_for(n)));
+    for (int n : {64, 100, 128, 240})
+        for (int m = 0; m < 3; ++m) TRY(set_max_dyn_smem(xpass2_for(n, m)));
     for (int a : {64, 100, 128})
         for (int b : {64, 100, 128}) {
             TRY(set_max_dyn_smem(plane2_for(a, b)));
@@ -514,6 +519,7 @@ struct ItemInfo {
     int dims[3];
     int lo[3], hi[3];          // bounds of voxels > 0; hi = -1 when none
     long long sum = 0;         // sum of values
+    long long sabs = 0;        // sum of |values|
     double sumsq = 0.0;
     std::vector<int4> vox;     // nonzero voxels (x, y, z, value)
 };
@@ -522,6 +528,7 @@ void analyse_item(const int32_t* a, int ex, int ey, int ez, ItemInfo* info) {
     info->dims[0] = ex; info->dims[1] = ey; info->dims[2] = ez;
     for (int k = 0; k < 3; ++k) { info->lo[k] = INT32_MAX; info->hi[k] = -1; }
     info->sum = 0;
+    info->sabs = 0;
     info->sumsq = 0.0;
     info->vox.clear();
     for (int i = 0; i < ex; ++i)
@@ -531,6 +538,7 @@ void analyse_item(const int32_t* a, int ex, int ey, int ez, ItemInfo* info) {
                 if (v == 0) continue;
                 info->vox.push_back(make_int4(i, j, k, v));
                 info->sum += v;
+                info->sabs += std::llabs((long long)v);
                 info->sumsq += (double)v * v;
                 if (v > 0) {
                     int c[3] = {i, j, k};
@@ -869,8 +877,7 @@ struct psb_tray {
         }
         od->sumI = info.sum;
         od->base = (double)phi_mean * (double)info.sum;
-        long long sabs = 0;  // |D'| <= sum|I| * max|phi - m|
-        for (const int4& q : info.vox) sabs += std::llabs((long long)q.w);
+        const long long sabs = info.sabs;  // |D'| <= sum|I| * max|phi - m|
         double maxD = (double)sabs * (double)phi_maxabs;
         const double eps = 1.1920928955078125e-07;
         od->delta = 2.0 * eps * std::sqrt(info.sumsq) * phi_norm + 0.5 * ulp32(maxD) + 1e-3;
@@ -946,13 +953,14 @@ struct psb_tray {
                      PlaneFn p1, size_t smem, ResultDev* d_out) {
         SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
         CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
+        const int ncols = g.F[1] * g.H;
+        XpassFn xf1 = xf ? xpass2_for(g.F[0], 1) : nullptr, xf2 = xf ? xpass2_for(g.F[0], 2) : nullptr;
         if (xf) {
-            PROF("k_xpass", st);
-            const int ncols = g.F[1] * g.H;
-            xf<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
-                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw);
+            PROF("k_xpass_coll", st);
+            xf1<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
+                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, nullptr, 0);
         } else {
-            PROF("k_xpass", st);
+            PROF("k_xpass_coll", st);
             const size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
             k_xpass<<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], n), PSB_THREADS, smx, st>>>(
                 d_odb, sb, d_Socc, d_Sphi, g.F[1], g.H, g.p[0].p, g.p[0].tw);
@@ -966,8 +974,14 @@ struct psb_tray {
         }
         CKL();
         if (interlock) TRY(flood_fill(d_odb, n, sp, nullptr, d_okplane));
+        if (xf) {
+            PROF("k_xpass_prox", st);
+            xf2<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
+                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, d_okplane, (long long)nx);
+        }
+        CKL();
         {
-            PROF("k_plane", st);
+            PROF("k_plane_prox", st);
             p1<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
         }
         CKL();
@@ -1089,7 +1103,7 @@ struct psb_tray {
                 PROF("k_xpass", st);
                 int ncols = g.F[1] * g.H;
                 xf<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, m), 256, xpass2_smem(g.F[0]), st>>>(
-                    odo, sbo, d_Socc, d_Sphi, ncols, g.p[0].tw);
+                    odo, sbo, d_Socc, d_Sphi, ncols, g.p[0].tw, nullptr, 0);
             } else {
                 PROF("k_xpass", st);
                 size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);

@@ -11,13 +11,18 @@
 // Fused x pass over a tile of PSB_XCOLS consecutive columns c = ky*Hz + kz
 // (contiguous in memory, so every row access of the tile is one 128-byte
 // segment): item forward along x (pass 1 reads global), products with the
-// tray's two spectra fused into the last forward pass, inverse along x for
-// both products (last pass writes global rows x < Xv).
+// tray's spectra fused into the first inverse pass, inverse along x (last
+// pass writes global rows x < Xv).
+//   MODE 0: both products (collision -> Pc, proximity -> Pd)
+//   MODE 1: the collision product only (Pc)
+//   MODE 2: the proximity product only (Pd), for orientations with an ok
+//           plane (okplane, see k_plane3), and stored only on those planes
 // grid: (ceil(Fy*Hz / PSB_XCOLS), n_orient), block 256
-template <int N>
+template <int N, int MODE>
 __global__ void __launch_bounds__(256)
 k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __restrict__ Socc,
-         const float2* __restrict__ Sphi, int ncols, const float2* __restrict__ g_tw) {
+         const float2* __restrict__ Sphi, int ncols, const float2* __restrict__ g_tw,
+         const unsigned char* __restrict__ okplane, long long okstride) {
     constexpr int C = PSB_XCOLS;
     constexpr int R0 = Plan2<N>::R0, R1 = Plan2<N>::R1;
     extern __shared__ float2 sm[];
@@ -29,10 +34,20 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
     float2* tw = sm;
     float2* A = tw + N;
     float2* X = A + N * C;
+    unsigned char* okp = (unsigned char*)(X + N * C);   // MODE 2: the orientation's plane flags
     const int tid = threadIdx.x, nthr = blockDim.x;
+    const int ex = od.e[0], Xv = od.valid[0];
+    if (MODE == 2) {
+        int any = 0;
+        for (int x = tid; x < Xv; x += nthr) {
+            const unsigned char f = okplane[(size_t)o * okstride + x];
+            okp[x] = f;
+            any |= f;
+        }
+        if (!__syncthreads_or(any)) return;
+    }
     load_twiddles(tw, g_tw, N, tid, nthr);
     __syncthreads();
-    const int ex = od.e[0], Xv = od.valid[0];
     const float2* Bi = sb.Bi + (size_t)o * sb.sB + c0;
     float2* Pc = sb.Pc + (size_t)o * sb.sP + c0;
     float2* Pd = sb.Pd + (size_t)o * sb.sP + c0;
@@ -45,27 +60,32 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
     tpass<N, R1, R0, -1, C, false>([&](int c, int n) { return A[n * C + c]; },
                                    [&](int c, int k, float2 v) { X[k * C + c] = v; }, nl, tw, tid, nthr);
     __syncthreads();
-    // products conj(I^) * S formed as the inverse's first pass loads them
-    tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return c_cmul(X[n * C + c], So[(size_t)n * ncols + c]); },
-                                 [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
-    __syncthreads();
-    tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
-                                  [&](int c, int x, float2 v) {
-                                      if (x < Xv) Pc[(size_t)x * ncols + c] = v;
-                                  },
-                                  nl, tw, tid, nthr);
-    __syncthreads();
+    if (MODE != 2) {
+        // products conj(I^) * S formed as the inverse's first pass loads them
+        tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return c_cmul(X[n * C + c], So[(size_t)n * ncols + c]); },
+                                     [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
+        __syncthreads();
+        tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
+                                      [&](int c, int x, float2 v) {
+                                          if (x < Xv) Pc[(size_t)x * ncols + c] = v;
+                                      },
+                                      nl, tw, tid, nthr);
+        if (MODE == 1) return;
+        __syncthreads();
+    }
     tpass<N, R0, 1, 1, C, false>([&](int c, int n) { return c_cmul(X[n * C + c], Sp[(size_t)n * ncols + c]); },
                                  [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
     __syncthreads();
     tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
                                   [&](int c, int x, float2 v) {
-                                      if (x < Xv) Pd[(size_t)x * ncols + c] = v;
+                                      if (x < Xv && (MODE != 2 || okp[x])) Pd[(size_t)x * ncols + c] = v;
                                   },
                                   nl, tw, tid, nthr);
 }
 
-constexpr size_t xpass2_smem(int N) { return sizeof(float2) * ((size_t)N + 2 * (size_t)N * PSB_XCOLS); }
+constexpr size_t xpass2_smem(int N) {
+    return sizeof(float2) * ((size_t)N + 2 * (size_t)N * PSB_XCOLS) + (size_t)N;  // + MODE 2 plane flags
+}
 
 // shared memory of k_plane2: twiddles, work buffer A and the y-inverted plane
 // Q (ny rows; it also holds the plane's free mask as one byte per (y, z)
