@@ -372,6 +372,95 @@ def run_many(args, rank, world, local_rank):
                        "parallelism": f"trays sharded over {world} GPU(s), {args.concurrency} concurrent streams each"}}
 
 
+def run_learned(args, rank, world, local_rank):
+    """Learned-proposal form (config 4): the config-2 distribution (128^3 tray,
+    100 items, 24 orientations), held-out seeds 0..9; each step packs every
+    seed twice, plain and with the trained proposal gating the search to its
+    top-k orientations (psacking_b200/proposal_weights.npz).  value = the
+    learned form's items placed/s; the plain form's rate and both densities
+    are reported beside it."""
+    import torch
+    from psacking_b200 import proposal as PR
+    from psacking_b200 import workloads
+    from psacking_b200.rotations import orientation_maps
+    torch.cuda.set_device(local_rank)
+    with np.load(PR.WEIGHTS) as z:
+        params, topk, margin = z["params"], int(z["topk"]), float(z["margin"])
+    prop = PR.Proposal(params)
+    maps = orientation_maps(N_ORIENT)
+    seeds = list(range(10))
+    seqs = [PR.sorted_by_volume(workloads.config2_items(s)) for s in seeds]
+    tray = PR.Tray(workloads.TRAY2)
+    stream_p = ctypes.c_void_p()
+    check(PR.lib(), PR.lib().psb_tray_stream(tray.h, ctypes.byref(stream_p)))
+    stream = torch.cuda.ExternalStream(stream_p.value, device=torch.device("cuda", local_rank))
+
+    def run(form):
+        ms, placed, dens, fb, gated = 0.0, 0, [], 0, 0
+        for seq in seqs:
+            check(PR.lib(), PR.lib().psb_tray_set(tray.h, tray.empty.ctypes.data, None))
+            arr, dims = PR._ptrs(seq)
+            check(PR.lib(), PR.lib().psb_pack_stage(tray.h, arr, dims.ctypes.data, len(seq)))
+            res = (PR.PsbResult * len(seq))()
+            final = np.zeros(workloads.TRAY2, np.int32)
+            stats = np.zeros(2, np.int32)
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            if form == "plain":
+                check(PR.lib(), PR.lib().psb_pack_staged(tray.h, maps.ctypes.data, N_ORIENT, 0, 0, res, None))
+            else:
+                check(PR.lib(), PR.lib().psb_pack_staged_prop(tray.h, prop.h, maps.ctypes.data, N_ORIENT, 0, 0, topk,
+                                                              margin, res, None, stats.ctypes.data))
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms += a.elapsed_time(b)
+            check(PR.lib(), PR.lib().psb_tray_get(tray.h, final.ctypes.data, None))
+            placed += sum(r.found for r in res)
+            dens.append(_density(final))
+            gated += int(stats[0])
+            fb += int(stats[1])
+        return ms, placed, float(np.mean(dens)), fb / max(1, gated)
+
+    for _ in range(args.warmup):
+        run("plain")
+        run("learned")
+    tot = {"plain": [0.0, 0, 0.0, 0.0], "learned": [0.0, 0, 0.0, 0.0]}
+    for _ in range(args.steps):
+        for form in ("plain", "learned"):
+            ms, placed, dens, fbr = run(form)
+            t = tot[form]
+            t[0] += ms
+            t[1] += placed
+            t[2] = dens
+            t[3] = fbr
+    value = tot["learned"][1] / (tot["learned"][0] / 1e3)
+    plain_v = tot["plain"][1] / (tot["plain"][0] / 1e3)
+    prop.close()
+    tray.close()
+    return {"metric": "items placed/s, learned-proposal form (config 4: 128^3 tray, 100 items, 24 orientations)",
+            "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(tot["learned"][0] / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FFT, network), bf16 (network weights)",
+            "data": "synthetic (seeded config-2 items, held-out seeds 0..9)",
+            "config": {"workload": f"config4: 10 held-out seeds x 100 items, top-{topk} of 24 orientations, "
+                                   f"full sweep below {margin} top-k softmax mass",
+                       "plain_items_per_s": round(plain_v, 3), "speedup_vs_plain": round(value / plain_v, 3),
+                       "density_plain": round(tot["plain"][2], 5), "density_learned": round(tot["learned"][2], 5),
+                       "density_gap_pp": round(100 * (tot["plain"][2] - tot["learned"][2]), 3),
+                       "fallback_rate": round(tot["learned"][3], 4),
+                       "parallelism": "one tray, one GPU"}}
+
+
+def _density(tray):
+    idx = np.argwhere(tray > 0)
+    if len(idx) == 0:
+        return 0.0
+    ext = idx.max(axis=0) - idx.min(axis=0) + 1
+    return float(len(idx) / np.prod(ext))
+
+
 def cpu_sample_setup():
     """The bounded CPU sample: the tray after the first item of the workload is
     placed, and the second item (24 orientations, interlocking-free)."""
@@ -421,7 +510,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--items", type=int, default=N_ITEMS, help="profiling only: shorter item stream")
     ap.add_argument("--value-only", action="store_true", help="profiling only: skip the e2e leg")
-    ap.add_argument("--workload", default="config3", choices=["config3", "config5"])
+    ap.add_argument("--workload", default="config3", choices=["config3", "config4", "config5"])
     ap.add_argument("--trays", type=int, default=64, help="config5: number of trays")
     ap.add_argument("--concurrency", type=int, default=8, help="config5: trays packed at once per GPU")
     args = ap.parse_args()
@@ -440,7 +529,12 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device("cuda", local_rank))
-    out = run_many(args, rank, world, local_rank) if args.workload == "config5" else run_ours(args, rank, world, local_rank)
+    if args.workload == "config5":
+        out = run_many(args, rank, world, local_rank)
+    elif args.workload == "config4":
+        out = run_learned(args, rank, world, local_rank)
+    else:
+        out = run_ours(args, rank, world, local_rank)
     if rank == 0 and out is not None:
         if world == 1 and not args.no_cpu_baseline and args.workload == "config3":
             item, tray = cpu_sample_setup()

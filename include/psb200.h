@@ -185,6 +185,68 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
 int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                     psb_result* out_placements, int32_t* final_tray);
 
+/* ---- detailed packing run and the learned orientation proposal ---------
+ * None of these has a counterpart in the reference: the learned-proposal
+ * form of the placement search (a small 3-D CNN that ranks an item's 24
+ * orientations so that only the best k are searched exactly) is an addition
+ * of this engine, described in psb_proposal.cuh.                          */
+
+/* psb_pack_staged, also returning every orientation's own result
+ * (per_orient: n_items x n_orient, may be NULL) and the 32x32 pooled height
+ * map of the tray before each item (hmaps: n_items x 1024 floats, may be
+ * NULL): the plain method's training data for the proposal network.       */
+int psb_pack_staged_detail(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock,
+                           int32_t id_offset, psb_result* out_placements, int32_t* final_tray,
+                           psb_result* per_orient, float* hmaps);
+
+typedef struct psb_proposal psb_proposal;   /* network weights and work buffers on one GPU */
+int psb_prop_create(psb_proposal** out);
+int psb_prop_destroy(psb_proposal* p);
+int psb_prop_num_params(size_t* n);
+/* Host FP32 parameter vector in the layer order of the network; weights are
+ * used as BF16 (round to nearest even), biases as FP32.  Resets Adam.     */
+int psb_prop_set_params(psb_proposal* p, const float* params, size_t n);
+int psb_prop_get_params(psb_proposal* p, float* params, size_t n);
+/* Forward pass over n_items items of 24 orientations each: d_grids
+ * [n_items*24][32^3], d_hmaps [n_items][1024] (device).  With d_target
+ * (soft targets [n_items][24]) and d_mask ([n_items][24], 1 = the
+ * orientation fits the tray): the masked softmax cross-entropy (h_loss)
+ * and every parameter's gradient (psb_prop_get_grads).  d_logits
+ * [n_items*24] may be NULL.                                               */
+int psb_prop_forward_backward(psb_proposal* p, const float* d_grids, const float* d_hmaps, const float* d_mask,
+                              const float* d_target, int n_items, float* d_logits, float* h_loss);
+int psb_prop_get_grads(psb_proposal* p, float* grads, size_t n);
+/* One Adam step on the last gradients. */
+int psb_prop_adam_step(psb_proposal* p, float lr, float beta1, float beta2, float eps);
+/* The network's item inputs: per item (host int32 arrays), its occupancy
+ * scaled into a 32^3 grid (s = ceil(max extent / 32), a cell holds the
+ * occupied fraction of its s^3 block), turned by each orientation map
+ * (src_axis[3], flip[3]) -> d_out [n_items][n_orient][32^3] (device).     */
+int psb_prop_item_grids(const int32_t* const* items, const int32_t* dims, int n_items,
+                        const int32_t* orient_maps, int n_orient, float* d_out);
+/* The network's tray input: per column 1 + highest occupied z (0 when empty)
+ * over nz, averaged over ceil(nx/32) x ceil(ny/32) blocks -> d_out [32*32]. */
+int psb_height_map(const int32_t* d_tray, int nx, int ny, int nz, float* d_out);
+/* The packing loop of psb_pack_staged with the proposal: before each item's
+ * search the network ranks its 24 orientations (orient_maps must be the 24
+ * of get_24_orientations) and only the top-k are searched, or all of them
+ * when the top-k softmax mass is below `margin`.  gate_stats (may be NULL)
+ * receives [items gated, full-sweep fallbacks].                           */
+int psb_pack_staged_prop(psb_tray* t, psb_proposal* prop, const int32_t* orient_maps, int n_orient, int interlock,
+                         int32_t id_offset, int topk, float margin, psb_result* out_placements,
+                         int32_t* final_tray, int32_t* gate_stats);
+
+/* ---- mesh voxelizer (voxelize_stl) --------------------------------------
+ * Replaces spectral_packing/bindings.cpp:285-302 (py_voxelize_stl) and
+ * packing.cpp:540-588 (voxelize): exact vertex merge, the box transform to
+ * `resolution` voxels along the longest side (5% margin, 16-bit fixed
+ * point), rasterization along the three axes with the parity bit per axis,
+ * surface voxels only (the reference compiles the inside fill out), tight
+ * bounding box.  tris: ntri x 3 vertices x (x, y, z) floats, as read from an
+ * STL file.  out must hold resolution^3 int32; it receives the tight grid
+ * (C order, values 0/1) and dims_out its shape ({0,0,0} when empty).       */
+int psb_voxelize_mesh(const float* tris, int ntri, int resolution, int32_t* out, int32_t* dims_out);
+
 /* Kernel variant switch (default on): FFT lengths 64, 100, 128, 240 use
  * the specialised two-pass kernels; off forces the generic mixed-radix path
  * (used by the tests to check both). */

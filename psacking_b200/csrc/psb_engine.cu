@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -26,6 +27,8 @@
 #include "psb_kernels3.cuh"
 #include "psb_kernels4.cuh"
 #include "psb_loop.cuh"
+#include "psb_proposal.cuh"
+#include "psb_voxel.cuh"
 
 namespace {
 
@@ -1348,6 +1351,203 @@ int linear_transform_product(const int32_t* a, const int32_t* b, int nx, int ny,
 }  // namespace
 
 // ===========================================================================
+// psb_proposal: the learned orientation proposal (network in psb_proposal.cuh)
+// ===========================================================================
+namespace {
+// flat parameter layout (the same order as the oracle's LAYERS)
+struct PropLayer {
+    size_t w, b;     // offsets of weight and bias
+    size_t nw, nb;
+};
+struct PropLayout {
+    PropLayer c[4], f1, f2, h1, h2;
+    size_t n = 0;
+    PropLayout() {
+        const int ci[4] = {1, 16, 32, 64}, co[4] = {16, 32, 64, 64};
+        auto add = [&](PropLayer& L, size_t nw, size_t nb) {
+            L.w = n; L.nw = nw; n += nw;
+            L.b = n; L.nb = nb; n += nb;
+        };
+        for (int i = 0; i < 4; ++i) add(c[i], (size_t)co[i] * ci[i] * 27, co[i]);
+        add(f1, 64 * 512, 64);
+        add(f2, 64 * PSB_PH * PSB_PH, 64);
+        add(h1, 64 * 128, 64);
+        add(h2, 64, 1);
+    }
+};
+const PropLayout kProp;
+}  // namespace
+
+struct psb_proposal {
+    int dev = 0;
+    cudaStream_t st = nullptr;     // own stream for training; the packing loop passes the tray's
+    float *P = nullptr, *G = nullptr, *M = nullptr, *V = nullptr;
+    uint16_t* P16 = nullptr;
+    unsigned char* isw = nullptr;
+    long long step = 0;
+    int capS = 0, capB = 0;
+    float *a0 = nullptr, *a1 = nullptr, *a2 = nullptr, *a3 = nullptr, *a4 = nullptr, *f1 = nullptr, *t = nullptr,
+          *hin = nullptr, *h1 = nullptr, *logit = nullptr, *dlogit = nullptr, *hm = nullptr;
+    float *da1 = nullptr, *da2 = nullptr, *da3 = nullptr, *da4 = nullptr, *df1 = nullptr, *dt = nullptr,
+          *dhin = nullptr, *dh1 = nullptr, *loss = nullptr;
+    int* stats = nullptr;          // gating: items seen, fallbacks
+
+    ~psb_proposal() { release(); }
+    void free_acts() {
+        for (float** q : {&a0, &a1, &a2, &a3, &a4, &f1, &t, &hin, &h1, &logit, &dlogit, &hm, &da1, &da2, &da3, &da4,
+                          &df1, &dt, &dhin, &dh1})
+            dfree(*q);
+        capS = capB = 0;
+    }
+    void release() {
+        cudaSetDevice(dev);
+        free_acts();
+        dfree(P); dfree(G); dfree(M); dfree(V); dfree(P16); dfree(isw); dfree(loss); dfree(stats);
+        if (st) cudaStreamDestroy(st);
+        st = nullptr;
+    }
+    int init() {
+        TRY(ensure_device());
+        CK(cudaGetDevice(&dev));
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        const size_t n = kProp.n;
+        TRY(dalloc(&P, n)); TRY(dalloc(&G, n)); TRY(dalloc(&M, n)); TRY(dalloc(&V, n));
+        TRY(dalloc(&P16, n)); TRY(dalloc(&isw, n)); TRY(dalloc(&loss, 1)); TRY(dalloc(&stats, 2));
+        std::vector<unsigned char> w(n, 0);
+        auto mark = [&](const PropLayer& L) { memset(w.data() + L.w, 1, L.nw); };
+        for (int i = 0; i < 4; ++i) mark(kProp.c[i]);
+        mark(kProp.f1); mark(kProp.f2); mark(kProp.h1); mark(kProp.h2);
+        CK(cudaMemcpy(isw, w.data(), n, cudaMemcpyHostToDevice));
+        CK(cudaMemset(P, 0, sizeof(float) * n));
+        CK(cudaMemset(M, 0, sizeof(float) * n));
+        CK(cudaMemset(V, 0, sizeof(float) * n));
+        CK(cudaMemset(P16, 0, sizeof(uint16_t) * n));
+        CK(cudaMemset(stats, 0, sizeof(int) * 2));
+        return PSB_OK;
+    }
+    int ensure(int S, int B) {
+        if (S <= capS && B <= capB) return PSB_OK;
+        free_acts();
+        S = std::max(S, capS);
+        B = std::max(B, capB);
+        const size_t s = (size_t)S;
+        TRY(dalloc(&a0, s * PSB_PG3)); TRY(dalloc(&a1, s * 16 * 4096)); TRY(dalloc(&a2, s * 32 * 512));
+        TRY(dalloc(&a3, s * 64 * 64)); TRY(dalloc(&a4, s * 512)); TRY(dalloc(&f1, s * 64));
+        TRY(dalloc(&t, (size_t)B * 64)); TRY(dalloc(&hin, s * 128)); TRY(dalloc(&h1, s * 64));
+        TRY(dalloc(&logit, s)); TRY(dalloc(&dlogit, s)); TRY(dalloc(&hm, (size_t)B * PSB_PH * PSB_PH));
+        TRY(dalloc(&da1, s * 16 * 4096)); TRY(dalloc(&da2, s * 32 * 512)); TRY(dalloc(&da3, s * 64 * 64));
+        TRY(dalloc(&da4, s * 512)); TRY(dalloc(&df1, s * 64)); TRY(dalloc(&dt, (size_t)B * 64));
+        TRY(dalloc(&dhin, s * 128)); TRY(dalloc(&dh1, s * 64));
+        capS = S;
+        capB = B;
+        return PSB_OK;
+    }
+
+    // forward over B items of no orientations: grids [B*no][32^3], hmaps
+    // [B][1024] (device) -> this->logit [B*no]
+    int forward(const float* grids, const float* hmaps, int B, int no, cudaStream_t s) {
+        const int S = B * no;
+        auto g1 = [](long long n) { return (unsigned)((n + 255) / 256); };
+        const int ci[4] = {1, 16, 32, 64}, co[4] = {16, 32, 64, 64}, D[4] = {32, 16, 8, 4};
+        const float* in[4] = {grids, a1, a2, a3};
+        float* out[4] = {a1, a2, a3, a4};
+        for (int i = 0; i < 4; ++i) {
+            const long long n = (long long)S * (D[i] / 2) * (D[i] / 2) * (D[i] / 2);
+            PROF("k_prop_conv", s);
+            k_conv_fwd<<<dim3(g1(n), co[i] / PSB_CPT), 256, sizeof(float) * PSB_CPT * ci[i] * 27, s>>>(
+                in[i], S, ci[i], D[i], P16 + kProp.c[i].w, P + kProp.c[i].b, out[i], co[i]);
+            CKL();
+        }
+        PROF("k_prop_head", s);
+        k_lin_fwd<<<g1((long long)S * 64), 256, 0, s>>>(a4, S, 512, P16 + kProp.f1.w, P + kProp.f1.b, 64, 1, f1);
+        CKL();
+        k_lin_fwd<<<g1((long long)B * 64), 256, 0, s>>>(hmaps, B, PSB_PH * PSB_PH, P16 + kProp.f2.w, P + kProp.f2.b,
+                                                        64, 1, t);
+        CKL();
+        k_concat<<<g1((long long)S * 128), 256, 0, s>>>(f1, t, S, no, hin);
+        CKL();
+        k_lin_fwd<<<g1((long long)S * 64), 256, 0, s>>>(hin, S, 128, P16 + kProp.h1.w, P + kProp.h1.b, 64, 1, h1);
+        CKL();
+        k_lin_fwd<<<g1(S), 256, 0, s>>>(h1, S, 64, P16 + kProp.h2.w, P + kProp.h2.b, 1, 0, logit);
+        CKL();
+        return PSB_OK;
+    }
+
+    // item branch only (conv stack + f1) for B items of no orientations
+    // whose grids are at `grids`; f1 left in this->f1 [B*no][64]
+    int item_features(const float* grids, int B, int no, cudaStream_t s) {
+        const int S = B * no;
+        auto g1 = [](long long n) { return (unsigned)((n + 255) / 256); };
+        const int ci[4] = {1, 16, 32, 64}, co[4] = {16, 32, 64, 64}, D[4] = {32, 16, 8, 4};
+        const float* in[4] = {grids, a1, a2, a3};
+        float* out[4] = {a1, a2, a3, a4};
+        for (int i = 0; i < 4; ++i) {
+            const long long n = (long long)S * (D[i] / 2) * (D[i] / 2) * (D[i] / 2);
+            PROF("k_prop_conv", s);
+            k_conv_fwd<<<dim3(g1(n), co[i] / PSB_CPT), 256, sizeof(float) * PSB_CPT * ci[i] * 27, s>>>(
+                in[i], S, ci[i], D[i], P16 + kProp.c[i].w, P + kProp.c[i].b, out[i], co[i]);
+            CKL();
+        }
+        k_lin_fwd<<<g1((long long)S * 64), 256, 0, s>>>(a4, S, 512, P16 + kProp.f1.w, P + kProp.f1.b, 64, 1, f1);
+        CKL();
+        return PSB_OK;
+    }
+
+    // loss and every parameter gradient (into G) after forward()
+    int backward(const float* grids, const float* hmaps, const float* target, const float* mask, int B, int no,
+                 cudaStream_t s) {
+        const int S = B * no;
+        auto g1 = [](long long n) { return (unsigned)((n + 255) / 256); };
+        CK(cudaMemsetAsync(G, 0, sizeof(float) * kProp.n, s));
+        CK(cudaMemsetAsync(loss, 0, sizeof(float), s));
+        k_softmax_ce<<<(B + 7) / 8, 256, 0, s>>>(logit, target, mask, B, no, dlogit, loss);
+        CKL();
+        k_lin_bwd_weight<<<dim3(g1(64), 1), 256, 0, s>>>(dlogit, h1, S, 1, 64, G + kProp.h2.w, G + kProp.h2.b);
+        CKL();
+        k_lin_bwd_data<<<g1((long long)S * 64), 256, 0, s>>>(dlogit, S, 1, P16 + kProp.h2.w, 64, h1, dh1);
+        CKL();
+        k_lin_bwd_weight<<<dim3(g1(128), 64), 256, 0, s>>>(dh1, hin, S, 64, 128, G + kProp.h1.w, G + kProp.h1.b);
+        CKL();
+        k_lin_bwd_data<<<g1((long long)S * 128), 256, 0, s>>>(dh1, S, 64, P16 + kProp.h1.w, 128, nullptr, dhin);
+        CKL();
+        k_split_item<<<g1((long long)S * 64), 256, 0, s>>>(dhin, f1, S, df1);
+        CKL();
+        k_split_tray<<<g1((long long)B * 64), 256, 0, s>>>(dhin, t, B, no, dt);
+        CKL();
+        k_lin_bwd_weight<<<dim3(g1(PSB_PH * PSB_PH), 64), 256, 0, s>>>(dt, hmaps, B, 64, PSB_PH * PSB_PH,
+                                                                       G + kProp.f2.w, G + kProp.f2.b);
+        CKL();
+        k_lin_bwd_weight<<<dim3(g1(512), 64), 256, 0, s>>>(df1, a4, S, 64, 512, G + kProp.f1.w, G + kProp.f1.b);
+        CKL();
+        k_lin_bwd_data<<<g1((long long)S * 512), 256, 0, s>>>(df1, S, 64, P16 + kProp.f1.w, 512, a4, da4);
+        CKL();
+        const int ci[4] = {1, 16, 32, 64}, co[4] = {16, 32, 64, 64}, D[4] = {32, 16, 8, 4};
+        const float* in[4] = {grids, a1, a2, a3};
+        float* dout[4] = {da1, da2, da3, da4};
+        for (int i = 3; i >= 0; --i) {
+            // enough CTAs: about 2048 (ci, co, chunk) triples
+            const int nch_goal = std::max(1, 2048 / (ci[i] * co[i]));
+            const int chunk = std::max(1, (S + nch_goal - 1) / nch_goal);
+            const int nch = (S + chunk - 1) / chunk;
+            {
+                PROF("k_prop_bwd_weight", s);
+                k_conv_bwd_weight<<<dim3(ci[i], co[i], nch), 256, 0, s>>>(dout[i], in[i], S, ci[i], D[i], co[i], chunk,
+                                                                          G + kProp.c[i].w, G + kProp.c[i].b);
+            }
+            CKL();
+            if (i > 0) {
+                const long long n = (long long)S * D[i] * D[i] * D[i];
+                PROF("k_prop_bwd_data", s);
+                k_conv_bwd_data<<<dim3(g1(n), ci[i]), 256, sizeof(float) * co[i] * 27, s>>>(
+                    dout[i], S, ci[i], D[i], P16 + kProp.c[i].w, co[i], in[i], 1, dout[i - 1]);
+                CKL();
+            }
+        }
+        return PSB_OK;
+    }
+};
+
+// ===========================================================================
 // C ABI
 // ===========================================================================
 extern "C" {
@@ -1793,8 +1993,56 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     return PSB_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Options of the packing loop beyond the plain form.
+struct PackOpts {
+    psb_proposal* prop = nullptr;   // learned proposal: gate each item's orientations
+    int topk = 4;
+    float margin = 0.f;
+    psb_result* per_orient = nullptr;   // n_items x n_orient results of every orientation
+    float* hmaps = nullptr;             // n_items x 1024 pooled height maps before each item
+    int32_t* gate_stats = nullptr;      // [items gated, fallbacks to the full sweep]
+};
+int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
+                     psb_result* out_placements, int32_t* final_tray, const PackOpts& opt);
+}  // namespace
+
+extern "C" {
+
 int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                     psb_result* out_placements, int32_t* final_tray) {
+    return pack_staged_impl(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray, PackOpts());
+}
+
+int psb_pack_staged_detail(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
+                           psb_result* out_placements, int32_t* final_tray, psb_result* per_orient, float* hmaps) {
+    PackOpts o;
+    o.per_orient = per_orient;
+    o.hmaps = hmaps;
+    return pack_staged_impl(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray, o);
+}
+
+int psb_pack_staged_prop(psb_tray* t, psb_proposal* prop, const int32_t* orient_maps, int n_orient, int interlock,
+                         int32_t id_offset, int topk, float margin, psb_result* out_placements, int32_t* final_tray,
+                         int32_t* gate_stats) {
+    if (!prop) return fail(PSB_ERR_ARG, "pack_staged_prop: null proposal");
+    if (n_orient != PSB_PNO) return fail(PSB_ERR_ARG, "the proposal network ranks exactly %d orientations", PSB_PNO);
+    if (topk < 1) return fail(PSB_ERR_ARG, "topk must be >= 1");
+    PackOpts o;
+    o.prop = prop;
+    o.topk = topk;
+    o.margin = margin;
+    o.gate_stats = gate_stats;
+    return pack_staged_impl(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray, o);
+}
+
+}  // extern "C"
+
+namespace {
+int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
+                     psb_result* out_placements, int32_t* final_tray, const PackOpts& opt) {
     if (!t || !orient_maps || n_orient <= 0 || !out_placements)
         return fail(PSB_ERR_ARG, "null pointer or bad orientation count");
     if (!t->ready) return fail(PSB_ERR_STATE, "tray not initialised");
@@ -1839,6 +2087,66 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
     memset(&ls0, 0, sizeof(ls0));
     ls0.id_offset = id_offset;
     CK(cudaMemcpyAsync(t->d_ls, &ls0, sizeof(ls0), cudaMemcpyHostToDevice, t->st));
+    // optional outputs and the proposal's inputs
+    ResultDev* d_per = nullptr;
+    float* d_hm = nullptr;
+    float* d_pgrid = nullptr;  // base grids of the staged items (proposal)
+    int* d_pG = nullptr;       // their scaled extents
+    int* d_pmaps = nullptr;
+    struct Cleanup {
+        psb_tray* t;
+        ResultDev** per;
+        float** hm;
+        float** pg;
+        int** pG;
+        int** pm;
+        ~Cleanup() { dfree(*per, t->st); dfree(*hm, t->st); dfree(*pg, t->st); dfree(*pG, t->st); dfree(*pm, t->st); }
+    } cleanup{t, &d_per, &d_hm, &d_pgrid, &d_pG, &d_pmaps};
+    if (opt.per_orient) TRY(dalloc(&d_per, (size_t)n_items * n_orient, t->st));
+    if (opt.hmaps || opt.prop) TRY(dalloc(&d_hm, (size_t)n_items * PSB_PH * PSB_PH, t->st));
+    float* d_feat = nullptr;   // item features of every orientation of every item [n_items][24][64]
+    struct FeatCleanup {
+        psb_tray* t;
+        float** f;
+        ~FeatCleanup() { dfree(*f, t->st); }
+    } feat_cleanup{t, &d_feat};
+    const int kChunk = 32;      // items per batched item-branch pass
+    if (opt.prop) {
+        TRY(opt.prop->ensure(n_orient * std::min(kChunk, n_items), 1));
+        TRY(dalloc(&d_feat, (size_t)n_items * n_orient * 64, t->st));
+        TRY(dalloc(&d_pgrid, (size_t)n_items * PSB_PG3, t->st));
+        TRY(dalloc(&d_pG, (size_t)n_items * 3, t->st));
+        TRY(dalloc(&d_pmaps, (size_t)n_orient * 6, t->st));
+        CK(cudaMemsetAsync(d_pgrid, 0, sizeof(float) * n_items * PSB_PG3, t->st));
+        std::vector<int> G(3 * (size_t)n_items);
+        for (int it = 0; it < n_items; ++it) {
+            const ItemInfo& inf = t->staged[it];
+            const int sc = std::max(1, (std::max(inf.dims[0], std::max(inf.dims[1], inf.dims[2])) + PSB_PG - 1) / PSB_PG);
+            for (int a = 0; a < 3; ++a) G[3 * it + a] = (inf.dims[a] + sc - 1) / sc;
+            const int nv = (int)inf.vox.size();
+            if (nv > 0)
+                k_base_grid<<<(nv + 255) / 256, 256, 0, t->st>>>(t->d_stage_vox + t->staged_voff[it], nv, sc,
+                                                                 d_pgrid + (size_t)it * PSB_PG3);
+            CKL();
+        }
+        CK(cudaMemcpyAsync(d_pG, G.data(), sizeof(int) * G.size(), cudaMemcpyHostToDevice, t->st));
+        CK(cudaMemcpyAsync(d_pmaps, orient_maps, sizeof(int) * 6 * n_orient, cudaMemcpyHostToDevice, t->st));
+        CK(cudaMemsetAsync(opt.prop->stats, 0, sizeof(int) * 2, t->st));
+        // the item branch does not depend on the tray: all items, in chunks
+        psb_proposal* pr = opt.prop;
+        for (int i0 = 0; i0 < n_items; i0 += kChunk) {
+            const int m = std::min(kChunk, n_items - i0);
+            {
+                PROF("k_prop_inputs", t->st);
+                k_orient_grids<<<dim3(PSB_PG3 / 256, n_orient, m), 256, 0, t->st>>>(
+                    d_pgrid + (size_t)i0 * PSB_PG3, d_pG + 3 * i0, d_pmaps, n_orient, pr->a0);
+            }
+            CKL();
+            TRY(pr->item_features(pr->a0, m, n_orient, t->st));
+            CK(cudaMemcpyAsync(d_feat + (size_t)i0 * n_orient * 64, pr->f1, sizeof(float) * m * n_orient * 64,
+                               cudaMemcpyDeviceToDevice, t->st));
+        }
+    }
     CK(cudaStreamSynchronize(t->st));
     // While no item is placed yet and ids start at 1, the next placement writes
     // distance sources (voxels == 1); the host waits on those few items and
@@ -1851,7 +2159,33 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
         for (int o = 0; o < n_orient; ++o) host_ods[o] = all[(size_t)it * n_orient + o];
         k_prep<<<(n_orient + 63) / 64, 64, 0, t->st>>>(d_odb, n_orient, t->d_ps);
         CKL();
+        if (d_hm) {
+            k_height_map<<<PSB_PH * PSB_PH, 256, 0, t->st>>>(t->d_tray, t->nx, t->ny, t->nz,
+                                                             d_hm + (size_t)it * PSB_PH * PSB_PH);
+            CKL();
+        }
+        if (opt.prop) {
+            psb_proposal* pr = opt.prop;
+            {
+                PROF("k_prop_head", t->st);
+                k_prop_tray_feat<<<64, 256, 0, t->st>>>(d_hm + (size_t)it * PSB_PH * PSB_PH, pr->P16 + kProp.f2.w,
+                                                        pr->P + kProp.f2.b, pr->t);
+                CKL();
+                k_prop_item_head<<<n_orient, 64, 0, t->st>>>(d_feat + (size_t)it * n_orient * 64, pr->t,
+                                                             pr->P16 + kProp.h1.w, pr->P + kProp.h1.b,
+                                                             pr->P16 + kProp.h2.w, pr->P + kProp.h2.b, pr->logit);
+            }
+            CKL();
+            {
+                PROF("k_gate", t->st);
+                k_gate<OrientDesc><<<1, 32, 0, t->st>>>(pr->logit, d_odb, n_orient, opt.topk, opt.margin, pr->stats);
+            }
+            CKL();
+        }
         TRY(t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res));
+        if (d_per)
+            CK(cudaMemcpyAsync(d_per + (size_t)it * n_orient, t->d_res, sizeof(ResultDev) * n_orient,
+                               cudaMemcpyDeviceToDevice, t->st));
         k_decide<<<1, 32, 0, t->st>>>(d_odb, t->d_res, n_orient, t->d_ls, t->d_dec + it, t->d_err);
         CKL();
         {
@@ -1879,7 +2213,23 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
     LoopState h;
     CK(cudaMemcpyAsync(dec.data(), t->d_dec, sizeof(DecisionDev) * n_items, cudaMemcpyDeviceToHost, t->st));
     CK(cudaMemcpyAsync(&h, t->d_ls, sizeof(h), cudaMemcpyDeviceToHost, t->st));
+    std::vector<ResultDev> per;
+    if (d_per) {
+        per.resize((size_t)n_items * n_orient);
+        CK(cudaMemcpyAsync(per.data(), d_per, sizeof(ResultDev) * per.size(), cudaMemcpyDeviceToHost, t->st));
+    }
+    if (opt.hmaps)
+        CK(cudaMemcpyAsync(opt.hmaps, d_hm, sizeof(float) * n_items * PSB_PH * PSB_PH, cudaMemcpyDeviceToHost,
+                           t->st));
+    int gst[2] = {0, 0};
+    if (opt.prop) CK(cudaMemcpyAsync(gst, opt.prop->stats, sizeof(gst), cudaMemcpyDeviceToHost, t->st));
     CK(cudaStreamSynchronize(t->st));
+    if (opt.gate_stats) { opt.gate_stats[0] = gst[0]; opt.gate_stats[1] = gst[1]; }
+    for (size_t i = 0; i < per.size(); ++i) {
+        const int o = (int)(i % n_orient);
+        to_result(per[i], o, &opt.per_orient[i]);
+        if (all[i].skip) opt.per_orient[i].diag |= 0x200u;
+    }
     for (int it = 0; it < n_items; ++it) {
         psb_result r;
         r.x = dec[it].x; r.y = dec[it].y; r.z = dec[it].z;
@@ -1904,6 +2254,10 @@ int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int i
     if (final_tray) TRY(psb_tray_get(t, final_tray, nullptr));
     return PSB_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items, const int32_t* orient_maps,
              int n_orient, int interlock, int32_t id_offset, psb_result* out_placements, int32_t* final_tray) {
@@ -1955,6 +2309,278 @@ int psb_pack_many(int n_trays, const int32_t* tray_dims, const int32_t* const* i
     for (auto& th : pool) th.join();
     for (int i = 0; i < n_trays; ++i)
         if (status[i] != PSB_OK) return fail(status[i], "pack_many: tray %d: %s", i, messages[i].c_str());
+    return PSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned orientation proposal
+// ---------------------------------------------------------------------------
+int psb_prop_create(psb_proposal** out) {
+    if (!out) return fail(PSB_ERR_ARG, "null pointer");
+    std::unique_ptr<psb_proposal> p(new psb_proposal());
+    TRY(p->init());
+    *out = p.release();
+    return PSB_OK;
+}
+
+int psb_prop_destroy(psb_proposal* p) {
+    delete p;
+    return PSB_OK;
+}
+
+int psb_prop_num_params(size_t* n) {
+    if (!n) return fail(PSB_ERR_ARG, "null pointer");
+    *n = kProp.n;
+    return PSB_OK;
+}
+
+int psb_prop_set_params(psb_proposal* p, const float* params, size_t n) {
+    if (!p || !params) return fail(PSB_ERR_ARG, "null pointer");
+    if (n != kProp.n) return fail(PSB_ERR_ARG, "expected %zu parameters, got %zu", kProp.n, n);
+    CK(cudaSetDevice(p->dev));
+    std::vector<uint16_t> h16(n);
+    for (size_t i = 0; i < n; ++i) h16[i] = bf16_bits(params[i]);
+    CK(cudaMemcpy(p->P, params, sizeof(float) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->P16, h16.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemset(p->M, 0, sizeof(float) * n));
+    CK(cudaMemset(p->V, 0, sizeof(float) * n));
+    p->step = 0;
+    return PSB_OK;
+}
+
+int psb_prop_get_params(psb_proposal* p, float* params, size_t n) {
+    if (!p || !params) return fail(PSB_ERR_ARG, "null pointer");
+    if (n != kProp.n) return fail(PSB_ERR_ARG, "expected %zu parameters, got %zu", kProp.n, n);
+    CK(cudaSetDevice(p->dev));
+    CK(cudaStreamSynchronize(p->st));
+    CK(cudaMemcpy(params, p->P, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    return PSB_OK;
+}
+
+int psb_prop_get_grads(psb_proposal* p, float* grads, size_t n) {
+    if (!p || !grads) return fail(PSB_ERR_ARG, "null pointer");
+    if (n != kProp.n) return fail(PSB_ERR_ARG, "expected %zu parameters, got %zu", kProp.n, n);
+    CK(cudaSetDevice(p->dev));
+    CK(cudaStreamSynchronize(p->st));
+    CK(cudaMemcpy(grads, p->G, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    return PSB_OK;
+}
+
+int psb_prop_forward_backward(psb_proposal* p, const float* d_grids, const float* d_hmaps, const float* d_mask,
+                              const float* d_target, int n_items, float* d_logits, float* h_loss) {
+    if (!p || !d_grids || !d_hmaps || n_items <= 0) return fail(PSB_ERR_ARG, "null pointer or empty batch");
+    if (d_target && !d_mask) return fail(PSB_ERR_ARG, "a target needs a mask");
+    CK(cudaSetDevice(p->dev));
+    const int S = n_items * PSB_PNO;
+    TRY(p->ensure(S, n_items));
+    TRY(p->forward(d_grids, d_hmaps, n_items, PSB_PNO, p->st));
+    if (d_target) TRY(p->backward(d_grids, d_hmaps, d_target, d_mask, n_items, PSB_PNO, p->st));
+    if (d_logits) CK(cudaMemcpyAsync(d_logits, p->logit, sizeof(float) * S, cudaMemcpyDeviceToDevice, p->st));
+    if (h_loss) {
+        float l = 0.f;
+        if (d_target) CK(cudaMemcpyAsync(&l, p->loss, sizeof(float), cudaMemcpyDeviceToHost, p->st));
+        CK(cudaStreamSynchronize(p->st));
+        *h_loss = l;
+    }
+    CK(cudaStreamSynchronize(p->st));
+    return PSB_OK;
+}
+
+int psb_prop_adam_step(psb_proposal* p, float lr, float beta1, float beta2, float eps) {
+    if (!p) return fail(PSB_ERR_ARG, "null pointer");
+    CK(cudaSetDevice(p->dev));
+    p->step += 1;
+    const float c1 = 1.f - std::pow(beta1, (float)p->step), c2 = 1.f - std::pow(beta2, (float)p->step);
+    const long long n = (long long)kProp.n;
+    k_adam<<<(unsigned)((n + 255) / 256), 256, 0, p->st>>>(p->P, p->G, p->M, p->V, p->P16, p->isw, n, lr, beta1,
+                                                            beta2, eps, c1, c2);
+    CKL();
+    CK(cudaStreamSynchronize(p->st));
+    return PSB_OK;
+}
+
+int psb_prop_item_grids(const int32_t* const* items, const int32_t* dims, int n_items, const int32_t* orient_maps,
+                        int n_orient, float* d_out) {
+    if (!items || !dims || !orient_maps || !d_out || n_items < 0 || n_orient <= 0)
+        return fail(PSB_ERR_ARG, "null pointer or bad count");
+    TRY(ensure_device());
+    if (n_items == 0) return PSB_OK;
+    std::vector<ItemInfo> infos(n_items);
+    std::vector<int> G(3 * (size_t)n_items), S(n_items);
+    size_t totv = 0;
+    for (int i = 0; i < n_items; ++i) {
+        const int ex = dims[3 * i], ey = dims[3 * i + 1], ez = dims[3 * i + 2];
+        if (!items[i] || ex <= 0 || ey <= 0 || ez <= 0) return fail(PSB_ERR_ARG, "item %d: bad array", i);
+        analyse_item(items[i], ex, ey, ez, &infos[i]);
+        S[i] = std::max(1, (std::max(ex, std::max(ey, ez)) + PSB_PG - 1) / PSB_PG);
+        for (int a = 0; a < 3; ++a) G[3 * i + a] = (infos[i].dims[a] + S[i] - 1) / S[i];
+        totv += infos[i].vox.size();
+    }
+    float* base = nullptr;
+    int4* vox = nullptr;
+    int *dG = nullptr, *dm = nullptr;
+    TRY(dalloc(&base, (size_t)n_items * PSB_PG3));
+    TRY(dalloc(&vox, std::max<size_t>(totv, 1)));
+    TRY(dalloc(&dG, G.size()));
+    TRY(dalloc(&dm, (size_t)6 * n_orient));
+    int rc = PSB_OK;
+    do {
+        if (cudaMemset(base, 0, sizeof(float) * n_items * PSB_PG3) != cudaSuccess) { rc = fail(PSB_ERR_CUDA, "memset"); break; }
+        size_t off = 0;
+        for (int i = 0; i < n_items && rc == PSB_OK; ++i) {
+            const size_t nv = infos[i].vox.size();
+            if (nv == 0) continue;
+            if (cudaMemcpy(vox + off, infos[i].vox.data(), sizeof(int4) * nv, cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = fail(PSB_ERR_CUDA, "copy");
+            k_base_grid<<<(unsigned)((nv + 255) / 256), 256>>>(vox + off, (int)nv, S[i], base + (size_t)i * PSB_PG3);
+            off += nv;
+        }
+        if (rc != PSB_OK) break;
+        if (cudaMemcpy(dG, G.data(), sizeof(int) * G.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dm, orient_maps, sizeof(int) * 6 * n_orient, cudaMemcpyHostToDevice) != cudaSuccess) {
+            rc = fail(PSB_ERR_CUDA, "copy");
+            break;
+        }
+        k_orient_grids<<<dim3(PSB_PG3 / 256, n_orient, n_items), 256>>>(base, dG, dm, n_orient, d_out);
+        if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess)
+            rc = fail(PSB_ERR_CUDA, "item grids: %s", cudaGetErrorString(cudaGetLastError()));
+    } while (0);
+    dfree(base); dfree(vox); dfree(dG); dfree(dm);
+    return rc;
+}
+
+int psb_height_map(const int32_t* d_tray, int nx, int ny, int nz, float* d_out) {
+    if (!d_tray || !d_out || nx <= 0 || ny <= 0 || nz <= 0) return fail(PSB_ERR_ARG, "bad arguments");
+    TRY(ensure_device());
+    k_height_map<<<PSB_PH * PSB_PH, 256>>>(d_tray, nx, ny, nz, d_out);
+    CKL();
+    CK(cudaDeviceSynchronize());
+    return PSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// mesh voxelizer (voxelize_stl: bindings.cpp:285-302, packing.cpp:540-588)
+// ---------------------------------------------------------------------------
+int psb_voxelize_mesh(const float* tris, int ntri, int resolution, int32_t* out, int32_t* dims_out) {
+    if (!tris || !out || !dims_out || ntri <= 0 || resolution <= 0)
+        return fail(PSB_ERR_ARG, "voxelize: null pointer, no triangles or bad resolution");
+    TRY(ensure_device());
+    // mergeVerticesExact (LibSL Mesh.cpp:350-392): the new index of a vertex
+    // is the rank of its position in lexicographic order
+    const int nv = 3 * ntri;
+    std::vector<std::pair<std::array<float, 3>, int>> all(nv);
+    for (int v = 0; v < nv; ++v) all[v] = {{tris[3 * v], tris[3 * v + 1], tris[3 * v + 2]}, v};
+    std::sort(all.begin(), all.end());
+    std::vector<int> newidx(nv);
+    std::vector<std::array<float, 3>> pos;
+    for (int v = 0; v < nv; ++v) {
+        if (pos.empty() || all[v].first != pos.back()) pos.push_back(all[v].first);
+        newidx[all[v].second] = (int)pos.size() - 1;
+    }
+    // box transform in float, composed and applied as LibSL's Matrix4x4 does
+    // (products accumulated from zero in index order; no fused multiply-add)
+    float lo[3], hi[3], ext[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = hi[a] = pos[0][a];
+        for (auto& p : pos) { lo[a] = std::min(lo[a], p[a]); hi[a] = std::max(hi[a], p[a]); }
+        ext[a] = hi[a] - lo[a];
+    }
+    const float emax = std::max(ext[0], std::max(ext[1], ext[2]));
+    if (!(emax > 0.f)) return fail(PSB_ERR_ARG, "voxelize: the mesh has no extent");
+    typedef std::array<std::array<float, 4>, 4> M4;
+    auto ident = []() { M4 m{}; for (int i = 0; i < 4; ++i) m[i][i] = 1.f; return m; };
+    auto scale = [&](float s) { M4 m = ident(); for (int i = 0; i < 3; ++i) m[i][i] = s; return m; };
+    auto trans = [&](const float* t) { M4 m = ident(); for (int i = 0; i < 3; ++i) m[i][3] = t[i]; return m; };
+    auto mul = [](const M4& a, const M4& b) {
+        M4 r{};
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) {
+                volatile float acc = 0.f;
+                for (int k = 0; k < 4; ++k) {
+                    volatile float prod = a[i][k] * b[k][j];
+                    acc = acc + prod;
+                }
+                r[i][j] = acc;
+            }
+        return r;
+    };
+    const float factor = 0.95f;
+    float t1[3], t2[3];
+    for (int a = 0; a < 3; ++a) {
+        volatile float h = (1.f - factor) * 0.5f;
+        t1[a] = h * ext[a];
+        t2[a] = -lo[a];
+    }
+    volatile float inv = 1.f / emax;
+    const M4 box = mul(mul(mul(mul(scale((float)resolution * (float)PSB_FP_SCALE), scale(inv)), trans(t1)),
+                           scale(factor)),
+                       trans(t2));
+    const float top = (float)resolution * (float)PSB_FP_SCALE - 1.f;
+    std::vector<int> pts(3 * pos.size());
+    for (size_t p = 0; p < pos.size(); ++p)
+        for (int i = 0; i < 3; ++i) {
+            volatile float acc = 0.f;
+            for (int k = 0; k < 3; ++k) {
+                volatile float prod = box[i][k] * pos[p][k];
+                acc = acc + prod;
+            }
+            acc = acc + box[i][3];
+            float r = ::roundf(acc);
+            r = std::min(std::max(r, 0.f), top);
+            pts[3 * p + i] = (int)r;
+        }
+    int dims[3];
+    for (int a = 0; a < 3; ++a) {
+        volatile float q = ext[a] / emax;
+        volatile float d = q * (float)resolution;
+        dims[a] = (int)(unsigned int)d;
+    }
+    const size_t V = (size_t)dims[0] * dims[1] * dims[2];
+    std::vector<int> tri(3 * (size_t)ntri);
+    for (int v = 0; v < nv; ++v) tri[v] = newidx[v];
+    std::vector<unsigned int> hv(V, 0u);
+    if (V > 0) {
+        int *dp = nullptr, *dt = nullptr;
+        unsigned int* dv = nullptr;
+        TRY(dalloc(&dp, pts.size()));
+        TRY(dalloc(&dt, tri.size()));
+        TRY(dalloc(&dv, V));
+        int rc = PSB_OK;
+        if (cudaMemcpy(dp, pts.data(), sizeof(int) * pts.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dt, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(dv, 0, sizeof(unsigned int) * V) != cudaSuccess) {
+            rc = fail(PSB_ERR_CUDA, "voxelize: upload failed");
+        } else {
+            const long long warps = 3LL * ntri;
+            PROF("k_voxel_raster", nullptr);
+            k_voxel_raster<<<(unsigned)((warps + 7) / 8), 256>>>(dp, dt, ntri, dims[0], dims[1], dims[2], dv);
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaMemcpy(hv.data(), dv, sizeof(unsigned int) * V, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) rc = fail(PSB_ERR_CUDA, "voxelize: %s", cudaGetErrorString(e));
+        }
+        dfree(dp); dfree(dt); dfree(dv);
+        TRY(rc);
+    }
+    // occupied = any axis bit; then the tight bounding box (make_voxel_grid_tight)
+    int lo3[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi3[3] = {-1, -1, -1};
+    for (int i = 0; i < dims[0]; ++i)
+        for (int j = 0; j < dims[1]; ++j)
+            for (int k = 0; k < dims[2]; ++k)
+                if (hv[((size_t)i * dims[1] + j) * dims[2] + k]) {
+                    const int c[3] = {i, j, k};
+                    for (int a = 0; a < 3; ++a) { lo3[a] = std::min(lo3[a], c[a]); hi3[a] = std::max(hi3[a], c[a]); }
+                }
+    if (hi3[0] < 0) {
+        dims_out[0] = dims_out[1] = dims_out[2] = 0;
+        return PSB_OK;
+    }
+    const int td[3] = {hi3[0] - lo3[0] + 1, hi3[1] - lo3[1] + 1, hi3[2] - lo3[2] + 1};
+    for (int i = 0; i < td[0]; ++i)
+        for (int j = 0; j < td[1]; ++j)
+            for (int k = 0; k < td[2]; ++k)
+                out[((size_t)i * td[1] + j) * td[2] + k] =
+                    hv[((size_t)(i + lo3[0]) * dims[1] + (j + lo3[1])) * dims[2] + (k + lo3[2])] ? 1 : 0;
+    for (int a = 0; a < 3; ++a) dims_out[a] = td[a];
     return PSB_OK;
 }
 
