@@ -51,9 +51,10 @@ __version__ = _core.__version__
 
 
 def voxelize_stl(path, resolution: int = VOXEL_RESOLUTION):
-    """The reference's mesh voxelizer (bindings.cpp:285-302) is upstream of the
-    placement search and not part of this engine."""
-    raise NotImplementedError("voxelize_stl: mesh voxelization is outside this engine")
+    """The reference's mesh voxelizer (bindings.cpp:285-302): surface voxels
+    of a binary or ASCII STL mesh, tight int32 grid (psacking_b200.voxelize)."""
+    from .voxelize import voxelize_stl as _v
+    return _v(path, resolution)
 
 
 __all__ = [
