@@ -256,6 +256,13 @@ int psb_set_fast_fft(int on);
  * spread over the CTA).  Same results; a tuning and comparison switch.
  * No counterpart in the reference (cuFFT there). */
 int psb_set_plane_variant(int v);
+/* The 24 orientations are 6 axis permutations x 4 flip patterns.  On: the
+ * z,y transforms of each permutation run once per item and the x pass reads
+ * every flip from them (row reversal, column map, conjugation, phase).  Off
+ * (the default, faster on B200): every orientation is transformed on its
+ * own.  Same results; a comparison switch.  No counterpart in the
+ * reference. */
+int psb_set_share_flips(int on);
 
 /* Many independent trays (the many-tray form of the benchmark set): tray i
  * has dims tray_dims[3i..3i+2] and items_per_tray[i] items, which follow the

@@ -489,6 +489,9 @@ PYBIND11_MODULE(_core, m) {
     m.def("device_count", &py_device_count);
     m.def("set_fast_fft", [](bool on) { psb_set_fast_fft(on ? 1 : 0); }, py::arg("on"),
           "Use the specialised two-pass FFT kernels where a plan exists (default) or force the generic path.");
+    m.def("set_share_flips", [](bool on) { check(psb_set_share_flips(on ? 1 : 0)); }, py::arg("on"),
+          "Share the z,y transforms among the flips of each axis permutation, or transform each orientation on "
+          "its own (the default).");
     m.def("set_plane_variant", [](int v) { check(psb_set_plane_variant(v)); }, py::arg("variant"),
           "Plane-pass kernel for the specialised lengths: 3 (warp-owned lines, default) or 2.");
     m.attr("VOXEL_RESOLUTION") = 128;

@@ -201,12 +201,15 @@ int g_smem_optin = 0;  // max dynamic shared memory per block of the current dev
 bool g_fast_fft = true;  // specialised two-pass kernels where a plan exists
 
 using XpassFn = void (*)(const OrientDesc*, SearchBufs, const float2*, const float2*, int, const float2*,
-                         const unsigned char*, long long);
+                         const unsigned char*, long long, BaseMap);
 using PlaneFn = void (*)(const OrientDesc*, SearchBufs, PlaneBufs, ScoreParams, const float2*, const float2*);
 
-// mode 0: both products, 1: collision only, 2: proximity only (gated)
-XpassFn xpass2_for(int n, int mode = 0) {
-#define PSB_XP(N) return mode == 1 ? k_xpass2<N, 1> : (mode == 2 ? k_xpass2<N, 2> : k_xpass2<N, 0>)
+// mode 0: both products, 1: collision only, 2: proximity only (gated);
+// shared: the slabs come from the orientation's permutation base
+XpassFn xpass2_for(int n, int mode = 0, bool shared = false) {
+#define PSB_XP(N)                                                                                     \
+    if (shared) return mode == 1 ? k_xpass2<N, 1, true> : (mode == 2 ? k_xpass2<N, 2, true> : k_xpass2<N, 0, true>); \
+    return mode == 1 ? k_xpass2<N, 1, false> : (mode == 2 ? k_xpass2<N, 2, false> : k_xpass2<N, 0, false>)
     switch (n) {
         case 64: PSB_XP(64);
         case 100: PSB_XP(100);
@@ -257,6 +260,20 @@ PlaneFn plane3_for(int ny, int nz, int field) {
 // launches with the flood fill between them, default) or 2 (both fields in
 // one CTA-wide launch, lazy flood fill)
 int g_plane_variant = 3;
+
+// z,y slab transforms shared across the flips of a permutation
+// (psb_kernels3.cuh).  Off by default: measured on the config-3 benchmark the
+// x pass's per-element index map and phase cost more (+13 ms per run) than
+// the 6-instead-of-24 slab transforms save (-3.4 ms: that launch is
+// latency-bound, not work-bound).
+bool g_share_flips = false;
+
+// the 6 axis permutations of an orientation map, as base indices
+int perm_index(const int* a) {
+    static const int tab[27] = {-1, -1, -1, -1, -1, 0, -1, 1, -1, -1, -1, 2, -1, -1, -1, 3, -1, -1,
+                                -1, 4, -1, 5, -1, -1, -1, -1, -1};
+    return tab[a[0] * 9 + a[1] * 3 + a[2]];
+}
 
 using FwdPlaneFn = void (*)(FwdSrc, const OrientDesc*, const float2*, const float2*);
 using XfwdFn = void (*)(const float2*, float2*, int, int, const int*, const float2*);
@@ -317,6 +334,7 @@ int set_smem_attrs() {
     if (dev < 64 && done[dev]) return PSB_OK;
     CK(cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (const char* e = getenv("PSB_PLANE_VARIANT")) g_plane_variant = atoi(e) == 2 ? 2 : 3;
+    if (const char* e = getenv("PSB_SHARE_FLIPS")) g_share_flips = atoi(e) != 0;
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
     TRY(set_max_dyn_smem(k_fft_mid<-1>));
@@ -325,7 +343,10 @@ int set_smem_attrs() {
     TRY(set_max_dyn_smem(k_plane));
     TRY(set_max_dyn_smem(k_dist_axis));
     for (int n : {64, 100, 128, 240})
-        for (int m = 0; m < 3; ++m) TRY(set_max_dyn_smem(xpass2_for(n, m)));
+        for (int m = 0; m < 3; ++m) {
+            TRY(set_max_dyn_smem(xpass2_for(n, m, false)));
+            TRY(set_max_dyn_smem(xpass2_for(n, m, true)));
+        }
     for (int a : {64, 100, 128})
         for (int b : {64, 100, 128}) {
             TRY(set_max_dyn_smem(plane2_for(a, b)));
@@ -562,6 +583,37 @@ double ulp32(double v) {
 
 }  // namespace
 
+// The item's 6 axis permutations as base descriptors (no flips), and each
+// orientation's base index.  A base is skipped when it does not fit the tray
+// (the same for all flips of it) or no orientation uses it.  Returns false
+// (no sharing possible) unless every orientation turns the same item: the
+// synchronous entry points take explicit arrays, which may be different
+// items described as identity maps.
+bool make_bases(std::vector<OrientDesc>* ods, std::vector<OrientDesc>* bases) {
+    for (auto& od : *ods)
+        if (od.item != (*ods)[0].item || od.b[0] != (*ods)[0].b[0] || od.b[1] != (*ods)[0].b[1] ||
+            od.b[2] != (*ods)[0].b[2])
+            return false;
+    bases->assign(6, OrientDesc());
+    for (auto& b : *bases) {
+        memset(&b, 0, sizeof(b));
+        b.skip = 1;
+        b.perm = -1;
+    }
+    std::vector<char> used(6, 0);
+    for (auto& od : *ods) {
+        const int p = perm_index(od.src_axis);
+        od.perm = p;
+        if (p < 0 || used[p]) continue;
+        OrientDesc b = od;
+        b.flip[0] = b.flip[1] = b.flip[2] = 0;
+        b.perm = p;
+        (*bases)[p] = b;
+        used[p] = 1;
+    }
+    return true;
+}
+
 // ===========================================================================
 // psb_tray: the device-resident tray context
 // ===========================================================================
@@ -597,6 +649,8 @@ struct psb_tray {
     MidDesc* d_midd = nullptr;  // pairs in the same order
     OrientDesc* d_od_all = nullptr;
     size_t od_all_cap = 0;
+    OrientDesc* d_base_all = nullptr;   // 6 axis-permutation bases per staged item
+    size_t base_all_cap = 0;
     DecisionDev* d_dec = nullptr;
     size_t dec_cap = 0;
 
@@ -617,6 +671,7 @@ struct psb_tray {
     unsigned long long* d_pmin = nullptr;   // per (orientation, x plane) minimum approximate score key
     int* d_needff = nullptr;                // lazy interlocking search: flood fill needed
     unsigned char* d_okplane = nullptr;     // per (orientation, x plane): holds an ok cell
+    OrientDesc* d_bases = nullptr;          // their descriptors (synchronous searches)
     unsigned int* d_diag = nullptr;
     unsigned int* d_errmax = nullptr;
     OrientDesc* d_od = nullptr;
@@ -631,6 +686,8 @@ struct psb_tray {
     int32_t* d_stage = nullptr;
     int4* d_stage_vox = nullptr;
     size_t stage_cap = 0, stage_vcap = 0;
+    void* h_stage = nullptr;   // pinned host staging buffer of psb_pack_stage
+    size_t h_stage_cap = 0;
 
     // item staging
     int32_t* d_items = nullptr;
@@ -643,7 +700,7 @@ struct psb_tray {
     void release_slots() {
         dfree(d_Ai, st); dfree(d_Bi, st); dfree(d_Pc, st); dfree(d_Pd, st); dfree(d_Dq, st); dfree(d_free, st); dfree(d_reach, st);
         dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
-        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_best, st);
+        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_bases, st); dfree(d_best, st);
         dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
@@ -652,12 +709,15 @@ struct psb_tray {
         release_slots();
         dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_pen, st);
         dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st); dfree(d_stage_vox, st);
-        dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_dec, st);
+        dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_base_all, st); dfree(d_dec, st);
         if (st) {
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
         }
         st = nullptr;
+        if (h_stage) cudaFreeHost(h_stage);
+        h_stage = nullptr;
+        h_stage_cap = 0;
     }
 
     int init(int x, int y, int z) {
@@ -731,7 +791,8 @@ struct psb_tray {
         TRY(dalloc(&d_blk, (size_t)((nx * ny + 255) / 256) * c, st));
         TRY(dalloc(&d_cand, (size_t)kCandCap * c, st)); TRY(dalloc(&d_ncand, c, st));
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c, st));
-        TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_okplane, (size_t)nx * c, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
+        TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_okplane, (size_t)nx * c, st));
+        TRY(dalloc(&d_bases, 6, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
         TRY(dalloc(&d_diag, c, st)); TRY(dalloc(&d_errmax, c, st)); TRY(dalloc(&d_od, c, st)); TRY(dalloc(&d_rzs, c, st)); TRY(dalloc(&d_mids, c, st));
         TRY(dalloc(&d_res, c, st));
         // item transform descriptors of each slot (orientation-relative)
@@ -888,7 +949,7 @@ struct psb_tray {
         od->item = d_item;
         od->vox = d_vx;
         od->nvox = (int)info.vox.size();
-        od->pad = 0;
+        od->perm = -1;
         od->sumsq = info.sumsq;
         od->sabs = sabs;
     }
@@ -953,15 +1014,16 @@ struct psb_tray {
     // selection over the ok cells.  An item that fits nowhere costs no
     // proximity transform, and every orientation's own result is exact.
     int search_split(const OrientDesc* d_odb, int n, const ScoreParams& sp, bool interlock, XpassFn xf, PlaneFn p0,
-                     PlaneFn p1, size_t smem, ResultDev* d_out) {
+                     PlaneFn p1, size_t smem, ResultDev* d_out, bool spec) {
         SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
         CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
         const int ncols = g.F[1] * g.H;
-        XpassFn xf1 = xf ? xpass2_for(g.F[0], 1) : nullptr, xf2 = xf ? xpass2_for(g.F[0], 2) : nullptr;
+        XpassFn xf1 = xf ? xpass2_for(g.F[0], 1, spec) : nullptr, xf2 = xf ? xpass2_for(g.F[0], 2, spec) : nullptr;
+        const BaseMap bm{g.F[1], g.H, g.F[2], g.p[1].tw, g.p[2].tw};
         if (xf) {
             PROF("k_xpass_coll", st);
             xf1<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
-                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, nullptr, 0);
+                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, nullptr, 0, bm);
         } else {
             PROF("k_xpass_coll", st);
             const size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
@@ -980,7 +1042,7 @@ struct psb_tray {
         if (xf) {
             PROF("k_xpass_prox", st);
             xf2<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
-                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, d_okplane, (long long)nx);
+                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, d_okplane, (long long)nx, bm);
         }
         CKL();
         {
@@ -1032,10 +1094,52 @@ struct psb_tray {
     // flood fill is skipped (k_line_check).  Otherwise the flood fill and a
     // second selection over the reachable cells run, gated on the device flag
     // d_needff, so the host never waits.
+    //
+    // With bases (d_bases / hbases: the item's 6 axis permutations, each
+    // orientation's OrientDesc::perm set), the split flow transforms only the
+    // bases and the x passes read their slabs (k_xpass2 SHARED).
     int search_async(const OrientDesc* d_odb, const std::vector<OrientDesc>& ods, int mode, bool interlock,
-                     ResultDev* d_out, bool lazy = true) {
+                     ResultDev* d_out, bool lazy = true, const OrientDesc* d_bases_in = nullptr,
+                     const std::vector<OrientDesc>* hbases = nullptr) {
         const int n = (int)ods.size();
-        TRY(ensure_slots(n));
+        // the caller reserves the slots (ensure_slots) before taking slot
+        // pointers such as d_out: growing them here would free those
+        if (cap < std::max(n, 6)) return fail(PSB_ERR_STATE, "search slots not reserved (%d < %d)", cap, std::max(n, 6));
+        XpassFn xf = g_fast_fft ? xpass2_for(g.F[0]) : nullptr;
+        if (xf && xpass2_smem(g.F[0]) + 64 > (size_t)g_smem_optin) xf = nullptr;
+        PlaneFn p0 = nullptr, p1 = nullptr;
+        size_t sm3 = 0;
+        if (g_fast_fft && g_plane_variant == 3) {
+            p0 = plane3_for(g.F[1], g.F[2], 0);
+            p1 = plane3_for(g.F[1], g.F[2], 1);
+            if (p0 && p1) sm3 = plane3_smem(g.F[1], g.F[2], ny) + 64;
+            if (!p0 || !p1 || sm3 > (size_t)g_smem_optin) p0 = p1 = nullptr;
+        }
+        FwdPlaneFn ffb = g_fast_fft ? fwd_plane_for(g.F[1], g.F[2]) : nullptr;
+        const bool spec = g_share_flips && d_bases_in && hbases && p0 && xf && ffb;
+        if (spec) {
+            // the bases' z,y forward into slab slots 0..5; the x passes read them
+            int bx = 1, by = 1;
+            for (auto& b : *hbases)
+                if (!b.skip) { bx = std::max(bx, b.e[0]); by = std::max(by, b.e[1]); }
+            const size_t smf = fwd_plane_smem(g.F[1], g.F[2], by) + 64;
+            if (smf <= (size_t)g_smem_optin) {
+                FwdSrc src{SRC_ITEM, nullptr, 0, 0, 0, nullptr, nullptr, d_Bi, sBi};
+                {
+                    PROF("k_fwd_plane", st);
+                    ffb<<<dim3(bx, 6), 256, smf, st>>>(src, d_bases_in, g.p[1].tw, g.p[2].tw);
+                }
+                CKL();
+                CK(cudaMemsetAsync(d_smin, 0xff, sizeof(unsigned long long) * n, st));
+                CK(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long) * n, st));
+                CK(cudaMemsetAsync(d_bestkey, 0xff, sizeof(unsigned long long) * n, st));
+                CK(cudaMemsetAsync(d_diag, 0, sizeof(unsigned int) * n, st));
+                CK(cudaMemsetAsync(d_errmax, 0, sizeof(unsigned int) * n, st));
+                CK(cudaMemsetAsync(d_ncand, 0, sizeof(int) * n, st));
+                CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
+                return search_split(d_odb, n, score_params(mode), interlock, xf, p0, p1, sm3, d_out, true);
+            }
+        }
         int exmax = 1, maxpairs = 1;
         for (auto& o : ods)
             if (!o.skip) {
@@ -1073,13 +1177,7 @@ struct psb_tray {
         CK(cudaMemsetAsync(d_ncand, 0, sizeof(int) * n, st));
         CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
         ScoreParams sp = score_params(mode);
-        XpassFn xf = g_fast_fft ? xpass2_for(g.F[0]) : nullptr;
-        if (xf && xpass2_smem(g.F[0]) + 64 > (size_t)g_smem_optin) xf = nullptr;
-        if (g_fast_fft && g_plane_variant == 3) {
-            PlaneFn p0 = plane3_for(g.F[1], g.F[2], 0), p1 = plane3_for(g.F[1], g.F[2], 1);
-            const size_t sm3 = plane3_smem(g.F[1], g.F[2], ny) + 64;
-            if (p0 && p1 && sm3 <= (size_t)g_smem_optin) return search_split(d_odb, n, sp, interlock, xf, p0, p1, sm3, d_out);
-        }
+        if (p0) return search_split(d_odb, n, sp, interlock, xf, p0, p1, sm3, d_out, false);
         PlaneFn pf = nullptr;
         size_t sm2 = 0;
         const int pthreads = PSB_PLANE_THREADS;
@@ -1106,7 +1204,7 @@ struct psb_tray {
                 PROF("k_xpass", st);
                 int ncols = g.F[1] * g.H;
                 xf<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, m), 256, xpass2_smem(g.F[0]), st>>>(
-                    odo, sbo, d_Socc, d_Sphi, ncols, g.p[0].tw, nullptr, 0);
+                    odo, sbo, d_Socc, d_Sphi, ncols, g.p[0].tw, nullptr, 0, BaseMap{0, 0, 0, nullptr, nullptr});
             } else {
                 PROF("k_xpass", st);
                 size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
@@ -1170,9 +1268,12 @@ struct psb_tray {
     int search(const std::vector<OrientDesc>& ods, int mode, bool interlock, std::vector<ResultDev>* res,
                bool lazy = true) {
         const int n = (int)ods.size();
-        TRY(ensure_slots(n));
-        CK(cudaMemcpyAsync(d_od, ods.data(), sizeof(OrientDesc) * n, cudaMemcpyHostToDevice, st));
-        TRY(search_async(d_od, ods, mode, interlock, d_res, lazy));
+        TRY(ensure_slots(std::max(n, 6)));
+        std::vector<OrientDesc> od2(ods), bases;
+        const bool share = make_bases(&od2, &bases);
+        CK(cudaMemcpyAsync(d_od, od2.data(), sizeof(OrientDesc) * n, cudaMemcpyHostToDevice, st));
+        if (share) CK(cudaMemcpyAsync(d_bases, bases.data(), sizeof(OrientDesc) * 6, cudaMemcpyHostToDevice, st));
+        TRY(search_async(d_od, od2, mode, interlock, d_res, lazy, share ? d_bases : nullptr, share ? &bases : nullptr));
         res->resize(n);
         unsigned int herr = 0;
         CK(cudaMemcpyAsync(res->data(), d_res, sizeof(ResultDev) * n, cudaMemcpyDeviceToHost, st));
@@ -1957,18 +2058,38 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     t->staged.clear();
     t->staged_off.clear();
     t->staged_voff.clear();
-    size_t tot = 0, totv = 0;
-    t->staged.resize(n_items);
     for (int it = 0; it < n_items; ++it) {
-        int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
+        const int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
         if (!items[it] || ex <= 0 || ey <= 0 || ez <= 0) return fail(PSB_ERR_ARG, "item %d: bad array", it);
-        size_t m = (size_t)ex * ey * ez;
-        if (has_negative(items[it], m)) return fail(PSB_ERR_ARG, "item %d holds negative values", it);
-        analyse_item(items[it], ex, ey, ez, &t->staged[it]);
+    }
+    // item analysis (bounds, sums, voxel lists) on all host cores
+    t->staged.resize(n_items);
+    std::vector<char> neg(n_items, 0);
+    {
+        std::atomic<int> next(0);
+        auto work = [&]() {
+            for (int it = next.fetch_add(1); it < n_items; it = next.fetch_add(1)) {
+                const int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
+                const size_t m = (size_t)ex * ey * ez;
+                if (has_negative(items[it], m)) { neg[it] = 1; continue; }
+                analyse_item(items[it], ex, ey, ez, &t->staged[it]);
+            }
+        };
+        const int nthr = std::max(1, std::min<int>(n_items / 8, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (int w = 1; w < nthr; ++w) pool.emplace_back(work);
+        work();
+        for (auto& th : pool) th.join();
+    }
+    for (int it = 0; it < n_items; ++it)
+        if (neg[it]) return fail(PSB_ERR_ARG, "item %d holds negative values", it);
+    size_t tot = 0, totv = 0;
+    for (int it = 0; it < n_items; ++it) {
+        const ItemInfo& inf = t->staged[it];
         t->staged_off.push_back(tot);
         t->staged_voff.push_back(totv);
-        tot += m;
-        totv += t->staged[it].vox.size();
+        tot += (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
+        totv += inf.vox.size();
     }
     if (tot > t->stage_cap) {
         dfree(t->d_stage, t->st);
@@ -1980,15 +2101,25 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
         t->stage_vcap = totv;
         TRY(dalloc(&t->d_stage_vox, totv, t->st));
     }
+    // one pinned staging buffer for the item arrays and voxel lists: two
+    // large copies instead of two small pageable ones per item
+    const size_t bytes = sizeof(int32_t) * tot + sizeof(int4) * totv;
+    if (bytes > t->h_stage_cap) {
+        if (t->h_stage) cudaFreeHost(t->h_stage);
+        t->h_stage = nullptr;
+        t->h_stage_cap = 0;
+        CK(cudaMallocHost(&t->h_stage, bytes));
+        t->h_stage_cap = bytes;
+    }
+    int32_t* hi = (int32_t*)t->h_stage;
+    int4* hv = (int4*)(hi + tot);
     for (int it = 0; it < n_items; ++it) {
         const ItemInfo& inf = t->staged[it];
-        size_t m = (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
-        CK(cudaMemcpyAsync(t->d_stage + t->staged_off[it], items[it], sizeof(int32_t) * m, cudaMemcpyHostToDevice,
-                           t->st));
-        if (!inf.vox.empty())
-            CK(cudaMemcpyAsync(t->d_stage_vox + t->staged_voff[it], inf.vox.data(), sizeof(int4) * inf.vox.size(),
-                               cudaMemcpyHostToDevice, t->st));
+        memcpy(hi + t->staged_off[it], items[it], sizeof(int32_t) * inf.dims[0] * inf.dims[1] * inf.dims[2]);
+        if (!inf.vox.empty()) memcpy(hv + t->staged_voff[it], inf.vox.data(), sizeof(int4) * inf.vox.size());
     }
+    if (tot) CK(cudaMemcpyAsync(t->d_stage, hi, sizeof(int32_t) * tot, cudaMemcpyHostToDevice, t->st));
+    if (totv) CK(cudaMemcpyAsync(t->d_stage_vox, hv, sizeof(int4) * totv, cudaMemcpyHostToDevice, t->st));
     CK(cudaStreamSynchronize(t->st));
     return PSB_OK;
 }
@@ -2062,7 +2193,9 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         if (final_tray) TRY(psb_tray_get(t, final_tray, nullptr));
         return PSB_OK;
     }
-    TRY(t->ensure_slots(n_orient));
+    // slots for the orientations and the item's 6 permutation bases; reserved
+    // here, before any slot pointer (d_res ...) is handed to a search
+    TRY(t->ensure_slots(std::max(n_orient, 6)));
     // every orientation of every item, described once (bounds, maps, sizes);
     // the error bounds are filled on the device by k_prep from the current
     // distance statistics
@@ -2072,11 +2205,26 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             t->describe(t->staged[it], orient_maps + 6 * o, orient_maps + 6 * o + 3,
                         t->d_stage + t->staged_off[it], t->d_stage_vox + t->staged_voff[it],
                         &all[(size_t)it * n_orient + o]);
+    // each item's 6 axis permutations (the flips of one share its spectrum)
+    std::vector<OrientDesc> allb((size_t)n_items * 6);
+    for (int it = 0; it < n_items; ++it) {
+        std::vector<OrientDesc> slice(all.begin() + (size_t)it * n_orient, all.begin() + (size_t)(it + 1) * n_orient);
+        std::vector<OrientDesc> b;
+        if (!make_bases(&slice, &b)) return fail(PSB_ERR_STATE, "item %d: orientations of different items", it);
+        std::copy(slice.begin(), slice.end(), all.begin() + (size_t)it * n_orient);
+        std::copy(b.begin(), b.end(), allb.begin() + (size_t)it * 6);
+    }
     if (all.size() > t->od_all_cap) {
         dfree(t->d_od_all, t->st);
         t->od_all_cap = all.size();
         TRY(dalloc(&t->d_od_all, t->od_all_cap, t->st));
     }
+    if (allb.size() > t->base_all_cap) {
+        dfree(t->d_base_all, t->st);
+        t->base_all_cap = allb.size();
+        TRY(dalloc(&t->d_base_all, t->base_all_cap, t->st));
+    }
+    CK(cudaMemcpyAsync(t->d_base_all, allb.data(), sizeof(OrientDesc) * allb.size(), cudaMemcpyHostToDevice, t->st));
     if ((size_t)n_items > t->dec_cap) {
         dfree(t->d_dec, t->st);
         t->dec_cap = n_items;
@@ -2182,7 +2330,9 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             }
             CKL();
         }
-        TRY(t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res));
+        std::vector<OrientDesc> hb(allb.begin() + (size_t)it * 6, allb.begin() + (size_t)(it + 1) * 6);
+        TRY(t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res, true, t->d_base_all + (size_t)it * 6,
+                            &hb));
         if (d_per)
             CK(cudaMemcpyAsync(d_per + (size_t)it * n_orient, t->d_res, sizeof(ResultDev) * n_orient,
                                cudaMemcpyDeviceToDevice, t->st));
@@ -2586,6 +2736,11 @@ int psb_voxelize_mesh(const float* tris, int ntri, int resolution, int32_t* out,
 
 int psb_set_fast_fft(int on) {
     g_fast_fft = on != 0;
+    return PSB_OK;
+}
+
+int psb_set_share_flips(int on) {
+    g_share_flips = on != 0;
     return PSB_OK;
 }
 

@@ -34,7 +34,7 @@ struct OrientDesc {
     const int32_t* item;      // device base item
     const int4* vox;          // device voxel list of the base item (x,y,z,value)
     int nvox;
-    int pad;
+    int perm;                 // index of its axis permutation among the item's 6 bases
     double sumsq;             // sum of squared item values
     long long sabs;           // sum of |item values|
 };

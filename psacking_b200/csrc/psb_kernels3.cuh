@@ -8,6 +8,28 @@
 
 #define PSB_XCOLS 16   // spectrum columns (ky*Hz + kz) per CTA in k_xpass2
 
+// ---------------------------------------------------------------------------
+// z,y transforms shared by the flips of one axis permutation
+// ---------------------------------------------------------------------------
+// The 24 orientations are 6 axis permutations x 4 sign patterns.  After the z
+// and y transforms, x is still in real space: with I_p the permuted
+// (unflipped) item and flips x_a -> e_a - 1 - x_a,
+//   G_o(x, ky, kz) = phase(ky, kz) * G_p(x', ky', kz')     (conjugated if z is flipped)
+// where x' = e_x - 1 - x on an x flip (a row reversal, no phase), and for the
+// half spectrum in z (real slices are Hermitian in (ky, kz)):
+//   z not flipped: ky' = -ky on a y flip, kz' = kz;
+//   z flipped:     ky' = -ky unless y is flipped too, kz' = kz, conjugate;
+//   phase = W_y^(ky (e_y - 1)) on a y flip * W_z^(kz (e_z - 1)) on a z flip,
+// W = exp(-2 pi i / F).  So k_fwd_plane runs once per permutation and the x
+// pass reads each orientation's slabs from its permutation's ("base" slots
+// 0..5 of the slab buffer).
+struct BaseMap {
+    int Fy, Hz, Fz;
+    const float2* twy;        // exp(-2 pi i n / Fy), n < Fy
+    const float2* twz;        // exp(-2 pi i n / Fz), n < Fz
+};
+
+
 // Fused x pass over a tile of PSB_XCOLS consecutive columns c = ky*Hz + kz
 // (contiguous in memory, so every row access of the tile is one 128-byte
 // segment): item forward along x (pass 1 reads global), products with the
@@ -18,11 +40,11 @@
 //   MODE 2: the proximity product only (Pd), for orientations with an ok
 //           plane (okplane, see k_plane3), and stored only on those planes
 // grid: (ceil(Fy*Hz / PSB_XCOLS), n_orient), block 256
-template <int N, int MODE>
+template <int N, int MODE, bool SHARED>
 __global__ void __launch_bounds__(256)
 k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __restrict__ Socc,
          const float2* __restrict__ Sphi, int ncols, const float2* __restrict__ g_tw,
-         const unsigned char* __restrict__ okplane, long long okstride) {
+         const unsigned char* __restrict__ okplane, long long okstride, BaseMap bm) {
     constexpr int C = PSB_XCOLS;
     constexpr int R0 = Plan2<N>::R0, R1 = Plan2<N>::R1;
     extern __shared__ float2 sm[];
@@ -47,14 +69,38 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
         if (!__syncthreads_or(any)) return;
     }
     load_twiddles(tw, g_tw, N, tid, nthr);
+    __shared__ int srccol[C];
+    __shared__ float2 colph[C];
+    const int sx = SHARED ? od.flip[0] : 0, sy = SHARED ? od.flip[1] : 0, sz = SHARED ? od.flip[2] : 0;
+    if (SHARED && tid < C) {
+        const int c = c0 + tid;
+        int sc = c;
+        float2 ph = make_float2(1.f, 0.f);
+        if (tid < nl) {
+            const int ky = c / bm.Hz, kz = c - (c / bm.Hz) * bm.Hz;
+            const int kys = (sy != sz) ? (ky == 0 ? 0 : bm.Fy - ky) : ky;
+            sc = kys * bm.Hz + kz;
+            if (sy) ph = c_mul(ph, bm.twy[(int)(((long long)ky * (od.e[1] - 1)) % bm.Fy)]);
+            if (sz) ph = c_mul(ph, bm.twz[(int)(((long long)kz * (od.e[2] - 1)) % bm.Fz)]);
+        }
+        srccol[tid] = sc - c0;
+        colph[tid] = ph;
+    }
     __syncthreads();
-    const float2* Bi = sb.Bi + (size_t)o * sb.sB + c0;
+    // the orientation's own slabs, or its permutation's (SHARED)
+    const float2* Bi = sb.Bi + (size_t)(SHARED ? od.perm : o) * sb.sB + c0;
     float2* Pc = sb.Pc + (size_t)o * sb.sP + c0;
     float2* Pd = sb.Pd + (size_t)o * sb.sP + c0;
     const float2* So = Socc + c0;
     const float2* Sp = Sphi + c0;
     tpass<N, R0, 1, -1, C, false>(
-        [&](int c, int n) { return n < ex ? Bi[(size_t)n * ncols + c] : make_float2(0.f, 0.f); },
+        [&](int c, int n) {
+            if (n >= ex) return make_float2(0.f, 0.f);
+            if (!SHARED) return Bi[(size_t)n * ncols + c];
+            float2 v = Bi[(size_t)(sx ? ex - 1 - n : n) * ncols + srccol[c]];
+            if (sz) v.y = -v.y;
+            return c_mul(v, colph[c]);
+        },
         [&](int c, int n, float2 v) { A[n * C + c] = v; }, nl, tw, tid, nthr);
     __syncthreads();
     tpass<N, R1, R0, -1, C, false>([&](int c, int n) { return A[n * C + c]; },

@@ -114,9 +114,9 @@ class BinPacker:
                 raise ValueError(f"Item {i} is not a numpy array")
             if item.ndim != 3:
                 raise ValueError(f"Item {i} must be 3D, got {item.ndim}D")
-            it = item.astype(np.int32)
+            it = np.asarray(item, dtype=np.int32)   # no copy when already int32
             processed.append(it)
-            volumes.append(int(np.sum(it > 0)))
+            volumes.append(int(np.count_nonzero(it > 0)))
         if sort_by_volume:
             order = list(np.argsort(volumes)[::-1])
         else:

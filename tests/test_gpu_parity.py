@@ -181,13 +181,15 @@ def test_caged_interlock_search(gpu_core, hole, variant):
     assert (tuple(got[0]), got[1], got[2], got[3]) == (tuple(want[0]), want[1], want[2], want[3])
 
 
-@pytest.fixture(params=["fast", "plane2", "generic"])
+@pytest.fixture(params=["fast", "share", "plane2", "generic"])
 def fft_variant(request, gpu_core):
     gpu_core.set_fast_fft(request.param != "generic")
     gpu_core.set_plane_variant(2 if request.param == "plane2" else 3)
+    gpu_core.set_share_flips(request.param == "share")
     yield request.param
     gpu_core.set_fast_fft(True)
     gpu_core.set_plane_variant(3)
+    gpu_core.set_share_flips(False)
 
 
 def test_search_config3_scale(gpu_core, fft_variant):
