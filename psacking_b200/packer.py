@@ -251,12 +251,17 @@ class BinPacker:
 
     def _calculate_stats(self, tray: np.ndarray):
         """packer.py:582-601: density = occupied / bounding-box volume."""
-        occupied = int(np.sum(tray > 0))
+        occ = tray > 0
+        occupied = int(np.count_nonzero(occ))
         if occupied == 0:
             return 0.0, 0, None
-        idx = np.argwhere(tray > 0)
-        lo = tuple(idx.min(axis=0).tolist())
-        hi = tuple(idx.max(axis=0).tolist())
+        # bounding box from per-axis projections (no coordinate list)
+        lo, hi = [], []
+        for axes in ((1, 2), (0, 2), (0, 1)):
+            nz = np.flatnonzero(occ.any(axis=axes))
+            lo.append(int(nz[0]))
+            hi.append(int(nz[-1]))
+        lo, hi = tuple(lo), tuple(hi)
         vol = int(np.prod([b - a + 1 for a, b in zip(lo, hi)]))
         return (float(occupied / vol) if vol > 0 else 0.0), occupied, (lo, hi)
 

@@ -338,3 +338,24 @@ def test_pack_many_matches_single_runs(gpu_core):
             assert np.array_equal(r.tray, one.tray)
             assert [(q.position, q.orientation_index, q.score) for q in r.placements] == \
                    [(q.position, q.orientation_index, q.score) for q in one.placements]
+
+
+# --------------------------------------------------------------------------
+# orientation sharding of one tray (one rank here: the same code path that
+# several ranks run, with the decision exchange reduced to the identity)
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("cfg", ["config2", "config3"])
+def test_orientation_sharded_packing_matches(gpu_core, cfg):
+    from psacking_b200 import BinPacker, workloads
+    from psacking_b200.shard import pack_orientation_sharded
+    if cfg == "config2":
+        items, tray, n, inter = workloads.config2_items(11)[:8], (96, 96, 96), 24, False
+    else:
+        items, tray, n, inter = workloads.config3_items(12)[:4], workloads.TRAY3, 24, True
+    ref = BinPacker(tray, num_orientations=n, interlocking_free=inter).pack_voxels(items)
+    got_tray, got = pack_orientation_sharded(items, tray, n, inter)
+    assert np.array_equal(got_tray, ref.tray)
+    for p, g in zip(ref.placements, got):
+        assert (p.success, p.position, p.orientation_index) == (g[0], g[1], g[2] if g[0] else 0)
+        if p.success:
+            assert p.score == g[3]
