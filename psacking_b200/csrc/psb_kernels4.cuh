@@ -36,6 +36,11 @@ struct WarpLine {
     __device__ __forceinline__ static int fetch(int j2, int r) { return r * (R0 + 1) + j2; }
 };
 
+// Row stride of the y-inverted plane: HZ rounded up to 2 (mod 4) floats2, so
+// the y pass's stores (8 lanes per column, rows 16 apart, 4 columns per warp)
+// fall on distinct banks
+__host__ __device__ constexpr int plane3_row(int NZ) { return ((NZ / 2 + 1) + 1) / 4 * 4 + 2; }
+
 inline size_t plane3_smem(int NY, int NZ, int ny) {
     auto known = [](int N) { return N == 64 || N == 100 || N == 128; };
     if (!known(NY) || !known(NZ)) return 0;   // no specialised plan for these lengths
@@ -52,7 +57,7 @@ inline size_t plane3_smem(int NY, int NZ, int ny) {
     const size_t wy = ((HZ + per(NY) - 1) / per(NY)) * per(NY) * slab(NY);      // y pass: one slab per column
     const size_t wz = (size_t)(PSB_PLANE3_THREADS / 32) * per(NZ) * slab(NZ);   // z pass: per warp
     // the plane buffer also holds the per-warp per-z minima at the end
-    const size_t q = std::max((size_t)ny * HZ, (size_t)(PSB_PLANE3_THREADS / 32) * NZ / 2 + 1);
+    const size_t q = std::max((size_t)ny * plane3_row(NZ), (size_t)(PSB_PLANE3_THREADS / 32) * NZ / 2 + 1);
     return sizeof(float2) * (NY + NZ + std::max(wy, wz) + q);
 }
 
@@ -69,6 +74,7 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     using LY = WarpLine<NY>;
     using LZ = WarpLine<NZ>;
     constexpr int HZ = NZ / 2 + 1;
+    constexpr int HZP = plane3_row(NZ);   // row stride of Q (see plane3_row)
     constexpr int NZW = (NZ + 31) / 32;
     constexpr int NWARP = PSB_PLANE3_THREADS / 32;
     constexpr int WY = ((HZ + LY::PER - 1) / LY::PER) * LY::PER * LY::SLAB;
@@ -146,7 +152,7 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
 #pragma unroll
                 for (int r = 0; r < LY::R1; ++r) {
                     const int y = j2 + r * LY::R0;
-                    if (y < Yv) Q[y * HZ + c] = u[r];
+                    if (y < Yv) Q[y * HZP + c] = u[r];
                 }
             }
         }
@@ -166,12 +172,12 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
             for (int r = 0; r < LZ::R0; ++r) {
                 const int k = zj + r * LZ::L;
                 if (k < HZ) {
-                    const float2 xa = Q[ya * HZ + k];
-                    const float2 xb = hb ? Q[yb * HZ + k] : make_float2(0.f, 0.f);
+                    const float2 xa = Q[ya * HZP + k];
+                    const float2 xb = hb ? Q[yb * HZP + k] : make_float2(0.f, 0.f);
                     v[r] = make_float2(xa.x - xb.y, xa.y + xb.x);
                 } else {
-                    const float2 xa = Q[ya * HZ + (NZ - k)];
-                    const float2 xb = hb ? Q[yb * HZ + (NZ - k)] : make_float2(0.f, 0.f);
+                    const float2 xa = Q[ya * HZP + (NZ - k)];
+                    const float2 xb = hb ? Q[yb * HZP + (NZ - k)] : make_float2(0.f, 0.f);
                     v[r] = make_float2(xa.x + xb.y, xb.x - xa.y);
                 }
             }
