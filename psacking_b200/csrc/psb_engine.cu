@@ -975,19 +975,10 @@ struct psb_tray {
         const int lines = nx * ny;
         const int nblk = (lines + 255) / 256;
         const dim3 gl(nblk, n);
+        CK(cudaMemsetAsync(d_total, 0, sizeof(int) * n, st));
         {
-            PROF("k_ff_count", st);
-            k_ff_count<<<gl, 256, 0, st>>>(d_odb, fb, sp, d_blk, nblk);
-        }
-        CKL();
-        {
-            PROF("k_ff_scan", st);
-            k_ff_scan<<<n, 32, 0, st>>>(d_odb, fb, d_blk, nblk);
-        }
-        CKL();
-        {
-            PROF("k_ff_emit", st);
-            k_ff_emit<<<gl, 256, 0, st>>>(d_odb, fb, sp, d_blk, nblk);
+            PROF("k_ff_runs", st);
+            k_ff_runs<<<gl, 256, 0, st>>>(d_odb, fb, sp);
         }
         CKL();
         {
@@ -1862,17 +1853,10 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
     int lines = nx * ny;
     const int nblk = (lines + 255) / 256;
     dim3 gl(nblk, 1);
+    CK(cudaMemsetAsync(t->d_total, 0, sizeof(int), t->st));
     {
-        PROF("k_ff_count", t->st);
-        k_ff_count<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp, t->d_blk, nblk);
-    }
-    {
-        PROF("k_ff_scan", t->st);
-        k_ff_scan<<<1, 32, 0, t->st>>>(t->d_od, fb, t->d_blk, nblk);
-    }
-    {
-        PROF("k_ff_emit", t->st);
-        k_ff_emit<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp, t->d_blk, nblk);
+        PROF("k_ff_runs", t->st);
+        k_ff_runs<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
     }
     {
         PROF("k_ff_union", t->st);

@@ -466,92 +466,48 @@ __device__ __forceinline__ uint32_t run_starts(const uint32_t* w, int i, uint32_
     return cur & ~((cur << 1) | prevtop);
 }
 
-// Per line: its number of z-runs.  Per 256-line block: the block's total
-// (blk[o][b]).  grid: (ceil(nx*ny/256), n_orient), block 256
-__global__ void __launch_bounds__(256)
-k_ff_count(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, int* __restrict__ blk, int nblk) {
-    if (fb.gate && !*fb.gate) return;
-    const int o = blockIdx.y;
-    const OrientDesc& od = orients[o];
-    const int line = blockIdx.x * blockDim.x + threadIdx.x;
-    int c = 0;
-    if (!od.skip && line < sp.nx * sp.ny) {
-        int x = line / sp.ny, y = line - x * sp.ny;
-        if (x < od.valid[0] && y < od.valid[1]) {
-            const uint32_t* w = fb.freebits + (size_t)o * fb.sBits + (size_t)line * sp.nzw;
-            uint32_t prevtop = 0;
-            for (int i = 0; i < sp.nzw; ++i) {
-                c += __popc(run_starts(w, i, prevtop));
-                prevtop = w[i] >> 31;
-            }
-        }
-    }
-    if (line < sp.nx * sp.ny) fb.cnt[(size_t)o * fb.sLine + line] = c;
-    c = __reduce_add_sync(0xffffffffu, c);
-    __shared__ int ws[8];
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int t = 0;
-        for (int i = 0; i < 8; ++i) t += ws[i];
-        blk[(size_t)o * nblk + blockIdx.x] = t;
-    }
-}
-
-// Exclusive scan of the block totals of one orientation (one warp per
-// orientation); total runs in fb.total.  grid: (n_orient), block 32
-__global__ void k_ff_scan(const OrientDesc* __restrict__ orients, FloodBufs fb, int* __restrict__ blk, int nblk) {
-    if (fb.gate && !*fb.gate) return;
-    const int o = blockIdx.x;
-    if (orients[o].skip) return;
-    int* b = blk + (size_t)o * nblk;
-    const int lane = threadIdx.x;
-    int carry = 0;
-    for (int base = 0; base < nblk; base += 32) {
-        const int i = base + lane;
-        const int v = i < nblk ? b[i] : 0;
-        int incl = v;
-        for (int d = 1; d < 32; d <<= 1) {
-            int u = __shfl_up_sync(0xffffffffu, incl, d);
-            if (lane >= d) incl += u;
-        }
-        if (i < nblk) b[i] = carry + incl - v;
-        carry += __shfl_sync(0xffffffffu, incl, 31);
-    }
-    if (lane == 0) fb.total[o] = carry;
-}
-
-// Per line: its offset (block prefix + scan inside the block) and its runs,
-// found by bit scanning (one step per run, not per z).
+// Per line (x, y): its free z-runs.  The line's slots are reserved with one
+// atomicAdd per warp on the orientation's run counter (total, zeroed first),
+// so the run order differs from launch to launch; reachability does not
+// depend on it.  Writes cnt/off per line and, per run, (z0 | z1 << 16), its
+// line, itself as parent and the seed flag (runs on the seed faces).
 // grid: (ceil(nx*ny/256), n_orient), block 256
 __global__ void __launch_bounds__(256)
-k_ff_emit(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, const int* __restrict__ blk, int nblk) {
+k_ff_runs(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
     if (fb.gate && !*fb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
     const int line = blockIdx.x * blockDim.x + threadIdx.x;
     const bool inl = line < sp.nx * sp.ny;
-    const int c = inl ? fb.cnt[(size_t)o * fb.sLine + line] : 0;
-    // block-level exclusive scan of c
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int x = inl ? line / sp.ny : 0, y = inl ? line - x * sp.ny : 0;
+    const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
+    const bool act = inl && x < Xv && y < Yv;
+    const int nzw = sp.nzw;
+    const uint32_t* w = fb.freebits + (size_t)o * fb.sBits + (size_t)line * nzw;
+    int c = 0;
+    if (act) {
+        uint32_t prevtop = 0;
+        for (int i = 0; i < nzw; ++i) {
+            c += __popc(run_starts(w, i, prevtop));
+            prevtop = w[i] >> 31;
+        }
+    }
+    // warp-aggregated reservation
+    const int lane = threadIdx.x & 31;
     int incl = c;
     for (int d = 1; d < 32; d <<= 1) {
-        int u = __shfl_up_sync(0xffffffffu, incl, d);
+        const int u = __shfl_up_sync(0xffffffffu, incl, d);
         if (lane >= d) incl += u;
     }
-    __shared__ int ws[8];
-    if (lane == 31) ws[wid] = incl;
-    __syncthreads();
-    int wpre = 0;
-    for (int i = 0; i < wid; ++i) wpre += ws[i];
-    int r = blk[(size_t)o * nblk + blockIdx.x] + wpre + incl - c;
+    int base = 0;
+    if (lane == 31 && incl > 0) base = atomicAdd(&fb.total[o], incl);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    int r = base + incl - c;
     if (!inl) return;
+    fb.cnt[(size_t)o * fb.sLine + line] = c;
     fb.off[(size_t)o * fb.sLine + line] = r;
     if (c == 0) return;
-    int x = line / sp.ny, y = line - x * sp.ny;
-    const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
-    const uint32_t* w = fb.freebits + (size_t)o * fb.sBits + (size_t)line * sp.nzw;
     const bool side = (x == 0) || (y == 0) || (od.hi[0] >= 0 && x == Xv - 1) || (od.hi[1] >= 0 && y == Yv - 1);
     int* rz = fb.rz + (size_t)o * fb.sRun;
     int* rl = fb.rline + (size_t)o * fb.sRun;
@@ -559,7 +515,6 @@ k_ff_emit(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, 
     int* fl = fb.rflag + (size_t)o * fb.sRun;
     // walk runs: start = first set bit at or after z, end = first clear bit after it
     int z = 0;
-    const int nzw = sp.nzw;
     while (z < Zv) {
         int wi = z >> 5;
         uint32_t m = w[wi] & (0xffffffffu << (z & 31));
@@ -567,7 +522,6 @@ k_ff_emit(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp, 
         if (!m) break;
         const int z0 = (wi << 5) + __ffs(m) - 1;
         if (z0 >= Zv) break;
-        // first zero at or after z0
         int wj = z0 >> 5;
         uint32_t inv = ~w[wj] & (0xffffffffu << (z0 & 31));
         while (!inv && ++wj < nzw) inv = ~w[wj];
