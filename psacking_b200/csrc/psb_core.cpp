@@ -452,6 +452,18 @@ int py_device_count() {
     return n;
 }
 
+// bindings.cpp:285-302 and 304-313: the STL reader and the .vox encoder live
+// in the package's Python modules (psacking_b200.voxelize, psacking_b200.vox);
+// the rasterization itself is psb_voxelize_mesh.  These keep the module's
+// export list equal to the reference's.
+py::object py_voxelize_stl(py::object path, int resolution) {
+    return py::module_::import("psacking_b200.voxelize").attr("voxelize_stl")(path, resolution);
+}
+
+void py_save_vox(py::object grid, py::object path) {
+    py::module_::import("psacking_b200.vox").attr("save_vox")(grid, path);
+}
+
 }  // namespace
 
 PYBIND11_MODULE(_core, m) {
@@ -486,6 +498,10 @@ PYBIND11_MODULE(_core, m) {
           "searches run the flood fill for all of them); False: only the best (lazy flood fill).");
     m.def("pack_many", &py_pack_many, py::arg("trays"), py::arg("orient_maps"), py::arg("interlock"),
           py::arg("concurrency") = 8);
+    m.def("voxelize_stl", &py_voxelize_stl, py::arg("path"), py::arg("resolution") = 128,
+          "Surface voxels of an STL mesh, tight int32 grid (GPU rasterizer).");
+    m.def("save_vox", &py_save_vox, py::arg("grid"), py::arg("path"),
+          "Save a voxel grid in the reference's .vox layout.");
     m.def("device_count", &py_device_count);
     m.def("set_fast_fft", [](bool on) { psb_set_fast_fft(on ? 1 : 0); }, py::arg("on"),
           "Use the specialised two-pass FFT kernels where a plan exists (default) or force the generic path.");

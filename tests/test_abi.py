@@ -17,6 +17,7 @@ REFERENCE_EXPORTS = [  # spectral_packing/bindings.cpp:681-924
     "dft_corr3", "calculate_distance", "collision_grid", "make_tight", "get_bounds",
     "gpu_tray_init", "gpu_tray_cleanup", "gpu_tray_is_initialized", "gpu_tray_search",
     "fft_search_batch", "fft_search_batch_interlocking_free", "interlocking_free_positions",
+    "voxelize_stl", "save_vox",
 ]
 
 
@@ -49,6 +50,15 @@ def test_core_module_mirrors_reference(core):
     import psacking_b200 as p
     for name in REFERENCE_EXPORTS + ["save_vox", "voxelize_stl", "BinPacker"]:
         assert hasattr(p, name), name
+
+
+def test_core_save_vox_writes_the_package_encoding(core, tmp_path):
+    from psacking_b200.vox import encode_vox
+    g = np.zeros((3, 4, 5), np.int32)
+    g[0, 1, 2] = 1
+    g[2, 3, 4] = 8
+    core.save_vox(g, str(tmp_path / "a.vox"))
+    assert (tmp_path / "a.vox").read_bytes() == encode_vox(g)
 
 
 def test_wrong_dimensions_raise(core):

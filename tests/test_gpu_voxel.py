@@ -39,5 +39,6 @@ def test_voxelize_stl_files(gpu_core, tmp_path):
     gb = p.voxelize_stl(str(b), 40)
     ga = p.voxelize_stl(str(a), 40)
     assert np.array_equal(gb, ga) and np.array_equal(gb, V.voxelize(tris, 40))
+    assert np.array_equal(gpu_core.voxelize_stl(str(b), 40), gb)   # the drop-in module's export
     with pytest.raises(RuntimeError, match="Voxelization failed"):
         p.voxelize_stl(str(tmp_path / "missing.stl"), 32)
