@@ -310,11 +310,10 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FFT), i64/f64 (exact tie guard)",
         "data": "synthetic (seeded config-3 shapes; Thingi10K unavailable)",
         "config": {"workload": f"config3: 240x123x100 tray, {args.items} items (extent 20-50), 24 orientations, "
-                               "interlocking-free (lazy flood fill), K=1",
+                               "interlocking-free (flood fill on every searched item), K=1",
                    "items_per_step": len(seq), "items_placed_per_step": placed, "orientations_per_step": ab["orientations"],
                    "l2": "256 MiB buffer written before every step", "parallelism": f"replicas x{world} (independent trays)",
                    "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag,
-                   "flood_fill_items": sum(1 for r in res if r.diag & 0x400),
                    "tie_guard": {"candidates_per_item_mean": round(statistics.mean(cands), 1),
                                  "candidates_per_item_max": max(cands),
                                  "max_fp32_error_over_bound": round(err_ratio, 4)}},

@@ -1,0 +1,337 @@
+// psb_filter.cuh — exact pre-filter of the collision search.
+//
+// A translation t is collision-free only if every voxel of the item lands on
+// an empty tray cell (packing.cpp:254-270 counts overlaps; with non-negative
+// item values and the binary occupancy a zero count means no overlap).  So
+// the translations where a SUBSET S of the item's voxels lands on empty cells
+// are a superset of the free ones.  With S a spread sample of up to
+// PSB_FSAMP voxels this superset ("candidates") is computed with bit
+// operations on a bit-packed copy of the tray: for each (x, y) column of
+// translations and all z at once, AND over s in S of the tray's free bits of
+// column (x + s.x, y + s.y) shifted down by s.z.  Nothing here guesses: an
+// orientation without any candidate has no free translation (its search is
+// skipped: not found, as the full search would say), and a plane without
+// candidates holds no free cell (the collision plane pass leaves its zero
+// words and skips it).  Every other cell is decided exactly: by the FFT
+// collision count, or, for an orientation left with few candidates (at most
+// the direct limit), by a direct check of each candidate against the item's
+// voxel columns (k_cand_verify); such a "direct" orientation also gets its
+// proximity as exact integer sums over the item's voxels (k_direct_score)
+// and needs no transform at all.
+#pragma once
+#include "psb_kernels2.cuh"
+#include "psb_loop.cuh"
+
+#define PSB_FSAMP 128          // sample voxels per item
+#define PSB_FILT_THREADS 128   // translations (y) per CTA row
+#define PSB_FBATCH 8           // filter samples whose loads are issued together
+
+// Free bits of the tray: tbits[(i*ny + j)*nq + q] holds z in [128q, 128q+128),
+// bit set when the cell is empty; bits at z >= nz are clear (not free).
+// One warp per column, one ballot per 32 cells.  grid: ceil(nx*ny / 8), block 256
+__global__ void k_tray_bits(const int32_t* __restrict__ tray, int nx, int ny, int nz, int nq,
+                            uint4* __restrict__ tbits) {
+    const int col = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (col >= nx * ny) return;
+    const int32_t* t = tray + (size_t)col * nz;
+    uint32_t* out = (uint32_t*)(tbits + (size_t)col * nq);
+    for (int w = 0; w < 4 * nq; ++w) {
+        const int z = 32 * w + lane;
+        const unsigned int b = __ballot_sync(0xffffffffu, z < nz && t[z] == 0);
+        if (lane == 0) out[w] = b;
+    }
+}
+
+// After a placement only the tray columns under the placed item's box
+// change: refresh those (gated on ls->placed_now; the chosen orientation and
+// position come from the loop state).  grid: ceil(max box columns / 8), block 256
+__global__ void k_tray_bits_box(const int32_t* __restrict__ tray, int nx, int ny, int nz, int nq,
+                                uint4* __restrict__ tbits, const LoopState* __restrict__ ls,
+                                const OrientDesc* __restrict__ od_item) {
+    if (!ls->placed_now) return;
+    const OrientDesc& od = od_item[ls->orient];
+    const int by = od.e[1];
+    const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k >= od.e[0] * by) return;
+    const int i = ls->px + k / by, j = ls->py + k % by;
+    if (i < 0 || j < 0 || i >= nx || j >= ny) return;
+    const int32_t* t = tray + ((size_t)i * ny + j) * nz;
+    uint32_t* out = (uint32_t*)(tbits + ((size_t)i * ny + j) * nq);
+    for (int w = 0; w < 4 * nq; ++w) {
+        const int z = 32 * w + lane;
+        const unsigned int b = __ballot_sync(0xffffffffu, z < nz && t[z] == 0);
+        if (lane == 0) out[w] = b;
+    }
+}
+
+__device__ __forceinline__ uint32_t low_bits(int n) { return n >= 32 ? 0xffffffffu : (n <= 0 ? 0u : (1u << n) - 1u); }
+
+// Candidate words of one x plane of one orientation: for rows y < Yv, the
+// words cand[(x*ny + y)*nzw + w] (the free-bit layout of the search, so the
+// collision pass can refine them in place), candplane[o][x] = "the plane
+// holds a candidate", and the orientation's candidate count.  Samples are
+// sorted by their word shift s.z / 32 so every shift is a compile-time
+// register index; lanes of a warp share the sample; loads go in batches; a
+// warp stops once none of its lanes holds a candidate.
+// grid: (max Xv, n_orient), block PSB_FILT_THREADS
+template <int NQ>
+__global__ void __launch_bounds__(PSB_FILT_THREADS)
+k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ tbits, int ny, int nzw,
+              uint32_t* __restrict__ cand, long long sBits, unsigned char* __restrict__ candplane, long long pstride,
+              int* __restrict__ ccount) {
+    constexpr int NW = 4 * NQ;
+    const int o = blockIdx.y, x = blockIdx.x;
+    const OrientDesc& od = orients[o];
+    if (od.skip || od.nsamp <= 0) return;
+    const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
+    if (x >= Xv || Yv <= 0 || Zv <= 0) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ int3 S[PSB_FSAMP];
+    __shared__ int bound[NW + 1];   // samples with shift k are S[bound[k] .. bound[k+1])
+    const int ns = min(od.nsamp, PSB_FSAMP);
+    if (warp == 0) {
+        int base = 0;
+        for (int k = 0; k < NW; ++k) {
+            if (lane == 0) bound[k] = base;
+            for (int s0 = 0; s0 < ns; s0 += 32) {
+                const int s = s0 + lane;
+                int c[3] = {0, 0, 0};
+                if (s < ns) {
+                    const int4 v = od.samp[s];
+                    orient_voxel(od, v.x, v.y, v.z, c);
+                }
+                const bool hit = s < ns && (c[2] >> 5) == k;
+                const unsigned int b = __ballot_sync(0xffffffffu, hit);
+                if (hit) S[base + __popc(b & ((1u << lane) - 1u))] = make_int3(c[0], c[1], c[2]);
+                base += __popc(b);
+            }
+        }
+        if (lane == 0) bound[NW] = base;
+    }
+    __syncthreads();
+    uint32_t* cw = cand + (size_t)o * sBits + (size_t)x * ny * nzw;
+    int any = 0, cnt = 0;
+    for (int y0 = warp * 32; y0 < Yv; y0 += PSB_FILT_THREADS) {
+        const int y = y0 + lane;
+        const bool act = y < Yv;
+        uint32_t c[NW];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) c[w] = act ? low_bits(Zv - 32 * w) : 0u;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            // shift of k whole words: word w of the shifted column is
+            // funnel(T[w + k], T[w + k + 1]) >> (s.z & 31)
+            const int s1 = bound[k + 1];
+            for (int s0 = bound[k]; s0 < s1; s0 += PSB_FBATCH) {
+                uint32_t a = 0u;
+#pragma unroll
+                for (int w = 0; w < NW; ++w) a |= c[w];
+                if (!__any_sync(0xffffffffu, a != 0u)) break;
+                uint4 v[PSB_FBATCH][NQ];
+                int off[PSB_FBATCH];
+#pragma unroll
+                for (int i = 0; i < PSB_FBATCH; ++i) {
+                    off[i] = 0;
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) v[i][q] = make_uint4(0u, 0u, 0u, 0u);
+                    if (s0 + i < s1) {
+                        const int3 p = S[s0 + i];
+                        off[i] = p.z & 31;
+                        if (act) {
+                            const uint4* col = tbits + ((size_t)(x + p.x) * ny + (y + p.y)) * NQ;
+#pragma unroll
+                            for (int q = 0; q < NQ; ++q) v[i][q] = __ldg(col + q);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < PSB_FBATCH; ++i) {
+                    if (s0 + i >= s1) break;
+                    uint32_t T[NW];
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) {
+                        T[4 * q] = v[i][q].x;
+                        T[4 * q + 1] = v[i][q].y;
+                        T[4 * q + 2] = v[i][q].z;
+                        T[4 * q + 3] = v[i][q].w;
+                    }
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) {
+                        const uint32_t lo = (w + k < NW) ? T[w + k] : 0u;
+                        const uint32_t hi = (w + k + 1 < NW) ? T[w + k + 1] : 0u;
+                        c[w] &= __funnelshift_r(lo, hi, off[i]);
+                    }
+                }
+            }
+        }
+        if (act) {
+#pragma unroll
+            for (int w = 0; w < NW; ++w)
+                if (w < nzw) {
+                    cw[(size_t)y * nzw + w] = c[w];
+                    any |= c[w] != 0u;
+                    cnt += __popc(c[w]);
+                }
+        }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
+    if (lane == 0 && cnt) atomicAdd(&ccount[o], cnt);
+    any = __syncthreads_or(any);
+    if (tid == 0) candplane[(size_t)o * pstride + x] = any ? 1 : 0;
+}
+
+// Stage 0 (after k_cand_filter, count = candidates): an orientation without
+// a candidate is skipped; one with at most direct_max candidates and an item
+// at most 64 cells high (two mask words per column) becomes direct.
+// Stage 1 (after k_cand_verify, count = verified free cells): a direct
+// orientation without a free cell is skipped.  grid: ceil(n / 128), block 128
+__global__ void k_cand_apply(OrientDesc* __restrict__ orients, int n, const int* __restrict__ count, int stage,
+                             int direct_max) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    OrientDesc& od = orients[o];
+    if (od.skip || od.nsamp <= 0) return;
+    if (stage == 0) {
+        if (count[o] == 0) od.skip = 1;
+        else if (count[o] <= direct_max && od.e[2] <= 64) od.direct = 1;
+    } else if (od.direct && count[o] == 0) {
+        od.skip = 1;
+    }
+}
+
+// Column masks of a direct orientation's item: for each (a, b) holding a
+// positive voxel, {a | b << 16, bits of c < 32, bits of 32 <= c < 64} in
+// cols[o][k], k < ncol[o] (any order).  grid: (max e[0], n), block 64
+__global__ void k_item_cols(const OrientDesc* __restrict__ orients, uint4* __restrict__ cols, long long cstride,
+                            int* __restrict__ ncol) {
+    const int o = blockIdx.y, a = blockIdx.x;
+    const OrientDesc& od = orients[o];
+    if (od.skip || !od.direct || a >= od.e[0]) return;
+    const int lane = threadIdx.x & 31;
+    for (int b0 = 0; b0 < od.e[1]; b0 += blockDim.x) {
+        const int b = b0 + threadIdx.x;
+        uint32_t m0 = 0u, m1 = 0u;
+        if (b < od.e[1])
+            for (int c = 0; c < od.e[2]; ++c)
+                if (__ldg(&od.item[orient_src_index(od, a, b, c)]) > 0) {
+                    if (c < 32) m0 |= 1u << c;
+                    else m1 |= 1u << (c - 32);
+                }
+        const bool has = (m0 | m1) != 0u;
+        const unsigned int bal = __ballot_sync(0xffffffffu, has);
+        int slot = 0;
+        if (lane == 0 && bal) slot = atomicAdd(&ncol[o], __popc(bal));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (has)
+            cols[(size_t)o * cstride + slot + __popc(bal & ((1u << lane) - 1u))] =
+                make_uint4((uint32_t)a | ((uint32_t)b << 16), m0, m1, 0u);
+    }
+}
+
+// Exact collision check of every candidate of a direct orientation: the
+// translation (x, y, z) is free when no item column (a, b) meets an occupied
+// cell of tray column (x + a, y + b) over z .. z + 63.  A warp takes one
+// candidate at a time, its lanes one item column each, and stops at the first
+// overlap.  The candidate words are refined in place into the free words;
+// free cells are counted (stage 1 of k_cand_apply) and, outside the
+// interlocking mode, flag their plane (okplane).
+// grid: (max Xv, n), block 128
+__global__ void __launch_bounds__(128)
+k_cand_verify(const OrientDesc* __restrict__ orients, const uint4* __restrict__ tbits, int ny, int nzw, int tq,
+              uint32_t* __restrict__ cand, long long sBits, const unsigned char* __restrict__ candplane,
+              long long pstride, const uint4* __restrict__ cols, long long cstride, const int* __restrict__ ncol,
+              int* __restrict__ vcount, unsigned char* __restrict__ okplane, int set_okplane) {
+    const int o = blockIdx.y, x = blockIdx.x;
+    const OrientDesc& od = orients[o];
+    if (od.skip || !od.direct || x >= od.valid[0]) return;
+    if (!candplane[(size_t)o * pstride + x]) return;   // no candidate: the words are zero already
+    const int Yv = od.valid[1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nc = ncol[o];
+    const uint4* cl = cols + (size_t)o * cstride;
+    const uint32_t* T = (const uint32_t*)tbits;
+    const int tw = 4 * tq;   // words per tray column
+    uint32_t* cw = cand + (size_t)o * sBits + (size_t)x * ny * nzw;
+    int nfree = 0;
+    for (int y = warp; y < Yv; y += 4) {
+        for (int wi = 0; wi < nzw; ++wi) {
+            uint32_t word = cw[(size_t)y * nzw + wi];
+            uint32_t keep = word;
+            while (word) {
+                const int bit = __ffs(word) - 1;
+                word &= word - 1u;
+                const int z = 32 * wi + bit;
+                const int sh = z >> 5, off = z & 31;
+                bool hit = false;
+                for (int k0 = 0; k0 < nc; k0 += 32) {
+                    const int k = k0 + lane;
+                    bool c = false;
+                    if (k < nc) {
+                        const uint4 r = __ldg(&cl[k]);
+                        const int a = (int)(r.x & 0xffffu), b = (int)(r.x >> 16);
+                        const uint32_t* tc = T + ((size_t)(x + a) * ny + (y + b)) * tw;
+                        const uint32_t t0 = __ldg(&tc[sh]);
+                        const uint32_t t1 = sh + 1 < nzw ? __ldg(&tc[sh + 1]) : 0u;
+                        const uint32_t f0 = __funnelshift_r(t0, t1, off);
+                        uint32_t f1 = 0u;
+                        if (r.z) {
+                            const uint32_t t2 = sh + 2 < nzw ? __ldg(&tc[sh + 2]) : 0u;
+                            f1 = __funnelshift_r(t1, t2, off);
+                        }
+                        c = ((r.y & ~f0) | (r.z & ~f1)) != 0u;
+                    }
+                    if (__any_sync(0xffffffffu, c)) {
+                        hit = true;
+                        break;
+                    }
+                }
+                if (hit) keep &= ~(1u << bit);
+            }
+            if (lane == 0) cw[(size_t)y * nzw + wi] = keep;
+            nfree += __popc(keep);
+        }
+    }
+    if (lane == 0 && nfree) atomicAdd(&vcount[o], nfree);
+    const int any = __syncthreads_or(nfree != 0);
+    if (set_okplane && any && tid == 0) okplane[(size_t)o * pstride + x] = 1;
+}
+
+// Exact score of every ok cell of a direct orientation (k_collect_plane
+// collected all of them): the proximity sum over the item's voxels in
+// integers (the exact value the reference's FFT rounds to), then the
+// reference's score.  One warp per cell.  grid: (blocks, n_orient), block 256
+__global__ void __launch_bounds__(256)
+k_direct_score(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ phi) {
+    if (sb.gate && !*sb.gate) return;
+    const int o = blockIdx.y;
+    const OrientDesc& od = orients[o];
+    if (od.skip || !od.direct) return;
+    const int n = min(sb.ncand[o], sb.cap);
+    const int* cand = sb.cand + (size_t)o * sb.cap;
+    double* cs = sb.cscore + (size_t)o * sb.cap;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int c = blockIdx.x * wpb + (threadIdx.x >> 5); c < n; c += gridDim.x * wpb) {
+        const int t = cand[c];
+        const int z = t % sp.nz;
+        const int y = (t / sp.nz) % sp.ny;
+        const int x = t / (sp.nz * sp.ny);
+        long long acc = 0;
+        for (int v = lane; v < od.nvox; v += 32) {
+            const int4 q = __ldg(&od.vox[v]);
+            int oc[3];
+            orient_voxel(od, q.x, q.y, q.z, oc);
+            acc += (long long)q.w * __ldg(&phi[((size_t)(x + oc[0]) * sp.ny + (y + oc[1])) * sp.nz + (z + oc[2])]);
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+        if (lane == 0) {
+            const double s = ref_score(sp, (double)acc, z);
+            cs[c] = s;
+            atomicMin(&sb.best[o], ord_key(s));
+        }
+    }
+}

@@ -37,6 +37,9 @@ struct OrientDesc {
     int perm;                 // index of its axis permutation among the item's 6 bases
     double sumsq;             // sum of squared item values
     long long sabs;           // sum of |item values|
+    const int4* samp;         // sample voxels of the base item for the candidate filter (psb_filter.cuh)
+    int nsamp;                // their count; 0: no filter
+    int direct;               // set on the device: few candidates, decided without transforms (psb_filter.cuh)
 };
 
 __device__ __forceinline__ int orient_src_index(const OrientDesc& d, int i0, int i1, int i2) {
@@ -260,6 +263,10 @@ struct SearchBufs {
     float2* Pc;          // per orientation stride sP
     float2* Pd;
     long long sB, sP;
+    // work counters of the collision kernels (algorithmic bytes of the
+    // measurement), or null: [0] x-pass orientations, [1] their item rows ex,
+    // [2] their stored product planes, [3] plane-pass planes, [4] their row pairs
+    unsigned long long* work;
 };
 
 __global__ void __launch_bounds__(PSB_THREADS)
@@ -358,6 +365,8 @@ struct PlaneBufs {
     const uint32_t* okbits;   // k_plane3 field 1: cells that count (free, or reachable)
     unsigned char* okplane;   // k_plane3: per (orientation, x plane) "has an ok cell"
     int set_okplane;          // k_plane3 field 0 sets okplane from the free cells
+    const unsigned char* candplane;  // k_plane3 field 0: per (orientation, x plane) "holds a candidate"
+                                     // (k_cand_filter wrote the candidate words); null: no filter ran
 };
 
 // Per (x-plane, orientation): inverse along y, C2R along z for the collision

@@ -131,15 +131,33 @@ k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScorePara
     if (od.skip || x >= od.valid[0]) return;
     const int Yv = od.valid[1], Zv = od.valid[2];
     if (Yv <= 0 || Zv <= 0) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int nw = (Zv + 31) >> 5;
+    const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits + (size_t)x * sp.ny * sp.nzw;
+    if (od.direct) {
+        // a direct orientation (psb_filter.cuh): every ok cell is a candidate,
+        // scored exactly by k_direct_score (at most the direct limit of them)
+        int* cand = sb.cand + (size_t)o * sb.cap;
+        for (int y = warp; y < Yv; y += nwarp)
+            for (int w = 0; w < nw; ++w) {
+                const int z = w * 32 + lane;
+                const bool take = z < Zv && ((bits[(size_t)y * sp.nzw + w] >> lane) & 1u);
+                const unsigned int tk = __ballot_sync(0xffffffffu, take);
+                if (!tk) continue;
+                int slot0 = 0;
+                if (lane == 0) slot0 = atomicAdd(&sb.ncand[o], __popc(tk));
+                slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+                const int slot = slot0 + __popc(tk & ((1u << lane) - 1u));
+                if (take && slot < sb.cap) cand[slot] = (int)(((size_t)x * sp.ny + y) * sp.nz + z);
+            }
+        return;
+    }
     const unsigned long long gk = sb.smin[o];
     if (gk == 0xffffffffffffffffULL) return;  // no ok cell in any plane
     const double pm = ord_val(gk);
     const double lim = pm + 2.0 * od.delta + 1e-4 + 8.0 * (fabs(pm) + 1.0) * 2.220446049250313e-16;
     const unsigned long long pk = sb.pmin[(size_t)o * sb.pstride + x];
     if (pk == 0xffffffffffffffffULL || ord_val(pk) > lim) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int nw = (Zv + 31) >> 5;
-    const uint32_t* bits = sb.okbits + (size_t)o * sb.sBits + (size_t)x * sp.ny * sp.nzw;
     const float* Dq = sb.Dq + (size_t)o * sb.sD + (size_t)x * sp.ny * sp.nz;
     const double base = od.base;
     // score(D) <= lim needs D <= lim - score(0) at that z, up to roundings:
@@ -208,7 +226,7 @@ k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp,
     if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
-    if (od.skip) return;
+    if (od.skip || od.direct) return;   // direct orientations: k_direct_score
     const int n = min(sb.ncand[o], sb.cap);
     const int* cand = sb.cand + (size_t)o * sb.cap;
     double* cs = sb.cscore + (size_t)o * sb.cap;
@@ -318,6 +336,7 @@ __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb
     r.diag = sb.diag[o] | (orients[o].exact ? 1u : 0u);
     if (sb.ncand[o] > sb.cap) r.diag |= 0x100u;
     if (sb.gate) r.diag |= 0x400u;  // the gated second selection (lazy flood fill) ran
+    if (orients[o].direct) r.diag |= 0x800u;  // decided without transforms (psb_filter.cuh)
     if (!orients[o].skip && sb.best[o] != 0xffffffffffffffffULL) {
         double s = ord_val(sb.best[o]);
         double cut = sp.mode == 0 ? 1000000000.0 : 1e29;

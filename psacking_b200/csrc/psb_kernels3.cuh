@@ -39,6 +39,8 @@ struct BaseMap {
 //   MODE 1: the collision product only (Pc)
 //   MODE 2: the proximity product only (Pd), for orientations with an ok
 //           plane (okplane, see k_plane3), and stored only on those planes
+// In MODE 1 a non-null okplane holds the candidate-filter plane flags: only
+// those planes' rows are stored.
 // grid: (ceil(Fy*Hz / PSB_XCOLS), n_orient), block 256
 template <int N, int MODE, bool SHARED>
 __global__ void __launch_bounds__(256)
@@ -50,7 +52,7 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
     extern __shared__ float2 sm[];
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
-    if (od.skip || od.valid[0] <= 0) return;
+    if (od.skip || od.direct || od.valid[0] <= 0) return;
     const int c0 = blockIdx.x * C;
     const int nl = min(C, ncols - c0);
     float2* tw = sm;
@@ -59,14 +61,27 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
     unsigned char* okp = (unsigned char*)(X + N * C);   // MODE 2: the orientation's plane flags
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int ex = od.e[0], Xv = od.valid[0];
-    if (MODE == 2) {
-        int any = 0;
+    // plane flags: MODE 2 the ok planes; MODE 1 (when given) the planes that
+    // hold a filter candidate (psb_filter.cuh): rows of other planes are not stored
+    const bool flags = MODE == 2 || (MODE == 1 && okplane != nullptr && od.nsamp > 0);
+    if (flags) {
+        int cnt = 0;
         for (int x = tid; x < Xv; x += nthr) {
             const unsigned char f = okplane[(size_t)o * okstride + x];
             okp[x] = f;
-            any |= f;
+            cnt += f;
         }
-        if (!__syncthreads_or(any)) return;
+        if (!__syncthreads_or(cnt)) return;
+        if (MODE == 1 && sb.work && blockIdx.x == 0) {
+            for (int d = 16; d > 0; d >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
+            if ((tid & 31) == 0 && cnt) atomicAdd(&sb.work[2], (unsigned long long)cnt);
+        }
+    } else if (MODE == 1 && sb.work && blockIdx.x == 0 && tid == 0) {
+        atomicAdd(&sb.work[2], (unsigned long long)Xv);
+    }
+    if (MODE == 1 && sb.work && blockIdx.x == 0 && tid == 0) {
+        atomicAdd(&sb.work[0], 1ull);
+        atomicAdd(&sb.work[1], (unsigned long long)od.e[0]);
     }
     load_twiddles(tw, g_tw, N, tid, nthr);
     __shared__ int srccol[C];
@@ -113,7 +128,7 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
         __syncthreads();
         tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
                                       [&](int c, int x, float2 v) {
-                                          if (x < Xv) Pc[(size_t)x * ncols + c] = v;
+                                          if (x < Xv && (!flags || okp[x])) Pc[(size_t)x * ncols + c] = v;
                                       },
                                       nl, tw, tid, nthr);
         if (MODE == 1) return;
@@ -124,13 +139,13 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
     __syncthreads();
     tpass<N, R1, R0, 1, C, false>([&](int c, int n) { return A[n * C + c]; },
                                   [&](int c, int x, float2 v) {
-                                      if (x < Xv && (MODE != 2 || okp[x])) Pd[(size_t)x * ncols + c] = v;
+                                      if (x < Xv && (!flags || okp[x])) Pd[(size_t)x * ncols + c] = v;
                                   },
                                   nl, tw, tid, nthr);
 }
 
 constexpr size_t xpass2_smem(int N) {
-    return sizeof(float2) * ((size_t)N + 2 * (size_t)N * PSB_XCOLS) + (size_t)N;  // + MODE 2 plane flags
+    return sizeof(float2) * ((size_t)N + 2 * (size_t)N * PSB_XCOLS) + (size_t)N;  // + plane flags
 }
 
 // shared memory of k_plane2: twiddles, work buffer A and the y-inverted plane
@@ -273,7 +288,7 @@ k_fwd_plane(FwdSrc src, const OrientDesc* __restrict__ orients, const float2* __
     OrientDesc od;
     if (src.kind == SRC_ITEM) {
         od = orients[b];
-        if (od.skip) return;
+        if (od.skip || od.direct) return;   // direct orientations need no transform
         n0 = od.e[0]; n1 = od.e[1]; n2 = od.e[2];
     }
     if (i >= n0) return;

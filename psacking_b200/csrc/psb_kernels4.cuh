@@ -82,7 +82,7 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     extern __shared__ float2 sm[];
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
-    if (od.skip) return;
+    if (od.skip || od.direct) return;   // direct orientations: psb_filter.cuh
     const int x = blockIdx.x;
     const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
     if (x >= Xv || Yv <= 0 || Zv <= 0) return;
@@ -91,6 +91,10 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
         if (tid == 0) pb.pmin[(size_t)o * pb.pstride + x] = 0xffffffffffffffffULL;
         return;
     }
+    // FIELD 0 after the candidate filter (psb_filter.cuh): a plane without a
+    // candidate holds no free cell, and the filter already wrote its words
+    const bool filtered = FIELD == 0 && pb.candplane != nullptr && od.nsamp > 0;
+    if (filtered && !pb.candplane[(size_t)o * pb.pstride + x]) return;
     const int ny = sp.ny, nzw = sp.nzw;
     const int npairs = (Yv + 1) / 2;
     float2* twy = sm;
@@ -99,12 +103,46 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     float2* Q = W + (WY > WZ ? WY : WZ);                    // y-inverted plane [y][HZ]
     load_twiddles(twy, g_twy, NY, tid, PSB_PLANE3_THREADS);
     load_twiddles(twz, g_twz, NZ, tid, PSB_PLANE3_THREADS);
-    __syncthreads();
     const float scale = sp.scale;
     unsigned int diag = 0;
     float* Dq = pb.Dq + (size_t)o * pb.sD + (size_t)x * ny * sp.nz;
     uint32_t* fbits = pb.freebits + (size_t)o * pb.sBits + (size_t)x * ny * nzw;
     const uint32_t* obits = pb.okbits + (size_t)o * pb.sBits + (size_t)x * ny * nzw;
+    // the row pairs the z pass computes: all of them, or (FIELD 0 filtered)
+    // those holding a candidate, or (FIELD 1) those holding an ok cell; the
+    // others' words stay zero and their proximity is never read
+    __shared__ int plist[(NY + 1) / 2];
+    __shared__ int nact;
+    if (warp == 0) {
+        const uint32_t* rows = FIELD == 0 ? fbits : obits;
+        const bool all = FIELD == 0 && !filtered;
+        int base = 0;
+        for (int p0 = 0; p0 < npairs; p0 += 32) {
+            const int p = p0 + lane;
+            bool on = p < npairs;
+            if (on && !all) {
+                uint32_t a = 0u;
+                for (int i = 0; i < nzw; ++i) {
+                    a |= rows[(size_t)(2 * p) * nzw + i];
+                    if (2 * p + 1 < Yv) a |= rows[(size_t)(2 * p + 1) * nzw + i];
+                }
+                on = a != 0u;
+            }
+            const unsigned int b = __ballot_sync(0xffffffffu, on);
+            if (on) plist[base + __popc(b & ((1u << lane) - 1u))] = p;
+            base += __popc(b);
+        }
+        if (lane == 0) nact = base;
+    }
+    __syncthreads();
+    if (nact == 0) {
+        if (FIELD == 1 && tid == 0) pb.pmin[(size_t)o * pb.pstride + x] = 0xffffffffffffffffULL;
+        return;
+    }
+    if (FIELD == 0 && sb.work && tid == 0) {
+        atomicAdd(&sb.work[3], 1ull);
+        atomicAdd(&sb.work[4], (unsigned long long)nact);
+    }
 
     // y pass: line (column) c = t*PER + lane / L, lane j = lane % L
     const int yl = lane / LY::L, yj = lane - yl * LY::L;
@@ -160,9 +198,11 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     }
     __syncthreads();
     // z pass: C2R of two rows per complex line (rows 2p, 2p+1)
-    for (int t = warp; t * LZ::PER < npairs; t += NWARP) {
-        const int p = t * LZ::PER + zl;
-        const bool act = zl < LZ::PER && p < npairs;
+    const int na = nact;
+    for (int t = warp; t * LZ::PER < na; t += NWARP) {
+        const int pi = t * LZ::PER + zl;
+        const bool act = zl < LZ::PER && pi < na;
+        const int p = act ? plist[pi] : 0;
         const int ya = 2 * p, yb = ya + 1;
         const bool hb = yb < Yv;
         float2* slab = W + (size_t)(warp * LZ::PER + (act ? zl : 0)) * LZ::SLAB;
