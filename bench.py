@@ -139,34 +139,33 @@ def sorted_items(items):
     return [np.ascontiguousarray(items[i].astype(np.int32)) for i in np.argsort(vols)[::-1]]
 
 
-def algorithmic_bytes(seq, maps, F):
-    """Bytes the two always-running transform kernels must move, summed over
-    the run, from the item shapes (every item is searched once in all
-    orientations that fit).
-      k_xpass_coll per orientation: read the occupancy half spectrum
-        (Fx*Fy*Hz*8 B), read the item's z,y-transformed columns (ex*Fy*Hz*8),
-        write the collision product for the valid planes (Xv*Fy*Hz*8).
-      k_plane_coll per orientation: read that product (Xv*Fy*Hz*8), write the
-        free bits of the valid planes (Xv*ny*ceil(nz/32)*4).
-    The proximity kernels (k_xpass_prox, k_plane_prox) run only on the planes
-    that hold a reachable cell and are reported by time only."""
+def orientations_searched(seq, maps):
+    """Orientations of the run that fit the tray (each is searched once)."""
     from psacking_b200.rotations import apply_map
+    return sum(1 for it in seq for row in maps
+               if all(apply_map(it, row).shape[a] <= TRAY[a] for a in range(3)))
+
+
+def algorithmic_bytes(work, F):
+    """Bytes the two collision kernels must move for the work they did, from
+    the engine's work counters (psb_tray_work) over the timed steps:
+      k_xpass_coll per orientation it transforms: read the occupancy half
+        spectrum (Fx*Fy*Hz*8 B), read the item's z,y-transformed columns
+        (ex*Fy*Hz*8), write the collision product of the planes it stores
+        (Fy*Hz*8 per plane: the valid planes, or with the candidate filter
+        only those holding a candidate);
+      k_plane_coll per plane it processes: read that plane's product
+        (Fy*Hz*8), write the free words of the row pairs it computes
+        (2*ceil(nz/32)*4 per pair).
+    Orientations and planes the candidate filter rules out move nothing.
+    The proximity kernels run only where a reachable cell exists and are
+    reported by time only."""
     Fx, Fy, Fz = F
     Hz = Fz // 2 + 1
-    xb = pb = 0
-    nor = 0
-    for it in seq:
-        for row in maps:
-            o = apply_map(it, row)
-            if any(o.shape[a] > TRAY[a] for a in range(3)):
-                continue
-            oi = np.argwhere(o > 0)
-            hi = oi.max(axis=0)
-            Xv = TRAY[0] - hi[0]
-            xb += Fx * Fy * Hz * 8 + o.shape[0] * Fy * Hz * 8 + Xv * Fy * Hz * 8
-            pb += Xv * Fy * Hz * 8 + Xv * TRAY[1] * ((TRAY[2] + 31) // 32) * 4
-            nor += 1
-    return {"k_xpass_coll": xb, "k_plane_coll": pb, "orientations": nor}
+    col = Fy * Hz * 8
+    xb = work[0] * Fx * col + work[1] * col + work[2] * col
+    pb = work[3] * col + work[4] * 2 * ((TRAY[2] + 31) // 32) * 4
+    return {"k_xpass_coll": xb, "k_plane_coll": pb}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -225,7 +224,10 @@ def run_ours(args, rank, world, local_rank):
     # records per item
     lib.psb_profile_filter(b"k_plane_coll,k_xpass_coll")
     lib.psb_profile_enable(1)
+    work = (ctypes.c_ulonglong * 8)()
+    check(lib, lib.psb_tray_work(t, None, 1))
     ms = [one_step(True) for _ in range(args.steps)]
+    check(lib, lib.psb_tray_work(t, work, 1))
     prof_top = parse_profile(lib)
     lib.psb_profile_enable(0)
     clk = clocks.stop()
@@ -286,14 +288,14 @@ def run_ours(args, rank, world, local_rank):
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    ab = algorithmic_bytes(seq, maps, F)
+    ab = algorithmic_bytes(list(work), F)
     dom = max((k for k in prof_top if k in ("k_xpass_coll", "k_plane_coll")), key=lambda k: prof_top[k][1],
               default=None)
     top = max(prof, key=lambda k: prof[k][1]) if prof else None
     roof = None
     if dom:
         n_l, ms_l = prof_top[dom]
-        per_launch_bytes = ab[dom] / (n_l / args.steps)
+        per_launch_bytes = ab[dom] / n_l
         achieved = per_launch_bytes / (ms_l / n_l / 1e3) / 1e9
         traffic = None
         tf = ROOT / "profiles" / f"{dom}_traffic.json"
@@ -311,7 +313,10 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded config-3 shapes; Thingi10K unavailable)",
         "config": {"workload": f"config3: 240x123x100 tray, {args.items} items (extent 20-50), 24 orientations, "
                                "interlocking-free (flood fill on every searched item), K=1",
-                   "items_per_step": len(seq), "items_placed_per_step": placed, "orientations_per_step": ab["orientations"],
+                   "items_per_step": len(seq), "items_placed_per_step": placed, "orientations_per_step": orientations_searched(seq, maps),
+                   "collision_work_per_step": {
+                       "xpass_orientations": work[0] / args.steps, "xpass_planes_stored": work[2] / args.steps,
+                       "plane_pass_planes": work[3] / args.steps, "plane_pass_row_pairs": work[4] / args.steps},
                    "l2": "256 MiB buffer written before every step", "parallelism": f"replicas x{world} (independent trays)",
                    "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag,
                    "tie_guard": {"candidates_per_item_mean": round(statistics.mean(cands), 1),

@@ -52,6 +52,8 @@ extern "C" {
 #define PSB_DIAG_FLOOD_FILL      0x400 /* interlocking search: the winner over the free cells
                                           had no straight free run to a seed face, so the
                                           flood fill and a second selection ran             */
+#define PSB_DIAG_DIRECT          0x800 /* few candidates left by the pre-filter: decided by direct
+                                          exact checks and exact proximity sums, no transforms */
 
 typedef struct psb_result {
     int32_t x, y, z;       /* placement of the item array origin, or -1,-1,-1      */
@@ -256,6 +258,18 @@ int psb_set_fast_fft(int on);
  * spread over the CTA).  Same results; a tuning and comparison switch.
  * No counterpart in the reference (cuFFT there). */
 int psb_set_plane_variant(int v);
+/* Candidate pre-filter of the packing loop (psb_pack*, default on): before
+ * an item's collision transforms, a bit-parallel test of up to 128 of its
+ * voxels against the tray proves most translations (and often whole
+ * orientations or x planes) blocked; those are skipped, every other cell is
+ * decided exactly as before.  Same placements either way; the switch exists
+ * for comparisons.  No counterpart in the reference. */
+int psb_set_cand_filter(int on);
+/* Orientations the pre-filter leaves with at most n candidate translations
+ * (default 2048; 0 disables) skip the transforms: each candidate is checked
+ * exactly against the item's voxel columns and the free ones are scored by
+ * exact integer proximity sums.  Same placements either way. */
+int psb_set_direct_max(int n);
 /* The 24 orientations are 6 axis permutations x 4 flip patterns.  On: the
  * z,y transforms of each permutation run once per item and the x pass reads
  * every flip from them (row reversal, column map, conjugation, phase).  Off
@@ -287,6 +301,12 @@ int psb_profile_report(char* buf, size_t len);
 int psb_tray_fft_dims(const psb_tray* t, int* F);
 /* The CUDA stream (cudaStream_t) a tray's kernels run on. */
 int psb_tray_stream(psb_tray* t, void** stream);
+/* Work counters of a tray's collision kernels since the last reset (the
+ * measurement's algorithmic bytes): out[0] collision x-pass orientations,
+ * out[1] the sum of their item x extents, out[2] their stored product planes,
+ * out[3] collision plane-pass planes, out[4] their row pairs; out[5..7] 0.
+ * out may be NULL; reset != 0 zeroes them after the copy. */
+int psb_tray_work(psb_tray* t, unsigned long long* out, int reset);
 
 #ifdef __cplusplus
 }

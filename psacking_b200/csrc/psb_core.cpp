@@ -505,6 +505,10 @@ PYBIND11_MODULE(_core, m) {
     m.def("device_count", &py_device_count);
     m.def("set_fast_fft", [](bool on) { psb_set_fast_fft(on ? 1 : 0); }, py::arg("on"),
           "Use the specialised two-pass FFT kernels where a plan exists (default) or force the generic path.");
+    m.def("set_cand_filter", [](bool on) { check(psb_set_cand_filter(on ? 1 : 0)); }, py::arg("on"),
+          "Candidate pre-filter of the packing loop (default on; same placements either way).");
+    m.def("set_direct_max", [](int n) { check(psb_set_direct_max(n)); }, py::arg("n"),
+          "Candidate limit below which the packing loop decides an orientation without transforms.");
     m.def("set_share_flips", [](bool on) { check(psb_set_share_flips(on ? 1 : 0)); }, py::arg("on"),
           "Share the z,y transforms among the flips of each axis permutation, or transform each orientation on "
           "its own (the default).");

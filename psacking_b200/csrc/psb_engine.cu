@@ -27,6 +27,7 @@
 #include "psb_kernels3.cuh"
 #include "psb_kernels4.cuh"
 #include "psb_loop.cuh"
+#include "psb_filter.cuh"
 #include "psb_proposal.cuh"
 #include "psb_voxel.cuh"
 
@@ -268,6 +269,14 @@ int g_plane_variant = 3;
 // latency-bound, not work-bound).
 bool g_share_flips = false;
 
+// exact candidate pre-filter of the packing loop's collision searches
+// (psb_filter.cuh); on by default
+bool g_cand_filter = true;
+// orientations left with at most this many candidates are decided directly
+// (exact checks against the item's columns, exact proximity sums) instead of
+// by transforms; 0 disables
+int g_direct_max = 2048;
+
 // the 6 axis permutations of an orientation map, as base indices
 int perm_index(const int* a) {
     static const int tab[27] = {-1, -1, -1, -1, -1, 0, -1, 1, -1, -1, -1, 2, -1, -1, -1, 3, -1, -1,
@@ -335,6 +344,8 @@ int set_smem_attrs() {
     CK(cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (const char* e = getenv("PSB_PLANE_VARIANT")) g_plane_variant = atoi(e) == 2 ? 2 : 3;
     if (const char* e = getenv("PSB_SHARE_FLIPS")) g_share_flips = atoi(e) != 0;
+    if (const char* e = getenv("PSB_CAND_FILTER")) g_cand_filter = atoi(e) != 0;
+    if (const char* e = getenv("PSB_DIRECT_MAX")) g_direct_max = std::max(0, atoi(e));
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
     TRY(set_max_dyn_smem(k_fft_mid<-1>));
@@ -546,7 +557,57 @@ struct ItemInfo {
     long long sabs = 0;        // sum of |values|
     double sumsq = 0.0;
     std::vector<int4> vox;     // nonzero voxels (x, y, z, value)
+    std::vector<int4> samp;    // candidate-filter samples (positive voxels, spread out)
 };
+
+// Up to PSB_FSAMP positive voxels spread over the item, for the candidate
+// filter.  Pool: in each cell of a 10x10x10 split of the item's box, the
+// voxel farthest from the box centre (extreme voxels are the ones that stop
+// an item from fitting a gap).  Order: farthest-point (each next sample is
+// the pool voxel farthest from those taken), starting from the voxel farthest
+// from the centre, so the filter's first samples already span the item.  Any
+// subset is exact for the filter; the spread only makes it sharp.
+void pick_samples(ItemInfo* info) {
+    info->samp.clear();
+    const int G = 10;
+    const int* d = info->dims;
+    const float cx = 0.5f * (d[0] - 1), cy = 0.5f * (d[1] - 1), cz = 0.5f * (d[2] - 1);
+    auto d2 = [](const int4& a, float x, float y, float z) {
+        return (a.x - x) * (a.x - x) + (a.y - y) * (a.y - y) + (a.z - z) * (a.z - z);
+    };
+    std::vector<int> best(G * G * G, -1);
+    std::vector<float> bd(G * G * G, 0.f);
+    for (size_t i = 0; i < info->vox.size(); ++i) {
+        const int4 v = info->vox[i];
+        if (v.w <= 0) continue;
+        const int cell = ((v.x * G / d[0]) * G + v.y * G / d[1]) * G + v.z * G / d[2];
+        const float dist = d2(v, cx, cy, cz);
+        if (best[cell] < 0 || dist > bd[cell]) { best[cell] = (int)i; bd[cell] = dist; }
+    }
+    std::vector<int4> pool;
+    for (int b : best)
+        if (b >= 0) pool.push_back(info->vox[b]);
+    if (pool.empty()) return;
+    size_t k = 0;
+    for (size_t i = 1; i < pool.size(); ++i)
+        if (d2(pool[i], cx, cy, cz) > d2(pool[k], cx, cy, cz)) k = i;
+    std::vector<float> dmin(pool.size(), 3.0e38f);
+    std::vector<char> taken(pool.size(), 0);
+    const size_t m = std::min(pool.size(), (size_t)PSB_FSAMP);
+    while (info->samp.size() < m) {
+        taken[k] = 1;
+        info->samp.push_back(pool[k]);
+        size_t nk = k;
+        float far = -1.f;
+        for (size_t i = 0; i < pool.size(); ++i) {
+            if (taken[i]) continue;
+            dmin[i] = std::min(dmin[i], d2(pool[i], (float)pool[k].x, (float)pool[k].y, (float)pool[k].z));
+            if (dmin[i] > far) { far = dmin[i]; nk = i; }
+        }
+        if (nk == k) break;
+        k = nk;
+    }
+}
 
 void analyse_item(const int32_t* a, int ex, int ey, int ez, ItemInfo* info) {
     info->dims[0] = ex; info->dims[1] = ey; info->dims[2] = ez;
@@ -671,6 +732,15 @@ struct psb_tray {
     unsigned long long* d_pmin = nullptr;   // per (orientation, x plane) minimum approximate score key
     int* d_needff = nullptr;                // lazy interlocking search: flood fill needed
     unsigned char* d_okplane = nullptr;     // per (orientation, x plane): holds an ok cell
+    unsigned char* d_candplane = nullptr;   // per (orientation, x plane): holds a filter candidate
+    bool cand_active = false;               // the current search's candidate words and planes are valid
+    bool direct_active = false;             // ... and direct orientations may exist
+    int *d_ccount = nullptr, *d_vcount = nullptr, *d_ncol = nullptr;   // per orientation: candidates,
+                                                                      // verified free cells, item columns
+    uint4* d_icols = nullptr;               // item column masks of direct orientations, stride nx*ny
+    uint4* d_tbits = nullptr;               // free bits of the tray (k_tray_bits), tq uint4 per column
+    int tq = 0;
+    unsigned long long* d_work = nullptr;   // collision-kernel work counters (SearchBufs::work)
     OrientDesc* d_bases = nullptr;          // their descriptors (synchronous searches)
     unsigned int* d_diag = nullptr;
     unsigned int* d_errmax = nullptr;
@@ -686,6 +756,9 @@ struct psb_tray {
     int32_t* d_stage = nullptr;
     int4* d_stage_vox = nullptr;
     size_t stage_cap = 0, stage_vcap = 0;
+    std::vector<size_t> staged_soff;   // the items' filter samples in d_stage_samp
+    int4* d_stage_samp = nullptr;
+    size_t stage_scap = 0;
     void* h_stage = nullptr;   // pinned host staging buffer of psb_pack_stage
     size_t h_stage_cap = 0;
 
@@ -700,7 +773,8 @@ struct psb_tray {
     void release_slots() {
         dfree(d_Ai, st); dfree(d_Bi, st); dfree(d_Pc, st); dfree(d_Pd, st); dfree(d_Dq, st); dfree(d_free, st); dfree(d_reach, st);
         dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
-        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_bases, st); dfree(d_best, st);
+        dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_candplane, st); dfree(d_bases, st); dfree(d_best, st);
+        dfree(d_ccount, st); d_vcount = d_ncol = nullptr; dfree(d_icols, st);
         dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
@@ -710,6 +784,8 @@ struct psb_tray {
         dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_pen, st);
         dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st); dfree(d_stage_vox, st);
         dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_base_all, st); dfree(d_dec, st);
+        dfree(d_tbits, st); dfree(d_stage_samp, st); dfree(d_work, st);
+        tq = 0;
         if (st) {
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
@@ -735,6 +811,8 @@ struct psb_tray {
         TRY(dalloc(&d_Socc, S, st)); TRY(dalloc(&d_Sphi, S, st));
         TRY(dalloc(&d_w1, (size_t)nx * ny * g.H, st)); TRY(dalloc(&d_w2, (size_t)nx * g.F[1] * g.H, st));
         TRY(dalloc(&d_pen, 3 * (size_t)nz, st)); TRY(dalloc(&d_rz, 4, st)); TRY(dalloc(&d_mid, 4, st)); TRY(dalloc(&d_stats, 4, st));
+        TRY(dalloc(&d_work, 8, st));
+        CK(cudaMemsetAsync(d_work, 0, sizeof(unsigned long long) * 8, st));
         TRY(dalloc(&d_err, 1, st)); TRY(dalloc(&d_first, 1, st)); TRY(dalloc(&d_needff, 1, st));
         TRY(dalloc(&d_ls, 1, st)); TRY(dalloc(&d_ps, 1, st)); TRY(dalloc(&d_rzd, 4, st)); TRY(dalloc(&d_midd, 8, st));
         CK(cudaStreamSynchronize(st));  // stream-ordered allocations complete before plain copies touch them
@@ -792,6 +870,11 @@ struct psb_tray {
         TRY(dalloc(&d_cand, (size_t)kCandCap * c, st)); TRY(dalloc(&d_ncand, c, st));
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c, st));
         TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_okplane, (size_t)nx * c, st));
+        TRY(dalloc(&d_candplane, (size_t)nx * c, st));
+        TRY(dalloc(&d_ccount, 3 * (size_t)c, st));
+        d_vcount = d_ccount + c;
+        d_ncol = d_ccount + 2 * c;
+        TRY(dalloc(&d_icols, (size_t)nx * ny * c, st));
         TRY(dalloc(&d_bases, 6, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
         TRY(dalloc(&d_diag, c, st)); TRY(dalloc(&d_errmax, c, st)); TRY(dalloc(&d_od, c, st)); TRY(dalloc(&d_rzs, c, st)); TRY(dalloc(&d_mids, c, st));
         TRY(dalloc(&d_res, c, st));
@@ -952,6 +1035,96 @@ struct psb_tray {
         od->perm = -1;
         od->sumsq = info.sumsq;
         od->sabs = sabs;
+        od->samp = nullptr;
+        od->nsamp = 0;
+        od->direct = 0;
+    }
+
+    // Free bits of the tray for the candidate filter, all columns.
+    int tray_bits() {
+        if (!d_tbits) {
+            tq = (nzw + 3) / 4;
+            TRY(dalloc(&d_tbits, (size_t)nx * ny * tq, st));
+        }
+        {
+            PROF("k_tray_bits", st);
+            k_tray_bits<<<(unsigned)(((size_t)nx * ny + 7) / 8), 256, 0, st>>>(d_tray, nx, ny, nz, tq, d_tbits);
+        }
+        CKL();
+        return PSB_OK;
+    }
+
+    // ... after the loop placed the item described by d_odb: only the columns
+    // under its box (gated on the loop's "placed" flag).
+    int tray_bits_placed(const OrientDesc* d_odb, const std::vector<OrientDesc>& ods) {
+        size_t box = 1;
+        for (auto& o : ods) box = std::max(box, (size_t)o.e[0] * o.e[1]);
+        {
+            PROF("k_tray_bits", st);
+            k_tray_bits_box<<<(unsigned)((box + 7) / 8), 256, 0, st>>>(d_tray, nx, ny, nz, tq, d_tbits, d_ls, d_odb);
+        }
+        CKL();
+        return PSB_OK;
+    }
+
+    // whether search_async takes the split flow (search_split) with the
+    // specialised x pass for this tray: only its kernels know direct
+    // orientations
+    bool split_flow() const {
+        if (!g_fast_fft || g_plane_variant != 3) return false;
+        if (!xpass2_for(g.F[0]) || xpass2_smem(g.F[0]) + 64 > (size_t)g_smem_optin) return false;
+        if (!plane3_for(g.F[1], g.F[2], 0) || !plane3_for(g.F[1], g.F[2], 1)) return false;
+        return plane3_smem(g.F[1], g.F[2], ny) + 64 <= (size_t)g_smem_optin;
+    }
+
+    // Candidate filter of one item's orientations (psb_filter.cuh): candidate
+    // words into the free-bit slots, plane flags, orientations without a
+    // candidate skipped; orientations with few candidates verified directly.
+    // The next search refines the other candidates.
+    int cand_filter(OrientDesc* d_odb, const std::vector<OrientDesc>& ods, bool interlock) {
+        int xmax = 0, emax = 0;
+        for (auto& o : ods)
+            if (!o.skip && o.nsamp > 0) {
+                xmax = std::max(xmax, o.valid[0]);
+                emax = std::max(emax, o.e[0]);
+            }
+        const int n = (int)ods.size();
+        const int dmax = split_flow() ? g_direct_max : 0;
+        if (xmax > 0) {
+            const dim3 grid(xmax, n);
+            CK(cudaMemsetAsync(d_ccount, 0, sizeof(int) * 3 * cap, st));
+            {
+                PROF("k_cand_filter", st);
+                if (tq == 1)
+                    k_cand_filter<1><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
+                                                                        d_candplane, (long long)nx, d_ccount);
+                else
+                    k_cand_filter<2><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
+                                                                        d_candplane, (long long)nx, d_ccount);
+            }
+            CKL();
+            k_cand_apply<<<(n + 127) / 128, 128, 0, st>>>(d_odb, n, d_ccount, 0, dmax);
+            CKL();
+            if (dmax > 0) {
+                // the okplane flags of the free cells (non-interlocking mode)
+                // are set here for direct orientations, so clear them first
+                CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
+                {
+                    PROF("k_cand_verify", st);
+                    k_item_cols<<<dim3(emax, n), 64, 0, st>>>(d_odb, d_icols, (long long)nx * ny, d_ncol);
+                    CKL();
+                    k_cand_verify<<<grid, 128, 0, st>>>(d_odb, d_tbits, ny, nzw, tq, d_free, sBits, d_candplane,
+                                                        (long long)nx, d_icols, (long long)nx * ny, d_ncol, d_vcount,
+                                                        d_okplane, interlock ? 0 : 1);
+                }
+                CKL();
+                k_cand_apply<<<(n + 127) / 128, 128, 0, st>>>(d_odb, n, d_vcount, 1, dmax);
+                CKL();
+            }
+        }
+        cand_active = true;
+        direct_active = dmax > 0 && xmax > 0;   // the okplane flags were cleared above
+        return PSB_OK;
     }
 
     ScoreParams score_params(int mode) const {
@@ -1006,15 +1179,19 @@ struct psb_tray {
     // proximity transform, and every orientation's own result is exact.
     int search_split(const OrientDesc* d_odb, int n, const ScoreParams& sp, bool interlock, XpassFn xf, PlaneFn p0,
                      PlaneFn p1, size_t smem, ResultDev* d_out, bool spec) {
-        SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP};
-        CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
+        SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP, d_work};
+        // (with direct orientations the candidate filter cleared the flags and
+        // set those of its verified planes already)
+        if (!direct_active) CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
         const int ncols = g.F[1] * g.H;
         XpassFn xf1 = xf ? xpass2_for(g.F[0], 1, spec) : nullptr, xf2 = xf ? xpass2_for(g.F[0], 2, spec) : nullptr;
         const BaseMap bm{g.F[1], g.H, g.F[2], g.p[1].tw, g.p[2].tw};
         if (xf) {
             PROF("k_xpass_coll", st);
+            // with the filter's plane flags, only rows of planes holding a
+            // candidate are stored (the plane pass skips the others)
             xf1<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
-                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, nullptr, 0, bm);
+                d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, cand_active ? d_candplane : nullptr, (long long)nx, bm);
         } else {
             PROF("k_xpass_coll", st);
             const size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
@@ -1023,7 +1200,8 @@ struct psb_tray {
         }
         CKL();
         const uint32_t* ok = interlock ? d_reach : d_free;
-        PlaneBufs pb{d_free, d_Dq, d_smin, d_diag, sBits, sD, d_pmin, (long long)nx, ok, d_okplane, interlock ? 0 : 1};
+        PlaneBufs pb{d_free, d_Dq,      d_smin,         d_diag, sBits, sD, d_pmin, (long long)nx, ok, d_okplane,
+                     interlock ? 0 : 1, cand_active ? d_candplane : nullptr};
         {
             PROF("k_plane_coll", st);
             p0<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
@@ -1060,6 +1238,11 @@ struct psb_tray {
             k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_tray, d_phi);
         }
         CKL();
+        if (direct_active) {
+            PROF("k_direct_score", st);
+            k_direct_score<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp, d_phi);
+            CKL();
+        }
         {
             PROF("k_tiebreak", st);
             k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp);
@@ -2042,6 +2225,7 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     t->staged.clear();
     t->staged_off.clear();
     t->staged_voff.clear();
+    t->staged_soff.clear();
     for (int it = 0; it < n_items; ++it) {
         const int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
         if (!items[it] || ex <= 0 || ey <= 0 || ez <= 0) return fail(PSB_ERR_ARG, "item %d: bad array", it);
@@ -2057,6 +2241,7 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
                 const size_t m = (size_t)ex * ey * ez;
                 if (has_negative(items[it], m)) { neg[it] = 1; continue; }
                 analyse_item(items[it], ex, ey, ez, &t->staged[it]);
+                pick_samples(&t->staged[it]);
             }
         };
         const int nthr = std::max(1, std::min<int>(n_items / 8, (int)std::thread::hardware_concurrency()));
@@ -2067,13 +2252,20 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     }
     for (int it = 0; it < n_items; ++it)
         if (neg[it]) return fail(PSB_ERR_ARG, "item %d holds negative values", it);
-    size_t tot = 0, totv = 0;
+    size_t tot = 0, totv = 0, tots = 0;
     for (int it = 0; it < n_items; ++it) {
         const ItemInfo& inf = t->staged[it];
         t->staged_off.push_back(tot);
         t->staged_voff.push_back(totv);
+        t->staged_soff.push_back(tots);
         tot += (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
         totv += inf.vox.size();
+        tots += inf.samp.size();
+    }
+    if (tots > t->stage_scap) {
+        dfree(t->d_stage_samp, t->st);
+        t->stage_scap = tots;
+        TRY(dalloc(&t->d_stage_samp, tots, t->st));
     }
     if (tot > t->stage_cap) {
         dfree(t->d_stage, t->st);
@@ -2087,7 +2279,7 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     }
     // one pinned staging buffer for the item arrays and voxel lists: two
     // large copies instead of two small pageable ones per item
-    const size_t bytes = sizeof(int32_t) * tot + sizeof(int4) * totv;
+    const size_t bytes = sizeof(int32_t) * tot + sizeof(int4) * (totv + tots);
     if (bytes > t->h_stage_cap) {
         if (t->h_stage) cudaFreeHost(t->h_stage);
         t->h_stage = nullptr;
@@ -2097,13 +2289,16 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     }
     int32_t* hi = (int32_t*)t->h_stage;
     int4* hv = (int4*)(hi + tot);
+    int4* hs = hv + totv;
     for (int it = 0; it < n_items; ++it) {
         const ItemInfo& inf = t->staged[it];
         memcpy(hi + t->staged_off[it], items[it], sizeof(int32_t) * inf.dims[0] * inf.dims[1] * inf.dims[2]);
         if (!inf.vox.empty()) memcpy(hv + t->staged_voff[it], inf.vox.data(), sizeof(int4) * inf.vox.size());
+        if (!inf.samp.empty()) memcpy(hs + t->staged_soff[it], inf.samp.data(), sizeof(int4) * inf.samp.size());
     }
     if (tot) CK(cudaMemcpyAsync(t->d_stage, hi, sizeof(int32_t) * tot, cudaMemcpyHostToDevice, t->st));
     if (totv) CK(cudaMemcpyAsync(t->d_stage_vox, hv, sizeof(int4) * totv, cudaMemcpyHostToDevice, t->st));
+    if (tots) CK(cudaMemcpyAsync(t->d_stage_samp, hs, sizeof(int4) * tots, cudaMemcpyHostToDevice, t->st));
     CK(cudaStreamSynchronize(t->st));
     return PSB_OK;
 }
@@ -2189,6 +2384,15 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             t->describe(t->staged[it], orient_maps + 6 * o, orient_maps + 6 * o + 3,
                         t->d_stage + t->staged_off[it], t->d_stage_vox + t->staged_voff[it],
                         &all[(size_t)it * n_orient + o]);
+    // candidate-filter samples (tray columns of at most 256 cells)
+    const bool filt = g_cand_filter && t->nzw <= 8;
+    if (filt)
+        for (int it = 0; it < n_items; ++it)
+            for (int o = 0; o < n_orient; ++o) {
+                OrientDesc& od = all[(size_t)it * n_orient + o];
+                od.samp = t->d_stage_samp + t->staged_soff[it];
+                od.nsamp = (int)t->staged[it].samp.size();
+            }
     // each item's 6 axis permutations (the flips of one share its spectrum)
     std::vector<OrientDesc> allb((size_t)n_items * 6);
     for (int it = 0; it < n_items; ++it) {
@@ -2285,6 +2489,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
     // queues the gated distance rebuild.  After that ids are >= 2, the
     // distance field is final and the rest of the run is queued without waits.
     bool first_pending = (id_offset == 0);
+    if (filt) TRY(t->tray_bits());
     std::vector<OrientDesc> host_ods(n_orient);
     for (int it = 0; it < n_items; ++it) {
         OrientDesc* d_odb = t->d_od_all + (size_t)it * n_orient;
@@ -2315,8 +2520,11 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             CKL();
         }
         std::vector<OrientDesc> hb(allb.begin() + (size_t)it * 6, allb.begin() + (size_t)(it + 1) * 6);
-        TRY(t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res, true, t->d_base_all + (size_t)it * 6,
-                            &hb));
+        if (filt) TRY(t->cand_filter(d_odb, host_ods, interlock != 0));
+        const int sst = t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res, true,
+                                        t->d_base_all + (size_t)it * 6, &hb);
+        t->cand_active = t->direct_active = false;
+        TRY(sst);
         if (d_per)
             CK(cudaMemcpyAsync(d_per + (size_t)it * n_orient, t->d_res, sizeof(ResultDev) * n_orient,
                                cudaMemcpyDeviceToDevice, t->st));
@@ -2335,6 +2543,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         k_place_done<<<1, 32, 0, t->st>>>(d_odb, t->d_ls, t->d_dec + it);
         CKL();
         TRY(t->rebuild_occ_gated());
+        if (filt) TRY(t->tray_bits_placed(d_odb, host_ods));
         if (first_pending) {
             TRY(t->rebuild_phi_gated());
             LoopState h;
@@ -2728,6 +2937,17 @@ int psb_set_share_flips(int on) {
     return PSB_OK;
 }
 
+int psb_set_cand_filter(int on) {
+    g_cand_filter = on != 0;
+    return PSB_OK;
+}
+
+int psb_set_direct_max(int n) {
+    if (n < 0 || n > kCandCap) return fail(PSB_ERR_ARG, "direct limit must be in [0, %d]", kCandCap);
+    g_direct_max = n;
+    return PSB_OK;
+}
+
 int psb_set_plane_variant(int v) {
     if (v != 2 && v != 3) return fail(PSB_ERR_ARG, "plane variant must be 2 or 3");
     g_plane_variant = v;
@@ -2790,6 +3010,17 @@ int psb_tray_fft_dims(const psb_tray* t, int* F) {
 int psb_tray_stream(psb_tray* t, void** stream) {
     if (!t || !stream) return fail(PSB_ERR_ARG, "null pointer");
     *stream = (void*)t->st;
+    return PSB_OK;
+}
+
+int psb_tray_work(psb_tray* t, unsigned long long* out, int reset) {
+    if (!t) return fail(PSB_ERR_ARG, "null pointer");
+    CK(cudaSetDevice(t->dev));
+    if (out) {
+        CK(cudaMemcpyAsync(out, t->d_work, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, t->st));
+        CK(cudaStreamSynchronize(t->st));
+    }
+    if (reset) CK(cudaMemsetAsync(t->d_work, 0, sizeof(unsigned long long) * 8, t->st));
     return PSB_OK;
 }
 

@@ -359,3 +359,70 @@ def test_orientation_sharded_packing_matches(gpu_core, cfg):
         assert (p.success, p.position, p.orientation_index) == (g[0], g[1], g[2] if g[0] else 0)
         if p.success:
             assert p.score == g[3]
+
+
+# --------------------------------------------------------------------------
+# candidate pre-filter of the packing loop: same results with and without it
+# --------------------------------------------------------------------------
+def _detail_run(items, tray_size, interlock):
+    from psacking_b200 import proposal as PR
+    from psacking_b200.rotations import orientation_maps
+    seq = PR.sorted_by_volume(items)
+    tray = PR.Tray(tray_size)
+    try:
+        res, per, _, final = tray.pack_detail(seq, orientation_maps(24), interlock)
+    finally:
+        tray.close()
+    key = lambda r: (r.found, r.x, r.y, r.z, r.score)  # noqa: E731
+    direct = sum(1 for r in per if r.diag & 0x800)
+    return [key(r) + (r.orientation,) for r in res], [key(r) for r in per], final, direct
+
+
+@pytest.mark.parametrize("case", ["config2-free", "config3-interlock", "config3-generic", "config3-plane2"])
+def test_cand_filter_same_results(gpu_core, case):
+    """Trays that fill up, so the filter skips orientations and planes and
+    decides orientations with few candidates directly: the placements, every
+    orientation's own result and the final tray are the same with the filter
+    off, on without the direct decisions, and on with them."""
+    from psacking_b200 import workloads
+    # (100, 64, 64): every axis has a specialised FFT length, so the default
+    # search takes the split flow that decides orientations directly
+    if case == "config2-free":
+        items, dims, il = workloads.config2_items(3)[:60], (100, 64, 64), False
+    else:
+        items, dims, il = workloads.config3_items(9)[:40], (100, 64, 64), True
+    gpu_core.set_fast_fft(case != "config3-generic")
+    gpu_core.set_plane_variant(2 if case == "config3-plane2" else 3)
+    try:
+        gpu_core.set_cand_filter(False)
+        want = _detail_run(items, dims, il)
+        gpu_core.set_cand_filter(True)
+        gpu_core.set_direct_max(0)
+        mid = _detail_run(items, dims, il)
+        gpu_core.set_direct_max(2048)
+        got = _detail_run(items, dims, il)
+    finally:
+        gpu_core.set_cand_filter(True)
+        gpu_core.set_direct_max(2048)
+        gpu_core.set_fast_fft(True)
+        gpu_core.set_plane_variant(3)
+    for run in (mid, got):
+        assert run[0] == want[0]
+        assert run[1] == want[1]
+        assert np.array_equal(run[2], want[2])
+    placed = sum(r[0] for r in want[0])
+    assert 0 < placed < len(items)   # the tray filled up: the filter had work to skip
+    assert want[3] == 0 and mid[3] == 0
+    if case in ("config2-free", "config3-interlock"):
+        assert got[3] > 0            # some orientations were decided directly
+    else:
+        assert got[3] == 0           # only the split flow decides directly
+
+
+def test_cand_filter_full_tray_against_oracle(gpu_core):
+    """A small tray packed until items stop fitting, against the oracle, in
+    both modes (the filter is on by default)."""
+    from psacking_b200 import workloads
+    items = workloads.config1_items(4)
+    run_both(items, (30, 30, 14), 6, True)
+    run_both(items, (30, 30, 14), 6, False)
