@@ -738,6 +738,8 @@ struct psb_tray {
     int *d_ccount = nullptr, *d_vcount = nullptr, *d_ncol = nullptr;   // per orientation: candidates,
                                                                       // verified free cells, item columns
     uint4* d_icols = nullptr;               // item column masks of direct orientations, stride nx*ny
+    int4* d_fsamp = nullptr;                // oriented, shift-sorted filter samples (k_cand_prep)
+    int* d_fbound = nullptr;                // their bucket bounds
     uint4* d_tbits = nullptr;               // free bits of the tray (k_tray_bits), tq uint4 per column
     int tq = 0;
     unsigned long long* d_work = nullptr;   // collision-kernel work counters (SearchBufs::work)
@@ -774,7 +776,7 @@ struct psb_tray {
         dfree(d_Ai, st); dfree(d_Bi, st); dfree(d_Pc, st); dfree(d_Pd, st); dfree(d_Dq, st); dfree(d_free, st); dfree(d_reach, st);
         dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
         dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_candplane, st); dfree(d_bases, st); dfree(d_best, st);
-        dfree(d_ccount, st); d_vcount = d_ncol = nullptr; dfree(d_icols, st);
+        dfree(d_ccount, st); d_vcount = d_ncol = nullptr; dfree(d_icols, st); dfree(d_fsamp, st); dfree(d_fbound, st);
         dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
@@ -875,6 +877,8 @@ struct psb_tray {
         d_vcount = d_ccount + c;
         d_ncol = d_ccount + 2 * c;
         TRY(dalloc(&d_icols, (size_t)nx * ny * c, st));
+        TRY(dalloc(&d_fsamp, (size_t)PSB_FSAMP * c, st));
+        TRY(dalloc(&d_fbound, (size_t)PSB_FBOUND * c, st));
         TRY(dalloc(&d_bases, 6, st)); TRY(dalloc(&d_best, c, st)); TRY(dalloc(&d_bestkey, c, st));
         TRY(dalloc(&d_diag, c, st)); TRY(dalloc(&d_errmax, c, st)); TRY(dalloc(&d_od, c, st)); TRY(dalloc(&d_rzs, c, st)); TRY(dalloc(&d_mids, c, st));
         TRY(dalloc(&d_res, c, st));
@@ -1095,12 +1099,17 @@ struct psb_tray {
             CK(cudaMemsetAsync(d_ccount, 0, sizeof(int) * 3 * cap, st));
             {
                 PROF("k_cand_filter", st);
-                if (tq == 1)
+                if (tq == 1) {
+                    k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
                     k_cand_filter<1><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
-                                                                        d_candplane, (long long)nx, d_ccount);
-                else
+                                                                        d_candplane, (long long)nx, d_ccount,
+                                                                        d_fsamp, d_fbound);
+                } else {
+                    k_cand_prep<2><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
                     k_cand_filter<2><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
-                                                                        d_candplane, (long long)nx, d_ccount);
+                                                                        d_candplane, (long long)nx, d_ccount,
+                                                                        d_fsamp, d_fbound);
+                }
             }
             CKL();
             k_cand_apply<<<(n + 127) / 128, 128, 0, st>>>(d_odb, n, d_ccount, 0, dmax);

@@ -25,6 +25,7 @@
 #define PSB_FSAMP 128          // sample voxels per item
 #define PSB_FILT_THREADS 128   // translations (y) per CTA row
 #define PSB_FBATCH 8           // filter samples whose loads are issued together
+#define PSB_FBOUND 9           // bucket bounds per orientation (up to 8 word shifts + 1)
 
 // Free bits of the tray: tbits[(i*ny + j)*nq + q] holds z in [128q, 128q+128),
 // bit set when the cell is empty; bits at z >= nz are clear (not free).
@@ -66,21 +67,53 @@ __global__ void k_tray_bits_box(const int32_t* __restrict__ tray, int nx, int ny
     }
 }
 
+// The samples of each orientation, oriented and sorted by their word shift
+// s.z / 32 (bucket k holds fs[o][bound[o][k] .. bound[o][k+1])), once per
+// item, so the filter's CTAs only load them.  One warp per orientation.
+// grid: n, block 32
+template <int NQ>
+__global__ void k_cand_prep(const OrientDesc* __restrict__ orients, int4* __restrict__ fs, int* __restrict__ fbound) {
+    constexpr int NW = 4 * NQ;
+    const int o = blockIdx.x, lane = threadIdx.x;
+    const OrientDesc& od = orients[o];
+    if (od.skip || od.nsamp <= 0) return;
+    const int ns = min(od.nsamp, PSB_FSAMP);
+    int4* S = fs + (size_t)o * PSB_FSAMP;
+    int* bound = fbound + (size_t)o * (PSB_FBOUND);
+    int base = 0;
+    for (int k = 0; k < NW; ++k) {
+        if (lane == 0) bound[k] = base;
+        for (int s0 = 0; s0 < ns; s0 += 32) {
+            const int s = s0 + lane;
+            int c[3] = {0, 0, 0};
+            if (s < ns) {
+                const int4 v = od.samp[s];
+                orient_voxel(od, v.x, v.y, v.z, c);
+            }
+            const bool hit = s < ns && (c[2] >> 5) == k;
+            const unsigned int b = __ballot_sync(0xffffffffu, hit);
+            if (hit) S[base + __popc(b & ((1u << lane) - 1u))] = make_int4(c[0], c[1], c[2], 0);
+            base += __popc(b);
+        }
+    }
+    if (lane == 0) bound[NW] = base;
+}
+
 __device__ __forceinline__ uint32_t low_bits(int n) { return n >= 32 ? 0xffffffffu : (n <= 0 ? 0u : (1u << n) - 1u); }
 
 // Candidate words of one x plane of one orientation: for rows y < Yv, the
 // words cand[(x*ny + y)*nzw + w] (the free-bit layout of the search, so the
 // collision pass can refine them in place), candplane[o][x] = "the plane
-// holds a candidate", and the orientation's candidate count.  Samples are
-// sorted by their word shift s.z / 32 so every shift is a compile-time
-// register index; lanes of a warp share the sample; loads go in batches; a
-// warp stops once none of its lanes holds a candidate.
+// holds a candidate", and the orientation's candidate count.  Samples come
+// sorted by their word shift s.z / 32 (k_cand_prep) so every shift is a
+// compile-time register index; lanes of a warp share the sample; loads go in
+// batches; a warp stops once none of its lanes holds a candidate.
 // grid: (max Xv, n_orient), block PSB_FILT_THREADS
 template <int NQ>
 __global__ void __launch_bounds__(PSB_FILT_THREADS)
 k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ tbits, int ny, int nzw,
               uint32_t* __restrict__ cand, long long sBits, unsigned char* __restrict__ candplane, long long pstride,
-              int* __restrict__ ccount) {
+              int* __restrict__ ccount, const int4* __restrict__ fs, const int* __restrict__ fbound) {
     constexpr int NW = 4 * NQ;
     const int o = blockIdx.y, x = blockIdx.x;
     const OrientDesc& od = orients[o];
@@ -91,25 +124,11 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
     __shared__ int3 S[PSB_FSAMP];
     __shared__ int bound[NW + 1];   // samples with shift k are S[bound[k] .. bound[k+1])
     const int ns = min(od.nsamp, PSB_FSAMP);
-    if (warp == 0) {
-        int base = 0;
-        for (int k = 0; k < NW; ++k) {
-            if (lane == 0) bound[k] = base;
-            for (int s0 = 0; s0 < ns; s0 += 32) {
-                const int s = s0 + lane;
-                int c[3] = {0, 0, 0};
-                if (s < ns) {
-                    const int4 v = od.samp[s];
-                    orient_voxel(od, v.x, v.y, v.z, c);
-                }
-                const bool hit = s < ns && (c[2] >> 5) == k;
-                const unsigned int b = __ballot_sync(0xffffffffu, hit);
-                if (hit) S[base + __popc(b & ((1u << lane) - 1u))] = make_int3(c[0], c[1], c[2]);
-                base += __popc(b);
-            }
-        }
-        if (lane == 0) bound[NW] = base;
+    for (int s = tid; s < ns; s += PSB_FILT_THREADS) {
+        const int4 v = __ldg(&fs[(size_t)o * PSB_FSAMP + s]);
+        S[s] = make_int3(v.x, v.y, v.z);
     }
+    if (tid <= NW) bound[tid] = __ldg(&fbound[(size_t)o * PSB_FBOUND + tid]);
     __syncthreads();
     uint32_t* cw = cand + (size_t)o * sBits + (size_t)x * ny * nzw;
     int any = 0, cnt = 0;
