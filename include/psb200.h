@@ -266,10 +266,15 @@ int psb_set_plane_variant(int v);
  * for comparisons.  No counterpart in the reference. */
 int psb_set_cand_filter(int on);
 /* Orientations the pre-filter leaves with at most n candidate translations
- * (default 2048; 0 disables) skip the transforms: each candidate is checked
+ * (default 1024; 0 disables) skip the transforms: each candidate is checked
  * exactly against the item's voxel columns and the free ones are scored by
  * exact integer proximity sums.  Same placements either way. */
 int psb_set_direct_max(int n);
+/* Pre-filter cut-off: a group of 32 translations stops testing samples when,
+ * after 32 samples, more than pct % of them still pass (open space, nothing
+ * to skip there); default 50, 0 tests every sample.  Any subset of samples
+ * keeps the filter exact, so results never depend on it. */
+int psb_set_filter_cut(int pct);
 /* The 24 orientations are 6 axis permutations x 4 flip patterns.  On: the
  * z,y transforms of each permutation run once per item and the x pass reads
  * every flip from them (row reversal, column map, conjugation, phase).  Off

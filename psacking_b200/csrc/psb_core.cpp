@@ -509,6 +509,8 @@ PYBIND11_MODULE(_core, m) {
           "Candidate pre-filter of the packing loop (default on; same placements either way).");
     m.def("set_direct_max", [](int n) { check(psb_set_direct_max(n)); }, py::arg("n"),
           "Candidate limit below which the packing loop decides an orientation without transforms.");
+    m.def("set_filter_cut", [](int pct) { check(psb_set_filter_cut(pct)); }, py::arg("pct"),
+          "Pre-filter cut-off percentage (default 50, 0 off; same placements either way).");
     m.def("set_share_flips", [](bool on) { check(psb_set_share_flips(on ? 1 : 0)); }, py::arg("on"),
           "Share the z,y transforms among the flips of each axis permutation, or transform each orientation on "
           "its own (the default).");

@@ -275,7 +275,10 @@ bool g_cand_filter = true;
 // orientations left with at most this many candidates are decided directly
 // (exact checks against the item's columns, exact proximity sums) instead of
 // by transforms; 0 disables
-int g_direct_max = 2048;
+int g_direct_max = 1024;
+// filter cut-off (k_cand_filter): a warp stops sampling when more than this
+// percentage of its translations survive the first samples; 0 disables
+int g_filter_cut = 50;
 
 // the 6 axis permutations of an orientation map, as base indices
 int perm_index(const int* a) {
@@ -346,6 +349,7 @@ int set_smem_attrs() {
     if (const char* e = getenv("PSB_SHARE_FLIPS")) g_share_flips = atoi(e) != 0;
     if (const char* e = getenv("PSB_CAND_FILTER")) g_cand_filter = atoi(e) != 0;
     if (const char* e = getenv("PSB_DIRECT_MAX")) g_direct_max = std::max(0, atoi(e));
+    if (const char* e = getenv("PSB_FILTER_CUT")) g_filter_cut = std::max(0, std::min(100, atoi(e)));
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
     TRY(set_max_dyn_smem(k_fft_mid<-1>));
@@ -1103,12 +1107,12 @@ struct psb_tray {
                     k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
                     k_cand_filter<1><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
                                                                         d_candplane, (long long)nx, d_ccount,
-                                                                        d_fsamp, d_fbound);
+                                                                        d_fsamp, d_fbound, g_filter_cut);
                 } else {
                     k_cand_prep<2><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
                     k_cand_filter<2><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
                                                                         d_candplane, (long long)nx, d_ccount,
-                                                                        d_fsamp, d_fbound);
+                                                                        d_fsamp, d_fbound, g_filter_cut);
                 }
             }
             CKL();
@@ -2954,6 +2958,12 @@ int psb_set_cand_filter(int on) {
 int psb_set_direct_max(int n) {
     if (n < 0 || n > kCandCap) return fail(PSB_ERR_ARG, "direct limit must be in [0, %d]", kCandCap);
     g_direct_max = n;
+    return PSB_OK;
+}
+
+int psb_set_filter_cut(int pct) {
+    if (pct < 0 || pct > 100) return fail(PSB_ERR_ARG, "filter cut-off must be a percentage in [0, 100]");
+    g_filter_cut = pct;
     return PSB_OK;
 }
 

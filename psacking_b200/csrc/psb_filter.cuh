@@ -26,6 +26,7 @@
 #define PSB_FILT_THREADS 128   // translations (y) per CTA row
 #define PSB_FBATCH 8           // filter samples whose loads are issued together
 #define PSB_FBOUND 9           // bucket bounds per orientation (up to 8 word shifts + 1)
+#define PSB_FCUT_AFTER 32      // samples before the cut-off test of k_cand_filter
 
 // Free bits of the tray: tbits[(i*ny + j)*nq + q] holds z in [128q, 128q+128),
 // bit set when the cell is empty; bits at z >= nz are clear (not free).
@@ -113,7 +114,7 @@ template <int NQ>
 __global__ void __launch_bounds__(PSB_FILT_THREADS)
 k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ tbits, int ny, int nzw,
               uint32_t* __restrict__ cand, long long sBits, unsigned char* __restrict__ candplane, long long pstride,
-              int* __restrict__ ccount, const int4* __restrict__ fs, const int* __restrict__ fbound) {
+              int* __restrict__ ccount, const int4* __restrict__ fs, const int* __restrict__ fbound, int cut_pct) {
     constexpr int NW = 4 * NQ;
     const int o = blockIdx.y, x = blockIdx.x;
     const OrientDesc& od = orients[o];
@@ -136,18 +137,48 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
         const int y = y0 + lane;
         const bool act = y < Yv;
         uint32_t c[NW];
+        int n0 = 0;
 #pragma unroll
-        for (int w = 0; w < NW; ++w) c[w] = act ? low_bits(Zv - 32 * w) : 0u;
+        for (int w = 0; w < NW; ++w) {
+            c[w] = act ? low_bits(Zv - 32 * w) : 0u;
+            n0 += __popc(c[w]);
+        }
+        // Cut-off: any subset of the samples gives a valid (wider) candidate
+        // set, so a warp whose translations still mostly survive after
+        // PSB_FCUT_AFTER samples (open space, nothing to skip) stops there.
+        bool stop = false, checked = cut_pct <= 0;
+        int done = 0;
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
             // shift of k whole words: word w of the shifted column is
             // funnel(T[w + k], T[w + k + 1]) >> (s.z & 31)
             const int s1 = bound[k + 1];
-            for (int s0 = bound[k]; s0 < s1; s0 += PSB_FBATCH) {
+            for (int s0 = bound[k]; s0 < s1 && !stop; s0 += PSB_FBATCH) {
                 uint32_t a = 0u;
+                int nb = 0;
 #pragma unroll
-                for (int w = 0; w < NW; ++w) a |= c[w];
-                if (!__any_sync(0xffffffffu, a != 0u)) break;
+                for (int w = 0; w < NW; ++w) {
+                    a |= c[w];
+                    nb += __popc(c[w]);
+                }
+                if (!__any_sync(0xffffffffu, a != 0u)) {
+                    stop = true;
+                    break;
+                }
+                if (!checked && done >= PSB_FCUT_AFTER) {
+                    checked = true;
+                    int t0 = n0, t1 = nb;
+#pragma unroll
+                    for (int d = 16; d > 0; d >>= 1) {
+                        t0 += __shfl_xor_sync(0xffffffffu, t0, d);
+                        t1 += __shfl_xor_sync(0xffffffffu, t1, d);
+                    }
+                    if ((long long)t1 * 100 > (long long)t0 * cut_pct) {
+                        stop = true;
+                        break;
+                    }
+                }
+                done += PSB_FBATCH;
                 uint4 v[PSB_FBATCH][NQ];
                 int off[PSB_FBATCH];
 #pragma unroll

@@ -383,7 +383,8 @@ def test_cand_filter_same_results(gpu_core, case):
     """Trays that fill up, so the filter skips orientations and planes and
     decides orientations with few candidates directly: the placements, every
     orientation's own result and the final tray are the same with the filter
-    off, on without the direct decisions, and on with them."""
+    off, on with every sample and no direct decisions, and on with the
+    defaults (sampling cut-off, direct decisions)."""
     from psacking_b200 import workloads
     # (100, 64, 64): every axis has a specialised FFT length, so the default
     # search takes the split flow that decides orientations directly
@@ -398,12 +399,15 @@ def test_cand_filter_same_results(gpu_core, case):
         want = _detail_run(items, dims, il)
         gpu_core.set_cand_filter(True)
         gpu_core.set_direct_max(0)
+        gpu_core.set_filter_cut(0)       # every sample tested
         mid = _detail_run(items, dims, il)
-        gpu_core.set_direct_max(2048)
+        gpu_core.set_direct_max(1024)
+        gpu_core.set_filter_cut(50)      # the defaults
         got = _detail_run(items, dims, il)
     finally:
         gpu_core.set_cand_filter(True)
-        gpu_core.set_direct_max(2048)
+        gpu_core.set_direct_max(1024)
+        gpu_core.set_filter_cut(50)
         gpu_core.set_fast_fft(True)
         gpu_core.set_plane_variant(3)
     for run in (mid, got):
