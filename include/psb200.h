@@ -262,7 +262,9 @@ int psb_set_plane_variant(int v);
  * an item's collision transforms, a bit-parallel test of up to 128 of its
  * voxels against the tray proves most translations (and often whole
  * orientations or x planes) blocked; those are skipped, every other cell is
- * decided exactly as before.  Same placements either way; the switch exists
+ * decided exactly as before.  It starts once the tray's occupied cells plus
+ * the items searched so far reach a quarter of the tray (before that it
+ * rarely rules anything out).  Same placements either way; the switch exists
  * for comparisons.  No counterpart in the reference. */
 int psb_set_cand_filter(int on);
 /* Orientations the pre-filter leaves with at most n candidate translations

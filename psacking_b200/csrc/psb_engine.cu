@@ -747,6 +747,7 @@ struct psb_tray {
     uint4* d_tbits = nullptr;               // free bits of the tray (k_tray_bits), tq uint4 per column
     int tq = 0;
     unsigned long long* d_work = nullptr;   // collision-kernel work counters (SearchBufs::work)
+    size_t occ = 0;                         // occupied cells of the tray, kept on the host
     OrientDesc* d_bases = nullptr;          // their descriptors (synchronous searches)
     unsigned int* d_diag = nullptr;
     unsigned int* d_errmax = nullptr;
@@ -998,6 +999,8 @@ struct psb_tray {
     int set(const int32_t* tray, const int32_t* phi) {
         CK(cudaSetDevice(dev));
         if (has_negative(tray, V)) return fail(PSB_ERR_ARG, "tray holds negative values; item ids must be >= 0");
+        occ = 0;
+        for (size_t i = 0; i < V; ++i) occ += tray[i] != 0;
         CK(cudaMemcpyAsync(d_tray, tray, sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
         if (phi) {
             CK(cudaMemcpyAsync(d_phi, phi, sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
@@ -2229,7 +2232,9 @@ int psb_tray_place(psb_tray* t, const int32_t* item, int ex, int ey, int ez, int
     int32_t dims[3] = {ex, ey, ez};
     std::vector<OrientDesc> ods;
     TRY(stage_arrays(t, items, dims, 1, &ods));
-    return t->place(ods[0], px, py, pz, item_id, nullptr);
+    TRY(t->place(ods[0], px, py, pz, item_id, nullptr));
+    t->occ += (size_t)std::max(0, ods[0].nvox);
+    return PSB_OK;
 }
 
 int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items) {
@@ -2503,6 +2508,12 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
     // distance field is final and the rest of the run is queued without waits.
     bool first_pending = (id_offset == 0);
     if (filt) TRY(t->tray_bits());
+    // The filter rules translations out only where occupied cells block
+    // them: while the tray's cells plus every item searched so far (placed
+    // or not: an upper bound of the occupancy) fill less than a quarter of
+    // the tray it rarely skips anything and only costs its kernels, so it
+    // starts after that.  Its results are exact either way.
+    size_t occ_est = t->occ;
     std::vector<OrientDesc> host_ods(n_orient);
     for (int it = 0; it < n_items; ++it) {
         OrientDesc* d_odb = t->d_od_all + (size_t)it * n_orient;
@@ -2533,7 +2544,8 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             CKL();
         }
         std::vector<OrientDesc> hb(allb.begin() + (size_t)it * 6, allb.begin() + (size_t)(it + 1) * 6);
-        if (filt) TRY(t->cand_filter(d_odb, host_ods, interlock != 0));
+        if (filt && occ_est * 4 >= t->V) TRY(t->cand_filter(d_odb, host_ods, interlock != 0));
+        occ_est += t->staged[it].vox.size();
         const int sst = t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res, true,
                                         t->d_base_all + (size_t)it * 6, &hb);
         t->cand_active = t->direct_active = false;
@@ -2596,6 +2608,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         r.n_candidates = dec[it].ncand;
         r.err_ratio = dec[it].err_ratio;
         out_placements[it] = r;
+        if (r.found) t->occ += t->staged[it].vox.size();   // a placement writes every item voxel
     }
     if (h.err & 1u) return fail(PSB_ERR_LIMIT, "flood fill union-find hit its iteration limit");
     if (h.err & 2u) return fail(PSB_ERR_LIMIT, "tie-guard candidates exceeded the capacity %d", kCandCap);
