@@ -1,0 +1,117 @@
+"""The candidate pre-filter's exactness argument and word arithmetic, on the
+CPU (no GPU call).
+
+The packing loop's pre-filter (psacking_b200/csrc/psb_filter.cuh) keeps, per
+(x, y) column of translations, the z bits where a sample S of the item's
+voxels lands on empty tray cells.  Two facts make it safe, checked here
+against the oracle's exact collision count (oracle/psb_oracle.py corr_direct,
+the reference's collision_grid semantics):
+  * every collision-free translation is a candidate, for ANY sample subset
+    (the filter may stop sampling early), and with all voxels sampled the
+    candidates are exactly the free translations;
+  * the kernel's word arithmetic (tray columns as 32-bit words, a sample at
+    height s.z shifting by s.z // 32 whole words and a funnel shift of
+    s.z % 32) gives the same bits as the plain boolean definition.
+"""
+import numpy as np
+import pytest
+
+from oracle import psb_oracle as O
+
+
+def free_translations(tray, item):
+    """Boolean [Xv, Yv, Zv]: collision-free translations (count == 0)."""
+    hi = np.argwhere(item > 0).max(axis=0)
+    c = O.corr_direct((tray != 0).astype(np.int64), (item > 0).astype(np.int64))
+    Xv, Yv, Zv = (np.array(tray.shape) - hi)
+    return c[:Xv, :Yv, :Zv] == 0
+
+
+def candidates(tray, item, samples):
+    """Boolean [Xv, Yv, Zv]: translations where every sample lands on an
+    empty cell (the filter's definition)."""
+    hi = np.argwhere(item > 0).max(axis=0)
+    Xv, Yv, Zv = (np.array(tray.shape) - hi)
+    empty = tray == 0
+    cand = np.ones((Xv, Yv, Zv), bool)
+    for sx, sy, sz in samples:
+        cand &= empty[sx:sx + Xv, sy:sy + Yv, sz:sz + Zv]
+    return cand
+
+
+def words_of(col_bits, nw):
+    """Bit list along z -> nw little-endian 32-bit words."""
+    w = [0] * nw
+    for z, b in enumerate(col_bits):
+        if b:
+            w[z >> 5] |= 1 << (z & 31)
+    return w
+
+
+def funnel_r(lo, hi, off):
+    return (((hi << 32) | lo) >> off) & 0xFFFFFFFF
+
+
+def candidates_words(tray, item, samples):
+    """The same candidates through the kernel's word arithmetic (k_cand_filter:
+    c[w] &= funnel(T[w + k], T[w + k + 1]) >> off, k = s.z // 32)."""
+    hi = np.argwhere(item > 0).max(axis=0)
+    nx, ny, nz = tray.shape
+    Xv, Yv, Zv = (nx - hi[0], ny - hi[1], nz - hi[2])
+    nw = 4 * ((((nz + 31) // 32) + 3) // 4)   # words per tray column (uint4 granules)
+    T = {(i, j): words_of(tray[i, j] == 0, nw) for i in range(nx) for j in range(ny)}
+    out = np.zeros((Xv, Yv, Zv), bool)
+    for x in range(Xv):
+        for y in range(Yv):
+            c = [(0xFFFFFFFF if Zv - 32 * w >= 32 else ((1 << max(0, Zv - 32 * w)) - 1)) for w in range(nw)]
+            for sx, sy, sz in samples:
+                sx, sy, sz = int(sx), int(sy), int(sz)   # Python ints: no 64-bit wrap in the shifts
+                col = T[(x + sx, y + sy)]
+                k, off = sz >> 5, sz & 31
+                for w in range(nw):
+                    lo = col[w + k] if w + k < nw else 0
+                    hi_w = col[w + k + 1] if w + k + 1 < nw else 0
+                    c[w] &= funnel_r(lo, hi_w, off)
+            for z in range(Zv):
+                out[x, y, z] = (c[z >> 5] >> (z & 31)) & 1
+    return out
+
+
+def random_case(rng, shape, fill):
+    tray = (rng.random(shape) < fill).astype(np.int32) * rng.integers(1, 5, shape).astype(np.int32)
+    e = rng.integers(2, 6, 3)
+    item = (rng.random(tuple(e)) < 0.6).astype(np.int32)
+    item[0, 0, 0] = 1
+    item[e[0] - 1, e[1] - 1, e[2] - 1] = 1
+    return tray, item
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_any_sample_subset_keeps_every_free_translation(seed):
+    rng = np.random.default_rng(seed)
+    tray, item = random_case(rng, (12, 11, 40), 0.15)
+    free = free_translations(tray, item)
+    vox = [tuple(int(c) for c in v) for v in np.argwhere(item > 0)]
+    for m in (1, 3, 8, len(vox)):
+        pick = rng.choice(len(vox), size=m, replace=False)
+        cand = candidates(tray, item, [vox[i] for i in pick])
+        assert not (free & ~cand).any()           # free is a subset of the candidates
+    assert np.array_equal(candidates(tray, item, vox), free)   # all voxels: exactly the free set
+
+
+@pytest.mark.parametrize("seed,nz", [(0, 20), (1, 40), (2, 70), (3, 100)])
+def test_word_arithmetic_matches_the_boolean_definition(seed, nz):
+    """Columns of 20..100 cells, so samples shift by 0..3 whole words and
+    candidates straddle word boundaries."""
+    rng = np.random.default_rng(100 + seed)
+    tray, item = random_case(rng, (7, 6, nz), 0.1)
+    h = nz - 3                                   # samples up to z = nz - 4: shifts of up to 3 words
+    item = np.zeros((3, 2, h), np.int32)
+    item[0, 0, 0] = item[2, 1, -1] = item[1, 0, h // 2] = 1
+    for z in (31, 32, 63, 64):                   # samples on word boundaries
+        if z < h:
+            item[z % 3, z % 2, z] = 1
+    vox = [tuple(int(c) for c in v) for v in np.argwhere(item > 0)]
+    got = candidates_words(tray, item, vox)
+    assert np.array_equal(got, candidates(tray, item, vox))
+    assert np.array_equal(got, free_translations(tray, item))
