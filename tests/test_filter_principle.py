@@ -99,16 +99,17 @@ def test_any_sample_subset_keeps_every_free_translation(seed):
     assert np.array_equal(candidates(tray, item, vox), free)   # all voxels: exactly the free set
 
 
-@pytest.mark.parametrize("seed,nz", [(0, 20), (1, 40), (2, 70), (3, 100)])
+@pytest.mark.parametrize("seed,nz", [(0, 20), (1, 40), (2, 70), (3, 100), (4, 150)])
 def test_word_arithmetic_matches_the_boolean_definition(seed, nz):
-    """Columns of 20..100 cells, so samples shift by 0..3 whole words and
-    candidates straddle word boundaries."""
+    """Columns of 20..150 cells, so samples shift by 0..4 whole words,
+    candidates straddle word boundaries, and columns of more than 128 cells
+    take two 16-byte granules (the kernel's NQ = 2 form, eight words)."""
     rng = np.random.default_rng(100 + seed)
     tray, item = random_case(rng, (7, 6, nz), 0.1)
-    h = nz - 3                                   # samples up to z = nz - 4: shifts of up to 3 words
+    h = nz - 3                                   # samples up to z = nz - 4: shifts of up to 4 words
     item = np.zeros((3, 2, h), np.int32)
     item[0, 0, 0] = item[2, 1, -1] = item[1, 0, h // 2] = 1
-    for z in (31, 32, 63, 64):                   # samples on word boundaries
+    for z in (31, 32, 63, 64, 127, 128):         # samples on word boundaries
         if z < h:
             item[z % 3, z % 2, z] = 1
     vox = [tuple(int(c) for c in v) for v in np.argwhere(item > 0)]
