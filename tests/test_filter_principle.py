@@ -9,6 +9,8 @@ the reference's collision_grid semantics):
   * every collision-free translation is a candidate, for ANY sample subset
     (the filter may stop sampling early), and with all voxels sampled the
     candidates are exactly the free translations;
+  * the direct check of k_cand_verify (item columns as two mask words against
+    shifted tray words) is exactly "collision count == 0";
   * the kernel's word arithmetic (tray columns as 32-bit words, a sample at
     height s.z shifting by s.z // 32 whole words and a funnel shift of
     s.z % 32) gives the same bits as the plain boolean definition.
@@ -116,3 +118,44 @@ def test_word_arithmetic_matches_the_boolean_definition(seed, nz):
     got = candidates_words(tray, item, vox)
     assert np.array_equal(got, candidates(tray, item, vox))
     assert np.array_equal(got, free_translations(tray, item))
+
+
+def verify_columns(tray, item, x, y, z):
+    """k_cand_verify's test of one translation: item column (a, b) as two
+    mask words (bits c < 32, 32 <= c < 64); tray column (x + a, y + b) as
+    empty-cell words; free when no mask bit meets a non-empty cell of
+    funnel(T[z // 32 + j], T[z // 32 + j + 1]) >> z % 32."""
+    nx, ny, nz = tray.shape
+    nzw = (nz + 31) // 32
+    for a in range(item.shape[0]):
+        for b in range(item.shape[1]):
+            col = item[a, b] > 0
+            if not col.any():
+                continue
+            m = words_of(col, 2)
+            T = words_of(tray[x + a, y + b] == 0, nzw)
+            sh, off = z >> 5, z & 31
+            t0 = T[sh]
+            t1 = T[sh + 1] if sh + 1 < nzw else 0
+            t2 = T[sh + 2] if sh + 2 < nzw else 0
+            f0 = funnel_r(t0, t1, off)
+            f1 = funnel_r(t1, t2, off) if m[1] else 0
+            if (m[0] & ~f0 & 0xFFFFFFFF) | (m[1] & ~f1 & 0xFFFFFFFF):
+                return False
+    return True
+
+
+@pytest.mark.parametrize("seed,nz", [(0, 40), (1, 70), (2, 100)])
+def test_direct_column_check_matches_the_collision_count(seed, nz):
+    """Items up to 64 cells high (two mask words), translations across word
+    boundaries: the direct check is exactly "collision count == 0"."""
+    rng = np.random.default_rng(200 + seed)
+    tray = (rng.random((9, 8, nz)) < 0.08).astype(np.int32)
+    h = min(nz - 4, 60)
+    item = (rng.random((3, 3, h)) < 0.15).astype(np.int32)
+    item[0, 0, 0] = item[2, 2, h - 1] = 1
+    free = free_translations(tray, item)
+    Xv, Yv, Zv = free.shape
+    got = np.array([[[verify_columns(tray, item, x, y, z) for z in range(Zv)] for y in range(Yv)]
+                    for x in range(Xv)])
+    assert np.array_equal(got, free)
