@@ -3,7 +3,7 @@ CPU (no GPU call).
 
 The packing loop's pre-filter (psacking_b200/csrc/psb_filter.cuh) keeps, per
 (x, y) column of translations, the z bits where a sample S of the item's
-voxels lands on empty tray cells.  Two facts make it safe, checked here
+voxels lands on empty tray cells.  Three facts make it safe, checked here
 against the oracle's exact collision count (oracle/psb_oracle.py corr_direct,
 the reference's collision_grid semantics):
   * every collision-free translation is a candidate, for ANY sample subset
