@@ -312,6 +312,15 @@ def bitrev8(x: int) -> int:
     return int('{:08b}'.format(x & 255)[::-1], 2)
 
 
+_BITREV8 = np.array([int('{:08b}'.format(v)[::-1], 2) for v in range(256)], dtype=np.int64)
+
+
+def block_keys(idx: np.ndarray) -> np.ndarray:
+    """block_key over an array of linear indices."""
+    idx = np.asarray(idx, dtype=np.int64)
+    return (idx & ~np.int64(255)) | _BITREV8[idx & 255]
+
+
 def block_key(idx: int) -> int:
     """Tie order of argmin_reduction_kernel (fft3.cu:527-563) + the host finish
     (fft3.cu:1352-1357): lowest 256-block first (strict < over blocks), then
@@ -320,8 +329,42 @@ def block_key(idx: int) -> int:
     return (idx & ~255) | bitrev8(idx & 255)
 
 
-def _search_fields(item, tray, phi, interlock):
-    """Collision, proximity and the candidate mask of one orientation."""
+class TraySpectra:
+    """FP64 half spectra of one tray state (binary occupancy and phi) on the
+    circular grid s >= n per axis, computed once and shared by every
+    orientation searched against that state.  The reference keeps the tray's
+    spectra on the device between orientations the same way
+    (GPUTrayContext::initialize, fft3.cu:1106-1175).  The occupancy has the
+    same zero set of correlations as the reference's ID-valued tray for
+    non-negative ids, and its counts are small enough to round exactly."""
+
+    def __init__(self, tray, phi):
+        tray, phi = as_grid(tray), as_grid(phi)
+        self.shape = tray.shape
+        self.s = tuple(_next_fast(n) for n in self.shape)
+        self.occ = _rfftn((tray > 0).astype(np.float64), self.s, WORKERS)
+        self.phi = _rfftn(phi.astype(np.float64), self.s, WORKERS)
+        self.tray = tray
+        self.phi_grid = phi
+
+    def corr(self, spec_item, which):
+        c = _irfftn(np.conj(spec_item) * (self.occ if which == "occ" else self.phi), self.s,
+                    WORKERS)[:self.shape[0], :self.shape[1], :self.shape[2]]
+        r = np.rint(c)
+        err = float(np.max(np.abs(c - r))) if c.size else 0.0
+        if err > 0.05:
+            raise AssertionError(f"FP64 correlation not exact (max rounding residue {err})")
+        return r.astype(np.int64)
+
+
+def _search_fields(item, tray, phi, interlock, spectra=None):
+    """Collision, proximity and the candidate mask of one orientation.
+
+    With `spectra` (a TraySpectra of this tray and phi) the FFT correlations
+    reuse the tray's spectra and the item's spectrum is computed once for both
+    fields; the proximity is then computed only when some translation is a
+    candidate (prox is None otherwise).  Results are identical on the cells
+    the search reads: the valid box, where the circular correlation is exact."""
     nx, ny, nz = tray.shape
     padded = pad_to(item, tray.shape)
     _, hi = bounds(padded)
@@ -330,17 +373,26 @@ def _search_fields(item, tray, phi, interlock):
     if Xv > 0 and Yv > 0 and Zv > 0:
         valid[:Xv, :Yv, :Zv] = True
     lin = False
-    coll = corr_exact(tray, padded, linear=lin)
-    prox = corr_exact(phi, padded, linear=lin)
+    big = int(np.count_nonzero(padded)) * tray.size > 30_000_000
+    if spectra is not None and big:
+        FI = _rfftn(padded.astype(np.float64), spectra.s, WORKERS)
+        coll = spectra.corr(FI, "occ")
+        prox = None
+    else:
+        FI = None
+        coll = corr_exact(tray, padded, linear=lin)
+        prox = corr_exact(phi, padded, linear=lin)
     ok = valid & (coll == 0)
-    if interlock:
+    if interlock and ok.any():
         ex = (nx - 1 - hi[0], ny - 1 - hi[1], nz - 1 - hi[2])
         ex = tuple(max(0, e) for e in ex)
         ok = flood_reach(ok, ex)
+    if prox is None and ok.any():
+        prox = spectra.corr(FI, "phi")
     return ok, prox
 
 
-def search_one(item, tray, phi, mode="block", interlock=False):
+def search_one(item, tray, phi, mode="block", interlock=False, spectra=None):
     """One orientation: ((x,y,z), found, score).
 
     mode="scan"  -> fft_search_placement scoring (packing.cpp:590-642)
@@ -350,7 +402,7 @@ def search_one(item, tray, phi, mode="block", interlock=False):
     tray = as_grid(tray)
     phi = as_grid(phi)
     nx, ny, nz = tray.shape
-    ok, prox = _search_fields(item, tray, phi, interlock)
+    ok, prox = _search_fields(item, tray, phi, interlock, spectra)
     cand = np.flatnonzero(ok.ravel())
     if len(cand) == 0:
         return (-1, -1, -1), False, 0.0
@@ -369,16 +421,14 @@ def search_one(item, tray, phi, mode="block", interlock=False):
         approx = pr.astype(np.float64) + ((P * qz) * qz) * qz
         m = approx.min()
         near = np.flatnonzero(approx <= m + abs(m) * 1e-14 + 1e-300)
-        best = None
-        for t in near:
-            sc_t = score_block(int(pr[t]), int(k[t]), nz)
-            key = (sc_t, block_key(int(cand[t])))
-            if best is None or key < best:
-                best = key
-        sc, idx = best[0], None
-        for t in near:
-            if score_block(int(pr[t]), int(k[t]), nz) == sc and block_key(int(cand[t])) == best[1]:
-                idx = int(cand[t])
+        # exact scores of the near-minimal cells, once per distinct (prox, k)
+        pk = np.stack([pr[near].astype(np.int64), k[near].astype(np.int64)], axis=1)
+        uniq, inv = np.unique(pk, axis=0, return_inverse=True)
+        sc_u = np.array([score_block(int(p), int(kk), nz) for p, kk in uniq])
+        sc_n = sc_u[np.ravel(inv)]
+        sc = float(sc_n.min())
+        tied = cand[near[sc_n == sc]]
+        idx = int(tied[int(np.argmin(block_keys(tied)))])
         if not sc < FOUND_CUT:
             return (-1, -1, -1), False, 0.0
     i, rem = divmod(idx, ny * nz)
@@ -404,7 +454,7 @@ def fft_search_placement_with_cache(item, tray, tray_distance, generation=0):
     return search_one(item, tray, tray_distance, mode="block")
 
 
-def fft_search_batch(orientations, tray, tray_distance, generation=0, interlock=False):
+def fft_search_batch(orientations, tray, tray_distance, generation=0, interlock=False, spectra=None):
     """fft_search_batch / _interlocking_free (fft3.cu:1549-1632): orientations
     larger than the tray are skipped; strict < keeps the first best."""
     tray = as_grid(tray)
@@ -413,7 +463,7 @@ def fft_search_batch(orientations, tray, tray_distance, generation=0, interlock=
         it = as_grid(it)
         if any(it.shape[a] > tray.shape[a] for a in range(3)):
             continue
-        pos, found, sc = search_one(it, tray, tray_distance, mode="block", interlock=interlock)
+        pos, found, sc = search_one(it, tray, tray_distance, mode="block", interlock=interlock, spectra=spectra)
         if found and sc < best[2]:
             best = (pos, True, sc, o)
     if not best[1]:
@@ -488,9 +538,13 @@ def orientations(grid, n=1):
 
 
 def pack_voxels(items, tray_size, num_orientations=1, interlocking_free=False,
-                sort_by_volume=True, initial_tray=None):
+                sort_by_volume=True, initial_tray=None, fast=False, progress=None):
     """BinPacker.pack_voxels (packer.py:366-544) over the oracle searches.
-    Returns (tray, placements) with placements as dicts in original order."""
+    Returns (tray, placements) with placements as dicts in original order.
+
+    fast=True shares each tray state's spectra between the orientations of an
+    item (TraySpectra); the answers are the same.  progress(n_done, placement)
+    is called after every item when given."""
     proc = [np.asarray(it).astype(np.int32) for it in items]
     vols = [int(np.sum(it > 0)) for it in proc]
     if sort_by_volume:
@@ -510,8 +564,11 @@ def pack_voxels(items, tray_size, num_orientations=1, interlocking_free=False,
         best = (None, float("inf"), 0, item)
         found_any = False
         ors = orientations(item, num_orientations)
+        spectra = None
         if num_orientations > 1 or interlocking_free:
             phi = calculate_distance(tray)
+            if fast:
+                spectra = TraySpectra(tray, phi)
         if interlocking_free:
             valid, vidx = [], []
             for o, r in enumerate(ors):
@@ -520,7 +577,7 @@ def pack_voxels(items, tray_size, num_orientations=1, interlocking_free=False,
                     valid.append(r)
                     vidx.append(o)
             if valid:
-                pos, found, sc, bo = fft_search_batch(valid, tray, phi, interlock=True)
+                pos, found, sc, bo = fft_search_batch(valid, tray, phi, interlock=True, spectra=spectra)
                 if found and bo >= 0:
                     best = (pos, sc, vidx[bo], valid[bo])
                     found_any = True
@@ -530,7 +587,7 @@ def pack_voxels(items, tray_size, num_orientations=1, interlocking_free=False,
                 if any(r.shape[a] > tray_size[a] for a in range(3)):
                     continue
                 if num_orientations > 1:
-                    pos, found, sc = fft_search_placement_with_cache(r, tray, phi)
+                    pos, found, sc = search_one(r, tray, phi, mode="block", spectra=spectra)
                 else:
                     pos, found, sc = fft_search_placement(r, tray)
                 if found and sc < best[1]:
@@ -544,6 +601,8 @@ def pack_voxels(items, tray_size, num_orientations=1, interlocking_free=False,
         else:
             placements.append(dict(item_index=int(orig), position=None, score=None,
                                    success=False, volume=vols[orig], orientation_index=0))
+        if progress is not None:
+            progress(len(placements), placements[-1])
     placements.sort(key=lambda p: p["item_index"])
     return tray, placements
 

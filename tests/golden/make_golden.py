@@ -2,11 +2,13 @@
 
 Run here (where the reference tree is mounted), never on the GPU box:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py <reference checkout>
 
 How it works: the reference's tests (tests/test_core.py, test_bindings.py,
 test_distance_1d.py, test_distance_3d.py, test_distance_correctness.py,
-test_flood_fill.py, test_orientations.py) import `spectral_packer`.  This script
+test_flood_fill.py, test_orientations.py, and the whole-run suites
+test_packer.py and test_interlocking.py, whose cage trays pin the
+interlocking-free behaviour) import `spectral_packer`.  This script
 puts a stand-in `spectral_packer` package on sys.path whose functions are the
 CPU oracle (oracle/psb_oracle.py) and record every call.  It then runs those
 reference tests with pytest.  A test passes only if the oracle's answers meet
@@ -35,6 +37,7 @@ REPO = HERE.parent.parent
 TEST_FILES = [
     "test_core.py", "test_bindings.py", "test_distance_1d.py", "test_distance_3d.py",
     "test_distance_correctness.py", "test_flood_fill.py", "test_orientations.py",
+    "test_packer.py", "test_interlocking.py",
 ]
 BIG = 65536
 
@@ -96,6 +99,15 @@ def get_orientations(grid, num_orientations=1):
 def get_24_orientations(grid):
     return O.orientations(grid, 24)
 
+class PlacementInfo:
+    def __init__(self, d):
+        self.item_index = d["item_index"]
+        self.position = d["position"]
+        self.score = d["score"]
+        self.success = d["success"]
+        self.volume = d["volume"]
+        self.orientation_index = d["orientation_index"]
+
 class PackingResult:
     def __init__(self, tray, placements):
         self.tray = tray
@@ -104,29 +116,43 @@ class PackingResult:
         self.num_failed = len(placements) - self.num_placed
         self.density = O.density(tray)
         self.total_volume = int((tray > 0).sum())
-
-class _P:
-    def __init__(self, d):
-        self.__dict__.update(d)
-        self.position = d["position"]
+        idx = np.argwhere(tray > 0)
+        self.bounding_box = (tuple(int(v) for v in idx.min(axis=0)), tuple(int(v) for v in idx.max(axis=0))) \
+            if len(idx) else None
+    def get_item_mask(self, item_id):
+        return self.tray == item_id
+    def summary(self):
+        return ("Packing Result Summary\n" f"Items placed: {self.num_placed}\n"
+                f"Packing density: {self.density:.1%}\n")
 
 class BinPacker:
     def __init__(self, tray_size, voxel_resolution=128, height_penalty=1e8,
                  num_orientations=1, interlocking_free=False):
+        if len(tray_size) != 3:
+            raise ValueError("tray_size must be a 3-tuple")
+        if any(s <= 0 for s in tray_size):
+            raise ValueError("tray_size dimensions must be positive")
+        if voxel_resolution <= 0:
+            raise ValueError("voxel_resolution must be positive")
         if num_orientations not in (1, 4, 6, 24):
             raise ValueError("num_orientations must be 1, 4, 6, or 24")
         self.tray_size = tuple(tray_size)
+        self.voxel_resolution = voxel_resolution
+        self.height_penalty = height_penalty
         self.num_orientations = num_orientations
         self.interlocking_free = interlocking_free
+    def __repr__(self):
+        return f"BinPacker(tray_size={self.tray_size}, voxel_resolution={self.voxel_resolution})"
     def pack_voxels(self, items, sort_by_volume=True, initial_tray=None):
         if len(items) == 0:
             raise ValueError("items list cannot be empty")
         tray, pl = O.pack_voxels(items, self.tray_size, self.num_orientations,
                                  self.interlocking_free, sort_by_volume, initial_tray)
         _rec("pack_voxels", ([np.array(i) for i in items], self.tray_size, self.num_orientations,
-                             self.interlocking_free, sort_by_volume),
+                             self.interlocking_free, sort_by_volume,
+                             None if initial_tray is None else _arr(O.as_grid(initial_tray))),
              (tray, [(p["position"], p["success"], p["orientation_index"], p["score"]) for p in pl]))
-        return PackingResult(tray, [_P(p) for p in pl])
+        return PackingResult(tray, [PlacementInfo(p) for p in pl])
     def pack_single(self, item, tray=None):
         if tray is None:
             tray = np.zeros(self.tray_size, dtype=np.int32)
@@ -176,8 +202,10 @@ def _pack(obj):
     return enc(obj), arrays
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     ref_tests = Path(ref_root) / "tests"
+    if not ref_tests.is_dir():
+        raise SystemExit(f"{ref_tests} is not a directory: pass the reference checkout")
     work = Path(tempfile.mkdtemp(prefix="psb_golden_"))
     try:
         (work / "spectral_packer").mkdir()
@@ -238,4 +266,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*(sys.argv[1:2]))
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <reference checkout>")
+    main(sys.argv[1])

@@ -40,11 +40,12 @@ def _replay(core, r):
         return core.place_in_tray(a[0], a[1], a[2], a[3])
     if fn == "pack_voxels":
         from psacking_b200 import BinPacker
-        items, tray_size, n_orient, interlock, sort = a
+        items, tray_size, n_orient, interlock, sort = a[:5]
+        initial = a[5] if len(a) > 5 else None
         outs = []
         for engine in ("native", "calls"):
             res = BinPacker(tuple(tray_size), num_orientations=n_orient, interlocking_free=interlock,
-                            engine=engine).pack_voxels(list(items), sort_by_volume=sort)
+                            engine=engine).pack_voxels(list(items), sort_by_volume=sort, initial_tray=initial)
             outs.append((res.tray, [(p.position, p.success, p.orientation_index, p.score) for p in res.placements]))
         assert same_output(outs[0], outs[1])
         return outs[0]

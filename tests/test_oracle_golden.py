@@ -21,8 +21,9 @@ FUNCS = {
 
 
 def _pack(a):
-    items, tray_size, n_orient, interlock, sort = a
-    tray, pl = O.pack_voxels(items, tuple(tray_size), n_orient, interlock, sort)
+    items, tray_size, n_orient, interlock, sort = a[:5]
+    initial = a[5] if len(a) > 5 else None
+    tray, pl = O.pack_voxels(items, tuple(tray_size), n_orient, interlock, sort, initial_tray=initial)
     return (tray, [(None if p["position"] is None else tuple(p["position"]), p["success"],
                     p["orientation_index"], p["score"]) for p in pl])
 

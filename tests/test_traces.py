@@ -1,0 +1,96 @@
+"""The golden packing traces (tests/golden/traces, made by
+tests/golden/make_traces.py with the oracle) are self-consistent and
+reproducible on CPU: replaying every record rebuilds a tray with the recorded
+SHA-256 and density, no record overlaps the tray it is placed in, and the
+oracle recomputes the short traces and the first items of the long ones."""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import psb_oracle as O
+from oracle.trace_replay import load_trace, oriented, replay_states, trace_items
+
+TRACES = sorted(p.stem for p in (Path(__file__).resolve().parent / "golden" / "traces").glob("*.json"))
+
+
+def test_traces_present():
+    assert {f"config1_seed{s}" for s in range(10)} <= set(TRACES)
+    assert "config2_seed0" in TRACES
+    assert "config3_seed1" in TRACES
+
+
+@pytest.mark.parametrize("name", TRACES)
+def test_trace_replays_to_recorded_tray(name):
+    tr = load_trace(name)
+    seq = trace_items(tr)
+    assert len(tr["records"]) == len(seq) == tr["n_items"]
+    final = replay_states(tr, seq, [len(seq)])[len(seq)]
+    assert hashlib.sha256(final.tobytes()).hexdigest() == tr["tray_sha256"]
+    assert O.density(final) == tr["density"]
+    assert sum(r[0] for r in tr["records"]) == tr["num_placed"] == int(final.max())
+
+
+@pytest.mark.parametrize("name", [f"config1_seed{s}" for s in range(10)])
+def test_oracle_recomputes_config1_traces(name):
+    tr = load_trace(name)
+    seq = trace_items(tr)
+    tray, pl = O.pack_voxels(seq, tuple(tr["tray"]), 1, False, sort_by_volume=False)
+    got = [[1, *p["position"], p["orientation_index"], p["score"]] if p["success"] else [0, -1, -1, -1, 0, 0.0]
+           for p in pl]
+    assert got == tr["records"]
+    assert hashlib.sha256(tray.tobytes()).hexdigest() == tr["tray_sha256"]
+
+
+@pytest.mark.parametrize("name,k", [("config2_seed0", 2), ("config3_seed1", 1)])
+def test_oracle_recomputes_trace_prefix(name, k):
+    """The first k items of a long trace, from the tray state replayed
+    before them, by the plain (uncached) oracle searches."""
+    tr = load_trace(name)
+    seq = trace_items(tr)
+    tray, pl = O.pack_voxels(seq[:k], tuple(tr["tray"]), tr["num_orientations"], tr["interlocking_free"],
+                             sort_by_volume=False)
+    got = [[1, *p["position"], p["orientation_index"], p["score"]] if p["success"] else [0, -1, -1, -1, 0, 0.0]
+           for p in pl]
+    assert got == tr["records"][:k]
+
+
+def test_replayed_states_are_placements_of_the_items():
+    tr = load_trace("config2_seed0")
+    seq = trace_items(tr)
+    states = replay_states(tr, seq, [0, 5, 6])
+    assert not states[0].any()
+    f, x, y, z, o, _ = tr["records"][5]
+    it = oriented(seq[5], o, tr["num_orientations"])
+    diff = states[6] != states[5]
+    if f:
+        assert diff.sum() == int((it > 0).sum())
+        sub = states[6][x:x + it.shape[0], y:y + it.shape[1], z:z + it.shape[2]]
+        assert np.array_equal(sub > 0, (it > 0) | (states[5][x:x + it.shape[0], y:y + it.shape[1],
+                                                              z:z + it.shape[2]] > 0))
+    else:
+        assert not diff.any()
+
+
+def test_bench_reference_sample_covers_the_stream():
+    import bench
+    seen = set()
+    for step in range(40):
+        pos = bench.ref_positions(step)
+        assert len(pos) == bench.REF_PER_STEP and all(0 <= p < bench.N_ITEMS for p in pos)
+        seen.update(pos)
+    assert len(seen) > 100   # the moving offset spreads the samples over the stream
+
+
+def test_oracle_spectra_cache_gives_the_same_runs():
+    """TraySpectra (one tray spectrum per item, shared by its orientations)
+    is an evaluation order of the same exact arithmetic."""
+    from oracle.trace_replay import load_workloads
+    W = load_workloads()
+    items = W.config2_items(7)[:4]
+    for inter in (False, True):
+        a = O.pack_voxels(items, (60, 50, 40), 24, inter)
+        b = O.pack_voxels(items, (60, 50, 40), 24, inter, fast=True)
+        assert a[1] == b[1] and np.array_equal(a[0], b[0])
