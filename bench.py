@@ -14,11 +14,18 @@ ours      value: the device-resident loop (psb_pack_staged) with the items
           e2e:   BinPacker.pack_voxels on host numpy arrays through the same
           C ABI, host->device item upload and device->host tray readback
           inside the timed region.
+          parity: every item's (found, position, orientation, score) of
+          the timed run against the oracle's trace of the same stream
+          (tests/golden/traces/config3_seed1.json).
 reference the reference's CPU implementation of the path, restated by the
           oracle (oracle/psb_oracle.py; the reference's own CPU path needs
-          FFTW3, absent on this image), on all host cores; each step is one
-          item (24 orientations, interlocking-free) searched and placed on a
-          tray that already holds the first item.
+          FFTW3, absent on this image), on all host cores.  Each step times
+          a systematic sample of the stream's items, each searched (24
+          orientations, interlocking-free) and placed on the tray state
+          replayed from the oracle's trace; value = the run's placed items /
+          (350 x mean seconds per item).  With oracle/_ref built, the line
+          also carries `cuda_reference`: the reference's own cuFFT module
+          and BinPacker timed the same way on the GPU.
 Multi-GPU (torchrun): every rank packs its own independent tray of its own
 item stream (no data-path collective); value = items placed on all ranks /
 max over ranks of the device time.
@@ -146,14 +153,15 @@ def orientations_searched(seq, maps):
                if all(apply_map(it, row).shape[a] <= TRAY[a] for a in range(3)))
 
 
-def algorithmic_bytes(work, F):
+def algorithmic_bytes(work, F, launches):
     """Bytes the two collision kernels must move for the work they did, from
     the engine's work counters (psb_tray_work) over the timed steps:
-      k_xpass_coll per orientation it transforms: read the occupancy half
-        spectrum (Fx*Fy*Hz*8 B), read the item's z,y-transformed columns
-        (ex*Fy*Hz*8), write the collision product of the planes it stores
-        (Fy*Hz*8 per plane: the valid planes, or with the candidate filter
-        only those holding a candidate);
+      k_xpass_coll per launch: read the occupancy half spectrum once
+        (Fx*Fy*Hz*8 B; every orientation of the launch reads the same
+        spectrum, which stays in L2); per orientation it transforms: read the
+        item's z,y-transformed columns (ex*Fy*Hz*8), write the collision
+        product of the planes it stores (Fy*Hz*8 per plane: the valid planes,
+        or with the candidate filter only those holding a candidate);
       k_plane_coll per plane it processes: read that plane's product
         (Fy*Hz*8), write the free words of the row pairs it computes
         (2*ceil(nz/32)*4 per pair).
@@ -163,9 +171,40 @@ def algorithmic_bytes(work, F):
     Fx, Fy, Fz = F
     Hz = Fz // 2 + 1
     col = Fy * Hz * 8
-    xb = work[0] * Fx * col + work[1] * col + work[2] * col
+    xb = launches.get("k_xpass_coll", 0) * Fx * col + work[1] * col + work[2] * col
     pb = work[3] * col + work[4] * 2 * ((TRAY[2] + 31) // 32) * 4
     return {"k_xpass_coll": xb, "k_plane_coll": pb}
+
+
+def kernel_source_sha():
+    """Hash of the engine's CUDA sources: a DRAM-traffic figure measured with
+    ncu on another build of the kernels is not reported."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in sorted((ROOT / "psacking_b200" / "csrc").glob("*.cu*")):
+        h.update(f.name.encode())
+        h.update(f.read_bytes())
+    return h.hexdigest()[:16]
+
+
+def as_record(r):
+    """A psb_result in the golden traces' record form."""
+    if not r.found:
+        return [0, -1, -1, -1, 0, 0.0]
+    return [1, int(r.x), int(r.y), int(r.z), int(r.orientation), float(r.score)]
+
+
+def trace_parity(recs):
+    """Item-by-item comparison with the oracle's trace of the stream."""
+    tf = ROOT / "tests" / "golden" / "traces" / f"{TRACE_NAME}.json"
+    if not tf.exists():
+        return {"checked": False, "why": f"{tf.name} missing"}
+    want = json.loads(tf.read_text())["records"]
+    if len(want) != len(recs):
+        return {"checked": False, "why": f"stream of {len(recs)} items, trace of {len(want)}"}
+    bad = [i for i, (a, b) in enumerate(zip(recs, want)) if a != b]
+    return {"checked": True, "items": len(recs), "identical": len(recs) - len(bad),
+            "first_mismatch": bad[0] if bad else None}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -243,6 +282,8 @@ def run_ours(args, rank, world, local_rank):
     cands = [r.n_candidates for r in res]
     err_ratio = max(r.err_ratio for r in res)
     same = placed_first == [(r.found, r.x, r.y, r.z, r.orientation) for r in res]
+    recs = [as_record(r) for r in res]
+    parity = trace_parity(recs) if rank == 0 else {"checked": False, "why": "no trace of this rank's stream"}
     total_ms = sum(ms)
     Fdims = (ctypes.c_int * 3)()
     check(lib, lib.psb_tray_fft_dims(t, Fdims))
@@ -267,6 +308,14 @@ def run_ours(args, rank, world, local_rank):
     if args.value_only:
         e2e_ms, r = [total_ms / args.steps], None
     e2e_placed = r.num_placed if r is not None else placed
+    e2e_same = None
+    if r is not None:
+        order = np.argsort([int(np.sum(i > 0)) for i in items])[::-1]
+        e2e_recs = []
+        for k in order:
+            p = r.placements[int(k)]
+            e2e_recs.append([1, *p.position, p.orientation_index, p.score] if p.success else [0, -1, -1, -1, 0, 0.0])
+        e2e_same = e2e_recs == recs
     h2d = sum(s.nbytes for s in seq) + sum(int(np.count_nonzero(s)) * 16 for s in seq) + tray0.nbytes
     d2h = tray0.nbytes + len(seq) * 40
     check(lib, lib.psb_tray_destroy(t))
@@ -288,7 +337,7 @@ def run_ours(args, rank, world, local_rank):
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    ab = algorithmic_bytes(list(work), F)
+    ab = algorithmic_bytes(list(work), F, {k: v[0] for k, v in prof_top.items()})
     dom = max((k for k in prof_top if k in ("k_xpass_coll", "k_plane_coll")), key=lambda k: prof_top[k][1],
               default=None)
     top = max(prof, key=lambda k: prof[k][1]) if prof else None
@@ -300,7 +349,9 @@ def run_ours(args, rank, world, local_rank):
         traffic = None
         tf = ROOT / "profiles" / f"{dom}_traffic.json"
         if tf.exists():
-            traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+            tj = json.loads(tf.read_text())
+            if tj.get("kernel_source_sha") == kernel_source_sha():
+                traffic = tj.get("bytes_per_launch")
         roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": int(per_launch_bytes), "avg_launch_ms": ms_l / n_l}
@@ -319,12 +370,13 @@ def run_ours(args, rank, world, local_rank):
                        "plane_pass_planes": work[3] / args.steps, "plane_pass_row_pairs": work[4] / args.steps},
                    "l2": "256 MiB buffer written before every step", "parallelism": f"replicas x{world} (independent trays)",
                    "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag,
+                   "parity_vs_oracle_trace": parity,
                    "tie_guard": {"candidates_per_item_mean": round(statistics.mean(cands), 1),
                                  "candidates_per_item_max": max(cands),
                                  "max_fp32_error_over_bound": round(err_ratio, 4)}},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_mean, 3),
-                "placements_match_value_leg": e2e_placed == placed},
+                "placements_match_value_leg": e2e_same},
         "gpu_launches": int(launches // args.steps * args.steps),
         "kernel_share": share, "top_kernel": top,
         "kernel_ms_per_step": {k: round(v[1], 3) for k, v in prof.items()},
@@ -465,44 +517,124 @@ def _density(tray):
     return float(len(idx) / np.prod(ext))
 
 
-def cpu_sample_setup():
-    """The bounded CPU sample: the tray after the first item of the workload is
-    placed, and the second item (24 orientations, interlocking-free)."""
-    from oracle import psb_oracle as O
-    items = sorted_items(workload(0))
-    tray = np.zeros(TRAY, np.int32)
-    tray, _ = O.pack_voxels([items[0]], TRAY, N_ORIENT, True, False)
-    return items[1], tray
+# ---------------------------------------------------------------------------
+# CPU sample (the oracle) and the reference's own GPU path, on tray states
+# replayed from the oracle's trace of the benchmark stream
+# ---------------------------------------------------------------------------
+TRACE_NAME = "config3_seed1"   # the oracle's trace of workload(0)
+REF_PER_STEP = 3               # items per reference-arm step
+CUDA_REF_POSITIONS = list(range(0, N_ITEMS, 25))   # the reference GPU path's sample
 
 
-def time_cpu_sample(item, tray):
+def ref_positions(step, m=REF_PER_STEP, n=N_ITEMS):
+    """A systematic sample of m search positions spread over the stream; the
+    offset moves with the step, so the steps together cover the stream."""
+    stride = n / m
+    off = (step * 37) % int(stride)
+    return [int(off + j * stride) for j in range(m)]
+
+
+def time_cpu_items(trace, seq, states, positions):
+    """The oracle's search + placement of each listed item against its
+    replayed tray state: (seconds per item, results in trace record form)."""
     from oracle import psb_oracle as O
-    t0 = time.perf_counter()
-    tray2, pl = O.pack_voxels([item], TRAY, N_ORIENT, True, False, initial_tray=tray)
-    dt = time.perf_counter() - t0
-    return dt, sum(1 for p in pl if p["success"])
+    from oracle.trace_replay import record
+    secs, recs = [], []
+    for pos in positions:
+        t0 = time.perf_counter()
+        _, pl = O.pack_voxels([seq[pos]], TRAY, N_ORIENT, True, False, initial_tray=states[pos], fast=True)
+        secs.append(time.perf_counter() - t0)
+        p = pl[0]
+        recs.append(record(p["success"], p["position"], p["orientation_index"], p["score"]))
+    return secs, recs
+
+
+def cuda_reference(timeout=600):
+    """The reference's own cuFFT path (oracle/_ref, built from the reference
+    sources by oracle/Makefile) on CUDA_REF_POSITIONS of the stream, in a
+    child process; None when it is not built or no GPU is visible."""
+    ref = ROOT / "oracle" / "_ref" / "spectral_packer"
+    if not ref.exists() or not list(ref.glob("_core*.so")):
+        return {"unavailable": "oracle/_ref not built (make -C oracle REF=<reference checkout>)"}
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        out = Path(td) / "ref.json"
+        cmd = [sys.executable, str(ROOT / "oracle" / "ref_cuda.py"), "sample", "--positions",
+               ",".join(str(p) for p in CUDA_REF_POSITIONS), "--out", str(out)]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": f"reference GPU sample exceeded {timeout} s"}
+        if r.returncode != 0 or not out.exists():
+            return {"unavailable": "reference GPU sample failed: " + (r.stderr.strip().splitlines() or ["?"])[-1]}
+        doc = json.loads(out.read_text())
+    return doc
+
+
+def cpu_baseline():
+    """The GPU arm's reported CPU baseline: the oracle on one step's sample."""
+    from oracle.trace_replay import load_trace, replay_states, trace_items
+    trace = load_trace(TRACE_NAME)
+    seq = trace_items(trace)
+    pos = ref_positions(0)
+    states = replay_states(trace, seq, pos)
+    secs, _ = time_cpu_items(trace, seq, states, pos)
+    v = trace["num_placed"] / (N_ITEMS * statistics.mean(secs))
+    return {"value": round(v, 5), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"items at search positions {pos} of the stream, 24 orientations, interlocking flood fill, "
+                      "placed, on tray states replayed from the oracle's trace; oracle FP64 FFTs on all host "
+                      f"cores; value = {trace['num_placed']} placed / ({N_ITEMS} x mean seconds per item)"}
 
 
 def run_reference(args):
-    item, tray = cpu_sample_setup()
-    for _ in range(args.warmup):
-        time_cpu_sample(item, tray)
-    tot, placed = 0.0, 0
-    for _ in range(args.steps):
-        dt, n = time_cpu_sample(item, tray)
-        tot += dt
-        placed += n
-    v = placed / tot
+    from oracle.trace_replay import load_trace, replay_states, trace_items
+    trace = load_trace(TRACE_NAME)
+    seq = trace_items(trace)
+    steps = [ref_positions(s) for s in range(args.warmup + args.steps)]
+    states = replay_states(trace, seq, [p for st in steps for p in st])
+    secs, same, n = [], 0, 0
+    step_ms = []
+    for s, pos in enumerate(steps):
+        t, recs = time_cpu_items(trace, seq, states, pos)
+        if s < args.warmup:
+            continue
+        secs += t
+        step_ms.append(1e3 * sum(t))
+        same += sum(1 for p, r in zip(pos, recs) if r == trace["records"][p])
+        n += len(pos)
+    per_item = statistics.mean(secs)
+    placed = trace["num_placed"]
+    v = placed / (N_ITEMS * per_item)
     cores = os.cpu_count()
-    cb = {"value": round(v, 5), "unit": UNIT, "cores": cores, "kind": "port",
-          "sample": "1 item (2nd of the config-3 stream) searched in 24 orientations with the interlocking "
-                    "flood fill and placed, tray holding the 1st item; FP64 FFTs on all host cores"}
-    return {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * tot / args.steps, 1),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/i64",
-            "data": "synthetic", "config": {"workload": "config3 sample (see cpu_baseline.sample)"},
-            "cpu_baseline": cb, "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0,
-                                        "d2h_bytes_per_step": 0}}
+    sample = (f"{REF_PER_STEP} items per step at search positions spread over the {N_ITEMS}-item stream "
+              f"(systematic sample, offset moving with the step), each searched in 24 orientations with the "
+              f"interlocking flood fill and placed on the tray state replayed from the oracle's trace; "
+              f"value = items placed in the whole run ({placed}) / ({N_ITEMS} x mean seconds per item)")
+    out = {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(statistics.mean(step_ms), 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/i64",
+           "data": "synthetic (seeded config-3 shapes; Thingi10K unavailable)",
+           "config": {"workload": f"config3: 240x123x100 tray, {N_ITEMS} items (extent 20-50), 24 orientations, "
+                                  "interlocking-free; timed on a systematic sample of the stream (see cpu_baseline)",
+                      "items_per_run": N_ITEMS, "items_placed_per_run": placed,
+                      "seconds_per_item": round(per_item, 4),
+                      "sample_parity_vs_trace": f"{same}/{n}"},
+           "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+           "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_cuda_reference:
+        cr = cuda_reference()
+        if "rows" in cr:
+            spi = cr["mean_seconds_per_item"]
+            out["cuda_reference"] = {
+                "value": round(placed / (N_ITEMS * spi), 3), "unit": UNIT, "seconds_per_item": round(spi, 4),
+                "kind": "reference (its own cuFFT module and Python BinPacker, built for sm_100a from its sources)",
+                "sample": f"{len(cr['rows'])} items at search positions {CUDA_REF_POSITIONS[0]}, "
+                          f"{CUDA_REF_POSITIONS[1]}, ... {CUDA_REF_POSITIONS[-1]}, each one "
+                          "BinPacker.pack_voxels([item], initial_tray=replayed state) call, wall clock",
+                "sample_parity_vs_trace": f"{sum(1 for r in cr['rows'] if r['same'])}/{len(cr['rows'])}"}
+        else:
+            out["cuda_reference"] = cr
+    return out
 
 
 def main():
@@ -512,6 +644,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cuda-reference", action="store_true",
+                    help="reference arm: skip the reference's own GPU path")
     ap.add_argument("--items", type=int, default=N_ITEMS, help="profiling only: shorter item stream")
     ap.add_argument("--value-only", action="store_true", help="profiling only: skip the e2e leg")
     ap.add_argument("--workload", default="config3", choices=["config3", "config4", "config5"])
@@ -541,11 +675,7 @@ def main():
         out = run_ours(args, rank, world, local_rank)
     if rank == 0 and out is not None:
         if world == 1 and not args.no_cpu_baseline and args.workload == "config3":
-            item, tray = cpu_sample_setup()
-            dt, n = time_cpu_sample(item, tray)
-            out["cpu_baseline"] = {"value": round(n / dt, 5), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                                   "sample": "1 item (2nd of the config-3 stream), 24 orientations, "
-                                             "interlocking flood fill, placed; oracle FP64 FFTs on all host cores"}
+            out["cpu_baseline"] = cpu_baseline()
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch

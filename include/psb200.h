@@ -54,6 +54,8 @@ extern "C" {
                                           flood fill and a second selection ran             */
 #define PSB_DIAG_DIRECT          0x800 /* few candidates left by the pre-filter: decided by direct
                                           exact checks and exact proximity sums, no transforms */
+#define PSB_DIAG_LATE_DIRECT    0x1000 /* few ok cells left after the collision pass: their proximity
+                                          by exact sums, no proximity transform                 */
 
 typedef struct psb_result {
     int32_t x, y, z;       /* placement of the item array origin, or -1,-1,-1      */
@@ -87,20 +89,24 @@ int psb_dft_corr3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, in
  * in the reference.  Some callers own every byte of device memory themselves
  * (a framework's caching allocator, a fixed memory budget) or must not call
  * cudaMalloc/cudaFree because those calls synchronise the device and are not
- * stream-ordered (latency-critical loops, code that will later be captured).
+ * stream-ordered (latency-critical loops next to other work on the GPU).
  * This variant computes exactly what psb_dft_corr3 computes, but:
  *   - d_a, d_b and d_out are DEVICE pointers to (nx,ny,nz) int32 grids that
- *     the caller provides; work is queued on `stream` (a cudaStream_t, NULL
- *     for the default stream) and the call returns without synchronising;
+ *     the caller provides; all work, including writing the transform
+ *     descriptors and twiddle tables, is queued on `stream` (a cudaStream_t,
+ *     NULL for the default stream) and the call returns without waiting for
+ *     the GPU;
  *   - its scratch is a fixed 3 MiB array in the library's device code, held
  *     by every GPU that loads the library until the process exits;
  *   - every axis must be <= 32 voxels; larger grids return PSB_ERR_LIMIT;
  *   - it calls no cudaMalloc/cudaFree or other allocating routine.
- * The first call on each device looks up the array's device address (make it
- * before any stream capture).  All calls share the one array: calls that
- * overlap on the GPU (different streams, or different host threads) race and
- * must be serialised by the caller; calls queued on one stream are safe.
- * Nothing in the array needs to start at zero: each call writes all it reads. */
+ * The first call on each device looks up the array's device address and
+ * keeps it (make that first call before any stream capture; the address is
+ * not looked up again, so do not use the function across a
+ * cudaDeviceReset).  All calls share the one array: calls that overlap on
+ * the GPU (different streams, or different host threads) race and must be
+ * serialised by the caller; calls queued on one stream are safe.  Nothing in
+ * the array needs to start at zero: each call writes all it reads. */
 int psb_dft_corr3_noalloc(const int32_t* d_a, const int32_t* d_b, int nx, int ny, int nz,
                           int32_t* d_out, void* stream);
 
@@ -277,6 +283,27 @@ int psb_set_direct_max(int n);
  * to skip there); default 50, 0 tests every sample.  Any subset of samples
  * keeps the filter exact, so results never depend on it. */
 int psb_set_filter_cut(int pct);
+/* Orientations left with at most n ok cells (free, or reachable in the
+ * interlocking mode) after the collision pass skip the proximity transforms:
+ * those cells are scored by exact integer proximity sums over the item's
+ * z-runs instead (default 1024; 0 disables).  Same placements either way.
+ * No counterpart in the reference. */
+int psb_set_late_direct_max(int n);
+/* Bound on the flood fill's union-find work per run lookup or merge
+ * (retries and path steps).  Past it the kernels stop following the chain,
+ * every access staying in bounds, and the search returns PSB_ERR_LIMIT
+ * instead of an answer.  n <= 0 restores the default (2^22, far above any
+ * chain a tray of 2^31 cells can form with path halving).  The reference
+ * bounds its flood fill by nx+ny+nz propagation sweeps instead
+ * (fft3.cu:437); this bound exists so that no device loop can spin. */
+int psb_set_uf_limit(int n);
+/* Test hooks, no counterpart in the reference: psb_debug_fail_alloc(n)
+ * makes the n-th device allocation of the engine from now on fail as a
+ * CUDA allocation error would (PSB_ERR_CUDA); 0 disarms it.
+ * psb_debug_live_allocs reports the engine's device allocations not yet
+ * freed, so a test can check that a failed call freed what it allocated. */
+int psb_debug_fail_alloc(int n);
+int psb_debug_live_allocs(long long* n);
 /* The 24 orientations are 6 axis permutations x 4 flip patterns.  On: the
  * z,y transforms of each permutation run once per item and the x pass reads
  * every flip from them (row reversal, column map, conjugation, phase).  Off

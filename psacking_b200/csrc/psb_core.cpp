@@ -516,6 +516,17 @@ PYBIND11_MODULE(_core, m) {
           "its own (the default).");
     m.def("set_plane_variant", [](int v) { check(psb_set_plane_variant(v)); }, py::arg("variant"),
           "Plane-pass kernel for the specialised lengths: 3 (warp-owned lines, default) or 2.");
+    m.def("set_late_direct_max", [](int n) { check(psb_set_late_direct_max(n)); }, py::arg("n"),
+          "Ok-cell limit below which an orientation skips the proximity transforms (0 off; same placements).");
+    m.def("set_uf_limit", [](int n) { check(psb_set_uf_limit(n)); }, py::arg("n"),
+          "Union-find step bound of the flood fill (n <= 0: the default); past it searches raise.");
+    m.def("debug_fail_alloc", [](int n) { check(psb_debug_fail_alloc(n)); }, py::arg("n"),
+          "Test hook: the n-th device allocation from now fails (0 disarms).");
+    m.def("debug_live_allocs", []() {
+        long long n = 0;
+        check(psb_debug_live_allocs(&n));
+        return n;
+    }, "Test hook: the engine's device allocations not yet freed.");
     m.attr("VOXEL_RESOLUTION") = 128;
     m.attr("HEIGHT_PENALTY") = 100000000.0;
     m.attr("__version__") = "0.1.0";

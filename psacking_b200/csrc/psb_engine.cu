@@ -279,6 +279,11 @@ int g_direct_max = 1024;
 // filter cut-off (k_cand_filter): a warp stops sampling when more than this
 // percentage of its translations survive the first samples; 0 disables
 int g_filter_cut = 50;
+// bound on the flood fill's union-find retries and path steps (psb_set_uf_limit)
+int g_uf_limit = PSB_UF_LIMIT;
+// orientations left with at most this many ok cells after the collision pass
+// skip the proximity transforms (psb_set_late_direct_max; 0 disables)
+int g_late_max = 1024;
 
 // the 6 axis permutations of an orientation map, as base indices
 int perm_index(const int* a) {
@@ -350,6 +355,7 @@ int set_smem_attrs() {
     if (const char* e = getenv("PSB_CAND_FILTER")) g_cand_filter = atoi(e) != 0;
     if (const char* e = getenv("PSB_DIRECT_MAX")) g_direct_max = std::max(0, atoi(e));
     if (const char* e = getenv("PSB_FILTER_CUT")) g_filter_cut = std::max(0, std::min(100, atoi(e)));
+    if (const char* e = getenv("PSB_LATE_MAX")) g_late_max = std::min(std::max(0, atoi(e)), kCandCap);
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
     TRY(set_max_dyn_smem(k_fft_mid<-1>));
@@ -378,15 +384,28 @@ int set_smem_attrs() {
 // Device allocations.  With a stream they are stream-ordered (the tray's own
 // stream), so creating and freeing trays never synchronises the whole device
 // while other trays are running.
+//
+// Test hooks (psb_debug_fail_alloc, psb_debug_live_allocs): the n-th
+// allocation from the moment the hook is armed fails as a CUDA error would,
+// and the allocations made here and not yet freed are counted, so the tests
+// can check that every failure path returns PSB_ERR_CUDA and frees what it
+// allocated.
+std::atomic<int> g_fail_alloc{0};
+std::atomic<long long> g_live_allocs{0};
+
 template <class T>
 int dalloc(T** p, size_t n, cudaStream_t s = nullptr) {
     *p = nullptr;
     if (n == 0) n = 1;
+    if (g_fail_alloc.load() > 0 && g_fail_alloc.fetch_sub(1) == 1)
+        return fail(PSB_ERR_CUDA, "device allocation of %zu B failed (injected by psb_debug_fail_alloc)",
+                    sizeof(T) * n);
     if (s) {
         CK(cudaMallocAsync((void**)p, sizeof(T) * n, s));
     } else {
         CK(cudaMalloc((void**)p, sizeof(T) * n));
     }
+    g_live_allocs.fetch_add(1);
     return PSB_OK;
 }
 
@@ -395,6 +414,7 @@ void dfree(T*& p, cudaStream_t s = nullptr) {
     if (p) {
         if (s) cudaFreeAsync(p, s);
         else cudaFree(p);
+        g_live_allocs.fetch_sub(1);
     }
     p = nullptr;
 }
@@ -477,6 +497,8 @@ int forward3(const Grid3& g, const RzDesc& rz_in, float2* w1, float2* w2, float2
     return forward3_dev(g, d_rz, d_mid, st);
 }
 
+int inverse3_dev(const Grid3& g, float2* w1, int32_t* out, const MidDesc* d_mid, cudaStream_t st);
+
 // inverse: spectrum [F0][F1][H] -> int32 grid (rounded, scaled by 1/(F0 F1 F2))
 int inverse3_int(const Grid3& g, float2* spec, float2* w1, float2* w2, int32_t* out, MidDesc* d_mid,
                  cudaStream_t st) {
@@ -486,6 +508,12 @@ int inverse3_int(const Grid3& g, float2* spec, float2* w1, float2* w2, int32_t* 
     // y: [n0][F1 -> n1][H]     (w2 -> w1 [n0][n1][H])
     m[1] = MidDesc{w2, w1, g.n[0], g.H, g.F[1], g.n[1], (long long)g.F[1] * g.H, (long long)g.n[1] * g.H, g.H, g.H, -1, 0};
     CK(cudaMemcpyAsync(d_mid, m, sizeof(m), cudaMemcpyHostToDevice, st));
+    return inverse3_dev(g, w1, out, d_mid, st);
+}
+
+// inverse with its two MidDescs already on the device (d_mid[0]: x pass
+// spectrum -> w2, d_mid[1]: y pass w2 -> w1), then the z C2R from w1
+int inverse3_dev(const Grid3& g, float2* w1, int32_t* out, const MidDesc* d_mid, cudaStream_t st) {
     {
         PROF("k_fft_mid_inv", st);
         k_fft_mid<1><<<dim3((g.F[1] * g.H + PSB_TILE - 1) / PSB_TILE, 1, 1), PSB_THREADS, smem_mid(g.F[0]), st>>>(
@@ -562,7 +590,41 @@ struct ItemInfo {
     double sumsq = 0.0;
     std::vector<int4> vox;     // nonzero voxels (x, y, z, value)
     std::vector<int4> samp;    // candidate-filter samples (positive voxels, spread out)
+    std::vector<int4> runs[3]; // runs of equal nonzero values along each source axis (build_runs)
 };
+
+// The item's runs along source axis s, in the layout orient_run reads
+// ({u, v, r0 | r1 << 16, value}, psb_kernels.cuh): the exact proximity and
+// collision sums of a translation then cost one pair of prefix-table loads
+// per run instead of one load per voxel.
+void build_runs(const int32_t* a, ItemInfo* info, int s) {
+    std::vector<int4>& out = info->runs[s];
+    out.clear();
+    const int* d = info->dims;
+    const int lo = s == 0 ? 1 : 0, hi = s == 2 ? 1 : 2;
+    int idx[3];
+    for (int u = 0; u < d[lo]; ++u)
+        for (int v = 0; v < d[hi]; ++v) {
+            int r0 = -1, w = 0;
+            for (int r = 0; r <= d[s]; ++r) {
+                int val = 0;
+                if (r < d[s]) {
+                    idx[lo] = u;
+                    idx[hi] = v;
+                    idx[s] = r;
+                    val = a[((size_t)idx[0] * d[1] + idx[1]) * d[2] + idx[2]];
+                }
+                if (r0 >= 0 && val != w) {
+                    out.push_back(make_int4(u, v, r0 | ((r - 1) << 16), w));
+                    r0 = -1;
+                }
+                if (r0 < 0 && val != 0) {
+                    r0 = r;
+                    w = val;
+                }
+            }
+        }
+}
 
 // Up to PSB_FSAMP positive voxels spread over the item, for the candidate
 // filter.  Pool: in each cell of a 10x10x10 split of the item's box, the
@@ -739,8 +801,12 @@ struct psb_tray {
     unsigned char* d_candplane = nullptr;   // per (orientation, x plane): holds a filter candidate
     bool cand_active = false;               // the current search's candidate words and planes are valid
     bool direct_active = false;             // ... and direct orientations may exist
+    bool late_active = false;               // the current search may hold late-direct orientations
     int *d_ccount = nullptr, *d_vcount = nullptr, *d_ncol = nullptr;   // per orientation: candidates,
                                                                       // verified free cells, item columns
+    int* d_okcount = nullptr;               // per orientation: ok cells after the collision pass
+    int* d_clist = nullptr;                 // per orientation: its filter candidates while few (k_cand_filter)
+    size_t clist_cap = 0;
     uint4* d_icols = nullptr;               // item column masks of direct orientations, stride nx*ny
     int4* d_fsamp = nullptr;                // oriented, shift-sorted filter samples (k_cand_prep)
     int* d_fbound = nullptr;                // their bucket bounds
@@ -769,11 +835,22 @@ struct psb_tray {
     void* h_stage = nullptr;   // pinned host staging buffer of psb_pack_stage
     size_t h_stage_cap = 0;
 
+    std::vector<std::array<size_t, 3>> staged_roff;   // the items' runs (per source axis) in d_stage_runs
+    int4* d_stage_runs = nullptr;
+    size_t stage_rcap = 0;
+
     // item staging
     int32_t* d_items = nullptr;
     size_t items_cap = 0;
     int4* d_vox = nullptr;
     size_t vox_cap = 0;
+    int4* d_runs = nullptr;
+    size_t runs_cap = 0;
+
+    // per-column prefix sums along z of the distance field and the occupancy
+    // (k_col_prefix), for the exact sums over an item's runs
+    int32_t* d_pphi = nullptr;
+    int32_t* d_pocc = nullptr;
 
     ~psb_tray() { release(); }
 
@@ -781,7 +858,7 @@ struct psb_tray {
         dfree(d_Ai, st); dfree(d_Bi, st); dfree(d_Pc, st); dfree(d_Pd, st); dfree(d_Dq, st); dfree(d_free, st); dfree(d_reach, st);
         dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
         dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_candplane, st); dfree(d_bases, st); dfree(d_best, st);
-        dfree(d_ccount, st); d_vcount = d_ncol = nullptr; dfree(d_icols, st); dfree(d_fsamp, st); dfree(d_fbound, st);
+        dfree(d_ccount, st); d_vcount = d_ncol = d_okcount = nullptr; dfree(d_icols, st); dfree(d_fsamp, st); dfree(d_fbound, st);
         dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
@@ -790,8 +867,10 @@ struct psb_tray {
         release_slots();
         dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_pen, st);
         dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st); dfree(d_stage_vox, st);
+        dfree(d_stage_runs, st); dfree(d_runs, st); dfree(d_pphi, st); dfree(d_pocc, st);
         dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_base_all, st); dfree(d_dec, st);
-        dfree(d_tbits, st); dfree(d_stage_samp, st); dfree(d_work, st);
+        dfree(d_tbits, st); dfree(d_stage_samp, st); dfree(d_work, st); dfree(d_clist, st);
+        clist_cap = 0;
         tq = 0;
         if (st) {
             cudaStreamSynchronize(st);
@@ -822,6 +901,7 @@ struct psb_tray {
         CK(cudaMemsetAsync(d_work, 0, sizeof(unsigned long long) * 8, st));
         TRY(dalloc(&d_err, 1, st)); TRY(dalloc(&d_first, 1, st)); TRY(dalloc(&d_needff, 1, st));
         TRY(dalloc(&d_ls, 1, st)); TRY(dalloc(&d_ps, 1, st)); TRY(dalloc(&d_rzd, 4, st)); TRY(dalloc(&d_midd, 8, st));
+        TRY(dalloc(&d_pphi, (size_t)nx * ny * (nz + 1), st)); TRY(dalloc(&d_pocc, (size_t)nx * ny * (nz + 1), st));
         CK(cudaStreamSynchronize(st));  // stream-ordered allocations complete before plain copies touch them
         CK(cudaMemset(d_err, 0, sizeof(unsigned int)));
         // SCAN-mode penalty table with the host libm pow (packing.cpp:630-631)
@@ -878,9 +958,10 @@ struct psb_tray {
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c, st));
         TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_okplane, (size_t)nx * c, st));
         TRY(dalloc(&d_candplane, (size_t)nx * c, st));
-        TRY(dalloc(&d_ccount, 3 * (size_t)c, st));
+        TRY(dalloc(&d_ccount, 4 * (size_t)c, st));
         d_vcount = d_ccount + c;
         d_ncol = d_ccount + 2 * c;
+        d_okcount = d_ccount + 3 * c;
         TRY(dalloc(&d_icols, (size_t)nx * ny * c, st));
         TRY(dalloc(&d_fsamp, (size_t)PSB_FSAMP * c, st));
         TRY(dalloc(&d_fbound, (size_t)PSB_FBOUND * c, st));
@@ -899,6 +980,30 @@ struct psb_tray {
         CK(cudaMemcpy(d_rzs, rz.data(), sizeof(RzDesc) * c, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(d_mids, md.data(), sizeof(MidDesc) * c, cudaMemcpyHostToDevice));
         cap = c;
+        return PSB_OK;
+    }
+
+    int ensure_runs(size_t n) {
+        if (n > runs_cap) {
+            dfree(d_runs, st);
+            runs_cap = std::max(n, (size_t)1 << 14);
+            TRY(dalloc(&d_runs, runs_cap, st));
+        }
+        return PSB_OK;
+    }
+
+    // prefix tables of the distance field (gated when gate is set) and of
+    // the occupancy
+    int prefix_phi(const int* gate) {
+        const int ncols = nx * ny;
+        k_col_prefix<0><<<(ncols + 7) / 8, 256, 0, st>>>(d_phi, d_pphi, ncols, nz, gate);
+        CKL();
+        return PSB_OK;
+    }
+    int prefix_occ() {
+        const int ncols = nx * ny;
+        k_col_prefix<1><<<(ncols + 7) / 8, 256, 0, st>>>(d_tray, d_pocc, ncols, nz, nullptr);
+        CKL();
         return PSB_OK;
     }
 
@@ -992,6 +1097,7 @@ struct psb_tray {
     int rebuild_phi_gated() {
         const int* need_phi = (const int*)((const char*)d_ls + offsetof(LoopState, need_phi));
         TRY(distance_on_device(d_tray, d_phi, nx, ny, nz, st, need_phi));
+        TRY(prefix_phi(need_phi));
         TRY(phi_stats(need_phi));
         return tray_forward(true, need_phi);
     }
@@ -1007,6 +1113,8 @@ struct psb_tray {
         } else {
             TRY(distance_on_device(d_tray, d_phi, nx, ny, nz, st));
         }
+        TRY(prefix_occ());
+        TRY(prefix_phi(nullptr));
         TRY(rebuild_occ());
         TRY(rebuild_phi_spectrum());
         CK(cudaStreamSynchronize(st));
@@ -1016,7 +1124,7 @@ struct psb_tray {
 
     // Fill an OrientDesc from an item's analysis and a signed permutation.
     void describe(const ItemInfo& info, const int* src_axis, const int* flip, const int32_t* d_item,
-                  const int4* d_vx, OrientDesc* od) const {
+                  const int4* d_vx, const int4* const* d_rn, OrientDesc* od) const {
         int n[3] = {nx, ny, nz};
         for (int a = 0; a < 3; ++a) {
             od->src_axis[a] = src_axis[a];
@@ -1049,6 +1157,8 @@ struct psb_tray {
         od->samp = nullptr;
         od->nsamp = 0;
         od->direct = 0;
+        od->runs = d_rn[src_axis[2]];
+        od->nruns = (int)info.runs[src_axis[2]].size();
     }
 
     // Free bits of the tray for the candidate filter, all columns.
@@ -1101,6 +1211,13 @@ struct psb_tray {
             }
         const int n = (int)ods.size();
         const int dmax = split_flow() ? g_direct_max : 0;
+        // candidate lists for the direct checks: dmax entries per orientation
+        const int ccap = std::max(dmax, 1);
+        if ((size_t)ccap * cap > clist_cap) {
+            dfree(d_clist, st);
+            clist_cap = (size_t)ccap * cap;
+            TRY(dalloc(&d_clist, clist_cap, st));
+        }
         if (xmax > 0) {
             const dim3 grid(xmax, n);
             CK(cudaMemsetAsync(d_ccount, 0, sizeof(int) * 3 * cap, st));
@@ -1110,12 +1227,14 @@ struct psb_tray {
                     k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
                     k_cand_filter<1><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
                                                                         d_candplane, (long long)nx, d_ccount,
-                                                                        d_fsamp, d_fbound, g_filter_cut);
+                                                                        d_fsamp, d_fbound, g_filter_cut, d_clist,
+                                                                        ccap, nz);
                 } else {
                     k_cand_prep<2><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
                     k_cand_filter<2><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
                                                                         d_candplane, (long long)nx, d_ccount,
-                                                                        d_fsamp, d_fbound, g_filter_cut);
+                                                                        d_fsamp, d_fbound, g_filter_cut, d_clist,
+                                                                        ccap, nz);
                 }
             }
             CKL();
@@ -1129,9 +1248,9 @@ struct psb_tray {
                     PROF("k_cand_verify", st);
                     k_item_cols<<<dim3(emax, n), 64, 0, st>>>(d_odb, d_icols, (long long)nx * ny, d_ncol);
                     CKL();
-                    k_cand_verify<<<grid, 128, 0, st>>>(d_odb, d_tbits, ny, nzw, tq, d_free, sBits, d_candplane,
-                                                        (long long)nx, d_icols, (long long)nx * ny, d_ncol, d_vcount,
-                                                        d_okplane, interlock ? 0 : 1);
+                    k_cand_verify_list<<<148 * 4, 256, sizeof(int) * (n + 1), st>>>(
+                        d_odb, n, d_tbits, ny, nz, nzw, tq, d_free, sBits, d_clist, ccap, d_ccount, d_icols,
+                        (long long)nx * ny, d_ncol, d_vcount, d_okplane, (long long)nx, interlock ? 0 : 1);
                 }
                 CKL();
                 k_cand_apply<<<(n + 127) / 128, 128, 0, st>>>(d_odb, n, d_vcount, 1, dmax);
@@ -1158,9 +1277,10 @@ struct psb_tray {
     // Flood fill (Algorithm 3) of every orientation's free bits into its
     // reach bits.  okplane, when set, receives the planes that hold a
     // reachable cell; gate, when set, makes every launch conditional.
-    int flood_fill(const OrientDesc* d_odb, int n, const ScoreParams& sp, const int* gate, unsigned char* okplane) {
+    int flood_fill(const OrientDesc* d_odb, int n, const ScoreParams& sp, const int* gate, unsigned char* okplane,
+                   int* okcount = nullptr) {
         FloodBufs fb{d_free, d_reach, sBits, d_cnt, d_off,   sLine, d_rz2,    d_rline,
-                     d_par,  d_rflag, sRun,  d_total, d_err, gate,  okplane, (long long)nx};
+                     d_par,  d_rflag, sRun,  d_total, d_err, gate,  okplane, (long long)nx, g_uf_limit, okcount};
         const int lines = nx * ny;
         const int nblk = (lines + 255) / 256;
         const dim3 gl(nblk, n);
@@ -1216,14 +1336,23 @@ struct psb_tray {
         }
         CKL();
         const uint32_t* ok = interlock ? d_reach : d_free;
+        // orientations left with few ok cells skip the proximity transforms
+        // (k_late_direct): count the ok cells of every orientation
+        const bool late = g_late_max > 0;
+        if (late) CK(cudaMemsetAsync(d_okcount, 0, sizeof(int) * n, st));
         PlaneBufs pb{d_free, d_Dq,      d_smin,         d_diag, sBits, sD, d_pmin, (long long)nx, ok, d_okplane,
-                     interlock ? 0 : 1, cand_active ? d_candplane : nullptr};
+                     interlock ? 0 : 1, cand_active ? d_candplane : nullptr, late ? d_okcount : nullptr};
         {
             PROF("k_plane_coll", st);
             p0<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
         }
         CKL();
-        if (interlock) TRY(flood_fill(d_odb, n, sp, nullptr, d_okplane));
+        if (interlock) TRY(flood_fill(d_odb, n, sp, nullptr, d_okplane, late ? d_okcount : nullptr));
+        if (late) {
+            k_late_direct<<<(n + 127) / 128, 128, 0, st>>>(const_cast<OrientDesc*>(d_odb), n, d_okcount, g_late_max);
+            CKL();
+            late_active = true;
+        }
         if (xf) {
             PROF("k_xpass_prox", st);
             xf2<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
@@ -1235,15 +1364,17 @@ struct psb_tray {
             p1<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
         }
         CKL();
-        return select_over(d_odb, n, sp, ok, nullptr, d_out);
+        return select_over(d_odb, n, sp, ok, nullptr, d_out, d_okplane);
     }
 
     // Selection over the ok cells from the plane minima: candidates in the
     // window of each orientation's minimum, exact re-score, tie rule, result.
+    // okplane (may be null): the planes that hold an ok cell (the split flow
+    // keeps them for every orientation)
     int select_over(const OrientDesc* d_odb, int n, const ScoreParams& sp, const uint32_t* ok, const int* gate,
-                    ResultDev* d_out) {
+                    ResultDev* d_out, const unsigned char* okplane = nullptr) {
         SelectBufs sel{ok,        sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
-                       d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate};
+                       d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate, okplane};
         {
             PROF("k_collect", st);
             k_collect_plane<<<dim3(nx, n), 256, 0, st>>>(d_odb, sel, sp);
@@ -1251,12 +1382,12 @@ struct psb_tray {
         CKL();
         {
             PROF("k_rescore", st);
-            k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_tray, d_phi);
+            k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_pocc, d_pphi);
         }
         CKL();
-        if (direct_active) {
+        if (direct_active || late_active) {
             PROF("k_direct_score", st);
-            k_direct_score<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp, d_phi);
+            k_direct_score<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp, d_pphi);
             CKL();
         }
         {
@@ -1463,7 +1594,10 @@ struct psb_tray {
         const bool share = make_bases(&od2, &bases);
         CK(cudaMemcpyAsync(d_od, od2.data(), sizeof(OrientDesc) * n, cudaMemcpyHostToDevice, st));
         if (share) CK(cudaMemcpyAsync(d_bases, bases.data(), sizeof(OrientDesc) * 6, cudaMemcpyHostToDevice, st));
-        TRY(search_async(d_od, od2, mode, interlock, d_res, lazy, share ? d_bases : nullptr, share ? &bases : nullptr));
+        const int sst = search_async(d_od, od2, mode, interlock, d_res, lazy, share ? d_bases : nullptr,
+                                     share ? &bases : nullptr);
+        late_active = false;
+        TRY(sst);
         res->resize(n);
         unsigned int herr = 0;
         CK(cudaMemcpyAsync(res->data(), d_res, sizeof(ResultDev) * n, cudaMemcpyDeviceToHost, st));
@@ -1497,9 +1631,11 @@ struct psb_tray {
         }
         k_place_write<<<blocks, 256, 0, st>>>(d_od, d_tray, nx, ny, nz, px, py, pz, id);
         CKL();
+        TRY(prefix_occ());
         TRY(rebuild_occ());
         if (id == 1 && od.nvox > 0) {  // only voxels equal to 1 are distance sources (fft3.cu:948)
             TRY(distance_on_device(d_tray, d_phi, nx, ny, nz, st));
+            TRY(prefix_phi(nullptr));
             TRY(rebuild_phi_spectrum());
         }
         CK(cudaStreamSynchronize(st));
@@ -1527,7 +1663,7 @@ void to_result(const ResultDev& r, int orient, psb_result* out) {
 // Upload a set of explicit orientation arrays and describe them.
 int stage_arrays(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n, std::vector<OrientDesc>* ods) {
     std::vector<ItemInfo> infos(n);
-    size_t tot = 0, totv = 0;
+    size_t tot = 0, totv = 0, totr = 0;
     for (int o = 0; o < n; ++o) {
         int ex = dims[3 * o], ey = dims[3 * o + 1], ez = dims[3 * o + 2];
         if (!items[o] || ex <= 0 || ey <= 0 || ez <= 0)
@@ -1535,11 +1671,14 @@ int stage_arrays(psb_tray* t, const int32_t* const* items, const int32_t* dims, 
         size_t m = (size_t)ex * ey * ez;
         if (has_negative(items[o], m)) return fail(PSB_ERR_ARG, "orientation %d holds negative values", o);
         analyse_item(items[o], ex, ey, ez, &infos[o]);
+        build_runs(items[o], &infos[o], 2);   // identity orientations: z-runs along the item's own z
         tot += m;
         totv += infos[o].vox.size();
+        totr += infos[o].runs[2].size();
     }
     TRY(t->ensure_staging(tot, totv));
-    size_t off = 0, offv = 0;
+    TRY(t->ensure_runs(totr));
+    size_t off = 0, offv = 0, offr = 0;
     ods->resize(n);
     for (int o = 0; o < n; ++o) {
         size_t m = (size_t)infos[o].dims[0] * infos[o].dims[1] * infos[o].dims[2];
@@ -1547,9 +1686,14 @@ int stage_arrays(psb_tray* t, const int32_t* const* items, const int32_t* dims, 
         if (!infos[o].vox.empty())
             CK(cudaMemcpyAsync(t->d_vox + offv, infos[o].vox.data(), sizeof(int4) * infos[o].vox.size(),
                                cudaMemcpyHostToDevice, t->st));
-        t->describe(infos[o], kIdentity, kNoFlip, t->d_items + off, t->d_vox + offv, &(*ods)[o]);
+        if (!infos[o].runs[2].empty())
+            CK(cudaMemcpyAsync(t->d_runs + offr, infos[o].runs[2].data(), sizeof(int4) * infos[o].runs[2].size(),
+                               cudaMemcpyHostToDevice, t->st));
+        const int4* rn[3] = {nullptr, nullptr, t->d_runs + offr};
+        t->describe(infos[o], kIdentity, kNoFlip, t->d_items + off, t->d_vox + offv, rn, &(*ods)[o]);
         off += m;
         offv += infos[o].vox.size();
+        offr += infos[o].runs[2].size();
     }
     CK(cudaStreamSynchronize(t->st));  // host vectors die at return
     return PSB_OK;
@@ -1889,6 +2033,30 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[64] = {nullptr};  // device address of the array, per device
+
+// The descriptors and twiddle tables of one call, passed by value to
+// k_noalloc_setup, which writes them into the array in stream order (no
+// host-to-device copy, so the call never waits for the GPU).
+struct NoAllocSetup {
+    RzDesc rz[2];          // z passes of a and b
+    MidDesc mid[6];        // y, x passes of a; of b; x, y passes of the inverse
+    RzDesc* d_rz;
+    MidDesc* d_mid;
+    float2* tw[3];         // twiddle tables, F[a] entries each
+    int F[3];
+};
+
+__global__ void k_noalloc_setup(NoAllocSetup s) {
+    if (blockIdx.x == 0 && threadIdx.x < 2) s.d_rz[threadIdx.x] = s.rz[threadIdx.x];
+    if (blockIdx.x == 0 && threadIdx.x < 6) s.d_mid[threadIdx.x] = s.mid[threadIdx.x];
+    // tw[a][i] = exp(-2 pi i / F), in double precision, rounded to float
+    for (int a = 0; a < 3; ++a)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.F[a]; i += gridDim.x * blockDim.x) {
+            double sn, cs;
+            sincospi(-2.0 * (double)i / (double)s.F[a], &sn, &cs);
+            s.tw[a][i] = make_float2((float)cs, (float)sn);
+        }
+}
 }  // namespace
 
 extern "C" {
@@ -1934,10 +2102,14 @@ int psb_dft_corr3_noalloc(const int32_t* d_a, const int32_t* d_b, int nx, int ny
         used += (n + 255) / 256 * 256;
         return r;
     };
-    float2* tw[3];
-    for (int a = 0; a < 3; ++a) tw[a] = (float2*)take(sizeof(float2) * g.F[a]);
-    RzDesc* d_rz = (RzDesc*)take(sizeof(RzDesc) * 2);
-    MidDesc* d_mid = (MidDesc*)take(sizeof(MidDesc) * 2);
+    NoAllocSetup su;
+    for (int a = 0; a < 3; ++a) {
+        su.tw[a] = (float2*)take(sizeof(float2) * g.F[a]);
+        su.F[a] = g.F[a];
+        g.p[a].tw = su.tw[a];
+    }
+    su.d_rz = (RzDesc*)take(sizeof(RzDesc) * 2);
+    su.d_mid = (MidDesc*)take(sizeof(MidDesc) * 6);
     float2* Sa = (float2*)take(sizeof(float2) * S);
     float2* Sb = (float2*)take(sizeof(float2) * S);
     float2* W1 = (float2*)take(sizeof(float2) * w1);
@@ -1946,24 +2118,23 @@ int psb_dft_corr3_noalloc(const int32_t* d_a, const int32_t* d_b, int nx, int ny
         return fail(PSB_ERR_LIMIT, "dft_corr3_noalloc: grid (%d,%d,%d) needs %zu B of scratch, the fixed array has %zu B",
                     nx, ny, nz, used, kNoAllocScratchBytes);
     cudaStream_t st = (cudaStream_t)stream;
-    // twiddle tables into the array (every byte the transforms read is
-    // written first in stream order, so nothing needs clearing)
-    for (int a = 0; a < 3; ++a) {
-        std::vector<float2> t(g.F[a]);
-        for (int i = 0; i < g.F[a]; ++i) {
-            double ang = -2.0 * M_PI * (double)i / (double)g.F[a];
-            t[i] = make_float2((float)std::cos(ang), (float)std::sin(ang));
-        }
-        CK(cudaMemcpyAsync(tw[a], t.data(), sizeof(float2) * g.F[a], cudaMemcpyHostToDevice, st));
-        g.p[a].tw = tw[a];
-    }
-    RzDesc ra{SRC_GRID_RAW, d_a, nx, ny, nz, 0, -1, nullptr};
-    RzDesc rb{SRC_GRID_RAW, d_b, nx, ny, nz, 0, -1, nullptr};
-    TRY(forward3(g, ra, W1, W2, Sa, d_rz, d_mid, st));
-    TRY(forward3(g, rb, W1, W2, Sb, d_rz + 1, d_mid, st));
+    su.rz[0] = RzDesc{SRC_GRID_RAW, d_a, nx, ny, nz, 0, -1, W1, nullptr, nullptr};
+    su.rz[1] = RzDesc{SRC_GRID_RAW, d_b, nx, ny, nz, 0, -1, W1, nullptr, nullptr};
+    forward_mids(g, W1, W2, Sa, nullptr, su.mid + 0);
+    forward_mids(g, W1, W2, Sb, nullptr, su.mid + 2);
+    // inverse: x [1][F0 -> n0][F1*H] (Sa -> W2), then y [n0][F1 -> n1][H] (W2 -> W1)
+    su.mid[4] = MidDesc{Sa, W2, 1, g.F[1] * g.H, g.F[0], g.n[0], 0, 0, g.F[1] * g.H, g.F[1] * g.H, -1, 0, nullptr};
+    su.mid[5] = MidDesc{W2, W1, g.n[0], g.H, g.F[1], g.n[1], (long long)g.F[1] * g.H, (long long)g.n[1] * g.H, g.H,
+                        g.H, -1, 0, nullptr};
+    // every byte the transforms read is written first in stream order, so
+    // nothing in the array needs clearing
+    k_noalloc_setup<<<4, 256, 0, st>>>(su);
+    CKL();
+    TRY(forward3_dev(g, su.d_rz + 0, su.d_mid + 0, st));
+    TRY(forward3_dev(g, su.d_rz + 1, su.d_mid + 2, st));
     k_spec_mul<<<grid1d(S), 256, 0, st>>>(Sa, Sb, Sa, S, 1);
     CKL();
-    TRY(inverse3_int(g, Sa, W1, W2, d_out, d_mid, st));
+    TRY(inverse3_dev(g, W1, d_out, su.d_mid + 4, st));
     return PSB_OK;
 }
 
@@ -2048,7 +2219,7 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
     CK(cudaMemsetAsync(t->d_err, 0, sizeof(unsigned int), t->st));
     ScoreParams sp = t->score_params(1);
     FloodBufs fb{t->d_free, t->d_reach, t->sBits, t->d_cnt, t->d_off, t->sLine, t->d_rz2, t->d_rline, t->d_par,
-                 t->d_rflag, t->sRun, t->d_total, t->d_err, nullptr, nullptr, 0};
+                 t->d_rflag, t->sRun, t->d_total, t->d_err, nullptr, nullptr, 0, g_uf_limit};
     int lines = nx * ny;
     const int nblk = (lines + 255) / 256;
     dim3 gl(nblk, 1);
@@ -2244,6 +2415,7 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     t->staged_off.clear();
     t->staged_voff.clear();
     t->staged_soff.clear();
+    t->staged_roff.clear();
     for (int it = 0; it < n_items; ++it) {
         const int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
         if (!items[it] || ex <= 0 || ey <= 0 || ez <= 0) return fail(PSB_ERR_ARG, "item %d: bad array", it);
@@ -2260,6 +2432,7 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
                 if (has_negative(items[it], m)) { neg[it] = 1; continue; }
                 analyse_item(items[it], ex, ey, ez, &t->staged[it]);
                 pick_samples(&t->staged[it]);
+                for (int a = 0; a < 3; ++a) build_runs(items[it], &t->staged[it], a);
             }
         };
         const int nthr = std::max(1, std::min<int>(n_items / 8, (int)std::thread::hardware_concurrency()));
@@ -2270,15 +2443,26 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     }
     for (int it = 0; it < n_items; ++it)
         if (neg[it]) return fail(PSB_ERR_ARG, "item %d holds negative values", it);
-    size_t tot = 0, totv = 0, tots = 0;
+    size_t tot = 0, totv = 0, tots = 0, totr = 0;
     for (int it = 0; it < n_items; ++it) {
         const ItemInfo& inf = t->staged[it];
         t->staged_off.push_back(tot);
         t->staged_voff.push_back(totv);
         t->staged_soff.push_back(tots);
+        std::array<size_t, 3> ro;
+        for (int a = 0; a < 3; ++a) {
+            ro[a] = totr;
+            totr += inf.runs[a].size();
+        }
+        t->staged_roff.push_back(ro);
         tot += (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
         totv += inf.vox.size();
         tots += inf.samp.size();
+    }
+    if (totr > t->stage_rcap) {
+        dfree(t->d_stage_runs, t->st);
+        t->stage_rcap = totr;
+        TRY(dalloc(&t->d_stage_runs, totr, t->st));
     }
     if (tots > t->stage_scap) {
         dfree(t->d_stage_samp, t->st);
@@ -2297,7 +2481,7 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     }
     // one pinned staging buffer for the item arrays and voxel lists: two
     // large copies instead of two small pageable ones per item
-    const size_t bytes = sizeof(int32_t) * tot + sizeof(int4) * (totv + tots);
+    const size_t bytes = sizeof(int32_t) * tot + sizeof(int4) * (totv + tots + totr);
     if (bytes > t->h_stage_cap) {
         if (t->h_stage) cudaFreeHost(t->h_stage);
         t->h_stage = nullptr;
@@ -2308,15 +2492,20 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     int32_t* hi = (int32_t*)t->h_stage;
     int4* hv = (int4*)(hi + tot);
     int4* hs = hv + totv;
+    int4* hr = hs + tots;
     for (int it = 0; it < n_items; ++it) {
         const ItemInfo& inf = t->staged[it];
         memcpy(hi + t->staged_off[it], items[it], sizeof(int32_t) * inf.dims[0] * inf.dims[1] * inf.dims[2]);
         if (!inf.vox.empty()) memcpy(hv + t->staged_voff[it], inf.vox.data(), sizeof(int4) * inf.vox.size());
         if (!inf.samp.empty()) memcpy(hs + t->staged_soff[it], inf.samp.data(), sizeof(int4) * inf.samp.size());
+        for (int a = 0; a < 3; ++a)
+            if (!inf.runs[a].empty())
+                memcpy(hr + t->staged_roff[it][a], inf.runs[a].data(), sizeof(int4) * inf.runs[a].size());
     }
     if (tot) CK(cudaMemcpyAsync(t->d_stage, hi, sizeof(int32_t) * tot, cudaMemcpyHostToDevice, t->st));
     if (totv) CK(cudaMemcpyAsync(t->d_stage_vox, hv, sizeof(int4) * totv, cudaMemcpyHostToDevice, t->st));
     if (tots) CK(cudaMemcpyAsync(t->d_stage_samp, hs, sizeof(int4) * tots, cudaMemcpyHostToDevice, t->st));
+    if (totr) CK(cudaMemcpyAsync(t->d_stage_runs, hr, sizeof(int4) * totr, cudaMemcpyHostToDevice, t->st));
     CK(cudaStreamSynchronize(t->st));
     return PSB_OK;
 }
@@ -2398,10 +2587,13 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
     // distance statistics
     std::vector<OrientDesc> all((size_t)n_items * n_orient);
     for (int it = 0; it < n_items; ++it)
-        for (int o = 0; o < n_orient; ++o)
+        for (int o = 0; o < n_orient; ++o) {
+            const int4* rn[3];
+            for (int a = 0; a < 3; ++a) rn[a] = t->d_stage_runs + t->staged_roff[it][a];
             t->describe(t->staged[it], orient_maps + 6 * o, orient_maps + 6 * o + 3,
-                        t->d_stage + t->staged_off[it], t->d_stage_vox + t->staged_voff[it],
+                        t->d_stage + t->staged_off[it], t->d_stage_vox + t->staged_voff[it], rn,
                         &all[(size_t)it * n_orient + o]);
+        }
     // candidate-filter samples (tray columns of at most 256 cells)
     const bool filt = g_cand_filter && t->nzw <= 8;
     if (filt)
@@ -2548,7 +2740,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         occ_est += t->staged[it].vox.size();
         const int sst = t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res, true,
                                         t->d_base_all + (size_t)it * 6, &hb);
-        t->cand_active = t->direct_active = false;
+        t->cand_active = t->direct_active = t->late_active = false;
         TRY(sst);
         if (d_per)
             CK(cudaMemcpyAsync(d_per + (size_t)it * n_orient, t->d_res, sizeof(ResultDev) * n_orient,
@@ -2563,6 +2755,14 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         {
             PROF("k_place_write", t->st);
             k_place_write_g<<<64, 256, 0, t->st>>>(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
+        }
+        CKL();
+        {
+            size_t box = 1;
+            for (auto& o : host_ods) box = std::max(box, (size_t)o.e[0] * o.e[1]);
+            PROF("k_occ_prefix", t->st);
+            k_occ_prefix_box<<<(unsigned)((box + 7) / 8), 256, 0, t->st>>>(t->d_tray, t->d_pocc, t->nx, t->ny, t->nz,
+                                                                            t->d_ls, d_odb);
         }
         CKL();
         k_place_done<<<1, 32, 0, t->st>>>(d_odb, t->d_ls, t->d_dec + it);
@@ -2977,6 +3177,28 @@ int psb_set_direct_max(int n) {
 int psb_set_filter_cut(int pct) {
     if (pct < 0 || pct > 100) return fail(PSB_ERR_ARG, "filter cut-off must be a percentage in [0, 100]");
     g_filter_cut = pct;
+    return PSB_OK;
+}
+
+int psb_set_late_direct_max(int n) {
+    if (n < 0) return fail(PSB_ERR_ARG, "late direct limit must be >= 0");
+    g_late_max = std::min(n, kCandCap);   // every ok cell of such an orientation is a candidate
+    return PSB_OK;
+}
+
+int psb_set_uf_limit(int n) {
+    g_uf_limit = n > 0 ? n : PSB_UF_LIMIT;
+    return PSB_OK;
+}
+
+int psb_debug_fail_alloc(int n) {
+    g_fail_alloc.store(n > 0 ? n : 0);
+    return PSB_OK;
+}
+
+int psb_debug_live_allocs(long long* n) {
+    if (!n) return fail(PSB_ERR_ARG, "null output");
+    *n = g_live_allocs.load();
     return PSB_OK;
 }
 

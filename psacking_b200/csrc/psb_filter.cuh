@@ -15,7 +15,7 @@
 // words and skips it).  Every other cell is decided exactly: by the FFT
 // collision count, or, for an orientation left with few candidates (at most
 // the direct limit), by a direct check of each candidate against the item's
-// voxel columns (k_cand_verify); such a "direct" orientation also gets its
+// voxel columns (k_cand_verify_list); such a "direct" orientation also gets its
 // proximity as exact integer sums over the item's voxels (k_direct_score)
 // and needs no transform at all.
 #pragma once
@@ -114,7 +114,8 @@ template <int NQ>
 __global__ void __launch_bounds__(PSB_FILT_THREADS)
 k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ tbits, int ny, int nzw,
               uint32_t* __restrict__ cand, long long sBits, unsigned char* __restrict__ candplane, long long pstride,
-              int* __restrict__ ccount, const int4* __restrict__ fs, const int* __restrict__ fbound, int cut_pct) {
+              int* __restrict__ ccount, const int4* __restrict__ fs, const int* __restrict__ fbound, int cut_pct,
+              int* __restrict__ clist, int ccap, int nz) {
     constexpr int NW = 4 * NQ;
     const int o = blockIdx.y, x = blockIdx.x;
     const OrientDesc& od = orients[o];
@@ -132,7 +133,7 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
     if (tid <= NW) bound[tid] = __ldg(&fbound[(size_t)o * PSB_FBOUND + tid]);
     __syncthreads();
     uint32_t* cw = cand + (size_t)o * sBits + (size_t)x * ny * nzw;
-    int any = 0, cnt = 0;
+    int any = 0;
     for (int y0 = warp * 32; y0 < Yv; y0 += PSB_FILT_THREADS) {
         const int y = y0 + lane;
         const bool act = y < Yv;
@@ -216,19 +217,42 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
                 }
             }
         }
+        int mine = 0;
         if (act) {
 #pragma unroll
             for (int w = 0; w < NW; ++w)
                 if (w < nzw) {
                     cw[(size_t)y * nzw + w] = c[w];
                     any |= c[w] != 0u;
-                    cnt += __popc(c[w]);
+                    mine += __popc(c[w]);
                 }
         }
-    }
+        // count, and list the candidates while the orientation has at most
+        // ccap of them (a list for the direct checks of k_cand_verify_list)
+        int incl = mine;
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
-    if (lane == 0 && cnt) atomicAdd(&ccount[o], cnt);
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+        int base = 0;
+        if (lane == 31 && incl) base = atomicAdd(&ccount[o], incl);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        int slot = base + incl - mine;
+        if (mine && slot < ccap) {
+            int* L = clist + (size_t)o * ccap;
+            const int t0 = (x * ny + y) * nz;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                uint32_t m = w < nzw ? c[w] : 0u;
+                while (m && slot < ccap) {
+                    const int bit = __ffs(m) - 1;
+                    m &= m - 1u;
+                    L[slot++] = t0 + 32 * w + bit;
+                }
+            }
+        }
+    }
     any = __syncthreads_or(any);
     if (tid == 0) candplane[(size_t)o * pstride + x] = any ? 1 : 0;
 }
@@ -236,7 +260,7 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
 // Stage 0 (after k_cand_filter, count = candidates): an orientation without
 // a candidate is skipped; one with at most direct_max candidates and an item
 // at most 64 cells high (two mask words per column) becomes direct.
-// Stage 1 (after k_cand_verify, count = verified free cells): a direct
+// Stage 1 (after k_cand_verify_list, count = verified free cells): a direct
 // orientation without a free cell is skipped.  grid: ceil(n / 128), block 128
 __global__ void k_cand_apply(OrientDesc* __restrict__ orients, int n, const int* __restrict__ count, int stage,
                              int direct_max) {
@@ -281,80 +305,83 @@ __global__ void k_item_cols(const OrientDesc* __restrict__ orients, uint4* __res
     }
 }
 
-// Exact collision check of every candidate of a direct orientation: the
-// translation (x, y, z) is free when no item column (a, b) meets an occupied
-// cell of tray column (x + a, y + b) over z .. z + 63.  A warp takes one
-// candidate at a time, its lanes one item column each, and stops at the first
-// overlap.  The candidate words are refined in place into the free words;
-// free cells are counted (stage 1 of k_cand_apply) and, outside the
-// interlocking mode, flag their plane (okplane).
-// grid: (max Xv, n), block 128
-__global__ void __launch_bounds__(128)
-k_cand_verify(const OrientDesc* __restrict__ orients, const uint4* __restrict__ tbits, int ny, int nzw, int tq,
-              uint32_t* __restrict__ cand, long long sBits, const unsigned char* __restrict__ candplane,
-              long long pstride, const uint4* __restrict__ cols, long long cstride, const int* __restrict__ ncol,
-              int* __restrict__ vcount, unsigned char* __restrict__ okplane, int set_okplane) {
-    const int o = blockIdx.y, x = blockIdx.x;
-    const OrientDesc& od = orients[o];
-    if (od.skip || !od.direct || x >= od.valid[0]) return;
-    if (!candplane[(size_t)o * pstride + x]) return;   // no candidate: the words are zero already
-    const int Yv = od.valid[1];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nc = ncol[o];
-    const uint4* cl = cols + (size_t)o * cstride;
+// Exact collision check of every candidate of the direct orientations, from
+// the candidate lists k_cand_filter wrote: the translation (x, y, z) is free
+// when no item column (a, b) meets an occupied cell of tray column
+// (x + a, y + b) over z .. z + 63.  The candidates of all orientations are
+// spread over the whole grid, one warp each, its lanes one item column each,
+// stopping at the first overlap.  A blocked candidate's bit is cleared in the
+// candidate words (which become the free words); free cells are counted
+// (stage 1 of k_cand_apply) and, outside the interlocking mode, flag their
+// plane (okplane).  grid: any, block 256; dynamic shared memory (n+1) ints
+__global__ void __launch_bounds__(256)
+k_cand_verify_list(const OrientDesc* __restrict__ orients, int n, const uint4* __restrict__ tbits, int ny, int nz,
+                   int nzw, int tq, uint32_t* __restrict__ cand, long long sBits, const int* __restrict__ clist,
+                   int ccap, const int* __restrict__ ccount, const uint4* __restrict__ cols, long long cstride,
+                   const int* __restrict__ ncol, int* __restrict__ vcount, unsigned char* __restrict__ okplane,
+                   long long pstride, int set_okplane) {
+    extern __shared__ int pre[];   // pre[o]: direct candidates of orientations before o
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int o = 0; o < n; ++o) {
+            pre[o] = acc;
+            const OrientDesc& od = orients[o];
+            if (!od.skip && od.direct == 1) acc += min(ccount[o], ccap);
+        }
+        pre[n] = acc;
+    }
+    __syncthreads();
+    const int total = pre[n];
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
     const uint32_t* T = (const uint32_t*)tbits;
     const int tw = 4 * tq;   // words per tray column
-    uint32_t* cw = cand + (size_t)o * sBits + (size_t)x * ny * nzw;
-    int nfree = 0;
-    for (int y = warp; y < Yv; y += 4) {
-        for (int wi = 0; wi < nzw; ++wi) {
-            uint32_t word = cw[(size_t)y * nzw + wi];
-            uint32_t keep = word;
-            while (word) {
-                const int bit = __ffs(word) - 1;
-                word &= word - 1u;
-                const int z = 32 * wi + bit;
-                const int sh = z >> 5, off = z & 31;
-                bool hit = false;
-                for (int k0 = 0; k0 < nc; k0 += 32) {
-                    const int k = k0 + lane;
-                    bool c = false;
-                    if (k < nc) {
-                        const uint4 r = __ldg(&cl[k]);
-                        const int a = (int)(r.x & 0xffffu), b = (int)(r.x >> 16);
-                        const uint32_t* tc = T + ((size_t)(x + a) * ny + (y + b)) * tw;
-                        const uint32_t t0 = __ldg(&tc[sh]);
-                        const uint32_t t1 = sh + 1 < nzw ? __ldg(&tc[sh + 1]) : 0u;
-                        const uint32_t f0 = __funnelshift_r(t0, t1, off);
-                        uint32_t f1 = 0u;
-                        if (r.z) {
-                            const uint32_t t2 = sh + 2 < nzw ? __ldg(&tc[sh + 2]) : 0u;
-                            f1 = __funnelshift_r(t1, t2, off);
-                        }
-                        c = ((r.y & ~f0) | (r.z & ~f1)) != 0u;
-                    }
-                    if (__any_sync(0xffffffffu, c)) {
-                        hit = true;
-                        break;
-                    }
+    for (int g = blockIdx.x * wpb + (threadIdx.x >> 5); g < total; g += gridDim.x * wpb) {
+        int o = 0;
+        while (pre[o + 1] <= g) ++o;
+        const int t = clist[(size_t)o * ccap + (g - pre[o])];
+        const int z = t % nz, y = (t / nz) % ny, x = t / (nz * ny);
+        const int nc = ncol[o];
+        const uint4* cl = cols + (size_t)o * cstride;
+        const int sh = z >> 5, off = z & 31;
+        bool hit = false;
+        for (int k0 = 0; k0 < nc && !hit; k0 += 32) {
+            const int k = k0 + lane;
+            bool c = false;
+            if (k < nc) {
+                const uint4 r = __ldg(&cl[k]);
+                const int a = (int)(r.x & 0xffffu), b = (int)(r.x >> 16);
+                const uint32_t* tc = T + ((size_t)(x + a) * ny + (y + b)) * tw;
+                const uint32_t t0 = __ldg(&tc[sh]);
+                const uint32_t t1 = sh + 1 < nzw ? __ldg(&tc[sh + 1]) : 0u;
+                const uint32_t f0 = __funnelshift_r(t0, t1, off);
+                uint32_t f1 = 0u;
+                if (r.z) {
+                    const uint32_t t2 = sh + 2 < nzw ? __ldg(&tc[sh + 2]) : 0u;
+                    f1 = __funnelshift_r(t1, t2, off);
                 }
-                if (hit) keep &= ~(1u << bit);
+                c = ((r.y & ~f0) | (r.z & ~f1)) != 0u;
             }
-            if (lane == 0) cw[(size_t)y * nzw + wi] = keep;
-            nfree += __popc(keep);
+            hit = __any_sync(0xffffffffu, c);
+        }
+        if (lane == 0) {
+            if (hit) {
+                atomicAnd(&cand[(size_t)o * sBits + ((size_t)x * ny + y) * nzw + sh], ~(1u << off));
+            } else {
+                atomicAdd(&vcount[o], 1);
+                if (set_okplane) okplane[(size_t)o * pstride + x] = 1;
+            }
         }
     }
-    if (lane == 0 && nfree) atomicAdd(&vcount[o], nfree);
-    const int any = __syncthreads_or(nfree != 0);
-    if (set_okplane && any && tid == 0) okplane[(size_t)o * pstride + x] = 1;
 }
 
 // Exact score of every ok cell of a direct orientation (k_collect_plane
-// collected all of them): the proximity sum over the item's voxels in
-// integers (the exact value the reference's FFT rounds to), then the
+// collected all of them): the proximity sum over the item's z-runs in
+// integers (the exact value the reference's FFT rounds to; pphi holds the
+// distance field's prefix sums along z, psb_kernels.cuh), then the
 // reference's score.  One warp per cell.  grid: (blocks, n_orient), block 256
 __global__ void __launch_bounds__(256)
-k_direct_score(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ phi) {
+k_direct_score(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pphi) {
     if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
@@ -370,11 +397,12 @@ k_direct_score(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParam
         const int y = (t / sp.nz) % sp.ny;
         const int x = t / (sp.nz * sp.ny);
         long long acc = 0;
-        for (int v = lane; v < od.nvox; v += 32) {
-            const int4 q = __ldg(&od.vox[v]);
-            int oc[3];
-            orient_voxel(od, q.x, q.y, q.z, oc);
-            acc += (long long)q.w * __ldg(&phi[((size_t)(x + oc[0]) * sp.ny + (y + oc[1])) * sp.nz + (z + oc[2])]);
+        for (int r = lane; r < od.nruns; r += 32) {
+            const int4 q = __ldg(&od.runs[r]);
+            int a, b, c0, c1;
+            orient_run(od, q, &a, &b, &c0, &c1);
+            const int32_t* P = pphi + ((size_t)(x + a) * sp.ny + (y + b)) * (sp.nz + 1) + z;
+            acc += (long long)q.w * (__ldg(&P[c1 + 1]) - __ldg(&P[c0]));
         }
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);

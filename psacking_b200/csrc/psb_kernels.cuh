@@ -40,7 +40,60 @@ struct OrientDesc {
     const int4* samp;         // sample voxels of the base item for the candidate filter (psb_filter.cuh)
     int nsamp;                // their count; 0: no filter
     int direct;               // set on the device: few candidates, decided without transforms (psb_filter.cuh)
+    const int4* runs;         // device z-runs of the base item along source axis src_axis[2] (item_run)
+    int nruns;
 };
+
+// A run of equal nonzero values along one source axis s of the base item:
+// {u, v, r0 | r1 << 16, value}, u and v the coordinates along the other two
+// source axes (u along the lower axis index), r0..r1 the range along s.
+// oriented position (a, b) of the run's column and its z range c0..c1 for
+// an orientation whose z axis comes from s (= d.src_axis[2]).
+__device__ __forceinline__ void orient_run(const OrientDesc& d, int4 q, int* a, int* b, int* c0, int* c1) {
+    const int s = d.src_axis[2];
+    const int lo = s == 0 ? 1 : 0;          // the lower of the two other source axes
+    const int va = d.src_axis[0] == lo ? q.x : q.y;
+    const int vb = d.src_axis[1] == lo ? q.x : q.y;
+    *a = d.flip[0] ? d.e[0] - 1 - va : va;
+    *b = d.flip[1] ? d.e[1] - 1 - vb : vb;
+    const int r0 = q.z & 0xffff, r1 = q.z >> 16;
+    *c0 = d.flip[2] ? d.e[2] - 1 - r1 : r0;
+    *c1 = d.flip[2] ? d.e[2] - 1 - r0 : r1;
+}
+
+// Prefix sums along z of every tray column: P[col * (nz + 1) + k] is the sum
+// over z < k of the column's distance values (MODE 0) or of its occupied
+// cells (MODE 1), so a run [c0, c1] of an item placed at height z collects
+// P[z + c1 + 1] - P[z + c0].  One warp per column (a shuffle scan per 32
+// cells).
+template <int MODE>
+__device__ __forceinline__ void col_prefix(const int32_t* __restrict__ src, int32_t* __restrict__ P, int nz,
+                                           int lane) {
+    int carry = 0;
+    if (lane == 0) P[0] = 0;
+    for (int z0 = 0; z0 < nz; z0 += 32) {
+        const int z = z0 + lane;
+        int v = 0;
+        if (z < nz) v = MODE == 0 ? src[z] : (src[z] != 0 ? 1 : 0);
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane >= d) v += u;
+        }
+        if (z < nz) P[z + 1] = carry + v;
+        carry += __shfl_sync(0xffffffffu, v, 31);
+    }
+}
+
+// every column; gated on *gate when given.  grid: ceil(ncols / 8), block 256
+template <int MODE>
+__global__ void k_col_prefix(const int32_t* __restrict__ src, int32_t* __restrict__ P, int ncols, int nz,
+                             const int* gate) {
+    if (gate && !*gate) return;
+    const int col = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (col >= ncols) return;
+    col_prefix<MODE>(src + (size_t)col * nz, P + (size_t)col * (nz + 1), nz, threadIdx.x & 31);
+}
 
 __device__ __forceinline__ int orient_src_index(const OrientDesc& d, int i0, int i1, int i2) {
     int o[3] = {i0, i1, i2};
@@ -367,6 +420,7 @@ struct PlaneBufs {
     int set_okplane;          // k_plane3 field 0 sets okplane from the free cells
     const unsigned char* candplane;  // k_plane3 field 0: per (orientation, x plane) "holds a candidate"
                                      // (k_cand_filter wrote the candidate words); null: no filter ran
+    int* okcount;             // k_plane3 field 0 with set_okplane: free cells per orientation (or null)
 };
 
 // Per (x-plane, orientation): inverse along y, C2R along z for the collision

@@ -3,7 +3,7 @@
 #pragma once
 #include "psb_kernels.cuh"
 
-#define PSB_UF_LIMIT (1 << 22)     // bound on union-find retries / path steps
+#define PSB_UF_LIMIT (1 << 22)     // default bound on union-find retries / path steps
 
 // ---------------------------------------------------------------------------
 // candidate selection and the exact tie guard
@@ -25,6 +25,7 @@ struct SelectBufs {
     unsigned long long* pmin;      // per (orientation, x plane) approx min key, stride pstride
     long long pstride;
     const int* gate;               // when set, the kernels run only if *gate != 0
+    const unsigned char* okplane;  // when set, per (orientation, x plane): holds an ok cell (stride pstride)
 };
 
 __device__ __forceinline__ bool okbit(const uint32_t* bits, const ScoreParams& sp, int x, int y, int z) {
@@ -137,6 +138,7 @@ k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScorePara
     if (od.direct) {
         // a direct orientation (psb_filter.cuh): every ok cell is a candidate,
         // scored exactly by k_direct_score (at most the direct limit of them)
+        if (sb.okplane && !sb.okplane[(size_t)o * sb.pstride + x]) return;   // no ok cell in this plane
         int* cand = sb.cand + (size_t)o * sb.cap;
         for (int y = warp; y < Yv; y += nwarp)
             for (int w = 0; w < nw; ++w) {
@@ -217,12 +219,13 @@ __global__ void k_sel_reset(SelectBufs sb, int n) {
 }
 
 // exact score of every candidate.  Regime (a): the FP32 value rounds to the
-// exact integer.  Regime (b): direct integer sums over the item's voxels
-// (proximity and collision), the FP64 guard.  One warp per candidate.
+// exact integer.  Regime (b): direct integer sums over the item's z-runs
+// (proximity and collision, from the per-column prefix sums pphi / pocc of
+// the distance field and the occupancy), the FP64 guard.
 // grid: (blocks, n_orient)
 __global__ void __launch_bounds__(256)
-k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ tray,
-          const int32_t* __restrict__ phi) {
+k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pocc,
+          const int32_t* __restrict__ pphi) {
     if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
@@ -244,9 +247,10 @@ k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp,
         }
         return;
     }
-    // regime (b): one CTA per candidate sums the item's voxels exactly
+    // regime (b): one CTA per candidate sums the item's runs exactly
     __shared__ long long red_acc[8], red_coll[8];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int nz1 = sp.nz + 1;
     for (int c = blockIdx.x; c < n; c += gridDim.x) {
         if (cs[c] > glim) {  // outside the orientation's window: provably not the minimum
             if (tid == 0) cs[c] = 1e300;
@@ -257,15 +261,15 @@ k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp,
         const int y = (t / sp.nz) % sp.ny;
         const int x = t / (sp.nz * sp.ny);
         long long acc = 0, coll = 0;
-        const int nv = od.nvox;
+        const int nr = od.nruns;
 #pragma unroll 4
-        for (int v = tid; v < nv; v += 256) {
-            const int4 q = __ldg(&od.vox[v]);
-            int oc[3];
-            orient_voxel(od, q.x, q.y, q.z, oc);
-            const size_t g = ((size_t)(x + oc[0]) * sp.ny + (y + oc[1])) * sp.nz + (z + oc[2]);
-            acc += (long long)q.w * __ldg(&phi[g]);
-            coll += (long long)q.w * (__ldg(&tray[g]) != 0);
+        for (int r = tid; r < nr; r += 256) {
+            const int4 q = __ldg(&od.runs[r]);
+            int a, b, c0, c1;
+            orient_run(od, q, &a, &b, &c0, &c1);
+            const size_t g = ((size_t)(x + a) * sp.ny + (y + b)) * nz1 + z;
+            acc += (long long)q.w * (__ldg(&pphi[g + c1 + 1]) - __ldg(&pphi[g + c0]));
+            coll += (long long)q.w * (__ldg(&pocc[g + c1 + 1]) - __ldg(&pocc[g + c0]));
         }
         for (int off = 16; off > 0; off >>= 1) {
             acc += __shfl_xor_sync(0xffffffffu, acc, off);
@@ -312,6 +316,19 @@ __global__ void k_tiebreak(const OrientDesc* __restrict__ orients, SelectBufs sb
     }
 }
 
+// After the collision pass (and, in the interlocking mode, the flood fill):
+// an orientation with at most late_max ok cells skips the proximity
+// transforms (direct = 2); k_collect_plane takes all its ok cells and
+// k_direct_score scores them by exact sums.  grid: ceil(n / 128), block 128
+__global__ void k_late_direct(OrientDesc* __restrict__ orients, int n, const int* __restrict__ okcount, int late_max) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    OrientDesc& od = orients[o];
+    if (od.skip || od.direct) return;
+    const int c = okcount[o];
+    if (c > 0 && c <= late_max) od.direct = 2;
+}
+
 struct ResultDev {
     int x, y, z, found;
     double score;
@@ -336,7 +353,8 @@ __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb
     r.diag = sb.diag[o] | (orients[o].exact ? 1u : 0u);
     if (sb.ncand[o] > sb.cap) r.diag |= 0x100u;
     if (sb.gate) r.diag |= 0x400u;  // the gated second selection (lazy flood fill) ran
-    if (orients[o].direct) r.diag |= 0x800u;  // decided without transforms (psb_filter.cuh)
+    if (orients[o].direct == 1) r.diag |= 0x800u;  // decided without transforms (psb_filter.cuh)
+    if (orients[o].direct == 2) r.diag |= 0x1000u; // few ok cells: proximity by exact sums (k_late_direct)
     if (!orients[o].skip && sb.best[o] != 0xffffffffffffffffULL) {
         double s = ord_val(sb.best[o]);
         double cut = sp.mode == 0 ? 1000000000.0 : 1e29;
@@ -449,9 +467,14 @@ struct FloodBufs {
     const int* gate;               // when set, the kernels run only if *gate != 0
     unsigned char* okplane;        // when set, k_ff_reach flags planes holding a reachable cell
     long long okstride;            // okplane stride per orientation
+    int limit;                     // union-find retries / path steps before err is set
+    int* okcount;                  // when set, k_ff_reach adds each orientation's reachable cells
 };
 
-__device__ __forceinline__ int run_find(int* parent, int x, unsigned int* err) {
+// Past `limit` steps both give up, set bit 0 of *err and return a valid run
+// index (not necessarily the root): every access stays in bounds and the
+// host reports PSB_ERR_LIMIT.
+__device__ __forceinline__ int run_find(int* parent, int x, unsigned int* err, int limit) {
     int it = 0;
     int p = __ldcg(&parent[x]);
     while (p != x) {
@@ -459,15 +482,15 @@ __device__ __forceinline__ int run_find(int* parent, int x, unsigned int* err) {
         if (gp != p) __stcg(&parent[x], gp);   // path halving; gp is an ancestor
         x = p;
         p = gp;
-        if (++it > PSB_UF_LIMIT) { atomicOr(err, 1u); return x; }
+        if (++it > limit) { atomicOr(err, 1u); return x; }
     }
     return x;
 }
 
-__device__ __forceinline__ void run_unite(int* parent, int a, int b, unsigned int* err) {
-    for (int it = 0; it < PSB_UF_LIMIT; ++it) {
-        a = run_find(parent, a, err);
-        b = run_find(parent, b, err);
+__device__ __forceinline__ void run_unite(int* parent, int a, int b, unsigned int* err, int limit) {
+    for (int it = 0; it < limit; ++it) {
+        a = run_find(parent, a, err, limit);
+        b = run_find(parent, b, err, limit);
         if (a == b) return;
         if (a > b) { int t = a; a = b; b = t; }
         int old = atomicCAS(&parent[b], b, a);   // link the larger root under the smaller
@@ -581,7 +604,7 @@ __global__ void k_ff_union(const OrientDesc* __restrict__ orients, FloodBufs fb,
         while (i < cL && j < cN) {
             int a = rz[oL + i], b = rz[oN + j];
             int a0 = a & 0xffff, a1 = a >> 16, b0 = b & 0xffff, b1 = b >> 16;
-            if (a0 <= b1 && b0 <= a1) run_unite(par, oL + i, oN + j, fb.err);
+            if (a0 <= b1 && b0 <= a1) run_unite(par, oL + i, oN + j, fb.err, fb.limit);
             if (a1 < b1) ++i; else ++j;
         }
     }
@@ -597,7 +620,7 @@ __global__ void k_ff_seed(const OrientDesc* __restrict__ orients, FloodBufs fb) 
     int* fl = fb.rflag + (size_t)o * fb.sRun;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         if (fl[r] & 1) {
-            int root = run_find(par, r, fb.err);
+            int root = run_find(par, r, fb.err, fb.limit);
             atomicOr(&fl[root], 2);
         }
     }
@@ -620,14 +643,22 @@ __global__ void k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb,
     int* par = fb.parent + (size_t)o * fb.sRun;
     const int* fl = fb.rflag + (size_t)o * fb.sRun;
     bool any = false;
+    int nreach = 0;
     for (int i = 0; i < cL; ++i) {
-        int root = run_find(par, oL + i, fb.err);
+        int root = run_find(par, oL + i, fb.err, fb.limit);
         if (!(__ldcg(&fl[root]) & 2)) continue;
         int a = rz[oL + i];
         for (int z = a & 0xffff; z <= (a >> 16); ++z) w[z >> 5] |= 1u << (z & 31);
+        nreach += (a >> 16) - (a & 0xffff) + 1;
         any = true;
     }
     if (any && fb.okplane) fb.okplane[(size_t)o * fb.okstride + x] = 1;
+    if (fb.okcount) {
+        // one atomic per group of lanes that arrive here together
+        const unsigned int m = __activemask();
+        const int c = __reduce_add_sync(m, nreach);
+        if ((threadIdx.x & 31) == __ffs(m) - 1 && c) atomicAdd(&fb.okcount[o], c);
+    }
 }
 
 // ---------------------------------------------------------------------------

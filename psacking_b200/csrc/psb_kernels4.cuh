@@ -156,6 +156,7 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
 #pragma unroll
     for (int i = 0; i < (FIELD == 1 ? LZ::B2 * LZ::R1 : 1); ++i) zmin[i] = INFINITY;
     unsigned int anyfree = 0u;
+    int nfree = 0;   // FIELD 0: free cells written by this lane
 
     const float2* P = (FIELD == 0 ? sb.Pc : sb.Pd) + (size_t)o * sb.sP + (size_t)x * NY * HZ;
     for (int t = warp; t * LY::PER < HZ; t += NWARP) {
@@ -304,6 +305,7 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
                     fbits[(size_t)ya * nzw + i] = wa[i];
                     if (hb) fbits[(size_t)yb * nzw + i] = wb[i];
                     anyfree |= wa[i] | wb[i];
+                    nfree += __popc(wa[i]) + (hb ? __popc(wb[i]) : 0);
                 }
             }
         }
@@ -314,6 +316,10 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
         if (lane == 0 && dg) atomicOr(&pb.diag[o], dg);
         if (pb.set_okplane && __any_sync(0xffffffffu, anyfree != 0u) && lane == 0)
             pb.okplane[(size_t)o * pb.pstride + x] = 1;
+        if (pb.set_okplane && pb.okcount) {
+            const int c = __reduce_add_sync(0xffffffffu, nfree);
+            if (lane == 0 && c) atomicAdd(&pb.okcount[o], c);
+        }
         return;
     }
     // FIELD 1: the plane's minimum approximate score over its ok cells (the

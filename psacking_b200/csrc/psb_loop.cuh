@@ -197,3 +197,20 @@ __global__ void k_stats_g(const int32_t* __restrict__ v, size_t n, const int* sh
         atomicMax((unsigned int*)&out[2], (unsigned int)mx);
     }
 }
+
+// After a placement only the columns under the placed item's box change:
+// refresh their occupancy prefix sums (k_col_prefix, MODE 1), gated on
+// ls->placed_now.  grid: ceil(max box columns / 8), block 256
+__global__ void k_occ_prefix_box(const int32_t* __restrict__ tray, int32_t* __restrict__ P, int nx, int ny, int nz,
+                                 const LoopState* __restrict__ ls, const OrientDesc* __restrict__ od_item) {
+    if (!ls->placed_now) return;
+    const OrientDesc& od = od_item[ls->orient];
+    const int by = od.e[1];
+    const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (k >= od.e[0] * by) return;
+    const int i = ls->px + k / by, j = ls->py + k % by;
+    if (i < 0 || j < 0 || i >= nx || j >= ny) return;
+    const size_t col = (size_t)i * ny + j;
+    col_prefix<1>(tray + col * nz, P + col * (nz + 1), nz, threadIdx.x & 31);
+}
+

@@ -1,0 +1,188 @@
+"""Device-side limits and host-side failures end in an error status, never in
+a spin or a leak.
+
+* The flood fill's union-find gives up after a bounded number of steps
+  (psb_set_uf_limit).  With the bound set to 1 on trays whose free space forms
+  long chains of z-runs, the searches and the packing loop return
+  PSB_ERR_LIMIT (RuntimeError in the drop-in module): the kernels returned.
+  With the default bound restored, the same calls give the oracle's answers,
+  so the context stayed usable.
+* Device allocation failures, injected at every allocation of a tray's
+  creation and of a packing run, return PSB_ERR_CUDA and free everything the
+  failed call allocated (the engine's live-allocation count returns to where
+  it was).
+"""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import psb_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+LIB = Path(__file__).resolve().parent.parent / "psacking_b200" / "libpsb200.so"
+PSB_ERR_CUDA, PSB_ERR_LIMIT = 2, 5
+
+
+def serpentine_tray(n=33, nz=3):
+    """Walls everywhere except a one-cell-high corridor at z = 1 that snakes
+    through the x-y plane and opens on the face x = 0: every free cell is
+    reachable, through one long chain of single-cell runs."""
+    tray = np.full((n, n, nz), 2, np.int32)
+    for y in range(1, n - 1, 2):
+        tray[1:n - 1, y, 1] = 0
+        if y + 2 < n - 1:
+            link_x = n - 2 if (y // 2) % 2 == 0 else 1
+            tray[link_x, y + 1, 1] = 0
+    tray[0, 1, 1] = 0
+    return tray
+
+
+def random_tray(seed, shape=(48, 40, 36), fill=0.3):
+    rng = np.random.default_rng(seed)
+    return (rng.random(shape) < fill).astype(np.int32) * 2
+
+
+def boxes_tray(seed, shape=(40, 40, 24), n_boxes=8):
+    """Mostly open space with a few solid boxes: one large free region made
+    of many z-runs, so the union-find merges long chains for every item."""
+    rng = np.random.default_rng(seed)
+    tray = np.zeros(shape, np.int32)
+    for _ in range(n_boxes):
+        e = [int(rng.integers(3, s // 3)) for s in shape]
+        o = [int(rng.integers(0, s - ee)) for s, ee in zip(shape, e)]
+        tray[o[0]:o[0] + e[0], o[1]:o[1] + e[1], o[2]:o[2] + e[2]] = 2
+    return tray
+
+
+@pytest.fixture
+def uf_limit(gpu_core):
+    yield gpu_core.set_uf_limit
+    gpu_core.set_uf_limit(0)
+
+
+def test_flood_fill_limit_returns_error_then_recovers(gpu_core, uf_limit):
+    item = np.ones((1, 1, 1), np.int32)
+    for tray in (serpentine_tray(), random_tray(1)):
+        want = O.interlocking_free_positions(tray, item)
+        uf_limit(1)
+        with pytest.raises(RuntimeError, match="iteration limit"):
+            gpu_core.interlocking_free_positions(tray, item)
+        uf_limit(0)
+        np.testing.assert_array_equal(gpu_core.interlocking_free_positions(tray, item), want)
+
+
+def test_search_limit_returns_error_then_recovers(gpu_core, uf_limit):
+    tray = boxes_tray(2)
+    phi = O.calculate_distance(tray)
+    ors = [np.ones((2, 1, 1), np.int32), np.ones((1, 2, 2), np.int32)]
+    want = O.fft_search_batch(ors, tray, phi, interlock=True)
+    uf_limit(1)
+    with pytest.raises(RuntimeError, match="iteration limit"):
+        gpu_core.gpu_tray_cleanup()
+        gpu_core.fft_search_batch_interlocking_free(ors, tray, phi, 1)
+    uf_limit(0)
+    gpu_core.gpu_tray_cleanup()
+    got = gpu_core.fft_search_batch_interlocking_free(ors, tray, phi, 1)
+    assert (tuple(got[0]), got[1], got[2], got[3]) == (tuple(want[0]), want[1], want[2], want[3])
+
+
+def test_packing_loop_limit_returns_error_then_recovers(gpu_core, uf_limit):
+    from psacking_b200 import BinPacker, workloads
+    items = workloads.config1_items(2)[:5]
+    tray = boxes_tray(3)
+    packer = BinPacker(tray.shape, num_orientations=4, interlocking_free=True)
+    uf_limit(1)
+    with pytest.raises(RuntimeError, match="iteration limit"):
+        packer.pack_voxels(items, initial_tray=tray)
+    uf_limit(0)
+    got = packer.pack_voxels(items, initial_tray=tray)
+    want_tray, want = O.pack_voxels(items, tray.shape, 4, True, initial_tray=tray)
+    np.testing.assert_array_equal(got.tray, want_tray)
+    assert [(p.success, p.position, p.orientation_index) for p in got.placements] == \
+           [(w["success"], w["position"], w["orientation_index"]) for w in want]
+
+
+class _Abi:
+    def __init__(self):
+        self.lib = lib = ctypes.CDLL(str(LIB))
+        P, I = ctypes.c_void_p, ctypes.c_int
+        lib.psb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        lib.psb_debug_fail_alloc.argtypes = [I]
+        lib.psb_debug_live_allocs.argtypes = [P]
+        lib.psb_tray_create.argtypes = [I, I, I, P]
+        lib.psb_tray_destroy.argtypes = [P]
+        lib.psb_tray_set.argtypes = [P, P, P]
+        lib.psb_pack.argtypes = [P, P, P, I, P, I, I, ctypes.c_int32, P, P]
+
+    def err(self):
+        buf = ctypes.create_string_buffer(1024)
+        self.lib.psb_last_error(buf, 1024)
+        return buf.value.decode()
+
+    def live(self):
+        n = ctypes.c_longlong(-1)
+        assert self.lib.psb_debug_live_allocs(ctypes.byref(n)) == 0
+        return n.value
+
+
+def test_injected_allocation_failures_are_clean():
+    abi = _Abi()
+    lib = abi.lib
+    base = abi.live()
+    # every allocation of a tray's creation, one at a time
+    failures = 0
+    for k in range(1, 64):
+        lib.psb_debug_fail_alloc(k)
+        t = ctypes.c_void_p()
+        st = lib.psb_tray_create(40, 36, 30, ctypes.byref(t))
+        lib.psb_debug_fail_alloc(0)
+        if st == 0:
+            assert lib.psb_tray_destroy(t) == 0
+            break
+        assert st == PSB_ERR_CUDA and "injected" in abi.err(), (k, st, abi.err())
+        assert not t.value
+        assert abi.live() == base, k
+        failures += 1
+    assert failures >= 10   # the tray allocates its grids, spectra and work buffers
+    # every allocation of a packing run (staging, slots, loop buffers)
+    from psacking_b200 import workloads
+    from psacking_b200.rotations import orientation_maps
+    items = [np.ascontiguousarray(i) for i in workloads.config1_items(5)[:4]]
+    ptrs = (ctypes.POINTER(ctypes.c_int32) * len(items))(
+        *[i.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) for i in items])
+    dims = np.array([i.shape for i in items], np.int32).ravel()
+    maps = np.ascontiguousarray(orientation_maps(4), np.int32)
+    tray0 = np.zeros((40, 36, 30), np.int32)
+
+    class Res(ctypes.Structure):
+        _fields_ = [("x", ctypes.c_int32), ("y", ctypes.c_int32), ("z", ctypes.c_int32),
+                    ("found", ctypes.c_int32), ("score", ctypes.c_double), ("orientation", ctypes.c_int32),
+                    ("diag", ctypes.c_uint32), ("n_candidates", ctypes.c_int32), ("err_ratio", ctypes.c_float)]
+
+    def pack(k):
+        t = ctypes.c_void_p()
+        assert lib.psb_tray_create(40, 36, 30, ctypes.byref(t)) == 0, abi.err()
+        assert lib.psb_tray_set(t, tray0.ctypes.data, None) == 0, abi.err()
+        res = (Res * len(items))()
+        out = np.zeros_like(tray0)
+        lib.psb_debug_fail_alloc(k)
+        st = lib.psb_pack(t, ptrs, dims.ctypes.data, len(items), maps.ctypes.data, 4, 1, 0, res, out.ctypes.data)
+        lib.psb_debug_fail_alloc(0)
+        msg = abi.err()
+        assert lib.psb_tray_destroy(t) == 0
+        return st, msg, res, out
+
+    failures = 0
+    for k in range(1, 128):
+        st, msg, res, out = pack(k)
+        assert abi.live() == base, k
+        if st == 0:
+            break
+        assert st == PSB_ERR_CUDA and "injected" in msg, (k, st, msg)
+        failures += 1
+    assert failures >= 3
+    want_tray, want = O.pack_voxels(items, tray0.shape, 4, True, sort_by_volume=False)
+    np.testing.assert_array_equal(out, want_tray)

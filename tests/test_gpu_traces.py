@@ -77,6 +77,20 @@ def test_native_loop_matches_trace_every_sample(gpu_core, name):
     _check(tr, res)
 
 
+@pytest.mark.parametrize("late", [0, 1 << 16])
+@pytest.mark.parametrize("name", ["config2_seed0", "config3_seed1"])
+def test_native_loop_matches_trace_late_direct(gpu_core, name, late):
+    """Orientations left with few ok cells after the collision pass take
+    exact proximity sums instead of the proximity transforms: none of them
+    (0), or practically all (2^16 cells)."""
+    gpu_core.set_late_direct_max(late)
+    try:
+        tr, res = _run(name)
+    finally:
+        gpu_core.set_late_direct_max(1024)
+    _check(tr, res)
+
+
 @pytest.mark.parametrize("name", ["config1_seed0", "config1_seed9", "config2_seed0", "config3_seed1"])
 def test_call_pattern_matches_trace(gpu_core, name):
     tr, res = _run(name, engine="calls")
