@@ -193,6 +193,28 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
 int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                     psb_result* out_placements, int32_t* final_tray);
 
+/* ---- orientation-sharded packing loop over several GPUs ------------------
+ * The greedy loop of psb_pack_staged with one tray's orientations spread
+ * over `world` ranks (one process and GPU each, every rank holding the whole
+ * tray): rank r searches the orientations o with o % world == r.  Per item,
+ * the rank's best (PSB_SHARD_RECORD_BYTES, with the global orientation
+ * index) is written to the device buffer d_local on the tray's stream
+ * (psb_tray_stream); then exchange(ctx) is called on the host, once per item
+ * in item order, and must queue on that stream the gathering of every rank's
+ * record into d_all (world records in rank order, e.g. an NCCL all-gather)
+ * and return 0.  The merged winner -- the smallest score, on equal scores the
+ * lowest orientation index, the reference's strict < over orientations
+ * (spectral_packing/fft3.cu:1625, spectral_packer/packer.py:500) -- is placed
+ * on every rank, so the trays stay identical without being exchanged and the
+ * results equal psb_pack_staged's.  world == 1 needs no exchange (NULL): the
+ * record is copied to d_all.  The reference packs on one GPU only; this
+ * entry point has no counterpart there. */
+#define PSB_SHARD_RECORD_BYTES 32
+typedef int (*psb_exchange_fn)(void* ctx);
+int psb_pack_staged_sharded(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
+                            int rank, int world, void* d_local, void* d_all, psb_exchange_fn exchange, void* ctx,
+                            psb_result* out_placements, int32_t* final_tray);
+
 /* ---- detailed packing run and the learned orientation proposal ---------
  * None of these has a counterpart in the reference: the learned-proposal
  * form of the placement search (a small 3-D CNN that ranks an item's 24

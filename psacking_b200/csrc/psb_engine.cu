@@ -2521,6 +2521,15 @@ struct PackOpts {
     psb_result* per_orient = nullptr;   // n_items x n_orient results of every orientation
     float* hmaps = nullptr;             // n_items x 1024 pooled height maps before each item
     int32_t* gate_stats = nullptr;      // [items gated, fallbacks to the full sweep]
+    // orientation sharding (psb_pack_staged_sharded): this rank searches the
+    // orientations o with o % world == rank; per item its decision goes to
+    // d_local, exchange(ctx) gathers every rank's into d_all, and the merged
+    // winner is placed
+    int rank = 0, world = 1;
+    void* d_local = nullptr;
+    void* d_all = nullptr;
+    psb_exchange_fn exchange = nullptr;
+    void* ctx = nullptr;
 };
 int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                      psb_result* out_placements, int32_t* final_tray, const PackOpts& opt);
@@ -2538,6 +2547,22 @@ int psb_pack_staged_detail(psb_tray* t, const int32_t* orient_maps, int n_orient
     PackOpts o;
     o.per_orient = per_orient;
     o.hmaps = hmaps;
+    return pack_staged_impl(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray, o);
+}
+
+int psb_pack_staged_sharded(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
+                            int rank, int world, void* d_local, void* d_all, psb_exchange_fn exchange, void* ctx,
+                            psb_result* out_placements, int32_t* final_tray) {
+    if (world < 1 || rank < 0 || rank >= world) return fail(PSB_ERR_ARG, "bad rank %d of world %d", rank, world);
+    if (!d_local || !d_all) return fail(PSB_ERR_ARG, "sharded packing needs the decision buffers");
+    if (world > 1 && !exchange) return fail(PSB_ERR_ARG, "sharded packing over %d ranks needs an exchange", world);
+    PackOpts o;
+    o.rank = rank;
+    o.world = world;
+    o.d_local = d_local;
+    o.d_all = d_all;
+    o.exchange = exchange;
+    o.ctx = ctx;
     return pack_staged_impl(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray, o);
 }
 
@@ -2594,6 +2619,11 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
                         t->d_stage + t->staged_off[it], t->d_stage_vox + t->staged_voff[it], rn,
                         &all[(size_t)it * n_orient + o]);
         }
+    // orientation sharding: the other ranks' orientations are not searched here
+    if (opt.world > 1)
+        for (int it = 0; it < n_items; ++it)
+            for (int o = 0; o < n_orient; ++o)
+                if (o % opt.world != opt.rank) all[(size_t)it * n_orient + o].skip = 1;
     // candidate-filter samples (tray columns of at most 256 cells)
     const bool filt = g_cand_filter && t->nzw <= 8;
     if (filt)
@@ -2745,8 +2775,20 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         if (d_per)
             CK(cudaMemcpyAsync(d_per + (size_t)it * n_orient, t->d_res, sizeof(ResultDev) * n_orient,
                                cudaMemcpyDeviceToDevice, t->st));
-        k_decide<<<1, 32, 0, t->st>>>(d_odb, t->d_res, n_orient, t->d_ls, t->d_dec + it, t->d_err);
+        ShardRecord* rec = opt.world > 1 || opt.d_local ? (ShardRecord*)opt.d_local : nullptr;
+        k_decide<<<1, 32, 0, t->st>>>(d_odb, t->d_res, n_orient, t->d_ls, t->d_dec + it, t->d_err, rec);
         CKL();
+        if (rec) {
+            // the exchange queues the gathering of every rank's record on the
+            // tray's stream; the merge then decides for all ranks alike
+            if (opt.exchange) {
+                if (opt.exchange(opt.ctx) != 0) return fail(PSB_ERR_STATE, "decision exchange failed at item %d", it);
+            } else {
+                CK(cudaMemcpyAsync(opt.d_all, opt.d_local, sizeof(ShardRecord), cudaMemcpyDeviceToDevice, t->st));
+            }
+            k_decide_merge<<<1, 1, 0, t->st>>>((const ShardRecord*)opt.d_all, opt.world, t->d_ls, t->d_dec + it);
+            CKL();
+        }
         {
             PROF("k_place_check", t->st);
             k_place_check_g<<<64, 256, 0, t->st>>>(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);

@@ -57,9 +57,19 @@ struct DecisionDev {
     float err_ratio;
 };
 
-// best over orientations (strict <: the first minimum wins), one warp
+// One rank's decision in the orientation-sharded loop
+// (psb_pack_staged_sharded): its best over the orientations it searched,
+// with the global orientation index.  32 bytes, exchanged between ranks.
+struct ShardRecord {
+    double score;
+    int found, orientation, x, y, z;
+    int pad;
+};
+
+// best over orientations (strict <: the first minimum wins), one warp.
+// rec (may be null): the same decision as a ShardRecord for the exchange.
 __global__ void k_decide(const OrientDesc* __restrict__ od, const ResultDev* __restrict__ res, int n,
-                         LoopState* ls, DecisionDev* out, const unsigned int* uf_err) {
+                         LoopState* ls, DecisionDev* out, const unsigned int* uf_err, ShardRecord* rec) {
     if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     const int best = best_result(od, res, n);
     unsigned int diag = 0;
@@ -102,6 +112,49 @@ __global__ void k_decide(const OrientDesc* __restrict__ od, const ResultDev* __r
     ls->need_phi = 0;
     ls->first = 0xffffffffffffffffULL;
     *out = d;
+    if (rec) {
+        ShardRecord r;
+        r.score = d.score;
+        r.found = d.found;
+        r.orientation = d.orientation;
+        r.x = d.x; r.y = d.y; r.z = d.z;
+        r.pad = 0;
+        *rec = r;
+    }
+}
+
+// The winner over every rank's record (rank order): the smallest score, on
+// equal scores the lowest orientation index -- the reference's strict < over
+// the orientations in order (fft3.cu:1625, packer.py:500); every rank then
+// places the same item the same way.  Overrides k_decide's local choice.
+// grid: 1, block 1
+__global__ void k_decide_merge(const ShardRecord* __restrict__ all, int world, LoopState* ls, DecisionDev* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int best = -1;
+    for (int r = 0; r < world; ++r) {
+        const ShardRecord& c = all[r];
+        if (!c.found) continue;
+        if (best < 0 || c.score < all[best].score ||
+            (c.score == all[best].score && c.orientation < all[best].orientation))
+            best = r;
+    }
+    if (best >= 0) {
+        const ShardRecord c = all[best];
+        out->x = c.x; out->y = c.y; out->z = c.z;
+        out->found = 1;
+        out->score = c.score;
+        out->orientation = c.orientation;
+        ls->do_place = 1;
+        ls->orient = c.orientation;
+        ls->px = c.x; ls->py = c.y; ls->pz = c.z;
+        ls->id = ls->id_offset + ls->placed + 1;
+    } else {
+        out->x = out->y = out->z = -1;
+        out->found = 0;
+        out->score = 0.0;
+        out->orientation = -1;
+        ls->do_place = 0;
+    }
 }
 
 __global__ void k_place_check_g(const OrientDesc* __restrict__ od_item, LoopState* ls, const int32_t* __restrict__ tray,

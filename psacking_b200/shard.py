@@ -96,63 +96,168 @@ def exchange_decision(local: Tuple, device=None) -> Tuple:
     return merge_decisions([tuple(o.tolist()) for o in out])
 
 
-def pack_orientation_sharded(items, tray_size, num_orientations: int = 24, interlocking_free: bool = False,
-                             sort_by_volume: bool = True, device=None):
-    """Pack one tray with its orientations spread over the ranks of the
-    initialised process group (one GPU per rank; a single process when none).
-    Returns (final tray, per-item (success, position, orientation, score)) in
-    the items' original order; identical on every rank and to
-    BinPacker(...).pack_voxels(items)."""
+RECORD_BYTES = 32   # PSB_SHARD_RECORD_BYTES: one rank's decision (score, found, orientation, x, y, z)
+
+ExchangeFn = None   # ctypes type of psb_exchange_fn, made on first use
+
+
+def _exchange_type():
+    import ctypes
+    global ExchangeFn
+    if ExchangeFn is None:
+        ExchangeFn = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
+    return ExchangeFn
+
+
+def nccl_exchange(local, gathered, stream):
+    """The exchange of psb_pack_staged_sharded over the initialised process
+    group: an all-gather of every rank's decision record, queued on the
+    engine's stream.  local: uint8 tensor of RECORD_BYTES, gathered: uint8
+    tensor of world * RECORD_BYTES, both on this rank's GPU."""
+    import torch
+    import torch.distributed as dist
+
+    def cb(_ctx):
+        try:
+            with torch.cuda.stream(stream):
+                dist.all_gather_into_tensor(gathered, local)
+            return 0
+        except Exception:  # noqa: BLE001  (reported as the engine's error)
+            return 1
+    return _exchange_type()(cb)
+
+
+class InProcessExchange:
+    """The exchange for `world` ranks running as threads of one process, each
+    with its own tray and stream on the same or different GPUs (used to run
+    the sharded loop where fewer GPUs than ranks are available).  Per item
+    every rank waits for its own stream, publishes its record on the host,
+    waits for the others (a host barrier with a timeout, no device-side
+    wait), and copies all records into its gathered buffer on its stream."""
+
+    def __init__(self, world: int, timeout: float = 120.0):
+        import threading
+        self.world = world
+        self.recs = [None] * world
+        self.barrier = threading.Barrier(world, timeout=timeout)
+
+    def callback(self, rank, local, gathered, stream):
+        import torch
+
+        def cb(_ctx):
+            try:
+                stream.synchronize()
+                self.recs[rank] = local.cpu()
+                self.barrier.wait()
+                with torch.cuda.stream(stream):
+                    gathered.copy_(torch.cat(self.recs).to(gathered.device))
+                stream.synchronize()
+                self.barrier.wait()
+                return 0
+            except Exception:  # noqa: BLE001
+                self.barrier.abort()
+                return 1
+        return _exchange_type()(cb)
+
+
+def pack_sharded_on_device(items, tray_size, num_orientations: int = 24, interlocking_free: bool = False,
+                           sort_by_volume: bool = True, rank: int = 0, world: int = 1, exchange=None,
+                           device=None):
+    """One rank of the orientation-sharded greedy loop on the device
+    (psb_pack_staged_sharded): this rank searches orientations o with
+    o % world == rank, decisions are exchanged per item by `exchange` (a
+    callable (local, gathered, stream) -> ctypes callback; None with world
+    == 1) and every rank places the merged winner.  Returns (final tray,
+    per-item (success, position, orientation, score)) in the items' original
+    order, identical on every rank and to BinPacker(...).pack_voxels(items)."""
     import ctypes
 
     import numpy as np
-    import torch.distributed as dist
+    import torch
 
     from .proposal import PsbResult, check, lib
-    from .rotations import apply_map, orientation_maps
+    from .rotations import orientation_maps
+
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    maps = np.ascontiguousarray(orientation_maps(num_orientations), np.int32)
+    arrs = [np.ascontiguousarray(np.asarray(i, dtype=np.int32)) for i in items]
+    vols = [int(np.count_nonzero(a > 0)) for a in arrs]
+    order = list(np.argsort(vols)[::-1]) if sort_by_volume else list(range(len(arrs)))
+    seq = [arrs[k] for k in order]
+    L = lib()
+    vp = ctypes.c_void_p
+    L.psb_tray_set.argtypes = [vp, vp, vp]
+    L.psb_pack_stage.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.psb_pack_staged_sharded.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int32, ctypes.c_int,
+                                          ctypes.c_int, vp, vp, vp, vp, vp, vp]
+    L.psb_tray_stream.argtypes = [vp, vp]
+    t = ctypes.c_void_p()
+    check(L.psb_tray_create(*[int(d) for d in tray_size], ctypes.byref(t)))
+    tray = np.zeros(tuple(int(d) for d in tray_size), np.int32)
+    res = (PsbResult * len(seq))()
+    try:
+        with torch.cuda.device(dev):
+            local = torch.zeros(RECORD_BYTES, dtype=torch.uint8, device=dev)
+            gathered = torch.zeros(RECORD_BYTES * world, dtype=torch.uint8, device=dev)
+            sp = ctypes.c_void_p()
+            check(L.psb_tray_stream(t, ctypes.byref(sp)))
+            stream = torch.cuda.ExternalStream(sp.value, device=dev)
+            cb = exchange(local, gathered, stream) if exchange is not None else None
+            check(L.psb_tray_set(t, tray.ctypes.data, None))
+            ptrs = (ctypes.c_void_p * len(seq))(*[a.ctypes.data for a in seq])
+            dims = np.ascontiguousarray(np.array([a.shape for a in seq], np.int32).ravel())
+            check(L.psb_pack_stage(t, ptrs, dims.ctypes.data, len(seq)))
+            torch.cuda.synchronize(dev)
+            check(L.psb_pack_staged_sharded(t, maps.ctypes.data, len(maps), 1 if interlocking_free else 0, 0,
+                                            rank, world, local.data_ptr(), gathered.data_ptr(),
+                                            ctypes.cast(cb, vp) if cb is not None else None, None, res,
+                                            tray.ctypes.data))
+    finally:
+        L.psb_tray_destroy(t)
+    out = [None] * len(arrs)
+    for r, k in zip(res, order):
+        out[k] = (True, (r.x, r.y, r.z), r.orientation, r.score) if r.found else (False, None, 0, None)
+    return tray, out
+
+
+def pack_orientation_sharded(items, tray_size, num_orientations: int = 24, interlocking_free: bool = False,
+                             sort_by_volume: bool = True, device=None):
+    """Pack one tray with its orientations spread over the ranks of the
+    initialised process group (one GPU per rank, NCCL; a single process when
+    none): the device-resident loop with the candidate pre-filter, one
+    decision record all-gathered per item.  Returns (final tray, per-item
+    (success, position, orientation, score)) in the items' original order;
+    identical on every rank and to BinPacker(...).pack_voxels(items)."""
+    import torch.distributed as dist
 
     rank, world = 0, 1
     if dist.is_available() and dist.is_initialized():
         rank, world = dist.get_rank(), dist.get_world_size()
-    maps = orientation_maps(num_orientations)
-    mine = orientation_shard(num_orientations, rank, world)
+    return pack_sharded_on_device(items, tray_size, num_orientations, interlocking_free, sort_by_volume, rank,
+                                  world, nccl_exchange if world > 1 else None, device)
+
+
+def pack_sharded_protocol(items, tray_size, num_orientations, interlocking_free, search, place, exchange,
+                          rank: int, world: int, sort_by_volume: bool = True):
+    """The sharded loop's host protocol with the search and the placement
+    supplied by the caller (the oracle in the CPU tests): per item in packing
+    order this rank searches its orientations, the ranks' records are
+    exchanged (exchange(local) -> merged record) and the winner is placed.
+    search(tray, item, orientations) -> (found, score, orientation, x, y, z)
+    with the global orientation index; place(tray, item, orientation, pos,
+    item_id) -> new tray.  Returns (tray, per-item records in search order)."""
+    import numpy as np
     arrs = [np.asarray(i, dtype=np.int32) for i in items]
     vols = [int(np.count_nonzero(a > 0)) for a in arrs]
     order = list(np.argsort(vols)[::-1]) if sort_by_volume else list(range(len(arrs)))
-    L = lib()
-    vp = ctypes.c_void_p
-    L.psb_tray_search.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
-    L.psb_tray_place.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                 ctypes.c_int, ctypes.c_int32]
-    L.psb_tray_set.argtypes = [vp, vp, vp]
-    L.psb_tray_get.argtypes = [vp, vp, vp]
-    t = ctypes.c_void_p()
-    check(L.psb_tray_create(*[int(d) for d in tray_size], ctypes.byref(t)))
+    mine = orientation_shard(num_orientations, rank, world)
     tray = np.zeros(tuple(int(d) for d in tray_size), np.int32)
-    mode = (1 if (interlocking_free or num_orientations > 1) else 0) | (0x10 if interlocking_free else 0)
-    out = [None] * len(arrs)
-    placed = 0
-    try:
-        check(L.psb_tray_set(t, tray.ctypes.data, None))
-        for k in order:
-            ors = [np.ascontiguousarray(apply_map(arrs[k], maps[o])) for o in mine]
-            local = (0, 0.0, -1, -1, -1, -1)
-            if ors:
-                ptrs = (ctypes.c_void_p * len(ors))(*[a.ctypes.data for a in ors])
-                dims = np.ascontiguousarray(np.array([a.shape for a in ors], np.int32).ravel())
-                r = PsbResult()
-                check(L.psb_tray_search(t, ptrs, dims.ctypes.data, len(ors), mode, ctypes.byref(r), None))
-                if r.found:
-                    local = (1, r.score, mine[r.orientation], r.x, r.y, r.z)
-            found, score, orient, x, y, z = exchange_decision(local, device=device)
-            if found:
-                it = np.ascontiguousarray(apply_map(arrs[k], maps[orient]))
-                placed += 1
-                check(L.psb_tray_place(t, it.ctypes.data, *it.shape, x, y, z, placed))
-                out[k] = (True, (x, y, z), orient, score)
-            else:
-                out[k] = (False, None, 0, None)
-        check(L.psb_tray_get(t, tray.ctypes.data, None))
-    finally:
-        L.psb_tray_destroy(t)
-    return tray, out
+    placed, recs = 0, []
+    for k in order:
+        local = search(tray, arrs[k], mine) if mine else (0, 0.0, -1, -1, -1, -1)
+        rec = exchange(local)
+        if rec[0]:
+            placed += 1
+            tray = place(tray, arrs[k], int(rec[2]), (int(rec[3]), int(rec[4]), int(rec[5])), placed)
+        recs.append(tuple(rec))
+    return tray, recs

@@ -115,3 +115,79 @@ def test_merge_decisions_rules():
     assert merge_decisions([(0, 0, -1, -1, -1, -1), (1, 3.0, 4, 1, 1, 1)]) == (1, 3.0, 4, 1, 1, 1)
     assert merge_decisions([(1, 3.0, 9, 0, 0, 0), (1, 3.0, 4, 1, 1, 1)])[2] == 4
     assert merge_decisions([(1, 2.0, 9, 0, 0, 0), (1, 3.0, 4, 1, 1, 1)])[2] == 9
+
+
+def _oracle_search(interlock, n_orient):
+    import numpy as np
+    from oracle import psb_oracle as O
+
+    def search(tray, item, mine):
+        phi = O.calculate_distance(tray)
+        ors = O.orientations(item, n_orient)
+        best = (0, 0.0, -1, -1, -1, -1)
+        for o in mine:
+            r = np.ascontiguousarray(ors[o])
+            if any(r.shape[a] > tray.shape[a] for a in range(3)):
+                continue
+            pos, found, sc = O.search_one(r, tray, phi, mode="block", interlock=interlock)
+            if found and (not best[0] or sc < best[1]):   # strict <: the first in index order wins
+                best = (1, sc, o, *pos)
+        return best
+
+    def place(tray, item, o, pos, item_id):
+        r = np.ascontiguousarray(O.orientations(item, n_orient)[o])
+        return O.place_in_tray(r, tray, pos, item_id)
+    return search, place
+
+
+def _loop_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        import importlib.util
+        from pathlib import Path
+        from psacking_b200.shard import exchange_decision, pack_sharded_protocol
+        spec = importlib.util.spec_from_file_location(
+            "wl", Path(__file__).resolve().parent.parent / "psacking_b200" / "workloads.py")
+        W = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(W)
+        items = W.config1_items(4)[:6]
+        search, place = _oracle_search(True, 6)
+        tray, recs = pack_sharded_protocol(items, (30, 30, 14), 6, True, search, place, exchange_decision, rank, world)
+        q.put((rank, tray, recs))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_sharded_packing_loop():
+    """The whole orientation-sharded packing loop at world size 2 (gloo):
+    each rank searches its own orientations with the oracle, the decision
+    records are all-gathered per item, and both ranks end with the same tray
+    and the same placements as the unsharded oracle run."""
+    import numpy as np
+    from oracle import psb_oracle as O
+    from oracle.trace_replay import load_workloads
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_loop_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=300) for _ in range(world)], key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, t0, r0), (_, t1, r1) = out
+    assert np.array_equal(t0, t1) and r0 == r1
+    items = load_workloads().config1_items(4)[:6]
+    want_tray, want = O.pack_voxels(items, (30, 30, 14), 6, True)
+    assert np.array_equal(t0, want_tray)
+    vols = [int((np.asarray(i) > 0).sum()) for i in items]
+    order = list(np.argsort(vols)[::-1])
+    for rec, k in zip(r0, order):
+        w = want[k]
+        assert bool(rec[0]) == w["success"]
+        if w["success"]:
+            assert (tuple(rec[3:6]), rec[2], rec[1]) == (w["position"], w["orientation_index"], w["score"])
