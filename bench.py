@@ -368,6 +368,9 @@ def run_ours(args, rank, world, local_rank):
                    "collision_work_per_step": {
                        "xpass_orientations": work[0] / args.steps, "xpass_planes_stored": work[2] / args.steps,
                        "plane_pass_planes": work[3] / args.steps, "plane_pass_row_pairs": work[4] / args.steps},
+                   "proximity_work_per_step": {
+                       "xpass_orientations": work[5] / args.steps, "planes": work[6] / args.steps,
+                       "plane_pass_row_pairs": work[7] / args.steps},
                    "l2": "256 MiB buffer written before every step", "parallelism": f"replicas x{world} (independent trays)",
                    "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag,
                    "parity_vs_oracle_trace": parity,

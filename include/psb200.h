@@ -308,7 +308,8 @@ int psb_set_filter_cut(int pct);
 /* Orientations left with at most n ok cells (free, or reachable in the
  * interlocking mode) after the collision pass skip the proximity transforms:
  * those cells are scored by exact integer proximity sums over the item's
- * z-runs instead (default 1024; 0 disables).  Same placements either way.
+ * z-runs instead (default 0: off, measured neutral on the benchmark).  Same
+ * placements either way.
  * No counterpart in the reference. */
 int psb_set_late_direct_max(int n);
 /* Bound on the flood fill's union-find work per run lookup or merge
@@ -357,10 +358,12 @@ int psb_profile_report(char* buf, size_t len);
 int psb_tray_fft_dims(const psb_tray* t, int* F);
 /* The CUDA stream (cudaStream_t) a tray's kernels run on. */
 int psb_tray_stream(psb_tray* t, void** stream);
-/* Work counters of a tray's collision kernels since the last reset (the
+/* Work counters of a tray's transform kernels since the last reset (the
  * measurement's algorithmic bytes): out[0] collision x-pass orientations,
  * out[1] the sum of their item x extents, out[2] their stored product planes,
- * out[3] collision plane-pass planes, out[4] their row pairs; out[5..7] 0.
+ * out[3] collision plane-pass planes, out[4] their row pairs, out[5]
+ * proximity x-pass orientations, out[6] their stored planes (also the
+ * proximity plane-pass planes), out[7] proximity plane-pass row pairs.
  * out may be NULL; reset != 0 zeroes them after the copy. */
 int psb_tray_work(psb_tray* t, unsigned long long* out, int reset);
 

@@ -282,8 +282,11 @@ int g_filter_cut = 50;
 // bound on the flood fill's union-find retries and path steps (psb_set_uf_limit)
 int g_uf_limit = PSB_UF_LIMIT;
 // orientations left with at most this many ok cells after the collision pass
-// skip the proximity transforms (psb_set_late_direct_max; 0 disables)
-int g_late_max = 1024;
+// skip the proximity transforms (psb_set_late_direct_max; 0 disables).  Off
+// by default: measured on the config-3 benchmark (items placed/s) 0: 1208.5,
+// 256: 1195.5, 1024: 1198.1, 4096: 1197.0 -- the orientations that reach the
+// proximity pass hold many ok cells.
+int g_late_max = 0;
 
 // the 6 axis permutations of an orientation map, as base indices
 int perm_index(const int* a) {

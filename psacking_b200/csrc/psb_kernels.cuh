@@ -316,9 +316,11 @@ struct SearchBufs {
     float2* Pc;          // per orientation stride sP
     float2* Pd;
     long long sB, sP;
-    // work counters of the collision kernels (algorithmic bytes of the
-    // measurement), or null: [0] x-pass orientations, [1] their item rows ex,
-    // [2] their stored product planes, [3] plane-pass planes, [4] their row pairs
+    // work counters of the transform kernels (algorithmic bytes of the
+    // measurement), or null: collision [0] x-pass orientations, [1] their item
+    // rows ex, [2] their stored product planes, [3] plane-pass planes, [4]
+    // their row pairs; proximity [5] x-pass orientations, [6] their stored
+    // planes (= plane-pass planes), [7] plane-pass row pairs
     unsigned long long* work;
 };
 

@@ -72,9 +72,10 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
             cnt += f;
         }
         if (!__syncthreads_or(cnt)) return;
-        if (MODE == 1 && sb.work && blockIdx.x == 0) {
+        if (MODE != 0 && sb.work && blockIdx.x == 0) {
             for (int d = 16; d > 0; d >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
-            if ((tid & 31) == 0 && cnt) atomicAdd(&sb.work[2], (unsigned long long)cnt);
+            if ((tid & 31) == 0 && cnt) atomicAdd(&sb.work[MODE == 1 ? 2 : 6], (unsigned long long)cnt);
+            if (MODE == 2 && tid == 0) atomicAdd(&sb.work[5], 1ull);
         }
     } else if (MODE == 1 && sb.work && blockIdx.x == 0 && tid == 0) {
         atomicAdd(&sb.work[2], (unsigned long long)Xv);

@@ -139,9 +139,13 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
         if (FIELD == 1 && tid == 0) pb.pmin[(size_t)o * pb.pstride + x] = 0xffffffffffffffffULL;
         return;
     }
-    if (FIELD == 0 && sb.work && tid == 0) {
-        atomicAdd(&sb.work[3], 1ull);
-        atomicAdd(&sb.work[4], (unsigned long long)nact);
+    if (sb.work && tid == 0) {
+        if (FIELD == 0) {
+            atomicAdd(&sb.work[3], 1ull);
+            atomicAdd(&sb.work[4], (unsigned long long)nact);
+        } else {
+            atomicAdd(&sb.work[7], (unsigned long long)nact);
+        }
     }
 
     // y pass: line (column) c = t*PER + lane / L, lane j = lane % L

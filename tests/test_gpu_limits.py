@@ -75,18 +75,23 @@ def test_flood_fill_limit_returns_error_then_recovers(gpu_core, uf_limit):
 
 
 def test_search_limit_returns_error_then_recovers(gpu_core, uf_limit):
+    """Every orientation's own result (per_orientation=True) runs the flood
+    fill for all of them; the drop-in batch search runs it only when its
+    winner has no straight free run to a seed face, which here it has."""
     tray = boxes_tray(2)
     phi = O.calculate_distance(tray)
     ors = [np.ones((2, 1, 1), np.int32), np.ones((1, 2, 2), np.int32)]
+    flags = 1 | 0x10   # PSB_MODE_BLOCK | PSB_FLAG_INTERLOCK
     want = O.fft_search_batch(ors, tray, phi, interlock=True)
+    gpu_core.gpu_tray_init(tray, phi)
     uf_limit(1)
     with pytest.raises(RuntimeError, match="iteration limit"):
-        gpu_core.gpu_tray_cleanup()
-        gpu_core.fft_search_batch_interlocking_free(ors, tray, phi, 1)
+        gpu_core.search_detail(ors, flags, per_orientation=True)
     uf_limit(0)
+    d = gpu_core.search_detail(ors, flags, per_orientation=True)
+    pos, found, score, bo = d["best"]
+    assert (tuple(pos), found, score, bo) == (tuple(want[0]), want[1], want[2], want[3])
     gpu_core.gpu_tray_cleanup()
-    got = gpu_core.fft_search_batch_interlocking_free(ors, tray, phi, 1)
-    assert (tuple(got[0]), got[1], got[2], got[3]) == (tuple(want[0]), want[1], want[2], want[3])
 
 
 def test_packing_loop_limit_returns_error_then_recovers(gpu_core, uf_limit):

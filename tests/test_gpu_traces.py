@@ -77,17 +77,17 @@ def test_native_loop_matches_trace_every_sample(gpu_core, name):
     _check(tr, res)
 
 
-@pytest.mark.parametrize("late", [0, 1 << 16])
+@pytest.mark.parametrize("late", [1024, 1 << 16])
 @pytest.mark.parametrize("name", ["config2_seed0", "config3_seed1"])
 def test_native_loop_matches_trace_late_direct(gpu_core, name, late):
     """Orientations left with few ok cells after the collision pass take
-    exact proximity sums instead of the proximity transforms: none of them
-    (0), or practically all (2^16 cells)."""
+    exact proximity sums instead of the proximity transforms (off by
+    default): up to 1024 ok cells, or practically all (2^16 cells)."""
     gpu_core.set_late_direct_max(late)
     try:
         tr, res = _run(name)
     finally:
-        gpu_core.set_late_direct_max(1024)
+        gpu_core.set_late_direct_max(0)
     _check(tr, res)
 
 
