@@ -762,6 +762,7 @@ struct psb_tray {
     float2* d_Sphi = nullptr;
     float2* d_w1 = nullptr;
     float2* d_w2 = nullptr;
+    float2* d_wocc = nullptr;   // z,y transforms of the occupancy's x slabs, kept between placements
     double* d_pen = nullptr;
     RzDesc* d_rz = nullptr;
     MidDesc* d_mid = nullptr;
@@ -805,6 +806,8 @@ struct psb_tray {
     bool cand_active = false;               // the current search's candidate words and planes are valid
     bool direct_active = false;             // ... and direct orientations may exist
     bool late_active = false;               // the current search may hold late-direct orientations
+    DecideArgs decide{nullptr, nullptr, nullptr, nullptr};   // the loop's decision, fused into the
+    bool fused = false;                                      // split flow's last selection step (done)
     int *d_ccount = nullptr, *d_vcount = nullptr, *d_ncol = nullptr;   // per orientation: candidates,
                                                                       // verified free cells, item columns
     int* d_okcount = nullptr;               // per orientation: ok cells after the collision pass
@@ -868,7 +871,7 @@ struct psb_tray {
     void release() {
         if (dev >= 0) cudaSetDevice(dev);
         release_slots();
-        dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_pen, st);
+        dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_wocc, st); dfree(d_pen, st);
         dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st); dfree(d_stage_vox, st);
         dfree(d_stage_runs, st); dfree(d_runs, st); dfree(d_pphi, st); dfree(d_pocc, st);
         dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_base_all, st); dfree(d_dec, st);
@@ -899,6 +902,7 @@ struct psb_tray {
         TRY(dalloc(&d_tray, V, st)); TRY(dalloc(&d_phi, V, st));
         TRY(dalloc(&d_Socc, S, st)); TRY(dalloc(&d_Sphi, S, st));
         TRY(dalloc(&d_w1, (size_t)nx * ny * g.H, st)); TRY(dalloc(&d_w2, (size_t)nx * g.F[1] * g.H, st));
+        TRY(dalloc(&d_wocc, (size_t)nx * g.F[1] * g.H, st));
         TRY(dalloc(&d_pen, 3 * (size_t)nz, st)); TRY(dalloc(&d_rz, 4, st)); TRY(dalloc(&d_mid, 4, st)); TRY(dalloc(&d_stats, 4, st));
         TRY(dalloc(&d_work, 8, st));
         CK(cudaMemsetAsync(d_work, 0, sizeof(unsigned long long) * 8, st));
@@ -1027,24 +1031,31 @@ struct psb_tray {
     // spectrum of the occupancy (phi = false) or of phi - mean (phi = true);
     // gated: only when *gate != 0 at run time.  Specialised kernels when the
     // FFT lengths have plans, the generic descriptor path otherwise.
-    int tray_forward(bool phi, const int* gate) {
+    //
+    // The occupancy's z,y slab transforms are kept (d_wocc): after a
+    // placement (slabs = the placed item's x extent at most, x0p = its x
+    // origin on the device) only the slabs under the item are transformed
+    // again, then the x pass runs over every column.
+    int tray_forward(bool phi, const int* gate, int slabs = 0, const int* x0p = nullptr) {
         FwdPlaneFn ff = g_fast_fft ? fwd_plane_for(g.F[1], g.F[2]) : nullptr;
         XfwdFn xf = g_fast_fft ? xfwd_for(g.F[0]) : nullptr;
         const size_t smf = fwd_plane_smem(g.F[1], g.F[2], ny) + 64;
         if (ff && xf && smf <= (size_t)g_smem_optin && xfwd_smem(g.F[0]) + 64 <= (size_t)g_smem_optin) {
             const int* mean_p = (const int*)((const char*)d_ps + offsetof(PhiStats, mean));
+            float2* w = phi ? d_w2 : d_wocc;
+            const bool part = !phi && x0p && slabs > 0 && slabs < nx;
             FwdSrc src{phi ? (int)SRC_GRID_SUB : (int)SRC_GRID_OCC, phi ? d_phi : d_tray, nx, ny, nz, mean_p, gate,
-                       d_w2, 0};
+                       w, 0, part ? x0p : nullptr};
             {
                 PROF("k_fwd_plane", st);
-                ff<<<dim3(nx, 1), 256, smf, st>>>(src, nullptr, g.p[1].tw, g.p[2].tw);
+                ff<<<dim3(part ? slabs : nx, 1), 256, smf, st>>>(src, nullptr, g.p[1].tw, g.p[2].tw);
             }
             CKL();
             {
                 PROF("k_xfwd", st);
                 const int ncols = g.F[1] * g.H;
                 xf<<<(ncols + PSB_XCOLS - 1) / PSB_XCOLS, 256, xfwd_smem(g.F[0]), st>>>(
-                    d_w2, phi ? d_Sphi : d_Socc, nx, ncols, gate, g.p[0].tw);
+                    w, phi ? d_Sphi : d_Socc, nx, ncols, gate, g.p[0].tw);
             }
             CKL();
             return PSB_OK;
@@ -1055,9 +1066,12 @@ struct psb_tray {
 
     // occupancy spectrum from the device tray
     int rebuild_occ() { return tray_forward(false, nullptr); }
-    // ... only when the current item of the asynchronous loop was placed
-    int rebuild_occ_gated() {
-        return tray_forward(false, (const int*)((const char*)d_ls + offsetof(LoopState, placed_now)));
+    // ... only when the current item of the asynchronous loop was placed,
+    // and then only the slabs under it (at most `slabs` of them from its x
+    // origin ls->px)
+    int rebuild_occ_gated(int slabs) {
+        return tray_forward(false, (const int*)((const char*)d_ls + offsetof(LoopState, placed_now)), slabs,
+                            (const int*)((const char*)d_ls + offsetof(LoopState, px)));
     }
 
     // mean, norm and max deviation of the distance field, on the device
@@ -1173,19 +1187,6 @@ struct psb_tray {
         {
             PROF("k_tray_bits", st);
             k_tray_bits<<<(unsigned)(((size_t)nx * ny + 7) / 8), 256, 0, st>>>(d_tray, nx, ny, nz, tq, d_tbits);
-        }
-        CKL();
-        return PSB_OK;
-    }
-
-    // ... after the loop placed the item described by d_odb: only the columns
-    // under its box (gated on the loop's "placed" flag).
-    int tray_bits_placed(const OrientDesc* d_odb, const std::vector<OrientDesc>& ods) {
-        size_t box = 1;
-        for (auto& o : ods) box = std::max(box, (size_t)o.e[0] * o.e[1]);
-        {
-            PROF("k_tray_bits", st);
-            k_tray_bits_box<<<(unsigned)((box + 7) / 8), 256, 0, st>>>(d_tray, nx, ny, nz, tq, d_tbits, d_ls, d_odb);
         }
         CKL();
         return PSB_OK;
@@ -1367,7 +1368,7 @@ struct psb_tray {
             p1<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
         }
         CKL();
-        return select_over(d_odb, n, sp, ok, nullptr, d_out, d_okplane);
+        return select_over(d_odb, n, sp, ok, nullptr, d_out, d_okplane, decide.ls != nullptr);
     }
 
     // Selection over the ok cells from the plane minima: candidates in the
@@ -1375,7 +1376,7 @@ struct psb_tray {
     // okplane (may be null): the planes that hold an ok cell (the split flow
     // keeps them for every orientation)
     int select_over(const OrientDesc* d_odb, int n, const ScoreParams& sp, const uint32_t* ok, const int* gate,
-                    ResultDev* d_out, const unsigned char* okplane = nullptr) {
+                    ResultDev* d_out, const unsigned char* okplane = nullptr, bool fuse = false) {
         SelectBufs sel{ok,        sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
                        d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate, okplane};
         {
@@ -1398,7 +1399,12 @@ struct psb_tray {
             k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp);
         }
         CKL();
-        {
+        if (fuse && !gate) {
+            // the packing loop's decision in the same launch
+            PROF("k_finalize", st);
+            k_finalize_decide<<<1, 128, 0, st>>>(d_odb, sel, sp, d_out, n, decide);
+            fused = true;
+        } else {
             PROF("k_finalize", st);
             k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_odb, sel, sp, d_out, n);
         }
@@ -2771,16 +2777,23 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         std::vector<OrientDesc> hb(allb.begin() + (size_t)it * 6, allb.begin() + (size_t)(it + 1) * 6);
         if (filt && occ_est * 4 >= t->V) TRY(t->cand_filter(d_odb, host_ods, interlock != 0));
         occ_est += t->staged[it].vox.size();
+        ShardRecord* rec = opt.world > 1 || opt.d_local ? (ShardRecord*)opt.d_local : nullptr;
+        // the decision below may be fused into the search's last launch
+        t->decide = DecideArgs{t->d_ls, t->d_dec + it, t->d_err, rec};
+        t->fused = false;
         const int sst = t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res, true,
                                         t->d_base_all + (size_t)it * 6, &hb);
         t->cand_active = t->direct_active = t->late_active = false;
+        t->decide = DecideArgs{nullptr, nullptr, nullptr, nullptr};
         TRY(sst);
         if (d_per)
             CK(cudaMemcpyAsync(d_per + (size_t)it * n_orient, t->d_res, sizeof(ResultDev) * n_orient,
                                cudaMemcpyDeviceToDevice, t->st));
-        ShardRecord* rec = opt.world > 1 || opt.d_local ? (ShardRecord*)opt.d_local : nullptr;
-        k_decide<<<1, 32, 0, t->st>>>(d_odb, t->d_res, n_orient, t->d_ls, t->d_dec + it, t->d_err, rec);
-        CKL();
+        if (!t->fused) {
+            k_decide<<<1, 32, 0, t->st>>>(d_odb, t->d_res, n_orient, t->d_ls, t->d_dec + it, t->d_err, rec);
+            CKL();
+        }
+        t->fused = false;
         if (rec) {
             // the exchange queues the gathering of every rank's record on the
             // tray's stream; the merge then decides for all ranks alike
@@ -2802,18 +2815,23 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             k_place_write_g<<<64, 256, 0, t->st>>>(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
         }
         CKL();
-        {
-            size_t box = 1;
-            for (auto& o : host_ods) box = std::max(box, (size_t)o.e[0] * o.e[1]);
-            PROF("k_occ_prefix", t->st);
-            k_occ_prefix_box<<<(unsigned)((box + 7) / 8), 256, 0, t->st>>>(t->d_tray, t->d_pocc, t->nx, t->ny, t->nz,
-                                                                            t->d_ls, d_odb);
-        }
-        CKL();
         k_place_done<<<1, 32, 0, t->st>>>(d_odb, t->d_ls, t->d_dec + it);
         CKL();
-        TRY(t->rebuild_occ_gated());
-        if (filt) TRY(t->tray_bits_placed(d_odb, host_ods));
+        {
+            // the placed item's columns: occupancy prefix sums and the
+            // filter's free bits (gated on the placement)
+            size_t box = 1;
+            for (auto& o : host_ods) box = std::max(box, (size_t)o.e[0] * o.e[1]);
+            PROF("k_box_refresh", t->st);
+            k_box_refresh<<<(unsigned)((box + 7) / 8), 256, 0, t->st>>>(t->d_tray, t->d_pocc, filt ? t->d_tbits : nullptr,
+                                                                         t->tq, t->nx, t->ny, t->nz, t->d_ls, d_odb);
+        }
+        CKL();
+        {
+            int slabs = 1;
+            for (auto& o : host_ods) slabs = std::max(slabs, o.e[0]);
+            TRY(t->rebuild_occ_gated(slabs));
+        }
         if (first_pending) {
             TRY(t->rebuild_phi_gated());
             LoopState h;

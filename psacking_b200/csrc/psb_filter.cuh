@@ -45,29 +45,6 @@ __global__ void k_tray_bits(const int32_t* __restrict__ tray, int nx, int ny, in
     }
 }
 
-// After a placement only the tray columns under the placed item's box
-// change: refresh those (gated on ls->placed_now; the chosen orientation and
-// position come from the loop state).  grid: ceil(max box columns / 8), block 256
-__global__ void k_tray_bits_box(const int32_t* __restrict__ tray, int nx, int ny, int nz, int nq,
-                                uint4* __restrict__ tbits, const LoopState* __restrict__ ls,
-                                const OrientDesc* __restrict__ od_item) {
-    if (!ls->placed_now) return;
-    const OrientDesc& od = od_item[ls->orient];
-    const int by = od.e[1];
-    const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (k >= od.e[0] * by) return;
-    const int i = ls->px + k / by, j = ls->py + k % by;
-    if (i < 0 || j < 0 || i >= nx || j >= ny) return;
-    const int32_t* t = tray + ((size_t)i * ny + j) * nz;
-    uint32_t* out = (uint32_t*)(tbits + ((size_t)i * ny + j) * nq);
-    for (int w = 0; w < 4 * nq; ++w) {
-        const int z = 32 * w + lane;
-        const unsigned int b = __ballot_sync(0xffffffffu, z < nz && t[z] == 0);
-        if (lane == 0) out[w] = b;
-    }
-}
-
 // The samples of each orientation, oriented and sorted by their word shift
 // s.z / 32 (bucket k holds fs[o][bound[o][k] .. bound[o][k+1])), once per
 // item, so the filter's CTAs only load them.  One warp per orientation.

@@ -338,11 +338,9 @@ struct ResultDev {
     int pad;
 };
 
-__global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, ResultDev* out,
-                           int n) {
-    if (sb.gate && !*sb.gate) return;
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n) return;
+// orientation o's result from the selection state
+__device__ __forceinline__ void finalize_one(const OrientDesc* __restrict__ orients, const SelectBufs& sb,
+                                             const ScoreParams& sp, ResultDev* out, int o) {
     ResultDev r;
     r.x = r.y = r.z = -1;
     r.found = 0;
@@ -368,6 +366,14 @@ __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb
         }
     }
     out[o] = r;
+}
+
+__global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, ResultDev* out,
+                           int n) {
+    if (sb.gate && !*sb.gate) return;
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    finalize_one(orients, sb, sp, out, o);
 }
 
 // Index of the best found result (smallest score; on equal scores the lowest

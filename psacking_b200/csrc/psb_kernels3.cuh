@@ -269,6 +269,7 @@ struct FwdSrc {
     const int* gate;     // when set, run only if *gate != 0
     float2* out;         // [n0][NY][HZ] per batch element
     long long out_stride;
+    const int* x0p;      // grid sources: when set, CTA i transforms slab *x0p + i (a placed item's planes)
 };
 
 // One x slab per CTA: each z line (real, zero-padded to NZ) is transformed as
@@ -284,7 +285,7 @@ k_fwd_plane(FwdSrc src, const OrientDesc* __restrict__ orients, const float2* __
     constexpr int RZ0 = Plan2<NZ>::R0, RZ1 = Plan2<NZ>::R1;
     extern __shared__ float2 sm[];
     if (src.gate && !*src.gate) return;
-    const int b = blockIdx.y, i = blockIdx.x;
+    const int b = blockIdx.y;
     int n0 = src.n0, n1 = src.n1, n2 = src.n2;
     OrientDesc od;
     if (src.kind == SRC_ITEM) {
@@ -292,7 +293,8 @@ k_fwd_plane(FwdSrc src, const OrientDesc* __restrict__ orients, const float2* __
         if (od.skip || od.direct) return;   // direct orientations need no transform
         n0 = od.e[0]; n1 = od.e[1]; n2 = od.e[2];
     }
-    if (i >= n0) return;
+    const int i = blockIdx.x + (src.x0p ? *src.x0p : 0);
+    if (i < 0 || i >= n0) return;
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int shift = (src.kind == SRC_GRID_SUB && src.subp) ? *src.subp : 0;
     float2* twy = sm;

@@ -68,9 +68,10 @@ struct ShardRecord {
 
 // best over orientations (strict <: the first minimum wins), one warp.
 // rec (may be null): the same decision as a ShardRecord for the exchange.
-__global__ void k_decide(const OrientDesc* __restrict__ od, const ResultDev* __restrict__ res, int n,
-                         LoopState* ls, DecisionDev* out, const unsigned int* uf_err, ShardRecord* rec) {
-    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+// (the body, run by one full warp)
+__device__ __forceinline__ void decide_warp(const OrientDesc* __restrict__ od, const ResultDev* __restrict__ res,
+                                            int n, LoopState* ls, DecisionDev* out, const unsigned int* uf_err,
+                                            ShardRecord* rec) {
     const int best = best_result(od, res, n);
     unsigned int diag = 0;
     int ncand = 0;
@@ -121,6 +122,29 @@ __global__ void k_decide(const OrientDesc* __restrict__ od, const ResultDev* __r
         r.pad = 0;
         *rec = r;
     }
+}
+
+__global__ void k_decide(const OrientDesc* __restrict__ od, const ResultDev* __restrict__ res, int n,
+                         LoopState* ls, DecisionDev* out, const unsigned int* uf_err, ShardRecord* rec) {
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    decide_warp(od, res, n, ls, out, uf_err, rec);
+}
+
+// The loop's decision fused into the selection's last step: every
+// orientation's result (k_finalize), then the best over them (k_decide), in
+// one block.  Arguments of the decision part:
+struct DecideArgs {
+    LoopState* ls;
+    DecisionDev* out;
+    const unsigned int* uf_err;
+    ShardRecord* rec;
+};
+// grid: 1, block 128
+__global__ void k_finalize_decide(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, ResultDev* res,
+                                  int n, DecideArgs da) {
+    for (int o = threadIdx.x; o < n; o += blockDim.x) finalize_one(orients, sb, sp, res, o);
+    __syncthreads();
+    if (threadIdx.x < 32) decide_warp(orients, res, n, da.ls, da.out, da.uf_err, da.rec);
 }
 
 // The winner over every rank's record (rank order): the smallest score, on
@@ -252,18 +276,30 @@ __global__ void k_stats_g(const int32_t* __restrict__ v, size_t n, const int* sh
 }
 
 // After a placement only the columns under the placed item's box change:
-// refresh their occupancy prefix sums (k_col_prefix, MODE 1), gated on
-// ls->placed_now.  grid: ceil(max box columns / 8), block 256
-__global__ void k_occ_prefix_box(const int32_t* __restrict__ tray, int32_t* __restrict__ P, int nx, int ny, int nz,
-                                 const LoopState* __restrict__ ls, const OrientDesc* __restrict__ od_item) {
+// refresh their occupancy prefix sums (k_col_prefix, MODE 1) and, when the
+// candidate filter keeps them (tbits != null, nq uint4 per column), their
+// free bits (k_tray_bits), gated on ls->placed_now.  One warp per column.
+// grid: ceil(max box columns / 8), block 256
+__global__ void k_box_refresh(const int32_t* __restrict__ tray, int32_t* __restrict__ P, uint4* __restrict__ tbits,
+                              int nq, int nx, int ny, int nz, const LoopState* __restrict__ ls,
+                              const OrientDesc* __restrict__ od_item) {
     if (!ls->placed_now) return;
     const OrientDesc& od = od_item[ls->orient];
     const int by = od.e[1];
     const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (k >= od.e[0] * by) return;
     const int i = ls->px + k / by, j = ls->py + k % by;
     if (i < 0 || j < 0 || i >= nx || j >= ny) return;
     const size_t col = (size_t)i * ny + j;
-    col_prefix<1>(tray + col * nz, P + col * (nz + 1), nz, threadIdx.x & 31);
+    const int32_t* t = tray + col * nz;
+    col_prefix<1>(t, P + col * (nz + 1), nz, lane);
+    if (tbits) {
+        uint32_t* out = (uint32_t*)(tbits + col * nq);
+        for (int w = 0; w < 4 * nq; ++w) {
+            const int z = 32 * w + lane;
+            const unsigned int b = __ballot_sync(0xffffffffu, z < nz && t[z] == 0);
+            if (lane == 0) out[w] = b;
+        }
+    }
 }
-

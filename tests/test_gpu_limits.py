@@ -95,9 +95,12 @@ def test_search_limit_returns_error_then_recovers(gpu_core, uf_limit):
 
 
 def test_packing_loop_limit_returns_error_then_recovers(gpu_core, uf_limit):
+    """A 64^3 tray (specialised FFT lengths): the loop's search runs the flood
+    fill for every item (other lengths take the lazy interlocking flow, which
+    skips it when the winner has a straight free run to a seed face)."""
     from psacking_b200 import BinPacker, workloads
     items = workloads.config1_items(2)[:5]
-    tray = boxes_tray(3)
+    tray = boxes_tray(3, shape=(64, 64, 64))
     packer = BinPacker(tray.shape, num_orientations=4, interlocking_free=True)
     uf_limit(1)
     with pytest.raises(RuntimeError, match="iteration limit"):

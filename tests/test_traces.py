@@ -94,3 +94,23 @@ def test_oracle_spectra_cache_gives_the_same_runs():
         a = O.pack_voxels(items, (60, 50, 40), 24, inter)
         b = O.pack_voxels(items, (60, 50, 40), 24, inter, fast=True)
         assert a[1] == b[1] and np.array_equal(a[0], b[0])
+
+
+def test_reference_gpu_divergences_are_fp32_rounding():
+    """The reference's own cuFFT search, run on a B200 on every item of the
+    benchmark stream from the oracle's tray states (the committed
+    tests/golden/ref_cuda_sample_config3.json), differs from the oracle only
+    where FP32 decides: 12 items get the same cell and orientation with a
+    score rounded to a neighbouring integer, and item 0 lands on another cell
+    whose exact score equals the oracle's (an exact tie on the empty tray,
+    broken by noise).  No choice of the reference is worse or invalid when
+    scored exactly."""
+    import json
+    from pathlib import Path
+    from oracle.classify_ref import classify
+    doc = json.loads((Path(__file__).resolve().parent / "golden" / "ref_cuda_sample_config3.json").read_text())
+    res = classify(doc)
+    assert res["items"] == 350
+    assert res["counts"] == {"same": 337, "same_cell": 12, "exact_tie": 1}
+    for r in res["rows"]:
+        assert abs(r["reference"][5] - r["oracle"][5]) <= 16.0
