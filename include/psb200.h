@@ -296,7 +296,7 @@ int psb_set_plane_variant(int v);
  * for comparisons.  No counterpart in the reference. */
 int psb_set_cand_filter(int on);
 /* Orientations the pre-filter leaves with at most n candidate translations
- * (default 1024; 0 disables) skip the transforms: each candidate is checked
+ * (default 4096; 0 disables) skip the transforms: each candidate is checked
  * exactly against the item's voxel columns and the free ones are scored by
  * exact integer proximity sums.  Same placements either way. */
 int psb_set_direct_max(int n);

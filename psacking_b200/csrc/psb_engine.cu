@@ -274,11 +274,18 @@ bool g_share_flips = false;
 bool g_cand_filter = true;
 // orientations left with at most this many candidates are decided directly
 // (exact checks against the item's columns, exact proximity sums) instead of
-// by transforms; 0 disables
-int g_direct_max = 1024;
+// by transforms; 0 disables.  Measured on the config-3 benchmark (items
+// placed/s): 1024: 1258.9, 2048: 1265.8, 4096: 1275.0 / 1277.2, 8192: 1268.1,
+// 16384: 1247.3.
+int g_direct_max = 4096;
 // filter cut-off (k_cand_filter): a warp stops sampling when more than this
 // percentage of its translations survive the first samples; 0 disables
 int g_filter_cut = 50;
+// k_cand_filter variant for trays of at most 128 cells per column (tuning:
+// 0 = 8-sample batches within 64 registers, 1 = 4-sample batches and 12
+// CTAs per SM, 2 = 8-sample batches without a register bound, 3 = 16-sample
+// batches); PSB_FILTER_VARIANT
+int g_filter_variant = 0;
 // bound on the flood fill's union-find retries and path steps (psb_set_uf_limit)
 int g_uf_limit = PSB_UF_LIMIT;
 // orientations left with at most this many ok cells after the collision pass
@@ -358,6 +365,7 @@ int set_smem_attrs() {
     if (const char* e = getenv("PSB_CAND_FILTER")) g_cand_filter = atoi(e) != 0;
     if (const char* e = getenv("PSB_DIRECT_MAX")) g_direct_max = std::max(0, atoi(e));
     if (const char* e = getenv("PSB_FILTER_CUT")) g_filter_cut = std::max(0, std::min(100, atoi(e)));
+    if (const char* e = getenv("PSB_FILTER_VARIANT")) g_filter_variant = std::max(0, std::min(3, atoi(e)));
     if (const char* e = getenv("PSB_LATE_MAX")) g_late_max = std::min(std::max(0, atoi(e)), kCandCap);
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
@@ -1229,10 +1237,13 @@ struct psb_tray {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
                     k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
-                    k_cand_filter<1><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
-                                                                        d_candplane, (long long)nx, d_ccount,
-                                                                        d_fsamp, d_fbound, g_filter_cut, d_clist,
-                                                                        ccap, nz);
+                    // the variant (sample batch, CTAs per SM bound) is a tuning switch
+                    auto kf = g_filter_variant == 1 ? k_cand_filter<1, 4, 12>
+                            : g_filter_variant == 2 ? k_cand_filter<1, 8, 1>
+                            : g_filter_variant == 3 ? k_cand_filter<1, 16, 1> : k_cand_filter<1>;
+                    kf<<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits, d_candplane,
+                                                          (long long)nx, d_ccount, d_fsamp, d_fbound, g_filter_cut,
+                                                          d_clist, ccap, nz);
                 } else {
                     k_cand_prep<2><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
                     k_cand_filter<2><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,

@@ -87,8 +87,8 @@ __device__ __forceinline__ uint32_t low_bits(int n) { return n >= 32 ? 0xfffffff
 // compile-time register index; lanes of a warp share the sample; loads go in
 // batches; a warp stops once none of its lanes holds a candidate.
 // grid: (max Xv, n_orient), block PSB_FILT_THREADS
-template <int NQ>
-__global__ void __launch_bounds__(PSB_FILT_THREADS)
+template <int NQ, int BATCH = PSB_FBATCH, int MINB = 8>
+__global__ void __launch_bounds__(PSB_FILT_THREADS, MINB)
 k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ tbits, int ny, int nzw,
               uint32_t* __restrict__ cand, long long sBits, unsigned char* __restrict__ candplane, long long pstride,
               int* __restrict__ ccount, const int4* __restrict__ fs, const int* __restrict__ fbound, int cut_pct,
@@ -131,7 +131,7 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
             // shift of k whole words: word w of the shifted column is
             // funnel(T[w + k], T[w + k + 1]) >> (s.z & 31)
             const int s1 = bound[k + 1];
-            for (int s0 = bound[k]; s0 < s1 && !stop; s0 += PSB_FBATCH) {
+            for (int s0 = bound[k]; s0 < s1 && !stop; s0 += BATCH) {
                 uint32_t a = 0u;
                 int nb = 0;
 #pragma unroll
@@ -156,11 +156,11 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
                         break;
                     }
                 }
-                done += PSB_FBATCH;
-                uint4 v[PSB_FBATCH][NQ];
-                int off[PSB_FBATCH];
+                done += BATCH;
+                uint4 v[BATCH][NQ];
+                int off[BATCH];
 #pragma unroll
-                for (int i = 0; i < PSB_FBATCH; ++i) {
+                for (int i = 0; i < BATCH; ++i) {
                     off[i] = 0;
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) v[i][q] = make_uint4(0u, 0u, 0u, 0u);
@@ -175,7 +175,7 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
                     }
                 }
 #pragma unroll
-                for (int i = 0; i < PSB_FBATCH; ++i) {
+                for (int i = 0; i < BATCH; ++i) {
                     if (s0 + i >= s1) break;
                     uint32_t T[NW];
 #pragma unroll

@@ -402,12 +402,12 @@ def test_cand_filter_same_results(gpu_core, case):
         gpu_core.set_direct_max(0)
         gpu_core.set_filter_cut(0)       # every sample tested
         mid = _detail_run(items, dims, il)
-        gpu_core.set_direct_max(1024)
+        gpu_core.set_direct_max(4096)
         gpu_core.set_filter_cut(50)      # the defaults
         got = _detail_run(items, dims, il)
     finally:
         gpu_core.set_cand_filter(True)
-        gpu_core.set_direct_max(1024)
+        gpu_core.set_direct_max(4096)
         gpu_core.set_filter_cut(50)
         gpu_core.set_fast_fft(True)
         gpu_core.set_plane_variant(3)

@@ -66,14 +66,15 @@ def test_native_loop_matches_trace_filter_off(gpu_core, name):
 @pytest.mark.parametrize("name", ["config3_seed1"])
 def test_native_loop_matches_trace_every_sample(gpu_core, name):
     """The pre-filter with every sample tested and direct decisions up to a
-    larger limit: more orientations decided without transforms."""
+    larger limit (16384 candidates): more orientations decided without
+    transforms."""
     gpu_core.set_filter_cut(0)
-    gpu_core.set_direct_max(4096)
+    gpu_core.set_direct_max(16384)
     try:
         tr, res = _run(name)
     finally:
         gpu_core.set_filter_cut(50)
-        gpu_core.set_direct_max(1024)
+        gpu_core.set_direct_max(4096)
     _check(tr, res)
 
 
