@@ -281,6 +281,9 @@ int g_direct_max = 4096;
 // filter cut-off (k_cand_filter): a warp stops sampling when more than this
 // percentage of its translations survive the first samples; 0 disables
 int g_filter_cut = 50;
+// CTA rows of the transform kernels when they take their orientations from
+// the active list (k_active_list); 0: one row per orientation (PSB_ACTIVE_GRID)
+int g_active_grid = 8;
 // k_cand_filter variant for trays of at most 128 cells per column (tuning:
 // 0 = 8-sample batches within 64 registers, 1 = 4-sample batches and 12
 // CTAs per SM, 2 = 8-sample batches without a register bound, 3 = 16-sample
@@ -365,6 +368,7 @@ int set_smem_attrs() {
     if (const char* e = getenv("PSB_CAND_FILTER")) g_cand_filter = atoi(e) != 0;
     if (const char* e = getenv("PSB_DIRECT_MAX")) g_direct_max = std::max(0, atoi(e));
     if (const char* e = getenv("PSB_FILTER_CUT")) g_filter_cut = std::max(0, std::min(100, atoi(e)));
+    if (const char* e = getenv("PSB_ACTIVE_GRID")) g_active_grid = std::max(0, atoi(e));
     if (const char* e = getenv("PSB_FILTER_VARIANT")) g_filter_variant = std::max(0, std::min(3, atoi(e)));
     if (const char* e = getenv("PSB_LATE_MAX")) g_late_max = std::min(std::max(0, atoi(e)), kCandCap);
     TRY(set_max_dyn_smem(k_rfft_z));
@@ -819,6 +823,9 @@ struct psb_tray {
     int *d_ccount = nullptr, *d_vcount = nullptr, *d_ncol = nullptr;   // per orientation: candidates,
                                                                       // verified free cells, item columns
     int* d_okcount = nullptr;               // per orientation: ok cells after the collision pass
+    int* d_act = nullptr;                   // the search's active orientations (k_active_list), and
+    int* d_nact = nullptr;                  // their count
+    bool act_ready = false;                 // the current search's active list is queued
     int* d_clist = nullptr;                 // per orientation: its filter candidates while few (k_cand_filter)
     size_t clist_cap = 0;
     uint4* d_icols = nullptr;               // item column masks of direct orientations, stride nx*ny
@@ -872,7 +879,8 @@ struct psb_tray {
         dfree(d_Ai, st); dfree(d_Bi, st); dfree(d_Pc, st); dfree(d_Pd, st); dfree(d_Dq, st); dfree(d_free, st); dfree(d_reach, st);
         dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
         dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_candplane, st); dfree(d_bases, st); dfree(d_best, st);
-        dfree(d_ccount, st); d_vcount = d_ncol = d_okcount = nullptr; dfree(d_icols, st); dfree(d_fsamp, st); dfree(d_fbound, st);
+        dfree(d_ccount, st); d_vcount = d_ncol = d_okcount = nullptr;
+        dfree(d_act, st); d_nact = nullptr; dfree(d_icols, st); dfree(d_fsamp, st); dfree(d_fbound, st);
         dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
@@ -973,6 +981,8 @@ struct psb_tray {
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c, st));
         TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_okplane, (size_t)nx * c, st));
         TRY(dalloc(&d_candplane, (size_t)nx * c, st));
+        TRY(dalloc(&d_act, (size_t)c + 1, st));
+        d_nact = d_act + c;
         TRY(dalloc(&d_ccount, 4 * (size_t)c, st));
         d_vcount = d_ccount + c;
         d_ncol = d_ccount + 2 * c;
@@ -1330,7 +1340,8 @@ struct psb_tray {
     // proximity transform, and every orientation's own result is exact.
     int search_split(const OrientDesc* d_odb, int n, const ScoreParams& sp, bool interlock, XpassFn xf, PlaneFn p0,
                      PlaneFn p1, size_t smem, ResultDev* d_out, bool spec) {
-        SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP, d_work};
+        SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP, d_work, act_ready ? d_act : nullptr, act_ready ? d_nact : nullptr};
+        const int rows = act_ready ? std::min(n, g_active_grid) : n;
         // (with direct orientations the candidate filter cleared the flags and
         // set those of its verified planes already)
         if (!direct_active) CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
@@ -1341,7 +1352,7 @@ struct psb_tray {
             PROF("k_xpass_coll", st);
             // with the filter's plane flags, only rows of planes holding a
             // candidate are stored (the plane pass skips the others)
-            xf1<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
+            xf1<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, rows), 256, xpass2_smem(g.F[0]), st>>>(
                 d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, cand_active ? d_candplane : nullptr, (long long)nx, bm);
         } else {
             PROF("k_xpass_coll", st);
@@ -1359,7 +1370,7 @@ struct psb_tray {
                      interlock ? 0 : 1, cand_active ? d_candplane : nullptr, late ? d_okcount : nullptr};
         {
             PROF("k_plane_coll", st);
-            p0<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
+            p0<<<dim3(nx, rows), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
         }
         CKL();
         if (interlock) TRY(flood_fill(d_odb, n, sp, nullptr, d_okplane, late ? d_okcount : nullptr));
@@ -1370,13 +1381,13 @@ struct psb_tray {
         }
         if (xf) {
             PROF("k_xpass_prox", st);
-            xf2<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, n), 256, xpass2_smem(g.F[0]), st>>>(
+            xf2<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, rows), 256, xpass2_smem(g.F[0]), st>>>(
                 d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, d_okplane, (long long)nx, bm);
         }
         CKL();
         {
             PROF("k_plane_prox", st);
-            p1<<<dim3(nx, n), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
+            p1<<<dim3(nx, rows), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
         }
         CKL();
         return select_over(d_odb, n, sp, ok, nullptr, d_out, d_okplane, decide.ls != nullptr);
@@ -1443,6 +1454,7 @@ struct psb_tray {
                      ResultDev* d_out, bool lazy = true, const OrientDesc* d_bases_in = nullptr,
                      const std::vector<OrientDesc>* hbases = nullptr) {
         const int n = (int)ods.size();
+        act_ready = false;
         // the caller reserves the slots (ensure_slots) before taking slot
         // pointers such as d_out: growing them here would free those
         if (cap < std::max(n, 6)) return fail(PSB_ERR_STATE, "search slots not reserved (%d < %d)", cap, std::max(n, 6));
@@ -1492,10 +1504,20 @@ struct psb_tray {
             if (!o.skip) eymax = std::max(eymax, o.e[1]);
         FwdPlaneFn ff = g_fast_fft ? fwd_plane_for(g.F[1], g.F[2]) : nullptr;
         const size_t smf = fwd_plane_smem(g.F[1], g.F[2], eymax) + 64;
+        act_ready = false;
         if (ff && smf <= (size_t)g_smem_optin) {
-            FwdSrc src{SRC_ITEM, nullptr, 0, 0, 0, nullptr, nullptr, d_Bi, sBi};
+            // the transforms take the active orientations from a list: a few
+            // CTA rows loop over them instead of a row per orientation
+            const int rows = g_active_grid > 0 ? std::min(n, g_active_grid) : n;
+            if (g_active_grid > 0) {
+                k_active_list<<<1, 32, 0, st>>>(d_odb, n, d_act, d_nact);
+                CKL();
+                act_ready = true;
+            }
+            FwdSrc src{SRC_ITEM, nullptr, 0, 0, 0, nullptr, nullptr, d_Bi, sBi, nullptr,
+                       act_ready ? d_act : nullptr, act_ready ? d_nact : nullptr};
             PROF("k_fwd_plane", st);
-            ff<<<dim3(exmax, n), 256, smf, st>>>(src, d_odb, g.p[1].tw, g.p[2].tw);
+            ff<<<dim3(exmax, rows), 256, smf, st>>>(src, d_odb, g.p[1].tw, g.p[2].tw);
         } else {
             {
                 PROF("k_rfft_z", st);

@@ -322,7 +322,27 @@ struct SearchBufs {
     // their row pairs; proximity [5] x-pass orientations, [6] their stored
     // planes (= plane-pass planes), [7] plane-pass row pairs
     unsigned long long* work;
+    // when set: the orientations to work on (k_active_list), *nact of them;
+    // CTA row y takes act[y], act[y + gridDim.y], ... instead of orientation y
+    const int* act;
+    const int* nact;
 };
+
+// The orientations a search's transforms work on (neither skipped nor
+// decided directly), compacted, so the transform kernels launch a few CTA
+// rows that loop over them instead of one row per orientation, most of which
+// would only read their descriptor and exit.  grid 1, block 32
+__global__ void k_active_list(const OrientDesc* __restrict__ od, int n, int* __restrict__ act, int* __restrict__ nact) {
+    int base = 0;
+    for (int o0 = 0; o0 < n; o0 += 32) {
+        const int o = o0 + threadIdx.x;
+        const bool on = o < n && !od[o].skip && !od[o].direct;
+        const unsigned int b = __ballot_sync(0xffffffffu, on);
+        if (on) act[base + __popc(b & ((1u << threadIdx.x) - 1u))] = o;
+        base += __popc(b);
+    }
+    if (threadIdx.x == 0) *nact = base;
+}
 
 __global__ void __launch_bounds__(PSB_THREADS)
 k_xpass(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __restrict__ Socc,

@@ -43,14 +43,13 @@ struct BaseMap {
 // those planes' rows are stored.
 // grid: (ceil(Fy*Hz / PSB_XCOLS), n_orient), block 256
 template <int N, int MODE, bool SHARED>
-__global__ void __launch_bounds__(256)
-k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __restrict__ Socc,
-         const float2* __restrict__ Sphi, int ncols, const float2* __restrict__ g_tw,
-         const unsigned char* __restrict__ okplane, long long okstride, BaseMap bm) {
+__device__ __forceinline__ void
+xpass2_body(const int o, const OrientDesc* __restrict__ orients, const SearchBufs& sb, const float2* __restrict__ Socc,
+            const float2* __restrict__ Sphi, int ncols, const float2* __restrict__ g_tw,
+            const unsigned char* __restrict__ okplane, long long okstride, const BaseMap& bm) {
     constexpr int C = PSB_XCOLS;
     constexpr int R0 = Plan2<N>::R0, R1 = Plan2<N>::R1;
     extern __shared__ float2 sm[];
-    const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip || od.direct || od.valid[0] <= 0) return;
     const int c0 = blockIdx.x * C;
@@ -143,6 +142,22 @@ k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __
                                       if (x < Xv && (!flags || okp[x])) Pd[(size_t)x * ncols + c] = v;
                                   },
                                   nl, tw, tid, nthr);
+}
+
+template <int N, int MODE, bool SHARED>
+__global__ void __launch_bounds__(256)
+k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __restrict__ Socc,
+         const float2* __restrict__ Sphi, int ncols, const float2* __restrict__ g_tw,
+         const unsigned char* __restrict__ okplane, long long okstride, BaseMap bm) {
+    if (!sb.act) {
+        xpass2_body<N, MODE, SHARED>(blockIdx.y, orients, sb, Socc, Sphi, ncols, g_tw, okplane, okstride, bm);
+        return;
+    }
+    const int na = *sb.nact;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        xpass2_body<N, MODE, SHARED>(sb.act[j], orients, sb, Socc, Sphi, ncols, g_tw, okplane, okstride, bm);
+        __syncthreads();   // shared memory is reused by the next orientation
+    }
 }
 
 constexpr size_t xpass2_smem(int N) {
@@ -270,6 +285,8 @@ struct FwdSrc {
     float2* out;         // [n0][NY][HZ] per batch element
     long long out_stride;
     const int* x0p;      // grid sources: when set, CTA i transforms slab *x0p + i (a placed item's planes)
+    const int* act;      // SRC_ITEM: when set, CTA row y takes orientations act[y], act[y + gridDim.y], ...
+    const int* nact;     //   (*nact of them, k_active_list)
 };
 
 // One x slab per CTA: each z line (real, zero-padded to NZ) is transformed as
@@ -277,15 +294,12 @@ struct FwdSrc {
 // along y.  Writes out[i][ky][kz] for all ky < NY.  Replaces k_rfft_z + the y
 // k_fft_mid of the generic path.  grid: (max slabs, batch), block 256
 template <int NY, int NZ>
-__global__ void __launch_bounds__(256)
-k_fwd_plane(FwdSrc src, const OrientDesc* __restrict__ orients, const float2* __restrict__ g_twy,
-            const float2* __restrict__ g_twz) {
+__device__ __forceinline__ void fwd_plane_body(const int b, const FwdSrc& src, const OrientDesc* __restrict__ orients,
+                                               const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
     constexpr int HZ = NZ / 2 + 1;
     constexpr int RY0 = Plan2<NY>::R0, RY1 = Plan2<NY>::R1;
     constexpr int RZ0 = Plan2<NZ>::R0, RZ1 = Plan2<NZ>::R1;
     extern __shared__ float2 sm[];
-    if (src.gate && !*src.gate) return;
-    const int b = blockIdx.y;
     int n0 = src.n0, n1 = src.n1, n2 = src.n2;
     OrientDesc od;
     if (src.kind == SRC_ITEM) {
@@ -335,6 +349,22 @@ k_fwd_plane(FwdSrc src, const OrientDesc* __restrict__ orients, const float2* __
     tpass<NY, RY1, RY0, -1, HZ, false>([&](int c, int n) { return A[n * HZ + c]; },
                                        [&](int c, int ky, float2 v) { out[(size_t)ky * HZ + c] = v; }, HZ, twy, tid,
                                        nthr);
+}
+
+template <int NY, int NZ>
+__global__ void __launch_bounds__(256)
+k_fwd_plane(FwdSrc src, const OrientDesc* __restrict__ orients, const float2* __restrict__ g_twy,
+            const float2* __restrict__ g_twz) {
+    if (src.gate && !*src.gate) return;
+    if (!src.act) {
+        fwd_plane_body<NY, NZ>(blockIdx.y, src, orients, g_twy, g_twz);
+        return;
+    }
+    const int na = *src.nact;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        fwd_plane_body<NY, NZ>(src.act[j], src, orients, g_twy, g_twz);
+        __syncthreads();   // shared memory is reused by the next orientation
+    }
 }
 
 inline size_t fwd_plane_smem(int NY, int NZ, int n1) {

@@ -68,9 +68,9 @@ inline size_t plane3_smem(int NY, int NZ, int ny) {
 // plane's minimum approximate score over its ok cells (pmin, smin).
 // grid: (nx, n_orient), block PSB_PLANE3_THREADS
 template <int NY, int NZ, int FIELD>
-__global__ void __launch_bounds__(PSB_PLANE3_THREADS, 2)
-k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, ScoreParams sp,
-         const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
+__device__ __forceinline__ void plane3_body(const int o, const OrientDesc* __restrict__ orients, const SearchBufs& sb,
+                                            const PlaneBufs& pb, const ScoreParams& sp,
+                                            const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
     using LY = WarpLine<NY>;
     using LZ = WarpLine<NZ>;
     constexpr int HZ = NZ / 2 + 1;
@@ -80,7 +80,6 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
     constexpr int WY = ((HZ + LY::PER - 1) / LY::PER) * LY::PER * LY::SLAB;
     constexpr int WZ = NWARP * LZ::PER * LZ::SLAB;
     extern __shared__ float2 sm[];
-    const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip || od.direct) return;   // direct orientations: psb_filter.cuh
     const int x = blockIdx.x;
@@ -359,5 +358,20 @@ k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, Sc
         for (int w = 0; w < NWARP; ++w) pm = fmin(pm, red[w]);
         pb.pmin[(size_t)o * pb.pstride + x] = pm < 1e299 ? ord_key(pm) : 0xffffffffffffffffULL;
         if (pm < 1e299) atomicMin(&pb.smin[o], ord_key(pm));
+    }
+}
+
+template <int NY, int NZ, int FIELD>
+__global__ void __launch_bounds__(PSB_PLANE3_THREADS, 2)
+k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, ScoreParams sp,
+         const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
+    if (!sb.act) {
+        plane3_body<NY, NZ, FIELD>(blockIdx.y, orients, sb, pb, sp, g_twy, g_twz);
+        return;
+    }
+    const int na = *sb.nact;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        plane3_body<NY, NZ, FIELD>(sb.act[j], orients, sb, pb, sp, g_twy, g_twz);
+        __syncthreads();   // shared memory is reused by the next orientation
     }
 }
