@@ -825,6 +825,8 @@ struct psb_tray {
     int* d_okcount = nullptr;               // per orientation: ok cells after the collision pass
     int* d_act = nullptr;                   // the search's active orientations (k_active_list), and
     int* d_nact = nullptr;                  // their count
+    int* d_srch = nullptr;                  // the searched orientations (not skipped), and
+    int* d_nsrch = nullptr;                 // their count
     bool act_ready = false;                 // the current search's active list is queued
     int* d_clist = nullptr;                 // per orientation: its filter candidates while few (k_cand_filter)
     size_t clist_cap = 0;
@@ -880,7 +882,7 @@ struct psb_tray {
         dfree(d_cnt, st); dfree(d_off, st); dfree(d_rz2, st); dfree(d_rline, st); dfree(d_par, st); dfree(d_rflag, st); dfree(d_total, st); dfree(d_blk, st);
         dfree(d_cand, st); dfree(d_ncand, st); dfree(d_cscore, st); dfree(d_smin, st); dfree(d_pmin, st); dfree(d_okplane, st); dfree(d_candplane, st); dfree(d_bases, st); dfree(d_best, st);
         dfree(d_ccount, st); d_vcount = d_ncol = d_okcount = nullptr;
-        dfree(d_act, st); d_nact = nullptr; dfree(d_icols, st); dfree(d_fsamp, st); dfree(d_fbound, st);
+        dfree(d_act, st); d_nact = d_srch = d_nsrch = nullptr; dfree(d_icols, st); dfree(d_fsamp, st); dfree(d_fbound, st);
         dfree(d_bestkey, st); dfree(d_diag, st); dfree(d_errmax, st); dfree(d_od, st); dfree(d_rzs, st); dfree(d_mids, st); dfree(d_res, st);
         cap = 0;
     }
@@ -981,8 +983,10 @@ struct psb_tray {
         TRY(dalloc(&d_cscore, (size_t)kCandCap * c, st));
         TRY(dalloc(&d_smin, c, st)); TRY(dalloc(&d_pmin, (size_t)nx * c, st)); TRY(dalloc(&d_okplane, (size_t)nx * c, st));
         TRY(dalloc(&d_candplane, (size_t)nx * c, st));
-        TRY(dalloc(&d_act, (size_t)c + 1, st));
+        TRY(dalloc(&d_act, 2 * (size_t)c + 2, st));
         d_nact = d_act + c;
+        d_srch = d_act + c + 1;
+        d_nsrch = d_srch + c;
         TRY(dalloc(&d_ccount, 4 * (size_t)c, st));
         d_vcount = d_ccount + c;
         d_ncol = d_ccount + 2 * c;
@@ -1305,10 +1309,12 @@ struct psb_tray {
     int flood_fill(const OrientDesc* d_odb, int n, const ScoreParams& sp, const int* gate, unsigned char* okplane,
                    int* okcount = nullptr) {
         FloodBufs fb{d_free, d_reach, sBits, d_cnt, d_off,   sLine, d_rz2,    d_rline,
-                     d_par,  d_rflag, sRun,  d_total, d_err, gate,  okplane, (long long)nx, g_uf_limit, okcount};
+                     d_par,  d_rflag, sRun,  d_total, d_err, gate,  okplane, (long long)nx, g_uf_limit, okcount,
+                     act_ready ? d_srch : nullptr, act_ready ? d_nsrch : nullptr};
+        const int rows = act_ready ? std::min(n, g_active_grid) : n;
         const int lines = nx * ny;
         const int nblk = (lines + 255) / 256;
-        const dim3 gl(nblk, n);
+        const dim3 gl(nblk, rows);
         CK(cudaMemsetAsync(d_total, 0, sizeof(int) * n, st));
         {
             PROF("k_ff_runs", st);
@@ -1322,7 +1328,7 @@ struct psb_tray {
         CKL();
         {
             PROF("k_ff_seed", st);
-            k_ff_seed<<<dim3(296, n), 256, 0, st>>>(d_odb, fb);
+            k_ff_seed<<<dim3(296, rows), 256, 0, st>>>(d_odb, fb);
         }
         CKL();
         {
@@ -1400,25 +1406,27 @@ struct psb_tray {
     int select_over(const OrientDesc* d_odb, int n, const ScoreParams& sp, const uint32_t* ok, const int* gate,
                     ResultDev* d_out, const unsigned char* okplane = nullptr, bool fuse = false) {
         SelectBufs sel{ok,        sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
-                       d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate, okplane};
+                       d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate, okplane,
+                       act_ready ? d_srch : nullptr, act_ready ? d_nsrch : nullptr};
+        const int rows = act_ready ? std::min(n, g_active_grid) : n;
         {
             PROF("k_collect", st);
-            k_collect_plane<<<dim3(nx, n), 256, 0, st>>>(d_odb, sel, sp);
+            k_collect_plane<<<dim3(nx, rows), 256, 0, st>>>(d_odb, sel, sp);
         }
         CKL();
         {
             PROF("k_rescore", st);
-            k_rescore<<<dim3(148, n), 256, 0, st>>>(d_odb, sel, sp, d_pocc, d_pphi);
+            k_rescore<<<dim3(148, rows), 256, 0, st>>>(d_odb, sel, sp, d_pocc, d_pphi);
         }
         CKL();
         if (direct_active || late_active) {
             PROF("k_direct_score", st);
-            k_direct_score<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp, d_pphi);
+            k_direct_score<<<dim3(64, rows), 256, 0, st>>>(d_odb, sel, sp, d_pphi);
             CKL();
         }
         {
             PROF("k_tiebreak", st);
-            k_tiebreak<<<dim3(64, n), 256, 0, st>>>(d_odb, sel, sp);
+            k_tiebreak<<<dim3(64, rows), 256, 0, st>>>(d_odb, sel, sp);
         }
         CKL();
         if (fuse && !gate) {
@@ -1510,7 +1518,7 @@ struct psb_tray {
             // CTA rows loop over them instead of a row per orientation
             const int rows = g_active_grid > 0 ? std::min(n, g_active_grid) : n;
             if (g_active_grid > 0) {
-                k_active_list<<<1, 32, 0, st>>>(d_odb, n, d_act, d_nact);
+                k_active_list<<<1, 32, 0, st>>>(d_odb, n, d_act, d_nact, d_srch, d_nsrch);
                 CKL();
                 act_ready = true;
             }

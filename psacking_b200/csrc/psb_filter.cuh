@@ -357,10 +357,8 @@ k_cand_verify_list(const OrientDesc* __restrict__ orients, int n, const uint4* _
 // integers (the exact value the reference's FFT rounds to; pphi holds the
 // distance field's prefix sums along z, psb_kernels.cuh), then the
 // reference's score.  One warp per cell.  grid: (blocks, n_orient), block 256
-__global__ void __launch_bounds__(256)
-k_direct_score(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pphi) {
+__device__ __forceinline__ void k_direct_score_body(const int o, const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pphi) {
     if (sb.gate && !*sb.gate) return;
-    const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip || !od.direct) return;
     const int n = min(sb.ncand[o], sb.cap);
@@ -388,5 +386,20 @@ k_direct_score(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParam
             cs[c] = s;
             atomicMin(&sb.best[o], ord_key(s));
         }
+    }
+}
+
+__global__ void __launch_bounds__(256)
+
+k_direct_score(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pphi) {
+    if (!sb.srch) {
+        const int o = blockIdx.y;
+        k_direct_score_body(o, orients, sb, sp, pphi);
+        return;
+    }
+    const int na = *sb.nsrch;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        const int o = sb.srch[j];
+        k_direct_score_body(o, orients, sb, sp, pphi);
     }
 }

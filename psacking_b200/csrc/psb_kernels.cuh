@@ -328,20 +328,30 @@ struct SearchBufs {
     const int* nact;
 };
 
-// The orientations a search's transforms work on (neither skipped nor
-// decided directly), compacted, so the transform kernels launch a few CTA
-// rows that loop over them instead of one row per orientation, most of which
-// would only read their descriptor and exit.  grid 1, block 32
-__global__ void k_active_list(const OrientDesc* __restrict__ od, int n, int* __restrict__ act, int* __restrict__ nact) {
-    int base = 0;
+// The orientations a search's transforms work on (act: neither skipped nor
+// decided directly) and the ones it searches at all (srch: not skipped; the
+// flood fill and the selection), compacted, so those kernels launch a few
+// CTA rows that loop over them instead of one row per orientation, most of
+// which would only read their descriptor and exit.  grid 1, block 32
+__global__ void k_active_list(const OrientDesc* __restrict__ od, int n, int* __restrict__ act, int* __restrict__ nact,
+                              int* __restrict__ srch, int* __restrict__ nsrch) {
+    int base = 0, sbase = 0;
+    const unsigned int below = (1u << threadIdx.x) - 1u;
     for (int o0 = 0; o0 < n; o0 += 32) {
         const int o = o0 + threadIdx.x;
-        const bool on = o < n && !od[o].skip && !od[o].direct;
+        const bool s = o < n && !od[o].skip;
+        const bool on = s && !od[o].direct;
         const unsigned int b = __ballot_sync(0xffffffffu, on);
-        if (on) act[base + __popc(b & ((1u << threadIdx.x) - 1u))] = o;
+        const unsigned int bs = __ballot_sync(0xffffffffu, s);
+        if (on) act[base + __popc(b & below)] = o;
+        if (s) srch[sbase + __popc(bs & below)] = o;
         base += __popc(b);
+        sbase += __popc(bs);
     }
-    if (threadIdx.x == 0) *nact = base;
+    if (threadIdx.x == 0) {
+        *nact = base;
+        *nsrch = sbase;
+    }
 }
 
 __global__ void __launch_bounds__(PSB_THREADS)

@@ -26,6 +26,8 @@ struct SelectBufs {
     long long pstride;
     const int* gate;               // when set, the kernels run only if *gate != 0
     const unsigned char* okplane;  // when set, per (orientation, x plane): holds an ok cell (stride pstride)
+    const int* srch;               // when set: the searched orientations (k_active_list), *nsrch of them;
+    const int* nsrch;              // CTA row y takes srch[y], srch[y + gridDim.y], ...
 };
 
 __device__ __forceinline__ bool okbit(const uint32_t* bits, const ScoreParams& sp, int x, int y, int z) {
@@ -124,10 +126,9 @@ k_plane_min(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams s
 // (2) candidate collection, one CTA per (x plane, orientation), one warp per
 // row y.  An FP32 per-z proximity threshold (rounded up, with slack) screens
 // the cells before the double-precision score.  grid: (nx, n_orient)
-__global__ void __launch_bounds__(256)
-k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+__device__ __forceinline__ void k_collect_plane_body(const int o, const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
     if (sb.gate && !*sb.gate) return;
-    const int o = blockIdx.y, x = blockIdx.x;
+    const int x = blockIdx.x;
     const OrientDesc& od = orients[o];
     if (od.skip || x >= od.valid[0]) return;
     const int Yv = od.valid[1], Zv = od.valid[2];
@@ -206,6 +207,21 @@ k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScorePara
     }
 }
 
+__global__ void __launch_bounds__(256)
+
+k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    if (!sb.srch) {
+        const int o = blockIdx.y;
+        k_collect_plane_body(o, orients, sb, sp);
+        return;
+    }
+    const int na = *sb.nsrch;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        const int o = sb.srch[j];
+        k_collect_plane_body(o, orients, sb, sp);
+    }
+}
+
 // per-orientation selection state back to "nothing seen" (the gated second
 // round of the lazy interlocking search)
 __global__ void k_sel_reset(SelectBufs sb, int n) {
@@ -223,11 +239,9 @@ __global__ void k_sel_reset(SelectBufs sb, int n) {
 // (proximity and collision, from the per-column prefix sums pphi / pocc of
 // the distance field and the occupancy), the FP64 guard.
 // grid: (blocks, n_orient)
-__global__ void __launch_bounds__(256)
-k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pocc,
+__device__ __forceinline__ void k_rescore_body(const int o, const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pocc,
           const int32_t* __restrict__ pphi) {
     if (sb.gate && !*sb.gate) return;
-    const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip || od.direct) return;   // direct orientations: k_direct_score
     const int n = min(sb.ncand[o], sb.cap);
@@ -294,6 +308,23 @@ k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp,
     }
 }
 
+__global__ void __launch_bounds__(256)
+
+k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pocc,
+          const int32_t* __restrict__ pphi) {
+    if (!sb.srch) {
+        const int o = blockIdx.y;
+        k_rescore_body(o, orients, sb, sp, pocc, pphi);
+        return;
+    }
+    const int na = *sb.nsrch;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        const int o = sb.srch[j];
+        k_rescore_body(o, orients, sb, sp, pocc, pphi);
+        __syncthreads();   // shared memory is reused by the next orientation
+    }
+}
+
 __device__ __forceinline__ unsigned int tie_key(int mode, int idx) {
     if (mode == 0) return (unsigned int)idx;
     return ((unsigned int)idx & ~255u) | (__brev((unsigned int)idx & 255u) >> 24);
@@ -303,9 +334,8 @@ __device__ __forceinline__ int untie_key(int mode, unsigned int key) {
     return (int)((key & ~255u) | (__brev(key & 255u) >> 24));
 }
 
-__global__ void k_tiebreak(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+__device__ __forceinline__ void k_tiebreak_body(const int o, const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
     if (sb.gate && !*sb.gate) return;
-    const int o = blockIdx.y;
     if (orients[o].skip) return;
     const int n = min(sb.ncand[o], sb.cap);
     const unsigned long long b = sb.best[o];
@@ -313,6 +343,20 @@ __global__ void k_tiebreak(const OrientDesc* __restrict__ orients, SelectBufs sb
     const double* cs = sb.cscore + (size_t)o * sb.cap;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         if (cs[c] < 1e299 && ord_key(cs[c]) == b) atomicMin(&sb.bestkey[o], (unsigned long long)tie_key(sp.mode, cand[c]));
+    }
+}
+
+__global__ void 
+k_tiebreak(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    if (!sb.srch) {
+        const int o = blockIdx.y;
+        k_tiebreak_body(o, orients, sb, sp);
+        return;
+    }
+    const int na = *sb.nsrch;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        const int o = sb.srch[j];
+        k_tiebreak_body(o, orients, sb, sp);
     }
 }
 
@@ -475,6 +519,8 @@ struct FloodBufs {
     long long okstride;            // okplane stride per orientation
     int limit;                     // union-find retries / path steps before err is set
     int* okcount;                  // when set, k_ff_reach adds each orientation's reachable cells
+    const int* srch;               // when set: the searched orientations (k_active_list), *nsrch of them;
+    const int* nsrch;              // CTA row y takes srch[y], srch[y + gridDim.y], ...
 };
 
 // Past `limit` steps both give up, set bit 0 of *err and return a valid run
@@ -520,10 +566,8 @@ __device__ __forceinline__ uint32_t run_starts(const uint32_t* w, int i, uint32_
 // depend on it.  Writes cnt/off per line and, per run, (z0 | z1 << 16), its
 // line, itself as parent and the seed flag (runs on the seed faces).
 // grid: (ceil(nx*ny/256), n_orient), block 256
-__global__ void __launch_bounds__(256)
-k_ff_runs(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+__device__ __forceinline__ void k_ff_runs_body(const int o, const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
     if (fb.gate && !*fb.gate) return;
-    const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
     const int line = blockIdx.x * blockDim.x + threadIdx.x;
@@ -585,10 +629,24 @@ k_ff_runs(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) 
     }
 }
 
+__global__ void __launch_bounds__(256)
+
+k_ff_runs(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    if (!fb.srch) {
+        const int o = blockIdx.y;
+        k_ff_runs_body(o, orients, fb, sp);
+        return;
+    }
+    const int na = *fb.nsrch;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        const int o = fb.srch[j];
+        k_ff_runs_body(o, orients, fb, sp);
+    }
+}
+
 // grid: (ceil(nx*ny/256), n_orient)
-__global__ void k_ff_union(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+__device__ __forceinline__ void k_ff_union_body(const int o, const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
     if (fb.gate && !*fb.gate) return;
-    const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
     const int line = blockIdx.x * blockDim.x + threadIdx.x;
@@ -616,10 +674,23 @@ __global__ void k_ff_union(const OrientDesc* __restrict__ orients, FloodBufs fb,
     }
 }
 
+__global__ void 
+k_ff_union(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    if (!fb.srch) {
+        const int o = blockIdx.y;
+        k_ff_union_body(o, orients, fb, sp);
+        return;
+    }
+    const int na = *fb.nsrch;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        const int o = fb.srch[j];
+        k_ff_union_body(o, orients, fb, sp);
+    }
+}
+
 // grid: (ceil(maxruns/256), n_orient)
-__global__ void k_ff_seed(const OrientDesc* __restrict__ orients, FloodBufs fb) {
+__device__ __forceinline__ void k_ff_seed_body(const int o, const OrientDesc* __restrict__ orients, FloodBufs fb) {
     if (fb.gate && !*fb.gate) return;
-    const int o = blockIdx.y;
     if (orients[o].skip) return;
     const int n = fb.total[o];
     int* par = fb.parent + (size_t)o * fb.sRun;
@@ -632,10 +703,23 @@ __global__ void k_ff_seed(const OrientDesc* __restrict__ orients, FloodBufs fb) 
     }
 }
 
+__global__ void 
+k_ff_seed(const OrientDesc* __restrict__ orients, FloodBufs fb) {
+    if (!fb.srch) {
+        const int o = blockIdx.y;
+        k_ff_seed_body(o, orients, fb);
+        return;
+    }
+    const int na = *fb.nsrch;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        const int o = fb.srch[j];
+        k_ff_seed_body(o, orients, fb);
+    }
+}
+
 // grid: (ceil(nx*ny/256), n_orient)
-__global__ void k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+__device__ __forceinline__ void k_ff_reach_body(const int o, const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
     if (fb.gate && !*fb.gate) return;
-    const int o = blockIdx.y;
     const OrientDesc& od = orients[o];
     if (od.skip) return;
     const int line = blockIdx.x * blockDim.x + threadIdx.x;
@@ -664,6 +748,20 @@ __global__ void k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb,
         const unsigned int m = __activemask();
         const int c = __reduce_add_sync(m, nreach);
         if ((threadIdx.x & 31) == __ffs(m) - 1 && c) atomicAdd(&fb.okcount[o], c);
+    }
+}
+
+__global__ void 
+k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    if (!fb.srch) {
+        const int o = blockIdx.y;
+        k_ff_reach_body(o, orients, fb, sp);
+        return;
+    }
+    const int na = *fb.nsrch;
+    for (int j = blockIdx.y; j < na; j += gridDim.y) {
+        const int o = fb.srch[j];
+        k_ff_reach_body(o, orients, fb, sp);
     }
 }
 
