@@ -284,6 +284,12 @@ int g_filter_cut = 50;
 // CTA rows of the transform kernels when they take their orientations from
 // the active list (k_active_list); 0: one row per orientation (PSB_ACTIVE_GRID)
 int g_active_grid = 8;
+// the flood fill and the selection kernels also loop over the searched
+// orientations' list (PSB_LIST_SELECT=1).  Off: measured slower (same box,
+// items placed/s: off 1243.3, on 1238.2; k_ff_union 9.4 -> 12.4 ms per run):
+// those kernels hold no shared memory, so a CTA row per orientation costs
+// little, and the list serialises orientations within a row.
+bool g_list_select = false;
 // k_cand_filter variant for trays of at most 128 cells per column (tuning:
 // 0 = 8-sample batches within 64 registers, 1 = 4-sample batches and 12
 // CTAs per SM, 2 = 8-sample batches without a register bound, 3 = 16-sample
@@ -369,6 +375,7 @@ int set_smem_attrs() {
     if (const char* e = getenv("PSB_DIRECT_MAX")) g_direct_max = std::max(0, atoi(e));
     if (const char* e = getenv("PSB_FILTER_CUT")) g_filter_cut = std::max(0, std::min(100, atoi(e)));
     if (const char* e = getenv("PSB_ACTIVE_GRID")) g_active_grid = std::max(0, atoi(e));
+    if (const char* e = getenv("PSB_LIST_SELECT")) g_list_select = atoi(e) != 0;
     if (const char* e = getenv("PSB_FILTER_VARIANT")) g_filter_variant = std::max(0, std::min(3, atoi(e)));
     if (const char* e = getenv("PSB_LATE_MAX")) g_late_max = std::min(std::max(0, atoi(e)), kCandCap);
     TRY(set_max_dyn_smem(k_rfft_z));
@@ -1308,10 +1315,11 @@ struct psb_tray {
     // reachable cell; gate, when set, makes every launch conditional.
     int flood_fill(const OrientDesc* d_odb, int n, const ScoreParams& sp, const int* gate, unsigned char* okplane,
                    int* okcount = nullptr) {
+        const bool lists = act_ready && g_list_select;
         FloodBufs fb{d_free, d_reach, sBits, d_cnt, d_off,   sLine, d_rz2,    d_rline,
                      d_par,  d_rflag, sRun,  d_total, d_err, gate,  okplane, (long long)nx, g_uf_limit, okcount,
-                     act_ready ? d_srch : nullptr, act_ready ? d_nsrch : nullptr};
-        const int rows = act_ready ? std::min(n, g_active_grid) : n;
+                     lists ? d_srch : nullptr, lists ? d_nsrch : nullptr};
+        const int rows = lists ? std::min(n, g_active_grid) : n;
         const int lines = nx * ny;
         const int nblk = (lines + 255) / 256;
         const dim3 gl(nblk, rows);
@@ -1405,10 +1413,11 @@ struct psb_tray {
     // keeps them for every orientation)
     int select_over(const OrientDesc* d_odb, int n, const ScoreParams& sp, const uint32_t* ok, const int* gate,
                     ResultDev* d_out, const unsigned char* okplane = nullptr, bool fuse = false) {
+        const bool lists = act_ready && g_list_select;
         SelectBufs sel{ok,        sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
                        d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate, okplane,
-                       act_ready ? d_srch : nullptr, act_ready ? d_nsrch : nullptr};
-        const int rows = act_ready ? std::min(n, g_active_grid) : n;
+                       lists ? d_srch : nullptr, lists ? d_nsrch : nullptr};
+        const int rows = lists ? std::min(n, g_active_grid) : n;
         {
             PROF("k_collect", st);
             k_collect_plane<<<dim3(nx, rows), 256, 0, st>>>(d_odb, sel, sp);
