@@ -281,6 +281,10 @@ int g_direct_max = 4096;
 // filter cut-off (k_cand_filter): a warp stops sampling when more than this
 // percentage of its translations survive the first samples; 0 disables
 int g_filter_cut = 50;
+// the candidate filter runs one CTA per x plane for all orientations with
+// the tray window in shared memory (k_cand_filter_plane) when it fits;
+// PSB_FILTER_PLANE=0 selects the CTA-per-(plane, orientation) kernel
+bool g_filter_plane = true;
 // CTA rows of the transform kernels when they take their orientations from
 // the active list (k_active_list); 0: one row per orientation (PSB_ACTIVE_GRID)
 int g_active_grid = 8;
@@ -377,6 +381,7 @@ int set_smem_attrs() {
     if (const char* e = getenv("PSB_ACTIVE_GRID")) g_active_grid = std::max(0, atoi(e));
     if (const char* e = getenv("PSB_LIST_SELECT")) g_list_select = atoi(e) != 0;
     if (const char* e = getenv("PSB_FILTER_VARIANT")) g_filter_variant = std::max(0, std::min(3, atoi(e)));
+    if (const char* e = getenv("PSB_FILTER_PLANE")) g_filter_plane = atoi(e) != 0;
     if (const char* e = getenv("PSB_LATE_MAX")) g_late_max = std::min(std::max(0, atoi(e)), kCandCap);
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
@@ -398,6 +403,8 @@ int set_smem_attrs() {
             TRY(set_max_dyn_smem(fwd_plane_for(a, b)));
         }
     for (int n : {64, 100, 128, 240}) TRY(set_max_dyn_smem(xfwd_for(n)));
+    TRY(set_max_dyn_smem(k_cand_filter_plane<1>));
+    TRY(set_max_dyn_smem(k_cand_filter_plane<2>));
     TRY(init_register_twiddles());
     if (dev < 64) done[dev] = true;
     return PSB_OK;
@@ -1254,7 +1261,21 @@ struct psb_tray {
         if (xmax > 0) {
             const dim3 grid(xmax, n);
             CK(cudaMemsetAsync(d_ccount, 0, sizeof(int) * 3 * cap, st));
-            {
+            const size_t smw = sizeof(uint4) * (size_t)emax * ny * tq + (size_t)n;
+            if (g_filter_plane && smw <= (size_t)g_smem_optin) {
+                PROF("k_cand_filter", st);
+                if (tq == 1) {
+                    k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
+                    k_cand_filter_plane<1><<<xmax, PSB_FILT_PLANE_THREADS, smw, st>>>(
+                        d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
+                        d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
+                } else {
+                    k_cand_prep<2><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
+                    k_cand_filter_plane<2><<<xmax, PSB_FILT_PLANE_THREADS, smw, st>>>(
+                        d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
+                        d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
+                }
+            } else {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
                     k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);

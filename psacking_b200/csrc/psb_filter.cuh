@@ -87,6 +87,157 @@ __device__ __forceinline__ uint32_t low_bits(int n) { return n >= 32 ? 0xfffffff
 // compile-time register index; lanes of a warp share the sample; loads go in
 // batches; a warp stops once none of its lanes holds a candidate.
 // grid: (max Xv, n_orient), block PSB_FILT_THREADS
+// The candidate words of one warp's rows (lane = row y0 + lane < Yv) for one
+// orientation and x plane: AND over the samples of the tray's free bits of
+// column (x + s.x, y + s.y) shifted down by s.z.  col(dx, yy) gives the NQ
+// uint4 free-bit words of tray column (x + dx, yy) (from global memory or a
+// shared-memory window), samp(i) the i-th shift-sorted sample; bound[k] ..
+// bound[k+1] are the samples with whole-word shift k (k_cand_prep).
+template <int NQ, int BATCH, class COLF, class SAMPF>
+__device__ __forceinline__ void filter_rows(int y0, int Yv, int Zv, COLF col, SAMPF samp, const int* bound, int cut_pct,
+                                            uint32_t (&c)[4 * NQ]) {
+    constexpr int NW = 4 * NQ;
+    const int lane = threadIdx.x & 31;
+    const int y = y0 + lane;
+    const bool act = y < Yv;
+    int n0 = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        c[w] = act ? low_bits(Zv - 32 * w) : 0u;
+        n0 += __popc(c[w]);
+    }
+    // Cut-off: any subset of the samples gives a valid (wider) candidate
+    // set, so a warp whose translations still mostly survive after
+    // PSB_FCUT_AFTER samples (open space, nothing to skip) stops there.
+    bool stop = false, checked = cut_pct <= 0;
+    int done = 0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        // shift of k whole words: word w of the shifted column is
+        // funnel(T[w + k], T[w + k + 1]) >> (s.z & 31)
+        const int s1 = bound[k + 1];
+        for (int s0 = bound[k]; s0 < s1 && !stop; s0 += BATCH) {
+            uint32_t a = 0u;
+            int nb = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                a |= c[w];
+                nb += __popc(c[w]);
+            }
+            if (!__any_sync(0xffffffffu, a != 0u)) {
+                stop = true;
+                break;
+            }
+            if (!checked && done >= PSB_FCUT_AFTER) {
+                checked = true;
+                int t0 = n0, t1 = nb;
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) {
+                    t0 += __shfl_xor_sync(0xffffffffu, t0, d);
+                    t1 += __shfl_xor_sync(0xffffffffu, t1, d);
+                }
+                if ((long long)t1 * 100 > (long long)t0 * cut_pct) {
+                    stop = true;
+                    break;
+                }
+            }
+            done += BATCH;
+            uint4 v[BATCH][NQ];
+            int off[BATCH];
+#pragma unroll
+            for (int i = 0; i < BATCH; ++i) {
+                off[i] = 0;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) v[i][q] = make_uint4(0u, 0u, 0u, 0u);
+                if (s0 + i < s1) {
+                    const int3 p = samp(s0 + i);
+                    off[i] = p.z & 31;
+                    if (act) {
+                        const uint4* cp = col(p.x, y + p.y);
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) v[i][q] = cp[q];
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < BATCH; ++i) {
+                if (s0 + i >= s1) break;
+                uint32_t T[NW];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    T[4 * q] = v[i][q].x;
+                    T[4 * q + 1] = v[i][q].y;
+                    T[4 * q + 2] = v[i][q].z;
+                    T[4 * q + 3] = v[i][q].w;
+                }
+#pragma unroll
+                for (int w = 0; w < NW; ++w) {
+                    const uint32_t lo = (w + k < NW) ? T[w + k] : 0u;
+                    const uint32_t hi = (w + k + 1 < NW) ? T[w + k + 1] : 0u;
+                    c[w] &= __funnelshift_r(lo, hi, off[i]);
+                }
+            }
+        }
+    }
+}
+
+// One warp's rows: store the candidate words, count them and list them while
+// the orientation has at most ccap (a list for the direct checks of
+// k_cand_verify_list); returns whether the rows hold a candidate.
+template <int NQ>
+__device__ __forceinline__ bool filter_store(const uint32_t (&c)[4 * NQ], int o, int x, int y0, int Yv, int ny,
+                                             int nzw, int nz, uint32_t* __restrict__ cw, int* __restrict__ ccount,
+                                             int* __restrict__ clist, int ccap) {
+    constexpr int NW = 4 * NQ;
+    const int lane = threadIdx.x & 31;
+    const int y = y0 + lane;
+    int mine = 0;
+    bool any = false;
+    if (y < Yv) {
+#pragma unroll
+        for (int w = 0; w < NW; ++w)
+            if (w < nzw) {
+                cw[(size_t)y * nzw + w] = c[w];
+                any |= c[w] != 0u;
+                mine += __popc(c[w]);
+            }
+    }
+    int incl = mine;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += u;
+    }
+    int base = 0;
+    if (lane == 31 && incl) base = atomicAdd(&ccount[o], incl);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    int slot = base + incl - mine;
+    if (mine && slot < ccap) {
+        int* L = clist + (size_t)o * ccap;
+        const int t0 = (x * ny + y) * nz;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            uint32_t m = w < nzw ? c[w] : 0u;
+            while (m && slot < ccap) {
+                const int bit = __ffs(m) - 1;
+                m &= m - 1u;
+                L[slot++] = t0 + 32 * w + bit;
+            }
+        }
+    }
+    return __any_sync(0xffffffffu, any);
+}
+
+// Candidate words of one x plane of one orientation: for rows y < Yv, the
+// words cand[(x*ny + y)*nzw + w] (the free-bit layout of the search, so the
+// collision pass can refine them in place), candplane[o][x] = "the plane
+// holds a candidate", the orientation's candidate count and, while there are
+// few, its candidate list.  Samples come sorted by their word shift s.z / 32
+// (k_cand_prep) so every shift is a compile-time register index; lanes of a
+// warp share the sample; loads go in batches; a warp stops once none of its
+// lanes holds a candidate.  The tray's free bits are read from global memory
+// (L1/L2); k_cand_filter_plane reads them from a shared-memory window.
+// grid: (max Xv, n_orient), block PSB_FILT_THREADS
 template <int NQ, int BATCH = PSB_FBATCH, int MINB = 8>
 __global__ void __launch_bounds__(PSB_FILT_THREADS, MINB)
 k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ tbits, int ny, int nzw,
@@ -99,7 +250,7 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
     if (od.skip || od.nsamp <= 0) return;
     const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
     if (x >= Xv || Yv <= 0 || Zv <= 0) return;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5;
     __shared__ int3 S[PSB_FSAMP];
     __shared__ int bound[NW + 1];   // samples with shift k are S[bound[k] .. bound[k+1])
     const int ns = min(od.nsamp, PSB_FSAMP);
@@ -112,126 +263,71 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
     uint32_t* cw = cand + (size_t)o * sBits + (size_t)x * ny * nzw;
     int any = 0;
     for (int y0 = warp * 32; y0 < Yv; y0 += PSB_FILT_THREADS) {
-        const int y = y0 + lane;
-        const bool act = y < Yv;
         uint32_t c[NW];
-        int n0 = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            c[w] = act ? low_bits(Zv - 32 * w) : 0u;
-            n0 += __popc(c[w]);
-        }
-        // Cut-off: any subset of the samples gives a valid (wider) candidate
-        // set, so a warp whose translations still mostly survive after
-        // PSB_FCUT_AFTER samples (open space, nothing to skip) stops there.
-        bool stop = false, checked = cut_pct <= 0;
-        int done = 0;
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-            // shift of k whole words: word w of the shifted column is
-            // funnel(T[w + k], T[w + k + 1]) >> (s.z & 31)
-            const int s1 = bound[k + 1];
-            for (int s0 = bound[k]; s0 < s1 && !stop; s0 += BATCH) {
-                uint32_t a = 0u;
-                int nb = 0;
-#pragma unroll
-                for (int w = 0; w < NW; ++w) {
-                    a |= c[w];
-                    nb += __popc(c[w]);
-                }
-                if (!__any_sync(0xffffffffu, a != 0u)) {
-                    stop = true;
-                    break;
-                }
-                if (!checked && done >= PSB_FCUT_AFTER) {
-                    checked = true;
-                    int t0 = n0, t1 = nb;
-#pragma unroll
-                    for (int d = 16; d > 0; d >>= 1) {
-                        t0 += __shfl_xor_sync(0xffffffffu, t0, d);
-                        t1 += __shfl_xor_sync(0xffffffffu, t1, d);
-                    }
-                    if ((long long)t1 * 100 > (long long)t0 * cut_pct) {
-                        stop = true;
-                        break;
-                    }
-                }
-                done += BATCH;
-                uint4 v[BATCH][NQ];
-                int off[BATCH];
-#pragma unroll
-                for (int i = 0; i < BATCH; ++i) {
-                    off[i] = 0;
-#pragma unroll
-                    for (int q = 0; q < NQ; ++q) v[i][q] = make_uint4(0u, 0u, 0u, 0u);
-                    if (s0 + i < s1) {
-                        const int3 p = S[s0 + i];
-                        off[i] = p.z & 31;
-                        if (act) {
-                            const uint4* col = tbits + ((size_t)(x + p.x) * ny + (y + p.y)) * NQ;
-#pragma unroll
-                            for (int q = 0; q < NQ; ++q) v[i][q] = __ldg(col + q);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < BATCH; ++i) {
-                    if (s0 + i >= s1) break;
-                    uint32_t T[NW];
-#pragma unroll
-                    for (int q = 0; q < NQ; ++q) {
-                        T[4 * q] = v[i][q].x;
-                        T[4 * q + 1] = v[i][q].y;
-                        T[4 * q + 2] = v[i][q].z;
-                        T[4 * q + 3] = v[i][q].w;
-                    }
-#pragma unroll
-                    for (int w = 0; w < NW; ++w) {
-                        const uint32_t lo = (w + k < NW) ? T[w + k] : 0u;
-                        const uint32_t hi = (w + k + 1 < NW) ? T[w + k + 1] : 0u;
-                        c[w] &= __funnelshift_r(lo, hi, off[i]);
-                    }
-                }
-            }
-        }
-        int mine = 0;
-        if (act) {
-#pragma unroll
-            for (int w = 0; w < NW; ++w)
-                if (w < nzw) {
-                    cw[(size_t)y * nzw + w] = c[w];
-                    any |= c[w] != 0u;
-                    mine += __popc(c[w]);
-                }
-        }
-        // count, and list the candidates while the orientation has at most
-        // ccap of them (a list for the direct checks of k_cand_verify_list)
-        int incl = mine;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, incl, d);
-            if (lane >= d) incl += u;
-        }
-        int base = 0;
-        if (lane == 31 && incl) base = atomicAdd(&ccount[o], incl);
-        base = __shfl_sync(0xffffffffu, base, 31);
-        int slot = base + incl - mine;
-        if (mine && slot < ccap) {
-            int* L = clist + (size_t)o * ccap;
-            const int t0 = (x * ny + y) * nz;
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-                uint32_t m = w < nzw ? c[w] : 0u;
-                while (m && slot < ccap) {
-                    const int bit = __ffs(m) - 1;
-                    m &= m - 1u;
-                    L[slot++] = t0 + 32 * w + bit;
-                }
-            }
-        }
+        filter_rows<NQ, BATCH>(
+            y0, Yv, Zv, [&](int dx, int yy) { return tbits + ((size_t)(x + dx) * ny + yy) * NQ; },
+            [&](int i) { return S[i]; }, bound, cut_pct, c);
+        any |= filter_store<NQ>(c, o, x, y0, Yv, ny, nzw, nz, cw, ccount, clist, ccap) ? 1 : 0;
     }
     any = __syncthreads_or(any);
     if (tid == 0) candplane[(size_t)o * pstride + x] = any ? 1 : 0;
+}
+
+// The same candidate words, one CTA per x plane for every orientation: the
+// tray's free bits of planes x .. x + E - 1 (E = the items' largest x extent)
+// are staged once in shared memory, and the CTA's warps take the
+// (orientation, 32-row block) tasks of the plane, reading samples from the
+// k_cand_prep buffers (L1-resident).  Staging the window replaces the L2
+// round trip of every sample load.  grid: max Xv, block PSB_FILT_PLANE_THREADS,
+// dynamic shared memory E * ny * NQ uint4 + n bytes of plane flags
+#define PSB_FILT_PLANE_THREADS 512
+template <int NQ>
+__global__ void __launch_bounds__(PSB_FILT_PLANE_THREADS, 1)
+k_cand_filter_plane(const OrientDesc* __restrict__ orients, int n, const uint4* __restrict__ tbits, int nx, int ny,
+                    int nzw, int E, uint32_t* __restrict__ cand, long long sBits,
+                    unsigned char* __restrict__ candplane, long long pstride, int* __restrict__ ccount,
+                    const int4* __restrict__ fs, const int* __restrict__ fbound, int cut_pct,
+                    int* __restrict__ clist, int ccap, int nz) {
+    constexpr int NW = 4 * NQ;
+    extern __shared__ uint4 win[];   // [E][ny][NQ]
+    const int x = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nwarp = PSB_FILT_PLANE_THREADS / 32;
+    unsigned char* flag = (unsigned char*)(win + (size_t)E * ny * NQ);
+    const int planes = min(E, nx - x);
+    const size_t nwords = (size_t)planes * ny * NQ;
+    const uint4* src = tbits + (size_t)x * ny * NQ;   // planes x .. x + planes - 1 are contiguous
+    for (size_t i = tid; i < nwords; i += PSB_FILT_PLANE_THREADS) win[i] = __ldg(&src[i]);
+    for (int o = tid; o < n; o += PSB_FILT_PLANE_THREADS) flag[o] = 0;
+    __syncthreads();
+    const int yblocks = (ny + 31) / 32;
+    for (int task = warp; task < n * yblocks; task += nwarp) {
+        const int o = task / yblocks, y0 = (task - o * yblocks) * 32;
+        const OrientDesc& od = orients[o];
+        if (od.skip || od.nsamp <= 0) continue;
+        const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
+        if (x >= Xv || y0 >= Yv || Zv <= 0) continue;
+        const int4* S = fs + (size_t)o * PSB_FSAMP;
+        int bound[NW + 1];
+#pragma unroll
+        for (int k = 0; k <= NW; ++k) bound[k] = __ldg(&fbound[(size_t)o * PSB_FBOUND + k]);
+        uint32_t c[NW];
+        filter_rows<NQ, PSB_FBATCH>(
+            y0, Yv, Zv, [&](int dx, int yy) { return win + ((size_t)dx * ny + yy) * NQ; },
+            [&](int i) {
+                const int4 v = __ldg(&S[i]);
+                return make_int3(v.x, v.y, v.z);
+            },
+            bound, cut_pct, c);
+        uint32_t* cw = cand + (size_t)o * sBits + (size_t)x * ny * nzw;
+        if (filter_store<NQ>(c, o, x, y0, Yv, ny, nzw, nz, cw, ccount, clist, ccap) && lane == 0) flag[o] = 1;
+    }
+    __syncthreads();
+    for (int o = tid; o < n; o += PSB_FILT_PLANE_THREADS) {
+        const OrientDesc& od = orients[o];
+        if (od.skip || od.nsamp <= 0 || x >= od.valid[0] || od.valid[1] <= 0 || od.valid[2] <= 0) continue;
+        candplane[(size_t)o * pstride + x] = flag[o];
+    }
 }
 
 // Stage 0 (after k_cand_filter, count = candidates): an orientation without
