@@ -200,6 +200,15 @@ int get_plan(int n, Plan1D* out) {
 
 int g_smem_optin = 0;  // max dynamic shared memory per block of the current device
 bool g_fast_fft = true;  // specialised two-pass kernels where a plan exists
+// Tray grids (circular, F >= n) may be padded further: when every axis
+// reaches a length with specialised kernels (x: 64, 100, 128, 240; y and z:
+// 64, 100, 128) for at most g_pad_max times the volume, those lengths are
+// taken, so the tray runs the specialised split flow (and its direct
+// decisions) instead of the generic kernels.  The circular correlation stays
+// exact for every translation the search scores (t + x <= n - 1 < F).
+// 0 disables (PSB_PAD_MAX).
+double g_pad_max = 2.0;
+
 
 using XpassFn = void (*)(const OrientDesc*, SearchBufs, const float2*, const float2*, int, const float2*,
                          const unsigned char*, long long, BaseMap);
@@ -281,10 +290,15 @@ int g_direct_max = 4096;
 // filter cut-off (k_cand_filter): a warp stops sampling when more than this
 // percentage of its translations survive the first samples; 0 disables
 int g_filter_cut = 50;
-// the candidate filter runs one CTA per x plane for all orientations with
-// the tray window in shared memory (k_cand_filter_plane) when it fits;
-// PSB_FILTER_PLANE=0 selects the CTA-per-(plane, orientation) kernel
-bool g_filter_plane = true;
+// the candidate filter as one CTA per x plane (and orientation group) with
+// the tray's free-bit window staged in shared memory (k_cand_filter_plane),
+// PSB_FILTER_PLANE=1 (or the group count).  Off: measured slower on the
+// config-3 benchmark (items placed/s: off 1283.7 / 1285.2; on with 1, 2, 3,
+// 4, 6 groups 1157.6, 1212.8, 1227.5, 1219.6, 1217.3): re-staging the
+// ~100 KB window for every CTA costs more L2 traffic than the per-sample L1
+// hits of the CTA-per-(plane, orientation) kernel.
+bool g_filter_plane = false;
+int g_filter_groups = 3;   // CTA rows of k_cand_filter_plane, each a third of the orientations
 // CTA rows of the transform kernels when they take their orientations from
 // the active list (k_active_list); 0: one row per orientation (PSB_ACTIVE_GRID)
 int g_active_grid = 8;
@@ -379,9 +393,14 @@ int set_smem_attrs() {
     if (const char* e = getenv("PSB_DIRECT_MAX")) g_direct_max = std::max(0, atoi(e));
     if (const char* e = getenv("PSB_FILTER_CUT")) g_filter_cut = std::max(0, std::min(100, atoi(e)));
     if (const char* e = getenv("PSB_ACTIVE_GRID")) g_active_grid = std::max(0, atoi(e));
+    if (const char* e = getenv("PSB_PAD_MAX")) g_pad_max = std::max(0.0, atof(e));
+    if (const char* e = getenv("PSB_FAST_FFT")) g_fast_fft = atoi(e) != 0;
     if (const char* e = getenv("PSB_LIST_SELECT")) g_list_select = atoi(e) != 0;
     if (const char* e = getenv("PSB_FILTER_VARIANT")) g_filter_variant = std::max(0, std::min(3, atoi(e)));
-    if (const char* e = getenv("PSB_FILTER_PLANE")) g_filter_plane = atoi(e) != 0;
+    if (const char* e = getenv("PSB_FILTER_PLANE")) {
+        g_filter_plane = atoi(e) != 0;
+        if (atoi(e) > 1) g_filter_groups = atoi(e);
+    }
     if (const char* e = getenv("PSB_LATE_MAX")) g_late_max = std::min(std::max(0, atoi(e)), kCandCap);
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
@@ -463,6 +482,15 @@ struct Grid3 {
     Plan1D p[3];
 };
 
+int next_special(int n, bool x_axis) {
+    const int xs[4] = {64, 100, 128, 240}, yz[3] = {64, 100, 128};
+    const int* set = x_axis ? xs : yz;
+    const int m = x_axis ? 4 : 3;
+    for (int i = 0; i < m; ++i)
+        if (set[i] >= n) return set[i];
+    return -1;
+}
+
 int make_grid3(int nx, int ny, int nz, bool linear, Grid3* g) {
     g->n[0] = nx; g->n[1] = ny; g->n[2] = nz;
     for (int a = 0; a < 3; ++a) {
@@ -470,8 +498,21 @@ int make_grid3(int nx, int ny, int nz, bool linear, Grid3* g) {
         g->F[a] = fft_len(want);
         if (g->F[a] < 0)
             return fail(PSB_ERR_ARG, "axis %d of length %d needs an FFT longer than %d", a, g->n[a], PSB_MAX_FFT);
-        TRY(get_plan(g->F[a], &g->p[a]));
     }
+    if (!linear && g_fast_fft && g_pad_max > 0.0) {
+        int P[3];
+        bool all = true;
+        for (int a = 0; a < 3; ++a) {
+            P[a] = next_special(g->n[a], a == 0);
+            all = all && P[a] > 0;
+        }
+        if (all && !(P[0] == g->F[0] && P[1] == g->F[1] && P[2] == g->F[2])) {
+            const double ratio = ((double)P[0] * P[1] * P[2]) / ((double)g->F[0] * g->F[1] * g->F[2]);
+            if (ratio <= g_pad_max)
+                for (int a = 0; a < 3; ++a) g->F[a] = P[a];
+        }
+    }
+    for (int a = 0; a < 3; ++a) TRY(get_plan(g->F[a], &g->p[a]));
     g->H = g->F[2] / 2 + 1;
     return PSB_OK;
 }
@@ -1266,12 +1307,12 @@ struct psb_tray {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
                     k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
-                    k_cand_filter_plane<1><<<xmax, PSB_FILT_PLANE_THREADS, smw, st>>>(
+                    k_cand_filter_plane<1><<<dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st>>>(
                         d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
                         d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
                 } else {
                     k_cand_prep<2><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
-                    k_cand_filter_plane<2><<<xmax, PSB_FILT_PLANE_THREADS, smw, st>>>(
+                    k_cand_filter_plane<2><<<dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st>>>(
                         d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
                         d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
                 }

@@ -278,11 +278,12 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
 // are staged once in shared memory, and the CTA's warps take the
 // (orientation, 32-row block) tasks of the plane, reading samples from the
 // k_cand_prep buffers (L1-resident).  Staging the window replaces the L2
-// round trip of every sample load.  grid: max Xv, block PSB_FILT_PLANE_THREADS,
+// round trip of every sample load.  grid: (max Xv, orientation groups),
+// block PSB_FILT_PLANE_THREADS,
 // dynamic shared memory E * ny * NQ uint4 + n bytes of plane flags
 #define PSB_FILT_PLANE_THREADS 512
 template <int NQ>
-__global__ void __launch_bounds__(PSB_FILT_PLANE_THREADS, 1)
+__global__ void __launch_bounds__(PSB_FILT_PLANE_THREADS, 2)
 k_cand_filter_plane(const OrientDesc* __restrict__ orients, int n, const uint4* __restrict__ tbits, int nx, int ny,
                     int nzw, int E, uint32_t* __restrict__ cand, long long sBits,
                     unsigned char* __restrict__ candplane, long long pstride, int* __restrict__ ccount,
@@ -300,9 +301,11 @@ k_cand_filter_plane(const OrientDesc* __restrict__ orients, int n, const uint4* 
     for (size_t i = tid; i < nwords; i += PSB_FILT_PLANE_THREADS) win[i] = __ldg(&src[i]);
     for (int o = tid; o < n; o += PSB_FILT_PLANE_THREADS) flag[o] = 0;
     __syncthreads();
+    // CTA row blockIdx.y takes the orientations o = blockIdx.y (mod gridDim.y)
     const int yblocks = (ny + 31) / 32;
-    for (int task = warp; task < n * yblocks; task += nwarp) {
-        const int o = task / yblocks, y0 = (task - o * yblocks) * 32;
+    const int nog = (n - (int)blockIdx.y + (int)gridDim.y - 1) / (int)gridDim.y;
+    for (int task = warp; task < nog * yblocks; task += nwarp) {
+        const int o = (task / yblocks) * gridDim.y + blockIdx.y, y0 = (task % yblocks) * 32;
         const OrientDesc& od = orients[o];
         if (od.skip || od.nsamp <= 0) continue;
         const int Xv = od.valid[0], Yv = od.valid[1], Zv = od.valid[2];
@@ -323,7 +326,7 @@ k_cand_filter_plane(const OrientDesc* __restrict__ orients, int n, const uint4* 
         if (filter_store<NQ>(c, o, x, y0, Yv, ny, nzw, nz, cw, ccount, clist, ccap) && lane == 0) flag[o] = 1;
     }
     __syncthreads();
-    for (int o = tid; o < n; o += PSB_FILT_PLANE_THREADS) {
+    for (int o = blockIdx.y + tid * gridDim.y; o < n; o += PSB_FILT_PLANE_THREADS * gridDim.y) {
         const OrientDesc& od = orients[o];
         if (od.skip || od.nsamp <= 0 || x >= od.valid[0] || od.valid[1] <= 0 || od.valid[2] <= 0) continue;
         candplane[(size_t)o * pstride + x] = flag[o];

@@ -121,6 +121,32 @@ def test_search_random(gpu_core, shape, flags):
         check_search(gpu_core, tray, items, flags)
 
 
+def test_search_padded_grid(gpu_core):
+    """A 90x70x110 tray is padded to the specialised lengths 100x100x128
+    (within twice the smooth lengths' volume): the circular correlation on
+    the longer grid must still give the oracle's exact answers."""
+    import ctypes
+    from psacking_b200.proposal import lib
+    shape = (90, 70, 110)
+    t = ctypes.c_void_p()
+    L = lib()
+    assert L.psb_tray_create(*shape, ctypes.byref(t)) == 0
+    F = (ctypes.c_int * 3)()
+    assert L.psb_tray_fft_dims(t, F) == 0
+    L.psb_tray_destroy(t)
+    assert tuple(F) == (100, 100, 128)
+    rng = np.random.default_rng(41)
+    for flags in (BLOCK | INTERLOCK, BLOCK, SCAN):
+        tray = random_tray(rng, shape, 0.3)
+        items = [random_item(rng, [12, 10, 14]) for _ in range(3)]
+        check_search(gpu_core, tray, items, flags)
+
+
+def test_padded_grid_packing(gpu_core):
+    from psacking_b200 import workloads
+    run_both(workloads.config2_items(21)[:8], (90, 70, 110), 6, True)
+
+
 def test_search_empty_and_full(gpu_core):
     tray = np.zeros((20, 20, 20), np.int32)
     it = np.ones((3, 3, 3), np.int32)
