@@ -397,14 +397,26 @@ k_cand_verify_list(const OrientDesc* __restrict__ orients, int n, const uint4* _
                    const int* __restrict__ ncol, int* __restrict__ vcount, unsigned char* __restrict__ okplane,
                    long long pstride, int set_okplane) {
     extern __shared__ int pre[];   // pre[o]: direct candidates of orientations before o
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        // warp 0: the orientations' counts loaded in parallel, an exclusive scan
         int acc = 0;
-        for (int o = 0; o < n; ++o) {
-            pre[o] = acc;
-            const OrientDesc& od = orients[o];
-            if (!od.skip && od.direct == 1) acc += min(ccount[o], ccap);
+        for (int o0 = 0; o0 < n; o0 += 32) {
+            const int o = o0 + threadIdx.x;
+            int c = 0;
+            if (o < n) {
+                const OrientDesc& od = orients[o];
+                if (!od.skip && od.direct == 1) c = min(ccount[o], ccap);
+            }
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, incl, d);
+                if ((int)threadIdx.x >= d) incl += u;
+            }
+            if (o < n) pre[o] = acc + incl - c;
+            acc += __shfl_sync(0xffffffffu, incl, 31);
         }
-        pre[n] = acc;
+        if (threadIdx.x == 0) pre[n] = acc;
     }
     __syncthreads();
     const int total = pre[n];
