@@ -401,6 +401,7 @@ int set_smem_attrs() {
         g_filter_plane = atoi(e) != 0;
         if (atoi(e) > 1) g_filter_groups = atoi(e);
     }
+    if (const char* e = getenv("PSB_PDL")) g_pdl = atoi(e) != 0;
     if (const char* e = getenv("PSB_LATE_MAX")) g_late_max = std::min(std::max(0, atoi(e)), kCandCap);
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
@@ -527,19 +528,19 @@ int forward3_dev(const Grid3& g, const RzDesc* d_rz, const MidDesc* d_mid, cudaS
     int npairs = (g.n[0] * g.n[1] + 1) / 2;
     {
         PROF("k_rfft_z", st);
-        k_rfft_z<<<dim3((npairs + PSB_PAIRS - 1) / PSB_PAIRS, 1), PSB_THREADS, smem_rz(g.F[2]), st>>>(
+        pdl(k_rfft_z, dim3((npairs + PSB_PAIRS - 1) / PSB_PAIRS, 1), PSB_THREADS, smem_rz(g.F[2]), st)(
             d_rz, nullptr, g.p[2].p, g.p[2].tw);
     }
     CKL();
     {
         PROF("k_fft_mid_fwd", st);
-        k_fft_mid<-1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.n[0], 1), PSB_THREADS, smem_mid(g.F[1]), st>>>(
+        pdl(k_fft_mid<-1>, dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.n[0], 1), PSB_THREADS, smem_mid(g.F[1]), st)(
             d_mid, nullptr, g.p[1].p, g.p[1].tw);
     }
     CKL();
     {
         PROF("k_fft_mid_fwd", st);
-        k_fft_mid<-1><<<dim3((g.F[1] * g.H + PSB_TILE - 1) / PSB_TILE, 1, 1), PSB_THREADS, smem_mid(g.F[0]), st>>>(
+        pdl(k_fft_mid<-1>, dim3((g.F[1] * g.H + PSB_TILE - 1) / PSB_TILE, 1, 1), PSB_THREADS, smem_mid(g.F[0]), st)(
             d_mid + 1, nullptr, g.p[0].p, g.p[0].tw);
     }
     CKL();
@@ -586,13 +587,13 @@ int inverse3_int(const Grid3& g, float2* spec, float2* w1, float2* w2, int32_t* 
 int inverse3_dev(const Grid3& g, float2* w1, int32_t* out, const MidDesc* d_mid, cudaStream_t st) {
     {
         PROF("k_fft_mid_inv", st);
-        k_fft_mid<1><<<dim3((g.F[1] * g.H + PSB_TILE - 1) / PSB_TILE, 1, 1), PSB_THREADS, smem_mid(g.F[0]), st>>>(
+        pdl(k_fft_mid<1>, dim3((g.F[1] * g.H + PSB_TILE - 1) / PSB_TILE, 1, 1), PSB_THREADS, smem_mid(g.F[0]), st)(
             d_mid, nullptr, g.p[0].p, g.p[0].tw);
     }
     CKL();
     {
         PROF("k_fft_mid_inv", st);
-        k_fft_mid<1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.n[0], 1), PSB_THREADS, smem_mid(g.F[1]), st>>>(
+        pdl(k_fft_mid<1>, dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.n[0], 1), PSB_THREADS, smem_mid(g.F[1]), st)(
             d_mid + 1, nullptr, g.p[1].p, g.p[1].tw);
     }
     CKL();
@@ -600,7 +601,7 @@ int inverse3_dev(const Grid3& g, float2* w1, int32_t* out, const MidDesc* d_mid,
     float scale = (float)(1.0 / ((double)g.F[0] * g.F[1] * g.F[2]));
     {
         PROF("k_irfft_z_int", st);
-        k_irfft_z_int<<<((nlines + 1) / 2 + PSB_PAIRS - 1) / PSB_PAIRS, PSB_THREADS, smem_rz(g.F[2]), st>>>(
+        pdl(k_irfft_z_int, ((nlines + 1) / 2 + PSB_PAIRS - 1) / PSB_PAIRS, PSB_THREADS, smem_rz(g.F[2]), st)(
             w1, out, nlines, g.n[2], scale, g.p[2].p, g.p[2].tw);
     }
     CKL();
@@ -613,7 +614,7 @@ int distance_on_device(const int32_t* d_grid, int32_t* d_out, int nx, int ny, in
     int far = nx + ny + nz + 10;  // fft3.cu:948
     {
         PROF("k_dist_init", st);
-        k_dist_init<<<grid1d(V), 256, 0, st>>>(d_grid, d_out, V, far, gate);
+        pdl(k_dist_init, grid1d(V), 256, 0, st)(d_grid, d_out, V, far, gate);
     }
     CKL();
     for (int axis = 0; axis < 3; ++axis) {
@@ -625,12 +626,12 @@ int distance_on_device(const int32_t* d_grid, int32_t* d_out, int nx, int ny, in
             long long blocks = (nlines + W - 1) / W;
             {
                 PROF("k_dist_axis", st);
-                k_dist_axis<<<(unsigned)blocks, 256, (size_t)W * L * 4, st>>>(d_out, axis, nx, ny, nz, (int)W, gate);
+                pdl(k_dist_axis, (unsigned)blocks, 256, (size_t)W * L * 4, st)(d_out, axis, nx, ny, nz, (int)W, gate);
             }
         } else {
             {
                 PROF("k_dist_axis_global", st);
-                k_dist_axis_global<<<(unsigned)((nlines + 255) / 256), 256, 0, st>>>(d_out, axis, nx, ny, nz, gate);
+                pdl(k_dist_axis_global, (unsigned)((nlines + 255) / 256), 256, 0, st)(d_out, axis, nx, ny, nz, gate);
             }
         }
         CKL();
@@ -1080,13 +1081,13 @@ struct psb_tray {
     // the occupancy
     int prefix_phi(const int* gate) {
         const int ncols = nx * ny;
-        k_col_prefix<0><<<(ncols + 7) / 8, 256, 0, st>>>(d_phi, d_pphi, ncols, nz, gate);
+        pdl(k_col_prefix<0>, (ncols + 7) / 8, 256, 0, st)(d_phi, d_pphi, ncols, nz, gate);
         CKL();
         return PSB_OK;
     }
     int prefix_occ() {
         const int ncols = nx * ny;
-        k_col_prefix<1><<<(ncols + 7) / 8, 256, 0, st>>>(d_tray, d_pocc, ncols, nz, nullptr);
+        pdl(k_col_prefix<1>, (ncols + 7) / 8, 256, 0, st)(d_tray, d_pocc, ncols, nz, nullptr);
         CKL();
         return PSB_OK;
     }
@@ -1125,13 +1126,13 @@ struct psb_tray {
                        w, 0, part ? x0p : nullptr};
             {
                 PROF("k_fwd_plane", st);
-                ff<<<dim3(part ? slabs : nx, 1), 256, smf, st>>>(src, nullptr, g.p[1].tw, g.p[2].tw);
+                pdl(ff, dim3(part ? slabs : nx, 1), 256, smf, st)(src, nullptr, g.p[1].tw, g.p[2].tw);
             }
             CKL();
             {
                 PROF("k_xfwd", st);
                 const int ncols = g.F[1] * g.H;
-                xf<<<(ncols + PSB_XCOLS - 1) / PSB_XCOLS, 256, xfwd_smem(g.F[0]), st>>>(
+                pdl(xf, (ncols + PSB_XCOLS - 1) / PSB_XCOLS, 256, xfwd_smem(g.F[0]), st)(
                     w, phi ? d_Sphi : d_Socc, nx, ncols, gate, g.p[0].tw);
             }
             CKL();
@@ -1158,17 +1159,17 @@ struct psb_tray {
         CK(cudaMemsetAsync(raw, 0, sizeof(unsigned long long) * 4, st));
         {
             PROF("k_stats", st);
-            k_stats_g<<<grid1d(V), 256, 0, st>>>(d_phi, V, nullptr, raw, gate);
+            pdl(k_stats_g, grid1d(V), 256, 0, st)(d_phi, V, nullptr, raw, gate);
         }
         CKL();
-        k_phi_mean<<<1, 1, 0, st>>>(d_ps, (unsigned long long)V, gate);
+        pdl(k_phi_mean, 1, 1, 0, st)(d_ps, (unsigned long long)V, gate);
         CKL();
         {
             PROF("k_stats", st);
-            k_stats_g<<<grid1d(V), 256, 0, st>>>(d_phi, V, mean_p, raw, gate);
+            pdl(k_stats_g, grid1d(V), 256, 0, st)(d_phi, V, mean_p, raw, gate);
         }
         CKL();
-        k_phi_norm<<<1, 1, 0, st>>>(d_ps, gate);
+        pdl(k_phi_norm, 1, 1, 0, st)(d_ps, gate);
         CKL();
         return PSB_OK;
     }
@@ -1263,7 +1264,7 @@ struct psb_tray {
         }
         {
             PROF("k_tray_bits", st);
-            k_tray_bits<<<(unsigned)(((size_t)nx * ny + 7) / 8), 256, 0, st>>>(d_tray, nx, ny, nz, tq, d_tbits);
+            pdl(k_tray_bits, (unsigned)(((size_t)nx * ny + 7) / 8), 256, 0, st)(d_tray, nx, ny, nz, tq, d_tbits);
         }
         CKL();
         return PSB_OK;
@@ -1306,37 +1307,37 @@ struct psb_tray {
             if (g_filter_plane && smw <= (size_t)g_smem_optin) {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
-                    k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
-                    k_cand_filter_plane<1><<<dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st>>>(
+                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound);
+                    pdl(k_cand_filter_plane<1>, dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st)(
                         d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
                         d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
                 } else {
-                    k_cand_prep<2><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
-                    k_cand_filter_plane<2><<<dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st>>>(
+                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound);
+                    pdl(k_cand_filter_plane<2>, dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st)(
                         d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
                         d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
                 }
             } else {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
-                    k_cand_prep<1><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
+                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound);
                     // the variant (sample batch, CTAs per SM bound) is a tuning switch
                     auto kf = g_filter_variant == 1 ? k_cand_filter<1, 4, 12>
                             : g_filter_variant == 2 ? k_cand_filter<1, 8, 1>
                             : g_filter_variant == 3 ? k_cand_filter<1, 16, 1> : k_cand_filter<1>;
-                    kf<<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits, d_candplane,
+                    pdl(kf, grid, PSB_FILT_THREADS, 0, st)(d_odb, d_tbits, ny, nzw, d_free, sBits, d_candplane,
                                                           (long long)nx, d_ccount, d_fsamp, d_fbound, g_filter_cut,
                                                           d_clist, ccap, nz);
                 } else {
-                    k_cand_prep<2><<<n, 32, 0, st>>>(d_odb, d_fsamp, d_fbound);
-                    k_cand_filter<2><<<grid, PSB_FILT_THREADS, 0, st>>>(d_odb, d_tbits, ny, nzw, d_free, sBits,
+                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound);
+                    pdl(k_cand_filter<2>, grid, PSB_FILT_THREADS, 0, st)(d_odb, d_tbits, ny, nzw, d_free, sBits,
                                                                         d_candplane, (long long)nx, d_ccount,
                                                                         d_fsamp, d_fbound, g_filter_cut, d_clist,
                                                                         ccap, nz);
                 }
             }
             CKL();
-            k_cand_apply<<<(n + 127) / 128, 128, 0, st>>>(d_odb, n, d_ccount, 0, dmax);
+            pdl(k_cand_apply, (n + 127) / 128, 128, 0, st)(d_odb, n, d_ccount, 0, dmax);
             CKL();
             if (dmax > 0) {
                 // the okplane flags of the free cells (non-interlocking mode)
@@ -1344,14 +1345,14 @@ struct psb_tray {
                 CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
                 {
                     PROF("k_cand_verify", st);
-                    k_item_cols<<<dim3(emax, n), 64, 0, st>>>(d_odb, d_icols, (long long)nx * ny, d_ncol);
+                    pdl(k_item_cols, dim3(emax, n), 64, 0, st)(d_odb, d_icols, (long long)nx * ny, d_ncol);
                     CKL();
-                    k_cand_verify_list<<<148 * 4, 256, sizeof(int) * (n + 1), st>>>(
+                    pdl(k_cand_verify_list, 148 * 4, 256, sizeof(int) * (n + 1), st)(
                         d_odb, n, d_tbits, ny, nz, nzw, tq, d_free, sBits, d_clist, ccap, d_ccount, d_icols,
                         (long long)nx * ny, d_ncol, d_vcount, d_okplane, (long long)nx, interlock ? 0 : 1);
                 }
                 CKL();
-                k_cand_apply<<<(n + 127) / 128, 128, 0, st>>>(d_odb, n, d_vcount, 1, dmax);
+                pdl(k_cand_apply, (n + 127) / 128, 128, 0, st)(d_odb, n, d_vcount, 1, dmax);
                 CKL();
             }
         }
@@ -1388,22 +1389,22 @@ struct psb_tray {
         CK(cudaMemsetAsync(d_total, 0, sizeof(int) * n, st));
         {
             PROF("k_ff_runs", st);
-            k_ff_runs<<<gl, 256, 0, st>>>(d_odb, fb, sp);
+            pdl(k_ff_runs, gl, 256, 0, st)(d_odb, fb, sp);
         }
         CKL();
         {
             PROF("k_ff_union", st);
-            k_ff_union<<<gl, 256, 0, st>>>(d_odb, fb, sp);
+            pdl(k_ff_union, gl, 256, 0, st)(d_odb, fb, sp);
         }
         CKL();
         {
             PROF("k_ff_seed", st);
-            k_ff_seed<<<dim3(296, rows), 256, 0, st>>>(d_odb, fb);
+            pdl(k_ff_seed, dim3(296, rows), 256, 0, st)(d_odb, fb);
         }
         CKL();
         {
             PROF("k_ff_reach", st);
-            k_ff_reach<<<gl, 256, 0, st>>>(d_odb, fb, sp);
+            pdl(k_ff_reach, gl, 256, 0, st)(d_odb, fb, sp);
         }
         CKL();
         return PSB_OK;
@@ -1428,12 +1429,12 @@ struct psb_tray {
             PROF("k_xpass_coll", st);
             // with the filter's plane flags, only rows of planes holding a
             // candidate are stored (the plane pass skips the others)
-            xf1<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, rows), 256, xpass2_smem(g.F[0]), st>>>(
+            pdl(xf1, dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, rows), 256, xpass2_smem(g.F[0]), st)(
                 d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, cand_active ? d_candplane : nullptr, (long long)nx, bm);
         } else {
             PROF("k_xpass_coll", st);
             const size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
-            k_xpass<<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], n), PSB_THREADS, smx, st>>>(
+            pdl(k_xpass, dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], n), PSB_THREADS, smx, st)(
                 d_odb, sb, d_Socc, d_Sphi, g.F[1], g.H, g.p[0].p, g.p[0].tw);
         }
         CKL();
@@ -1446,24 +1447,24 @@ struct psb_tray {
                      interlock ? 0 : 1, cand_active ? d_candplane : nullptr, late ? d_okcount : nullptr};
         {
             PROF("k_plane_coll", st);
-            p0<<<dim3(nx, rows), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
+            pdl(p0, dim3(nx, rows), PSB_PLANE3_THREADS, smem, st)(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
         }
         CKL();
         if (interlock) TRY(flood_fill(d_odb, n, sp, nullptr, d_okplane, late ? d_okcount : nullptr));
         if (late) {
-            k_late_direct<<<(n + 127) / 128, 128, 0, st>>>(const_cast<OrientDesc*>(d_odb), n, d_okcount, g_late_max);
+            pdl(k_late_direct, (n + 127) / 128, 128, 0, st)(const_cast<OrientDesc*>(d_odb), n, d_okcount, g_late_max);
             CKL();
             late_active = true;
         }
         if (xf) {
             PROF("k_xpass_prox", st);
-            xf2<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, rows), 256, xpass2_smem(g.F[0]), st>>>(
+            pdl(xf2, dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, rows), 256, xpass2_smem(g.F[0]), st)(
                 d_odb, sb, d_Socc, d_Sphi, ncols, g.p[0].tw, d_okplane, (long long)nx, bm);
         }
         CKL();
         {
             PROF("k_plane_prox", st);
-            p1<<<dim3(nx, rows), PSB_PLANE3_THREADS, smem, st>>>(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
+            pdl(p1, dim3(nx, rows), PSB_PLANE3_THREADS, smem, st)(d_odb, sb, pb, sp, g.p[1].tw, g.p[2].tw);
         }
         CKL();
         return select_over(d_odb, n, sp, ok, nullptr, d_out, d_okplane, decide.ls != nullptr);
@@ -1482,32 +1483,32 @@ struct psb_tray {
         const int rows = lists ? std::min(n, g_active_grid) : n;
         {
             PROF("k_collect", st);
-            k_collect_plane<<<dim3(nx, rows), 256, 0, st>>>(d_odb, sel, sp);
+            pdl(k_collect_plane, dim3(nx, rows), 256, 0, st)(d_odb, sel, sp);
         }
         CKL();
         {
             PROF("k_rescore", st);
-            k_rescore<<<dim3(148, rows), 256, 0, st>>>(d_odb, sel, sp, d_pocc, d_pphi);
+            pdl(k_rescore, dim3(148, rows), 256, 0, st)(d_odb, sel, sp, d_pocc, d_pphi);
         }
         CKL();
         if (direct_active || late_active) {
             PROF("k_direct_score", st);
-            k_direct_score<<<dim3(64, rows), 256, 0, st>>>(d_odb, sel, sp, d_pphi);
+            pdl(k_direct_score, dim3(64, rows), 256, 0, st)(d_odb, sel, sp, d_pphi);
             CKL();
         }
         {
             PROF("k_tiebreak", st);
-            k_tiebreak<<<dim3(64, rows), 256, 0, st>>>(d_odb, sel, sp);
+            pdl(k_tiebreak, dim3(64, rows), 256, 0, st)(d_odb, sel, sp);
         }
         CKL();
         if (fuse && !gate) {
             // the packing loop's decision in the same launch
             PROF("k_finalize", st);
-            k_finalize_decide<<<1, 128, 0, st>>>(d_odb, sel, sp, d_out, n, decide);
+            pdl(k_finalize_decide, 1, 128, 0, st)(d_odb, sel, sp, d_out, n, decide);
             fused = true;
         } else {
             PROF("k_finalize", st);
-            k_finalize<<<(n + 127) / 128, 128, 0, st>>>(d_odb, sel, sp, d_out, n);
+            pdl(k_finalize, (n + 127) / 128, 128, 0, st)(d_odb, sel, sp, d_out, n);
         }
         CKL();
         return PSB_OK;
@@ -1559,7 +1560,7 @@ struct psb_tray {
                 FwdSrc src{SRC_ITEM, nullptr, 0, 0, 0, nullptr, nullptr, d_Bi, sBi};
                 {
                     PROF("k_fwd_plane", st);
-                    ffb<<<dim3(bx, 6), 256, smf, st>>>(src, d_bases_in, g.p[1].tw, g.p[2].tw);
+                    pdl(ffb, dim3(bx, 6), 256, smf, st)(src, d_bases_in, g.p[1].tw, g.p[2].tw);
                 }
                 CKL();
                 CK(cudaMemsetAsync(d_smin, 0xff, sizeof(unsigned long long) * n, st));
@@ -1589,24 +1590,24 @@ struct psb_tray {
             // CTA rows loop over them instead of a row per orientation
             const int rows = g_active_grid > 0 ? std::min(n, g_active_grid) : n;
             if (g_active_grid > 0) {
-                k_active_list<<<1, 32, 0, st>>>(d_odb, n, d_act, d_nact, d_srch, d_nsrch);
+                pdl(k_active_list, 1, 32, 0, st)(d_odb, n, d_act, d_nact, d_srch, d_nsrch);
                 CKL();
                 act_ready = true;
             }
             FwdSrc src{SRC_ITEM, nullptr, 0, 0, 0, nullptr, nullptr, d_Bi, sBi, nullptr,
                        act_ready ? d_act : nullptr, act_ready ? d_nact : nullptr};
             PROF("k_fwd_plane", st);
-            ff<<<dim3(exmax, rows), 256, smf, st>>>(src, d_odb, g.p[1].tw, g.p[2].tw);
+            pdl(ff, dim3(exmax, rows), 256, smf, st)(src, d_odb, g.p[1].tw, g.p[2].tw);
         } else {
             {
                 PROF("k_rfft_z", st);
-                k_rfft_z<<<dim3((maxpairs + PSB_PAIRS - 1) / PSB_PAIRS, n), PSB_THREADS, smem_rz(g.F[2]), st>>>(
+                pdl(k_rfft_z, dim3((maxpairs + PSB_PAIRS - 1) / PSB_PAIRS, n), PSB_THREADS, smem_rz(g.F[2]), st)(
                     d_rzs, d_odb, g.p[2].p, g.p[2].tw);
             }
             CKL();
             {
                 PROF("k_fft_mid_fwd", st);
-                k_fft_mid<-1><<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, exmax, n), PSB_THREADS, smem_mid(g.F[1]), st>>>(
+                pdl(k_fft_mid<-1>, dim3((g.H + PSB_TILE - 1) / PSB_TILE, exmax, n), PSB_THREADS, smem_mid(g.F[1]), st)(
                     d_mids, d_odb, g.p[1].p, g.p[1].tw);
             }
         }
@@ -1645,21 +1646,21 @@ struct psb_tray {
             if (xf) {
                 PROF("k_xpass", st);
                 int ncols = g.F[1] * g.H;
-                xf<<<dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, m), 256, xpass2_smem(g.F[0]), st>>>(
+                pdl(xf, dim3((ncols + PSB_XCOLS - 1) / PSB_XCOLS, m), 256, xpass2_smem(g.F[0]), st)(
                     odo, sbo, d_Socc, d_Sphi, ncols, g.p[0].tw, nullptr, 0, BaseMap{0, 0, 0, nullptr, nullptr});
             } else {
                 PROF("k_xpass", st);
                 size_t smx = sizeof(float2) * (g.F[0] + 4 * PSB_TILE * g.F[0]);
-                k_xpass<<<dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], m), PSB_THREADS, smx, st>>>(
+                pdl(k_xpass, dim3((g.H + PSB_TILE - 1) / PSB_TILE, g.F[1], m), PSB_THREADS, smx, st)(
                     odo, sbo, d_Socc, d_Sphi, g.F[1], g.H, g.p[0].p, g.p[0].tw);
             }
             CKL();
             if (pf) {
                 PROF("k_plane", st);
-                pf<<<dim3(nx, m), pthreads, sm2, st>>>(odo, sbo, pbo, sp, g.p[1].tw, g.p[2].tw);
+                pdl(pf, dim3(nx, m), pthreads, sm2, st)(odo, sbo, pbo, sp, g.p[1].tw, g.p[2].tw);
             } else {
                 PROF("k_plane", st);
-                k_plane<<<dim3(nx, m), PSB_THREADS, smp, st>>>(odo, sbo, pbo, sp, g.F[1], g.F[2], g.p[1].p,
+                pdl(k_plane, dim3(nx, m), PSB_THREADS, smp, st)(odo, sbo, pbo, sp, g.F[1], g.F[2], g.p[1].p,
                                                                 g.p[2].p, g.p[1].tw, g.p[2].tw);
             }
             CKL();
@@ -1672,11 +1673,11 @@ struct psb_tray {
             TRY(flood_fill(d_odb, n, sp, gate, nullptr));
             SelectBufs sel{d_reach,   sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
                            d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, gate};
-            k_sel_reset<<<1, 128, 0, st>>>(sel, n);
+            pdl(k_sel_reset, 1, 128, 0, st)(sel, n);
             CKL();
             {
                 PROF("k_plane_min", st);
-                k_plane_min<<<dim3(nx, n), PSB_PMIN_THREADS, 0, st>>>(d_odb, sel, sp);
+                pdl(k_plane_min, dim3(nx, n), PSB_PMIN_THREADS, 0, st)(d_odb, sel, sp);
             }
             CKL();
             return select(d_reach, gate);
@@ -1687,7 +1688,7 @@ struct psb_tray {
             SelectBufs sel{d_free,    sBits,  d_Dq,     sD,       d_smin, d_cand,        d_ncand, d_cscore, d_best,
                            d_bestkey, d_diag, d_errmax, kCandCap, d_pmin, (long long)nx, nullptr};
             PROF("k_plane_min", st);
-            k_plane_min<<<dim3(nx, n), PSB_PMIN_THREADS, 0, st>>>(d_odb, sel, sp);
+            pdl(k_plane_min, dim3(nx, n), PSB_PMIN_THREADS, 0, st)(d_odb, sel, sp);
             CKL();
         }
         if (!interlock) {
@@ -1698,7 +1699,7 @@ struct psb_tray {
             TRY(select(d_free, nullptr));
             {
                 PROF("k_line_check", st);
-                k_line_check<<<1, 192, 0, st>>>(d_odb, d_out, n, d_free, sBits, sp, d_needff);
+                pdl(k_line_check, 1, 192, 0, st)(d_odb, d_out, n, d_free, sBits, sp, d_needff);
             }
             CKL();
             TRY(reach_select(d_needff));
@@ -1738,7 +1739,7 @@ struct psb_tray {
         CK(cudaMemcpyAsync(d_od, &od, sizeof(OrientDesc), cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(d_first, 0xff, sizeof(unsigned long long), st));
         int blocks = std::max(1, std::min(1024, (od.nvox + 255) / 256));
-        k_place_check<<<blocks, 256, 0, st>>>(d_od, d_tray, nx, ny, nz, px, py, pz, d_first);
+        pdl(k_place_check, blocks, 256, 0, st)(d_od, d_tray, nx, ny, nz, px, py, pz, d_first);
         CKL();
         unsigned long long first = 0;
         CK(cudaMemcpyAsync(&first, d_first, sizeof(first), cudaMemcpyDeviceToHost, st));
@@ -1750,7 +1751,7 @@ struct psb_tray {
                         "(place_in_tray): Item to be placed intersects with contents of tray at position (%d, %d, %d)",
                         i, j, k);
         }
-        k_place_write<<<blocks, 256, 0, st>>>(d_od, d_tray, nx, ny, nz, px, py, pz, id);
+        pdl(k_place_write, blocks, 256, 0, st)(d_od, d_tray, nx, ny, nz, px, py, pz, id);
         CKL();
         TRY(prefix_occ());
         TRY(rebuild_occ());
@@ -1894,7 +1895,7 @@ int linear_transform_product(const int32_t* a, const int32_t* b, int nx, int ny,
     TRY(forward3(g, rb, W1, W2, Sb, d_rz + 1, d_mid, st));
     {
         PROF("k_spec_mul", st);
-        k_spec_mul<<<grid1d(S), 256, 0, st>>>(Sa, Sb, Sa, S, conj_b);
+        pdl(k_spec_mul, grid1d(S), 256, 0, st)(Sa, Sb, Sa, S, conj_b);
     }
     CKL();
     CK(cudaStreamSynchronize(st));
@@ -2010,21 +2011,21 @@ struct psb_proposal {
         for (int i = 0; i < 4; ++i) {
             const long long n = (long long)S * (D[i] / 2) * (D[i] / 2) * (D[i] / 2);
             PROF("k_prop_conv", s);
-            k_conv_fwd<<<dim3(g1(n), co[i] / PSB_CPT), 256, sizeof(float) * PSB_CPT * ci[i] * 27, s>>>(
+            pdl(k_conv_fwd, dim3(g1(n), co[i] / PSB_CPT), 256, sizeof(float) * PSB_CPT * ci[i] * 27, s)(
                 in[i], S, ci[i], D[i], P16 + kProp.c[i].w, P + kProp.c[i].b, out[i], co[i]);
             CKL();
         }
         PROF("k_prop_head", s);
-        k_lin_fwd<<<g1((long long)S * 64), 256, 0, s>>>(a4, S, 512, P16 + kProp.f1.w, P + kProp.f1.b, 64, 1, f1);
+        pdl(k_lin_fwd, g1((long long)S * 64), 256, 0, s)(a4, S, 512, P16 + kProp.f1.w, P + kProp.f1.b, 64, 1, f1);
         CKL();
-        k_lin_fwd<<<g1((long long)B * 64), 256, 0, s>>>(hmaps, B, PSB_PH * PSB_PH, P16 + kProp.f2.w, P + kProp.f2.b,
+        pdl(k_lin_fwd, g1((long long)B * 64), 256, 0, s)(hmaps, B, PSB_PH * PSB_PH, P16 + kProp.f2.w, P + kProp.f2.b,
                                                         64, 1, t);
         CKL();
-        k_concat<<<g1((long long)S * 128), 256, 0, s>>>(f1, t, S, no, hin);
+        pdl(k_concat, g1((long long)S * 128), 256, 0, s)(f1, t, S, no, hin);
         CKL();
-        k_lin_fwd<<<g1((long long)S * 64), 256, 0, s>>>(hin, S, 128, P16 + kProp.h1.w, P + kProp.h1.b, 64, 1, h1);
+        pdl(k_lin_fwd, g1((long long)S * 64), 256, 0, s)(hin, S, 128, P16 + kProp.h1.w, P + kProp.h1.b, 64, 1, h1);
         CKL();
-        k_lin_fwd<<<g1(S), 256, 0, s>>>(h1, S, 64, P16 + kProp.h2.w, P + kProp.h2.b, 1, 0, logit);
+        pdl(k_lin_fwd, g1(S), 256, 0, s)(h1, S, 64, P16 + kProp.h2.w, P + kProp.h2.b, 1, 0, logit);
         CKL();
         return PSB_OK;
     }
@@ -2040,11 +2041,11 @@ struct psb_proposal {
         for (int i = 0; i < 4; ++i) {
             const long long n = (long long)S * (D[i] / 2) * (D[i] / 2) * (D[i] / 2);
             PROF("k_prop_conv", s);
-            k_conv_fwd<<<dim3(g1(n), co[i] / PSB_CPT), 256, sizeof(float) * PSB_CPT * ci[i] * 27, s>>>(
+            pdl(k_conv_fwd, dim3(g1(n), co[i] / PSB_CPT), 256, sizeof(float) * PSB_CPT * ci[i] * 27, s)(
                 in[i], S, ci[i], D[i], P16 + kProp.c[i].w, P + kProp.c[i].b, out[i], co[i]);
             CKL();
         }
-        k_lin_fwd<<<g1((long long)S * 64), 256, 0, s>>>(a4, S, 512, P16 + kProp.f1.w, P + kProp.f1.b, 64, 1, f1);
+        pdl(k_lin_fwd, g1((long long)S * 64), 256, 0, s)(a4, S, 512, P16 + kProp.f1.w, P + kProp.f1.b, 64, 1, f1);
         CKL();
         return PSB_OK;
     }
@@ -2056,26 +2057,26 @@ struct psb_proposal {
         auto g1 = [](long long n) { return (unsigned)((n + 255) / 256); };
         CK(cudaMemsetAsync(G, 0, sizeof(float) * kProp.n, s));
         CK(cudaMemsetAsync(loss, 0, sizeof(float), s));
-        k_softmax_ce<<<(B + 7) / 8, 256, 0, s>>>(logit, target, mask, B, no, dlogit, loss);
+        pdl(k_softmax_ce, (B + 7) / 8, 256, 0, s)(logit, target, mask, B, no, dlogit, loss);
         CKL();
-        k_lin_bwd_weight<<<dim3(g1(64), 1), 256, 0, s>>>(dlogit, h1, S, 1, 64, G + kProp.h2.w, G + kProp.h2.b);
+        pdl(k_lin_bwd_weight, dim3(g1(64), 1), 256, 0, s)(dlogit, h1, S, 1, 64, G + kProp.h2.w, G + kProp.h2.b);
         CKL();
-        k_lin_bwd_data<<<g1((long long)S * 64), 256, 0, s>>>(dlogit, S, 1, P16 + kProp.h2.w, 64, h1, dh1);
+        pdl(k_lin_bwd_data, g1((long long)S * 64), 256, 0, s)(dlogit, S, 1, P16 + kProp.h2.w, 64, h1, dh1);
         CKL();
-        k_lin_bwd_weight<<<dim3(g1(128), 64), 256, 0, s>>>(dh1, hin, S, 64, 128, G + kProp.h1.w, G + kProp.h1.b);
+        pdl(k_lin_bwd_weight, dim3(g1(128), 64), 256, 0, s)(dh1, hin, S, 64, 128, G + kProp.h1.w, G + kProp.h1.b);
         CKL();
-        k_lin_bwd_data<<<g1((long long)S * 128), 256, 0, s>>>(dh1, S, 64, P16 + kProp.h1.w, 128, nullptr, dhin);
+        pdl(k_lin_bwd_data, g1((long long)S * 128), 256, 0, s)(dh1, S, 64, P16 + kProp.h1.w, 128, nullptr, dhin);
         CKL();
-        k_split_item<<<g1((long long)S * 64), 256, 0, s>>>(dhin, f1, S, df1);
+        pdl(k_split_item, g1((long long)S * 64), 256, 0, s)(dhin, f1, S, df1);
         CKL();
-        k_split_tray<<<g1((long long)B * 64), 256, 0, s>>>(dhin, t, B, no, dt);
+        pdl(k_split_tray, g1((long long)B * 64), 256, 0, s)(dhin, t, B, no, dt);
         CKL();
-        k_lin_bwd_weight<<<dim3(g1(PSB_PH * PSB_PH), 64), 256, 0, s>>>(dt, hmaps, B, 64, PSB_PH * PSB_PH,
+        pdl(k_lin_bwd_weight, dim3(g1(PSB_PH * PSB_PH), 64), 256, 0, s)(dt, hmaps, B, 64, PSB_PH * PSB_PH,
                                                                        G + kProp.f2.w, G + kProp.f2.b);
         CKL();
-        k_lin_bwd_weight<<<dim3(g1(512), 64), 256, 0, s>>>(df1, a4, S, 64, 512, G + kProp.f1.w, G + kProp.f1.b);
+        pdl(k_lin_bwd_weight, dim3(g1(512), 64), 256, 0, s)(df1, a4, S, 64, 512, G + kProp.f1.w, G + kProp.f1.b);
         CKL();
-        k_lin_bwd_data<<<g1((long long)S * 512), 256, 0, s>>>(df1, S, 64, P16 + kProp.f1.w, 512, a4, da4);
+        pdl(k_lin_bwd_data, g1((long long)S * 512), 256, 0, s)(df1, S, 64, P16 + kProp.f1.w, 512, a4, da4);
         CKL();
         const int ci[4] = {1, 16, 32, 64}, co[4] = {16, 32, 64, 64}, D[4] = {32, 16, 8, 4};
         const float* in[4] = {grids, a1, a2, a3};
@@ -2087,14 +2088,14 @@ struct psb_proposal {
             const int nch = (S + chunk - 1) / chunk;
             {
                 PROF("k_prop_bwd_weight", s);
-                k_conv_bwd_weight<<<dim3(ci[i], co[i], nch), 256, 0, s>>>(dout[i], in[i], S, ci[i], D[i], co[i], chunk,
+                pdl(k_conv_bwd_weight, dim3(ci[i], co[i], nch), 256, 0, s)(dout[i], in[i], S, ci[i], D[i], co[i], chunk,
                                                                           G + kProp.c[i].w, G + kProp.c[i].b);
             }
             CKL();
             if (i > 0) {
                 const long long n = (long long)S * D[i] * D[i] * D[i];
                 PROF("k_prop_bwd_data", s);
-                k_conv_bwd_data<<<dim3(g1(n), ci[i]), 256, sizeof(float) * co[i] * 27, s>>>(
+                pdl(k_conv_bwd_data, dim3(g1(n), ci[i]), 256, sizeof(float) * co[i] * 27, s)(
                     dout[i], S, ci[i], D[i], P16 + kProp.c[i].w, co[i], in[i], 1, dout[i - 1]);
                 CKL();
             }
@@ -2168,6 +2169,7 @@ struct NoAllocSetup {
 };
 
 __global__ void k_noalloc_setup(NoAllocSetup s) {
+    pdl_enter();
     if (blockIdx.x == 0 && threadIdx.x < 2) s.d_rz[threadIdx.x] = s.rz[threadIdx.x];
     if (blockIdx.x == 0 && threadIdx.x < 6) s.d_mid[threadIdx.x] = s.mid[threadIdx.x];
     // tw[a][i] = exp(-2 pi i / F), in double precision, rounded to float
@@ -2249,11 +2251,11 @@ int psb_dft_corr3_noalloc(const int32_t* d_a, const int32_t* d_b, int nx, int ny
                         g.H, -1, 0, nullptr};
     // every byte the transforms read is written first in stream order, so
     // nothing in the array needs clearing
-    k_noalloc_setup<<<4, 256, 0, st>>>(su);
+    pdl(k_noalloc_setup, 4, 256, 0, st)(su);
     CKL();
     TRY(forward3_dev(g, su.d_rz + 0, su.d_mid + 0, st));
     TRY(forward3_dev(g, su.d_rz + 1, su.d_mid + 2, st));
-    k_spec_mul<<<grid1d(S), 256, 0, st>>>(Sa, Sb, Sa, S, 1);
+    pdl(k_spec_mul, grid1d(S), 256, 0, st)(Sa, Sb, Sa, S, 1);
     CKL();
     TRY(inverse3_dev(g, W1, d_out, su.d_mid + 4, st));
     return PSB_OK;
@@ -2334,7 +2336,7 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
     int32_t* dcoll = (int32_t*)t->d_Dq;  // slot 0 proximity buffer reused as int32 scratch
     CK(cudaMemcpyAsync(dcoll, coll.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, t->st));
     CK(cudaMemcpyAsync(t->d_od, &od, sizeof(od), cudaMemcpyHostToDevice, t->st));
-    k_bits_from_coll<<<grid1d((size_t)nx * ny), 256, 0, t->st>>>(dcoll, t->d_free, nx, ny, nz, t->nzw, od.valid[0],
+    pdl(k_bits_from_coll, grid1d((size_t)nx * ny), 256, 0, t->st)(dcoll, t->d_free, nx, ny, nz, t->nzw, od.valid[0],
                                                                    od.valid[1], od.valid[2]);
     CKL();
     CK(cudaMemsetAsync(t->d_err, 0, sizeof(unsigned int), t->st));
@@ -2347,21 +2349,21 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
     CK(cudaMemsetAsync(t->d_total, 0, sizeof(int), t->st));
     {
         PROF("k_ff_runs", t->st);
-        k_ff_runs<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+        pdl(k_ff_runs, gl, 256, 0, t->st)(t->d_od, fb, sp);
     }
     {
         PROF("k_ff_union", t->st);
-        k_ff_union<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+        pdl(k_ff_union, gl, 256, 0, t->st)(t->d_od, fb, sp);
     }
     {
         PROF("k_ff_seed", t->st);
-        k_ff_seed<<<dim3(296, 1), 256, 0, t->st>>>(t->d_od, fb);
+        pdl(k_ff_seed, dim3(296, 1), 256, 0, t->st)(t->d_od, fb);
     }
     {
         PROF("k_ff_reach", t->st);
-        k_ff_reach<<<gl, 256, 0, t->st>>>(t->d_od, fb, sp);
+        pdl(k_ff_reach, gl, 256, 0, t->st)(t->d_od, fb, sp);
     }
-    k_bits_to_mask<<<grid1d(V), 256, 0, t->st>>>(t->d_reach, dcoll, nx, ny, nz, t->nzw);
+    pdl(k_bits_to_mask, grid1d(V), 256, 0, t->st)(t->d_reach, dcoll, nx, ny, nz, t->nzw);
     CKL();
     unsigned int herr = 0;
     CK(cudaMemcpyAsync(out, dcoll, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, t->st));
@@ -2822,7 +2824,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             for (int a = 0; a < 3; ++a) G[3 * it + a] = (inf.dims[a] + sc - 1) / sc;
             const int nv = (int)inf.vox.size();
             if (nv > 0)
-                k_base_grid<<<(nv + 255) / 256, 256, 0, t->st>>>(t->d_stage_vox + t->staged_voff[it], nv, sc,
+                pdl(k_base_grid, (nv + 255) / 256, 256, 0, t->st)(t->d_stage_vox + t->staged_voff[it], nv, sc,
                                                                  d_pgrid + (size_t)it * PSB_PG3);
             CKL();
         }
@@ -2835,7 +2837,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             const int m = std::min(kChunk, n_items - i0);
             {
                 PROF("k_prop_inputs", t->st);
-                k_orient_grids<<<dim3(PSB_PG3 / 256, n_orient, m), 256, 0, t->st>>>(
+                pdl(k_orient_grids, dim3(PSB_PG3 / 256, n_orient, m), 256, 0, t->st)(
                     d_pgrid + (size_t)i0 * PSB_PG3, d_pG + 3 * i0, d_pmaps, n_orient, pr->a0);
             }
             CKL();
@@ -2861,10 +2863,10 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
     for (int it = 0; it < n_items; ++it) {
         OrientDesc* d_odb = t->d_od_all + (size_t)it * n_orient;
         for (int o = 0; o < n_orient; ++o) host_ods[o] = all[(size_t)it * n_orient + o];
-        k_prep<<<(n_orient + 63) / 64, 64, 0, t->st>>>(d_odb, n_orient, t->d_ps);
+        pdl(k_prep, (n_orient + 63) / 64, 64, 0, t->st)(d_odb, n_orient, t->d_ps);
         CKL();
         if (d_hm) {
-            k_height_map<<<PSB_PH * PSB_PH, 256, 0, t->st>>>(t->d_tray, t->nx, t->ny, t->nz,
+            pdl(k_height_map, PSB_PH * PSB_PH, 256, 0, t->st)(t->d_tray, t->nx, t->ny, t->nz,
                                                              d_hm + (size_t)it * PSB_PH * PSB_PH);
             CKL();
         }
@@ -2872,17 +2874,17 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             psb_proposal* pr = opt.prop;
             {
                 PROF("k_prop_head", t->st);
-                k_prop_tray_feat<<<64, 256, 0, t->st>>>(d_hm + (size_t)it * PSB_PH * PSB_PH, pr->P16 + kProp.f2.w,
+                pdl(k_prop_tray_feat, 64, 256, 0, t->st)(d_hm + (size_t)it * PSB_PH * PSB_PH, pr->P16 + kProp.f2.w,
                                                         pr->P + kProp.f2.b, pr->t);
                 CKL();
-                k_prop_item_head<<<n_orient, 64, 0, t->st>>>(d_feat + (size_t)it * n_orient * 64, pr->t,
+                pdl(k_prop_item_head, n_orient, 64, 0, t->st)(d_feat + (size_t)it * n_orient * 64, pr->t,
                                                              pr->P16 + kProp.h1.w, pr->P + kProp.h1.b,
                                                              pr->P16 + kProp.h2.w, pr->P + kProp.h2.b, pr->logit);
             }
             CKL();
             {
                 PROF("k_gate", t->st);
-                k_gate<OrientDesc><<<1, 32, 0, t->st>>>(pr->logit, d_odb, n_orient, opt.topk, opt.margin, pr->stats);
+                pdl(k_gate<OrientDesc>, 1, 32, 0, t->st)(pr->logit, d_odb, n_orient, opt.topk, opt.margin, pr->stats);
             }
             CKL();
         }
@@ -2902,7 +2904,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             CK(cudaMemcpyAsync(d_per + (size_t)it * n_orient, t->d_res, sizeof(ResultDev) * n_orient,
                                cudaMemcpyDeviceToDevice, t->st));
         if (!t->fused) {
-            k_decide<<<1, 32, 0, t->st>>>(d_odb, t->d_res, n_orient, t->d_ls, t->d_dec + it, t->d_err, rec);
+            pdl(k_decide, 1, 32, 0, t->st)(d_odb, t->d_res, n_orient, t->d_ls, t->d_dec + it, t->d_err, rec);
             CKL();
         }
         t->fused = false;
@@ -2914,20 +2916,20 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             } else {
                 CK(cudaMemcpyAsync(opt.d_all, opt.d_local, sizeof(ShardRecord), cudaMemcpyDeviceToDevice, t->st));
             }
-            k_decide_merge<<<1, 1, 0, t->st>>>((const ShardRecord*)opt.d_all, opt.world, t->d_ls, t->d_dec + it);
+            pdl(k_decide_merge, 1, 1, 0, t->st)((const ShardRecord*)opt.d_all, opt.world, t->d_ls, t->d_dec + it);
             CKL();
         }
         {
             PROF("k_place_check", t->st);
-            k_place_check_g<<<64, 256, 0, t->st>>>(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
+            pdl(k_place_check_g, 64, 256, 0, t->st)(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
         }
         CKL();
         {
             PROF("k_place_write", t->st);
-            k_place_write_g<<<64, 256, 0, t->st>>>(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
+            pdl(k_place_write_g, 64, 256, 0, t->st)(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
         }
         CKL();
-        k_place_done<<<1, 32, 0, t->st>>>(d_odb, t->d_ls, t->d_dec + it);
+        pdl(k_place_done, 1, 32, 0, t->st)(d_odb, t->d_ls, t->d_dec + it);
         CKL();
         {
             // the placed item's columns: occupancy prefix sums and the
@@ -2935,7 +2937,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             size_t box = 1;
             for (auto& o : host_ods) box = std::max(box, (size_t)o.e[0] * o.e[1]);
             PROF("k_box_refresh", t->st);
-            k_box_refresh<<<(unsigned)((box + 7) / 8), 256, 0, t->st>>>(t->d_tray, t->d_pocc, filt ? t->d_tbits : nullptr,
+            pdl(k_box_refresh, (unsigned)((box + 7) / 8), 256, 0, t->st)(t->d_tray, t->d_pocc, filt ? t->d_tbits : nullptr,
                                                                          t->tq, t->nx, t->ny, t->nz, t->d_ls, d_odb);
         }
         CKL();
@@ -3136,7 +3138,7 @@ int psb_prop_adam_step(psb_proposal* p, float lr, float beta1, float beta2, floa
     p->step += 1;
     const float c1 = 1.f - std::pow(beta1, (float)p->step), c2 = 1.f - std::pow(beta2, (float)p->step);
     const long long n = (long long)kProp.n;
-    k_adam<<<(unsigned)((n + 255) / 256), 256, 0, p->st>>>(p->P, p->G, p->M, p->V, p->P16, p->isw, n, lr, beta1,
+    pdl(k_adam, (unsigned)((n + 255) / 256), 256, 0, p->st)(p->P, p->G, p->M, p->V, p->P16, p->isw, n, lr, beta1,
                                                             beta2, eps, c1, c2);
     CKL();
     CK(cudaStreamSynchronize(p->st));

@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "psb_pdl.cuh"
+
 #define PSB_MAX_FFT 512
 #define PSB_MAX_STAGES 12
 

@@ -33,6 +33,7 @@
 // One warp per column, one ballot per 32 cells.  grid: ceil(nx*ny / 8), block 256
 __global__ void k_tray_bits(const int32_t* __restrict__ tray, int nx, int ny, int nz, int nq,
                             uint4* __restrict__ tbits) {
+    pdl_enter();
     const int col = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (col >= nx * ny) return;
@@ -51,6 +52,7 @@ __global__ void k_tray_bits(const int32_t* __restrict__ tray, int nx, int ny, in
 // grid: n, block 32
 template <int NQ>
 __global__ void k_cand_prep(const OrientDesc* __restrict__ orients, int4* __restrict__ fs, int* __restrict__ fbound) {
+    pdl_enter();
     constexpr int NW = 4 * NQ;
     const int o = blockIdx.x, lane = threadIdx.x;
     const OrientDesc& od = orients[o];
@@ -244,6 +246,7 @@ k_cand_filter(const OrientDesc* __restrict__ orients, const uint4* __restrict__ 
               uint32_t* __restrict__ cand, long long sBits, unsigned char* __restrict__ candplane, long long pstride,
               int* __restrict__ ccount, const int4* __restrict__ fs, const int* __restrict__ fbound, int cut_pct,
               int* __restrict__ clist, int ccap, int nz) {
+    pdl_enter();
     constexpr int NW = 4 * NQ;
     const int o = blockIdx.y, x = blockIdx.x;
     const OrientDesc& od = orients[o];
@@ -289,6 +292,7 @@ k_cand_filter_plane(const OrientDesc* __restrict__ orients, int n, const uint4* 
                     unsigned char* __restrict__ candplane, long long pstride, int* __restrict__ ccount,
                     const int4* __restrict__ fs, const int* __restrict__ fbound, int cut_pct,
                     int* __restrict__ clist, int ccap, int nz) {
+    pdl_enter();
     constexpr int NW = 4 * NQ;
     extern __shared__ uint4 win[];   // [E][ny][NQ]
     const int x = blockIdx.x;
@@ -340,6 +344,7 @@ k_cand_filter_plane(const OrientDesc* __restrict__ orients, int n, const uint4* 
 // orientation without a free cell is skipped.  grid: ceil(n / 128), block 128
 __global__ void k_cand_apply(OrientDesc* __restrict__ orients, int n, const int* __restrict__ count, int stage,
                              int direct_max) {
+    pdl_enter();
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
     OrientDesc& od = orients[o];
@@ -357,6 +362,7 @@ __global__ void k_cand_apply(OrientDesc* __restrict__ orients, int n, const int*
 // cols[o][k], k < ncol[o] (any order).  grid: (max e[0], n), block 64
 __global__ void k_item_cols(const OrientDesc* __restrict__ orients, uint4* __restrict__ cols, long long cstride,
                             int* __restrict__ ncol) {
+    pdl_enter();
     const int o = blockIdx.y, a = blockIdx.x;
     const OrientDesc& od = orients[o];
     if (od.skip || !od.direct || a >= od.e[0]) return;
@@ -396,6 +402,7 @@ k_cand_verify_list(const OrientDesc* __restrict__ orients, int n, const uint4* _
                    int ccap, const int* __restrict__ ccount, const uint4* __restrict__ cols, long long cstride,
                    const int* __restrict__ ncol, int* __restrict__ vcount, unsigned char* __restrict__ okplane,
                    long long pstride, int set_okplane) {
+    pdl_enter();
     extern __shared__ int pre[];   // pre[o]: direct candidates of orientations before o
     if (threadIdx.x < 32) {
         // warp 0: the orientations' counts loaded in parallel, an exclusive scan
@@ -503,6 +510,7 @@ __device__ __forceinline__ void k_direct_score_body(const int o, const OrientDes
 __global__ void __launch_bounds__(256)
 
 k_direct_score(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pphi) {
+    pdl_enter();
     if (!sb.srch) {
         const int o = blockIdx.y;
         k_direct_score_body(o, orients, sb, sp, pphi);

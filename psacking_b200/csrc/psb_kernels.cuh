@@ -89,6 +89,7 @@ __device__ __forceinline__ void col_prefix(const int32_t* __restrict__ src, int3
 template <int MODE>
 __global__ void k_col_prefix(const int32_t* __restrict__ src, int32_t* __restrict__ P, int ncols, int nz,
                              const int* gate) {
+    pdl_enter();
     if (gate && !*gate) return;
     const int col = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (col >= ncols) return;
@@ -133,6 +134,7 @@ struct RzDesc {
 __global__ void __launch_bounds__(PSB_THREADS)
 k_rfft_z(const RzDesc* __restrict__ descs, const OrientDesc* __restrict__ orients,
          AxisPlan plan, const float2* __restrict__ g_tw) {
+    pdl_enter();
     extern __shared__ float2 sm[];
     const RzDesc d = descs[blockIdx.y];
     if (d.gate && !*d.gate) return;
@@ -198,6 +200,7 @@ k_rfft_z(const RzDesc* __restrict__ descs, const OrientDesc* __restrict__ orient
 __global__ void __launch_bounds__(PSB_THREADS)
 k_irfft_z_int(const float2* __restrict__ in, int32_t* __restrict__ out, int nlines, int n2,
               float scale, AxisPlan plan, const float2* __restrict__ g_tw) {
+    pdl_enter();
     extern __shared__ float2 sm[];
     const int N = plan.n, Hz = N / 2 + 1;
     const int npairs = (nlines + 1) / 2;
@@ -255,6 +258,7 @@ template <int DIR>
 __global__ void __launch_bounds__(PSB_THREADS)
 k_fft_mid(const MidDesc* __restrict__ descs, const OrientDesc* __restrict__ orients, AxisPlan plan,
           const float2* __restrict__ g_tw) {
+    pdl_enter();
     extern __shared__ float2 sm[];
     MidDesc d = descs[blockIdx.z];
     if (d.gate && !*d.gate) return;
@@ -296,6 +300,7 @@ k_fft_mid(const MidDesc* __restrict__ descs, const OrientDesc* __restrict__ orie
 // out = conj(b) * a (corr) or a * b (conv)
 __global__ void k_spec_mul(const float2* __restrict__ a, const float2* __restrict__ b, float2* __restrict__ out,
                            size_t n, int conj_b) {
+    pdl_enter();
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         float2 x = a[i], y = b[i];
         out[i] = conj_b ? c_cmul(y, x) : c_mul(x, y);
@@ -335,6 +340,7 @@ struct SearchBufs {
 // which would only read their descriptor and exit.  grid 1, block 32
 __global__ void k_active_list(const OrientDesc* __restrict__ od, int n, int* __restrict__ act, int* __restrict__ nact,
                               int* __restrict__ srch, int* __restrict__ nsrch) {
+    pdl_enter();
     int base = 0, sbase = 0;
     const unsigned int below = (1u << threadIdx.x) - 1u;
     for (int o0 = 0; o0 < n; o0 += 32) {
@@ -357,6 +363,7 @@ __global__ void k_active_list(const OrientDesc* __restrict__ od, int n, int* __r
 __global__ void __launch_bounds__(PSB_THREADS)
 k_xpass(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __restrict__ Socc,
         const float2* __restrict__ Sphi, int Fy, int Hz, AxisPlan plan, const float2* __restrict__ g_tw) {
+    pdl_enter();
     extern __shared__ float2 sm[];
     const int o = blockIdx.z;
     const OrientDesc& od = orients[o];
@@ -464,6 +471,7 @@ struct PlaneBufs {
 __global__ void __launch_bounds__(PSB_THREADS)
 k_plane(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, ScoreParams sp, int Fy, int Fz,
         AxisPlan py, AxisPlan pz, const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
+    pdl_enter();
     extern __shared__ float2 sm[];
     const int o = blockIdx.y;
     const OrientDesc& od = orients[o];

@@ -68,6 +68,7 @@ __device__ __forceinline__ float ford_val(unsigned int k) {
 #define PSB_PMIN_THREADS (PSB_PMIN_ZL * PSB_PMIN_RG)
 __global__ void __launch_bounds__(PSB_PMIN_THREADS)
 k_plane_min(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    pdl_enter();
     if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.y, x = blockIdx.x;
     const OrientDesc& od = orients[o];
@@ -210,6 +211,7 @@ __device__ __forceinline__ void k_collect_plane_body(const int o, const OrientDe
 __global__ void __launch_bounds__(256)
 
 k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    pdl_enter();
     if (!sb.srch) {
         const int o = blockIdx.y;
         k_collect_plane_body(o, orients, sb, sp);
@@ -225,6 +227,7 @@ k_collect_plane(const OrientDesc* __restrict__ orients, SelectBufs sb, ScorePara
 // per-orientation selection state back to "nothing seen" (the gated second
 // round of the lazy interlocking search)
 __global__ void k_sel_reset(SelectBufs sb, int n) {
+    pdl_enter();
     if (sb.gate && !*sb.gate) return;
     for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x) {
         sb.smin[o] = 0xffffffffffffffffULL;
@@ -312,6 +315,7 @@ __global__ void __launch_bounds__(256)
 
 k_rescore(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, const int32_t* __restrict__ pocc,
           const int32_t* __restrict__ pphi) {
+    pdl_enter();
     if (!sb.srch) {
         const int o = blockIdx.y;
         k_rescore_body(o, orients, sb, sp, pocc, pphi);
@@ -348,6 +352,7 @@ __device__ __forceinline__ void k_tiebreak_body(const int o, const OrientDesc* _
 
 __global__ void 
 k_tiebreak(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp) {
+    pdl_enter();
     if (!sb.srch) {
         const int o = blockIdx.y;
         k_tiebreak_body(o, orients, sb, sp);
@@ -365,6 +370,7 @@ k_tiebreak(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp
 // transforms (direct = 2); k_collect_plane takes all its ok cells and
 // k_direct_score scores them by exact sums.  grid: ceil(n / 128), block 128
 __global__ void k_late_direct(OrientDesc* __restrict__ orients, int n, const int* __restrict__ okcount, int late_max) {
+    pdl_enter();
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
     OrientDesc& od = orients[o];
@@ -414,6 +420,7 @@ __device__ __forceinline__ void finalize_one(const OrientDesc* __restrict__ orie
 
 __global__ void k_finalize(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, ResultDev* out,
                            int n) {
+    pdl_enter();
     if (sb.gate && !*sb.gate) return;
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
@@ -459,6 +466,7 @@ __device__ __forceinline__ int best_result(const OrientDesc* __restrict__ orient
 // grid: 1, block 192 (one warp per ray)
 __global__ void k_line_check(const OrientDesc* __restrict__ orients, const ResultDev* __restrict__ res, int n,
                              const uint32_t* __restrict__ freebits, long long sBits, ScoreParams sp, int* need_ff) {
+    pdl_enter();
     __shared__ int s_best, s_clear;
     if (threadIdx.x < 32) {
         const int best = best_result(orients, res, n);
@@ -632,6 +640,7 @@ __device__ __forceinline__ void k_ff_runs_body(const int o, const OrientDesc* __
 __global__ void __launch_bounds__(256)
 
 k_ff_runs(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    pdl_enter();
     if (!fb.srch) {
         const int o = blockIdx.y;
         k_ff_runs_body(o, orients, fb, sp);
@@ -676,6 +685,7 @@ __device__ __forceinline__ void k_ff_union_body(const int o, const OrientDesc* _
 
 __global__ void 
 k_ff_union(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    pdl_enter();
     if (!fb.srch) {
         const int o = blockIdx.y;
         k_ff_union_body(o, orients, fb, sp);
@@ -705,6 +715,7 @@ __device__ __forceinline__ void k_ff_seed_body(const int o, const OrientDesc* __
 
 __global__ void 
 k_ff_seed(const OrientDesc* __restrict__ orients, FloodBufs fb) {
+    pdl_enter();
     if (!fb.srch) {
         const int o = blockIdx.y;
         k_ff_seed_body(o, orients, fb);
@@ -753,6 +764,7 @@ __device__ __forceinline__ void k_ff_reach_body(const int o, const OrientDesc* _
 
 __global__ void 
 k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp) {
+    pdl_enter();
     if (!fb.srch) {
         const int o = blockIdx.y;
         k_ff_reach_body(o, orients, fb, sp);
@@ -770,6 +782,7 @@ k_ff_reach(const OrientDesc* __restrict__ orients, FloodBufs fb, ScoreParams sp)
 // ---------------------------------------------------------------------------
 __global__ void k_dist_init(const int32_t* __restrict__ g, int32_t* __restrict__ d, size_t V, int far,
                             const int* gate) {
+    pdl_enter();
     if (gate && !*gate) return;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < V; i += (size_t)gridDim.x * blockDim.x)
         d[i] = g[i] == 1 ? 0 : far;
@@ -782,6 +795,7 @@ __global__ void k_dist_init(const int32_t* __restrict__ g, int32_t* __restrict__
 //   axis y: lines l = x*nz+z,        base = x*ny*nz + z,       stride = nz
 //   axis z: lines l = x*ny+y,        base = l*nz,              stride = 1
 __global__ void k_dist_axis(int32_t* __restrict__ d, int axis, int nx, int ny, int nz, int W, const int* gate) {
+    pdl_enter();
     extern __shared__ int32_t sd[];
     if (gate && !*gate) return;
     const int L = axis == 0 ? nx : (axis == 1 ? ny : nz);
@@ -829,6 +843,7 @@ __global__ void k_dist_axis(int32_t* __restrict__ d, int axis, int nx, int ny, i
 
 // fallback for very long lines: sequential in global memory, one thread per line
 __global__ void k_dist_axis_global(int32_t* __restrict__ d, int axis, int nx, int ny, int nz, const int* gate) {
+    pdl_enter();
     if (gate && !*gate) return;
     const int L = axis == 0 ? nx : (axis == 1 ? ny : nz);
     const long long nlines = axis == 0 ? (long long)ny * nz : (axis == 1 ? (long long)nx * nz : (long long)nx * ny);
@@ -843,6 +858,7 @@ __global__ void k_dist_axis_global(int32_t* __restrict__ d, int axis, int nx, in
 // sum and sum of squares (around a shift) for the distance spectrum's mean
 // subtraction; also the max absolute deviation.
 __global__ void k_stats(const int32_t* __restrict__ v, size_t n, int shift, unsigned long long* out) {
+    pdl_enter();
     long long s = 0, s2 = 0;
     int mx = 0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -865,6 +881,7 @@ __global__ void k_stats(const int32_t* __restrict__ v, size_t n, int shift, unsi
 
 // any negative value?
 __global__ void k_any_negative(const int32_t* __restrict__ v, size_t n, unsigned int* flag) {
+    pdl_enter();
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         if (v[i] < 0) { atomicOr(flag, 1u); return; }
 }
@@ -875,6 +892,7 @@ __global__ void k_any_negative(const int32_t* __restrict__ v, size_t n, unsigned
 // first tray cell (row-major) where an item voxel > 0 meets a tray voxel > 0
 __global__ void k_place_check(const OrientDesc* __restrict__ od_p, const int32_t* __restrict__ tray, int nx, int ny,
                               int nz, int px, int py, int pz, unsigned long long* first) {
+    pdl_enter();
     const OrientDesc od = *od_p;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < od.nvox; v += gridDim.x * blockDim.x) {
         int4 q = od.vox[v];
@@ -890,6 +908,7 @@ __global__ void k_place_check(const OrientDesc* __restrict__ od_p, const int32_t
 
 __global__ void k_place_write(const OrientDesc* __restrict__ od_p, int32_t* __restrict__ tray, int nx, int ny, int nz,
                               int px, int py, int pz, int32_t id) {
+    pdl_enter();
     const OrientDesc od = *od_p;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < od.nvox; v += gridDim.x * blockDim.x) {
         int4 q = od.vox[v];
@@ -905,6 +924,7 @@ __global__ void k_place_write(const OrientDesc* __restrict__ od_p, int32_t* __re
 
 // collision_grid post-pass: out-of-tray positions raised to max(c, 1)
 __global__ void k_oob_raise(int32_t* __restrict__ c, int nx, int ny, int nz, int hx, int hy, int hz) {
+    pdl_enter();
     size_t V = (size_t)nx * ny * nz;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < V; t += (size_t)gridDim.x * blockDim.x) {
         int k = (int)(t % nz), j = (int)((t / nz) % ny), i = (int)(t / ((size_t)ny * nz));
@@ -916,6 +936,7 @@ __global__ void k_oob_raise(int32_t* __restrict__ c, int nx, int ny, int nz, int
 // labels for interlocking_free_positions: free = collision 0 and in bounds
 __global__ void k_bits_from_coll(const int32_t* __restrict__ c, uint32_t* __restrict__ bits, int nx, int ny, int nz,
                                  int nzw, int Xv, int Yv, int Zv) {
+    pdl_enter();
     size_t nl = (size_t)nx * ny;
     for (size_t line = blockIdx.x * (size_t)blockDim.x + threadIdx.x; line < nl;
          line += (size_t)gridDim.x * blockDim.x) {
@@ -930,6 +951,7 @@ __global__ void k_bits_from_coll(const int32_t* __restrict__ c, uint32_t* __rest
 
 __global__ void k_bits_to_mask(const uint32_t* __restrict__ bits, int32_t* __restrict__ out, int nx, int ny, int nz,
                                int nzw) {
+    pdl_enter();
     size_t V = (size_t)nx * ny * nz;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < V; t += (size_t)gridDim.x * blockDim.x) {
         size_t line = t / nz;

@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(256)
 k_xpass2(const OrientDesc* __restrict__ orients, SearchBufs sb, const float2* __restrict__ Socc,
          const float2* __restrict__ Sphi, int ncols, const float2* __restrict__ g_tw,
          const unsigned char* __restrict__ okplane, long long okstride, BaseMap bm) {
+    pdl_enter();
     if (!sb.act) {
         xpass2_body<N, MODE, SHARED>(blockIdx.y, orients, sb, Socc, Sphi, ncols, g_tw, okplane, okstride, bm);
         return;
@@ -182,6 +183,7 @@ template <int NY, int NZ>
 __global__ void __launch_bounds__(PSB_PLANE_THREADS, 2)
 k_plane2(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, ScoreParams sp,
          const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
+    pdl_enter();
     constexpr int HZ = NZ / 2 + 1;
     constexpr int RY0 = Plan2<NY>::R0, RY1 = Plan2<NY>::R1;
     constexpr int RZ0 = Plan2<NZ>::R0, RZ1 = Plan2<NZ>::R1;
@@ -355,6 +357,7 @@ template <int NY, int NZ>
 __global__ void __launch_bounds__(256)
 k_fwd_plane(FwdSrc src, const OrientDesc* __restrict__ orients, const float2* __restrict__ g_twy,
             const float2* __restrict__ g_twz) {
+    pdl_enter();
     if (src.gate && !*src.gate) return;
     if (!src.act) {
         fwd_plane_body<NY, NZ>(blockIdx.y, src, orients, g_twy, g_twz);
@@ -379,6 +382,7 @@ template <int N>
 __global__ void __launch_bounds__(256)
 k_xfwd(const float2* __restrict__ in, float2* __restrict__ out, int n0, int ncols, const int* gate,
        const float2* __restrict__ g_tw) {
+    pdl_enter();
     constexpr int C = PSB_XCOLS;
     constexpr int R0 = Plan2<N>::R0, R1 = Plan2<N>::R1;
     extern __shared__ float2 sm[];

@@ -365,6 +365,7 @@ template <int NY, int NZ, int FIELD>
 __global__ void __launch_bounds__(PSB_PLANE3_THREADS, 2)
 k_plane3(const OrientDesc* __restrict__ orients, SearchBufs sb, PlaneBufs pb, ScoreParams sp,
          const float2* __restrict__ g_twy, const float2* __restrict__ g_twz) {
+    pdl_enter();
     if (!sb.act) {
         plane3_body<NY, NZ, FIELD>(blockIdx.y, orients, sb, pb, sp, g_twy, g_twz);
         return;

@@ -32,6 +32,7 @@ struct LoopState {
 
 // error bound and base of every orientation of one item (psb_tray::describe)
 __global__ void k_prep(OrientDesc* __restrict__ od, int n, const PhiStats* __restrict__ ps) {
+    pdl_enter();
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
     OrientDesc& d = od[o];
@@ -126,6 +127,7 @@ __device__ __forceinline__ void decide_warp(const OrientDesc* __restrict__ od, c
 
 __global__ void k_decide(const OrientDesc* __restrict__ od, const ResultDev* __restrict__ res, int n,
                          LoopState* ls, DecisionDev* out, const unsigned int* uf_err, ShardRecord* rec) {
+    pdl_enter();
     if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     decide_warp(od, res, n, ls, out, uf_err, rec);
 }
@@ -142,6 +144,7 @@ struct DecideArgs {
 // grid: 1, block 128
 __global__ void k_finalize_decide(const OrientDesc* __restrict__ orients, SelectBufs sb, ScoreParams sp, ResultDev* res,
                                   int n, DecideArgs da) {
+    pdl_enter();
     for (int o = threadIdx.x; o < n; o += blockDim.x) finalize_one(orients, sb, sp, res, o);
     __syncthreads();
     if (threadIdx.x < 32) decide_warp(orients, res, n, da.ls, da.out, da.uf_err, da.rec);
@@ -153,6 +156,7 @@ __global__ void k_finalize_decide(const OrientDesc* __restrict__ orients, Select
 // places the same item the same way.  Overrides k_decide's local choice.
 // grid: 1, block 1
 __global__ void k_decide_merge(const ShardRecord* __restrict__ all, int world, LoopState* ls, DecisionDev* out) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     int best = -1;
     for (int r = 0; r < world; ++r) {
@@ -183,6 +187,7 @@ __global__ void k_decide_merge(const ShardRecord* __restrict__ all, int world, L
 
 __global__ void k_place_check_g(const OrientDesc* __restrict__ od_item, LoopState* ls, const int32_t* __restrict__ tray,
                                 int nx, int ny, int nz) {
+    pdl_enter();
     if (!ls->do_place) return;
     const OrientDesc& od = od_item[ls->orient];
     const int px = ls->px, py = ls->py, pz = ls->pz;
@@ -200,6 +205,7 @@ __global__ void k_place_check_g(const OrientDesc* __restrict__ od_item, LoopStat
 
 __global__ void k_place_write_g(const OrientDesc* __restrict__ od_item, const LoopState* ls, int32_t* __restrict__ tray,
                                 int nx, int ny, int nz) {
+    pdl_enter();
     if (!ls->do_place || ls->first != 0xffffffffffffffffULL) return;
     const OrientDesc& od = od_item[ls->orient];
     const int px = ls->px, py = ls->py, pz = ls->pz, id = ls->id;
@@ -219,6 +225,7 @@ __global__ void k_place_write_g(const OrientDesc* __restrict__ od_item, const Lo
 // "free" cell that the exact check rejects) marks the item unplaced and
 // raises the run's error word
 __global__ void k_place_done(const OrientDesc* __restrict__ od_item, LoopState* ls, DecisionDev* out) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (!ls->do_place) return;
     if (ls->first != 0xffffffffffffffffULL) {
@@ -238,6 +245,7 @@ __global__ void k_place_done(const OrientDesc* __restrict__ od_item, LoopState* 
 // distance statistics on the device: mean after the first k_stats pass,
 // norm and max after the second
 __global__ void k_phi_mean(PhiStats* ps, unsigned long long V, const int* gate) {
+    pdl_enter();
     if (gate && !*gate) return;
     const long long sum = (long long)ps->raw[0];
     ps->mean = (int)llround((double)sum / (double)V);
@@ -245,6 +253,7 @@ __global__ void k_phi_mean(PhiStats* ps, unsigned long long V, const int* gate) 
 }
 
 __global__ void k_phi_norm(PhiStats* ps, const int* gate) {
+    pdl_enter();
     if (gate && !*gate) return;
     ps->norm = sqrt((double)(long long)ps->raw[1]);
     ps->maxabs = (int)(unsigned int)(ps->raw[2] & 0xffffffffULL);
@@ -253,6 +262,7 @@ __global__ void k_phi_norm(PhiStats* ps, const int* gate) {
 // k_stats with a device-side shift and a gate
 __global__ void k_stats_g(const int32_t* __restrict__ v, size_t n, const int* shiftp, unsigned long long* out,
                           const int* gate) {
+    pdl_enter();
     if (gate && !*gate) return;
     const int shift = shiftp ? *shiftp : 0;
     long long s = 0, s2 = 0;
@@ -283,6 +293,7 @@ __global__ void k_stats_g(const int32_t* __restrict__ v, size_t n, const int* sh
 __global__ void k_box_refresh(const int32_t* __restrict__ tray, int32_t* __restrict__ P, uint4* __restrict__ tbits,
                               int nq, int nx, int ny, int nz, const LoopState* __restrict__ ls,
                               const OrientDesc* __restrict__ od_item) {
+    pdl_enter();
     if (!ls->placed_now) return;
     const OrientDesc& od = od_item[ls->orient];
     const int by = od.e[1];

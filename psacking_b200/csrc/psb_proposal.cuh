@@ -19,6 +19,8 @@
 #pragma once
 #include <stdint.h>
 
+#include "psb_pdl.cuh"
+
 #define PSB_PG 32          // item grid side
 #define PSB_PG3 (PSB_PG * PSB_PG * PSB_PG)
 #define PSB_PH 32          // pooled height-map side
@@ -43,6 +45,7 @@ __device__ __forceinline__ float bf16_val(uint16_t h) { return __uint_as_float((
 // base grid of one item from its voxel list: cell floor(v / s) gains 1/s^3,
 // s = ceil(max extent / 32).  grid: (ceil(nvox/256)), block 256; out zeroed
 __global__ void k_base_grid(const int4* __restrict__ vox, int nvox, int s, float* __restrict__ out) {
+    pdl_enter();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nvox) return;
     const int4 q = vox[v];
@@ -56,6 +59,7 @@ __global__ void k_base_grid(const int4* __restrict__ vox, int nvox, int s, float
 // grid: (PSB_PG3 / 256, no, B), block 256
 __global__ void k_orient_grids(const float* __restrict__ base, const int* __restrict__ G, const int* __restrict__ maps,
                                int no, float* __restrict__ out) {
+    pdl_enter();
     const int b = blockIdx.z, o = blockIdx.y;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= PSB_PG3) return;
@@ -81,6 +85,7 @@ __global__ void k_orient_grids(const float* __restrict__ base, const int* __rest
 // top down and a ballot finds the highest occupied one.
 // grid: 1024, block 256
 __global__ void k_height_map(const int32_t* __restrict__ tray, int nx, int ny, int nz, float* __restrict__ out) {
+    pdl_enter();
     const int cell = blockIdx.x;  // 0..1023
     const int ci = cell / PSB_PH, cj = cell % PSB_PH;
     const int bx = (nx + PSB_PH - 1) / PSB_PH, by = (ny + PSB_PH - 1) / PSB_PH;
@@ -131,6 +136,7 @@ __global__ void k_height_map(const int32_t* __restrict__ tray, int nx, int ny, i
 #define PSB_CPT 4
 __global__ void k_conv_fwd(const float* __restrict__ in, int S, int Ci, int D, const uint16_t* __restrict__ w,
                            const float* __restrict__ bias, float* __restrict__ out, int Co) {
+    pdl_enter();
     extern __shared__ float ws[];   // [PSB_CPT][Ci*27]
     const int c0 = blockIdx.y * PSB_CPT;
     for (int i = threadIdx.x; i < PSB_CPT * Ci * 27; i += blockDim.x) {
@@ -178,6 +184,7 @@ __global__ void k_conv_fwd(const float* __restrict__ in, int S, int Ci, int D, c
 // grid: (ceil(S*D^3/256), Ci), block 256; smem Co*27 floats
 __global__ void k_conv_bwd_data(const float* __restrict__ dout, int S, int Ci, int D, const uint16_t* __restrict__ w,
                                 int Co, const float* __restrict__ in, int mask_relu, float* __restrict__ din) {
+    pdl_enter();
     extern __shared__ float ws[];
     const int ci = blockIdx.y;
     for (int i = threadIdx.x; i < Co * 27; i += blockDim.x) {
@@ -217,6 +224,7 @@ __global__ void k_conv_bwd_data(const float* __restrict__ dout, int S, int Ci, i
 // 0) with atomics.  grid: (Ci, Co, nchunk), block 256; dw, db zeroed first
 __global__ void k_conv_bwd_weight(const float* __restrict__ dout, const float* __restrict__ in, int S, int Ci, int D,
                                   int Co, int chunk, float* __restrict__ dw, float* __restrict__ db) {
+    pdl_enter();
     const int ci = blockIdx.x, co = blockIdx.y;
     const int s0 = blockIdx.z * chunk, s1 = min(S, s0 + chunk);
     const int Do = D / 2, Do3 = Do * Do * Do, D3 = D * D * D;
@@ -274,6 +282,7 @@ __global__ void k_conv_bwd_weight(const float* __restrict__ dout, const float* _
 // forward; relu applied when relu != 0.  grid: ceil(S*N/256)
 __global__ void k_lin_fwd(const float* __restrict__ x, int S, int K, const uint16_t* __restrict__ w,
                           const float* __restrict__ b, int N, int relu, float* __restrict__ y) {
+    pdl_enter();
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)S * N) return;
     const int s = (int)(idx / N), n = (int)(idx % N);
@@ -288,6 +297,7 @@ __global__ void k_lin_fwd(const float* __restrict__ x, int S, int K, const uint1
 // grid: ceil(S*K/256)
 __global__ void k_lin_bwd_data(const float* __restrict__ dy, int S, int N, const uint16_t* __restrict__ w, int K,
                                const float* __restrict__ xmask, float* __restrict__ dx) {
+    pdl_enter();
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)S * K) return;
     const int s = (int)(idx / K), k = (int)(idx % K);
@@ -301,6 +311,7 @@ __global__ void k_lin_bwd_data(const float* __restrict__ dy, int S, int N, const
 // column of threads also sums the bias
 __global__ void k_lin_bwd_weight(const float* __restrict__ dy, const float* __restrict__ x, int S, int N, int K,
                                  float* __restrict__ dw, float* __restrict__ db) {
+    pdl_enter();
     const int n = blockIdx.y;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K) return;
@@ -316,6 +327,7 @@ __global__ void k_lin_bwd_weight(const float* __restrict__ dy, const float* __re
 
 // head input: [f1[s] | t[s / no]] (64 + 64).  grid: ceil(S*128/256)
 __global__ void k_concat(const float* __restrict__ f1, const float* __restrict__ t, int S, int no, float* __restrict__ hin) {
+    pdl_enter();
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)S * 128) return;
     const int s = (int)(idx / 128), c = (int)(idx % 128);
@@ -326,6 +338,7 @@ __global__ void k_concat(const float* __restrict__ f1, const float* __restrict__
 // dt[b] = sum over its orientations of dhin[:, 64:] * (t > 0).  grid: ceil(S*64/256) and ceil(B*64/256)
 __global__ void k_split_item(const float* __restrict__ dhin, const float* __restrict__ f1, int S,
                              float* __restrict__ df1) {
+    pdl_enter();
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)S * 64) return;
     const int s = (int)(idx / 64), c = (int)(idx % 64);
@@ -333,6 +346,7 @@ __global__ void k_split_item(const float* __restrict__ dhin, const float* __rest
 }
 __global__ void k_split_tray(const float* __restrict__ dhin, const float* __restrict__ t, int B, int no,
                              float* __restrict__ dt) {
+    pdl_enter();
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= B * 64) return;
     const int b = idx / 64, c = idx % 64;
@@ -347,6 +361,7 @@ __global__ void k_split_tray(const float* __restrict__ dhin, const float* __rest
 __global__ void k_softmax_ce(const float* __restrict__ logit, const float* __restrict__ target,
                              const float* __restrict__ mask, int B, int no, float* __restrict__ dlogit,
                              float* __restrict__ loss) {
+    pdl_enter();
     const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     // items counted in the mean (the same for every warp)
@@ -387,6 +402,7 @@ __global__ void k_softmax_ce(const float* __restrict__ logit, const float* __res
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
                        uint16_t* __restrict__ p16, const unsigned char* __restrict__ is_weight, long long n, float lr,
                        float b1, float b2, float eps, float c1, float c2) {
+    pdl_enter();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float gi = g[i];
@@ -407,6 +423,7 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
 // output.  grid: 64, block 256
 __global__ void k_prop_tray_feat(const float* __restrict__ hmap, const uint16_t* __restrict__ w2,
                                  const float* __restrict__ b2, float* __restrict__ t) {
+    pdl_enter();
     const int n = blockIdx.x;
     float acc = 0.f;
     for (int k = threadIdx.x; k < PSB_PH * PSB_PH; k += blockDim.x)
@@ -428,6 +445,7 @@ __global__ void k_prop_item_head(const float* __restrict__ f1, const float* __re
                                  const uint16_t* __restrict__ wh1, const float* __restrict__ bh1,
                                  const uint16_t* __restrict__ wh2, const float* __restrict__ bh2,
                                  float* __restrict__ logit) {
+    pdl_enter();
     const int o = blockIdx.x, n = threadIdx.x;
     __shared__ float in[128];
     __shared__ float red[2];
@@ -454,6 +472,7 @@ __global__ void k_prop_item_head(const float* __restrict__ f1, const float* __re
 template <class OD>
 __global__ void k_gate(const float* __restrict__ logit, OD* __restrict__ od, int n, int topk, float margin,
                        int* __restrict__ stats) {
+    pdl_enter();
     const int lane = threadIdx.x;
     if (lane >= 32) return;
     const bool fit = lane < n && !od[lane].skip;

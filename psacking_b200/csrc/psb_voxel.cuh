@@ -14,6 +14,8 @@
 #pragma once
 #include <stdint.h>
 
+#include "psb_pdl.cuh"
+
 #define PSB_FP_POW 16
 #define PSB_FP_SCALE (1 << PSB_FP_POW)
 
@@ -45,6 +47,7 @@ __device__ __forceinline__ bool vox_in_triangle(long long i, long long j, const 
 // merged vertex indices, vox [X][Y][Z] axis bits.  grid: ceil(3*m / 8), block 256
 __global__ void k_voxel_raster(const int* __restrict__ pts, const int* __restrict__ tris, int m, int X, int Y, int Z,
                                unsigned int* __restrict__ vox) {
+    pdl_enter();
     const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (w >= 3 * m) return;
