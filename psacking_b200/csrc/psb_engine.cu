@@ -659,7 +659,8 @@ struct ItemInfo {
     long long sum = 0;         // sum of values
     long long sabs = 0;        // sum of |values|
     double sumsq = 0.0;
-    std::vector<int4> vox;     // nonzero voxels (x, y, z, value)
+    long long nvox = 0;        // nonzero voxels
+    std::vector<int4> vox;     // their list (x, y, z, value), when asked for
     std::vector<int4> samp;    // candidate-filter samples (positive voxels, spread out)
     std::vector<int4> runs[3]; // runs of equal nonzero values along each source axis (build_runs)
 };
@@ -704,7 +705,7 @@ void build_runs(const int32_t* a, ItemInfo* info, int s) {
 // the pool voxel farthest from those taken), starting from the voxel farthest
 // from the centre, so the filter's first samples already span the item.  Any
 // subset is exact for the filter; the spread only makes it sharp.
-void pick_samples(ItemInfo* info) {
+void pick_samples(const int32_t* a, ItemInfo* info) {
     info->samp.clear();
     const int G = 10;
     const int* d = info->dims;
@@ -712,18 +713,23 @@ void pick_samples(ItemInfo* info) {
     auto d2 = [](const int4& a, float x, float y, float z) {
         return (a.x - x) * (a.x - x) + (a.y - y) * (a.y - y) + (a.z - z) * (a.z - z);
     };
-    std::vector<int> best(G * G * G, -1);
+    std::vector<int4> best(G * G * G, make_int4(0, 0, 0, 0));   // w = 0: cell empty
     std::vector<float> bd(G * G * G, 0.f);
-    for (size_t i = 0; i < info->vox.size(); ++i) {
-        const int4 v = info->vox[i];
-        if (v.w <= 0) continue;
-        const int cell = ((v.x * G / d[0]) * G + v.y * G / d[1]) * G + v.z * G / d[2];
-        const float dist = d2(v, cx, cy, cz);
-        if (best[cell] < 0 || dist > bd[cell]) { best[cell] = (int)i; bd[cell] = dist; }
-    }
+    // the item's cells in row-major order (the first farthest voxel of a cell wins)
+    for (int i = 0; i < d[0]; ++i)
+        for (int j = 0; j < d[1]; ++j) {
+            const int32_t* line = a + ((size_t)i * d[1] + j) * d[2];
+            for (int k = 0; k < d[2]; ++k) {
+                if (line[k] <= 0) continue;
+                const int4 v = make_int4(i, j, k, line[k]);
+                const int cell = ((i * G / d[0]) * G + j * G / d[1]) * G + k * G / d[2];
+                const float dist = d2(v, cx, cy, cz);
+                if (best[cell].w == 0 || dist > bd[cell]) { best[cell] = v; bd[cell] = dist; }
+            }
+        }
     std::vector<int4> pool;
-    for (int b : best)
-        if (b >= 0) pool.push_back(info->vox[b]);
+    for (const int4& b : best)
+        if (b.w != 0) pool.push_back(b);
     if (pool.empty()) return;
     size_t k = 0;
     for (size_t i = 1; i < pool.size(); ++i)
@@ -746,19 +752,21 @@ void pick_samples(ItemInfo* info) {
     }
 }
 
-void analyse_item(const int32_t* a, int ex, int ey, int ez, ItemInfo* info) {
+void analyse_item(const int32_t* a, int ex, int ey, int ez, ItemInfo* info, bool keep_vox = true) {
     info->dims[0] = ex; info->dims[1] = ey; info->dims[2] = ez;
     for (int k = 0; k < 3; ++k) { info->lo[k] = INT32_MAX; info->hi[k] = -1; }
     info->sum = 0;
     info->sabs = 0;
     info->sumsq = 0.0;
+    info->nvox = 0;
     info->vox.clear();
     for (int i = 0; i < ex; ++i)
         for (int j = 0; j < ey; ++j)
             for (int k = 0; k < ez; ++k) {
                 int v = a[((size_t)i * ey + j) * ez + k];
                 if (v == 0) continue;
-                info->vox.push_back(make_int4(i, j, k, v));
+                info->nvox += 1;
+                if (keep_vox) info->vox.push_back(make_int4(i, j, k, v));
                 info->sum += v;
                 info->sabs += std::llabs((long long)v);
                 info->sumsq += (double)v * v;
@@ -904,10 +912,9 @@ struct psb_tray {
 
     // items of a packing run, staged once (psb_pack_stage)
     std::vector<ItemInfo> staged;
-    std::vector<size_t> staged_off, staged_voff;
+    std::vector<size_t> staged_off;
     int32_t* d_stage = nullptr;
-    int4* d_stage_vox = nullptr;
-    size_t stage_cap = 0, stage_vcap = 0;
+    size_t stage_cap = 0;
     std::vector<size_t> staged_soff;   // the items' filter samples in d_stage_samp
     int4* d_stage_samp = nullptr;
     size_t stage_scap = 0;
@@ -946,7 +953,7 @@ struct psb_tray {
         if (dev >= 0) cudaSetDevice(dev);
         release_slots();
         dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_wocc, st); dfree(d_pen, st);
-        dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st); dfree(d_stage_vox, st);
+        dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st);
         dfree(d_stage_runs, st); dfree(d_runs, st); dfree(d_pphi, st); dfree(d_pocc, st);
         dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_base_all, st); dfree(d_dec, st);
         dfree(d_tbits, st); dfree(d_stage_samp, st); dfree(d_work, st); dfree(d_clist, st);
@@ -1245,7 +1252,7 @@ struct psb_tray {
         od->exact = (od->delta >= 0.4 || maxD >= 8388608.0) ? 1 : 0;
         od->item = d_item;
         od->vox = d_vx;
-        od->nvox = (int)info.vox.size();
+        od->nvox = (int)info.nvox;
         od->perm = -1;
         od->sumsq = info.sumsq;
         od->sabs = sabs;
@@ -2536,7 +2543,6 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     CK(cudaSetDevice(t->dev));
     t->staged.clear();
     t->staged_off.clear();
-    t->staged_voff.clear();
     t->staged_soff.clear();
     t->staged_roff.clear();
     for (int it = 0; it < n_items; ++it) {
@@ -2553,8 +2559,9 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
                 const int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
                 const size_t m = (size_t)ex * ey * ez;
                 if (has_negative(items[it], m)) { neg[it] = 1; continue; }
-                analyse_item(items[it], ex, ey, ez, &t->staged[it]);
-                pick_samples(&t->staged[it]);
+                // the packing loop places items by their runs: no voxel list
+                analyse_item(items[it], ex, ey, ez, &t->staged[it], false);
+                pick_samples(items[it], &t->staged[it]);
                 for (int a = 0; a < 3; ++a) build_runs(items[it], &t->staged[it], a);
             }
         };
@@ -2566,11 +2573,10 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
     }
     for (int it = 0; it < n_items; ++it)
         if (neg[it]) return fail(PSB_ERR_ARG, "item %d holds negative values", it);
-    size_t tot = 0, totv = 0, tots = 0, totr = 0;
+    size_t tot = 0, tots = 0, totr = 0;
     for (int it = 0; it < n_items; ++it) {
         const ItemInfo& inf = t->staged[it];
         t->staged_off.push_back(tot);
-        t->staged_voff.push_back(totv);
         t->staged_soff.push_back(tots);
         std::array<size_t, 3> ro;
         for (int a = 0; a < 3; ++a) {
@@ -2579,7 +2585,6 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
         }
         t->staged_roff.push_back(ro);
         tot += (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
-        totv += inf.vox.size();
         tots += inf.samp.size();
     }
     if (totr > t->stage_rcap) {
@@ -2597,14 +2602,9 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
         t->stage_cap = tot;
         TRY(dalloc(&t->d_stage, tot, t->st));
     }
-    if (totv > t->stage_vcap) {
-        dfree(t->d_stage_vox, t->st);
-        t->stage_vcap = totv;
-        TRY(dalloc(&t->d_stage_vox, totv, t->st));
-    }
-    // one pinned staging buffer for the item arrays and voxel lists: two
-    // large copies instead of two small pageable ones per item
-    const size_t bytes = sizeof(int32_t) * tot + sizeof(int4) * (totv + tots + totr);
+    // one pinned staging buffer for the item arrays, samples and runs: three
+    // large copies instead of small pageable ones per item
+    const size_t bytes = sizeof(int32_t) * tot + sizeof(int4) * (tots + totr);
     if (bytes > t->h_stage_cap) {
         if (t->h_stage) cudaFreeHost(t->h_stage);
         t->h_stage = nullptr;
@@ -2613,20 +2613,29 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
         t->h_stage_cap = bytes;
     }
     int32_t* hi = (int32_t*)t->h_stage;
-    int4* hv = (int4*)(hi + tot);
-    int4* hs = hv + totv;
+    int4* hs = (int4*)(hi + tot);
     int4* hr = hs + tots;
-    for (int it = 0; it < n_items; ++it) {
-        const ItemInfo& inf = t->staged[it];
-        memcpy(hi + t->staged_off[it], items[it], sizeof(int32_t) * inf.dims[0] * inf.dims[1] * inf.dims[2]);
-        if (!inf.vox.empty()) memcpy(hv + t->staged_voff[it], inf.vox.data(), sizeof(int4) * inf.vox.size());
-        if (!inf.samp.empty()) memcpy(hs + t->staged_soff[it], inf.samp.data(), sizeof(int4) * inf.samp.size());
-        for (int a = 0; a < 3; ++a)
-            if (!inf.runs[a].empty())
-                memcpy(hr + t->staged_roff[it][a], inf.runs[a].data(), sizeof(int4) * inf.runs[a].size());
+    {
+        // the copies into the pinned buffer, items spread over the host cores
+        std::atomic<int> next(0);
+        auto work = [&]() {
+            for (int it = next.fetch_add(1); it < n_items; it = next.fetch_add(1)) {
+                const ItemInfo& inf = t->staged[it];
+                memcpy(hi + t->staged_off[it], items[it], sizeof(int32_t) * inf.dims[0] * inf.dims[1] * inf.dims[2]);
+                if (!inf.samp.empty())
+                    memcpy(hs + t->staged_soff[it], inf.samp.data(), sizeof(int4) * inf.samp.size());
+                for (int a = 0; a < 3; ++a)
+                    if (!inf.runs[a].empty())
+                        memcpy(hr + t->staged_roff[it][a], inf.runs[a].data(), sizeof(int4) * inf.runs[a].size());
+            }
+        };
+        const int nthr = std::max(1, std::min<int>(n_items / 8, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (int w = 1; w < nthr; ++w) pool.emplace_back(work);
+        work();
+        for (auto& th : pool) th.join();
     }
     if (tot) CK(cudaMemcpyAsync(t->d_stage, hi, sizeof(int32_t) * tot, cudaMemcpyHostToDevice, t->st));
-    if (totv) CK(cudaMemcpyAsync(t->d_stage_vox, hv, sizeof(int4) * totv, cudaMemcpyHostToDevice, t->st));
     if (tots) CK(cudaMemcpyAsync(t->d_stage_samp, hs, sizeof(int4) * tots, cudaMemcpyHostToDevice, t->st));
     if (totr) CK(cudaMemcpyAsync(t->d_stage_runs, hr, sizeof(int4) * totr, cudaMemcpyHostToDevice, t->st));
     CK(cudaStreamSynchronize(t->st));
@@ -2739,7 +2748,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             const int4* rn[3];
             for (int a = 0; a < 3; ++a) rn[a] = t->d_stage_runs + t->staged_roff[it][a];
             t->describe(t->staged[it], orient_maps + 6 * o, orient_maps + 6 * o + 3,
-                        t->d_stage + t->staged_off[it], t->d_stage_vox + t->staged_voff[it], rn,
+                        t->d_stage + t->staged_off[it], nullptr, rn,
                         &all[(size_t)it * n_orient + o]);
         }
     // orientation sharding: the other ranks' orientations are not searched here
@@ -2822,10 +2831,10 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             const ItemInfo& inf = t->staged[it];
             const int sc = std::max(1, (std::max(inf.dims[0], std::max(inf.dims[1], inf.dims[2])) + PSB_PG - 1) / PSB_PG);
             for (int a = 0; a < 3; ++a) G[3 * it + a] = (inf.dims[a] + sc - 1) / sc;
-            const int nv = (int)inf.vox.size();
-            if (nv > 0)
-                pdl(k_base_grid, (nv + 255) / 256, 256, 0, t->st)(t->d_stage_vox + t->staged_voff[it], nv, sc,
-                                                                 d_pgrid + (size_t)it * PSB_PG3);
+            const int nr = (int)inf.runs[2].size();
+            if (nr > 0)
+                pdl(k_base_grid_runs, (nr + 255) / 256, 256, 0, t->st)(t->d_stage_runs + t->staged_roff[it][2], nr,
+                                                                      sc, d_pgrid + (size_t)it * PSB_PG3);
             CKL();
         }
         CK(cudaMemcpyAsync(d_pG, G.data(), sizeof(int) * G.size(), cudaMemcpyHostToDevice, t->st));
@@ -2890,7 +2899,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         }
         std::vector<OrientDesc> hb(allb.begin() + (size_t)it * 6, allb.begin() + (size_t)(it + 1) * 6);
         if (filt && occ_est * 4 >= t->V) TRY(t->cand_filter(d_odb, host_ods, interlock != 0));
-        occ_est += t->staged[it].vox.size();
+        occ_est += (size_t)t->staged[it].nvox;
         ShardRecord* rec = opt.world > 1 || opt.d_local ? (ShardRecord*)opt.d_local : nullptr;
         // the decision below may be fused into the search's last launch
         t->decide = DecideArgs{t->d_ls, t->d_dec + it, t->d_err, rec};
@@ -2985,7 +2994,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         r.n_candidates = dec[it].ncand;
         r.err_ratio = dec[it].err_ratio;
         out_placements[it] = r;
-        if (r.found) t->occ += t->staged[it].vox.size();   // a placement writes every item voxel
+        if (r.found) t->occ += (size_t)t->staged[it].nvox;   // a placement writes every item voxel
     }
     if (h.err & 1u) return fail(PSB_ERR_LIMIT, "flood fill union-find hit its iteration limit");
     if (h.err & 2u) return fail(PSB_ERR_LIMIT, "tie-guard candidates exceeded the capacity %d", kCandCap);

@@ -185,21 +185,29 @@ __global__ void k_decide_merge(const ShardRecord* __restrict__ all, int world, L
     }
 }
 
+// The decided placement, walked by the item's z-runs (each run a contiguous
+// stretch of one tray column): the check records the smallest tray index an
+// item cell would overwrite, the write then fills the free cells with the id.
+// grid: 64, block 256
 __global__ void k_place_check_g(const OrientDesc* __restrict__ od_item, LoopState* ls, const int32_t* __restrict__ tray,
                                 int nx, int ny, int nz) {
     pdl_enter();
     if (!ls->do_place) return;
     const OrientDesc& od = od_item[ls->orient];
     const int px = ls->px, py = ls->py, pz = ls->pz;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < od.nvox; v += gridDim.x * blockDim.x) {
-        int4 q = od.vox[v];
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < od.nruns; r += gridDim.x * blockDim.x) {
+        const int4 q = od.runs[r];
         if (q.w <= 0) continue;
-        int oc[3];
-        orient_voxel(od, q.x, q.y, q.z, oc);
-        int i = px + oc[0], j = py + oc[1], k = pz + oc[2];
-        if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) continue;
-        size_t t = ((size_t)i * ny + j) * nz + k;
-        if (tray[t] > 0) atomicMin(&ls->first, (unsigned long long)t);
+        int a, b, c0, c1;
+        orient_run(od, q, &a, &b, &c0, &c1);
+        const int i = px + a, j = py + b;
+        if (i < 0 || j < 0 || i >= nx || j >= ny) continue;
+        const size_t col = ((size_t)i * ny + j) * nz;
+        for (int k = max(0, pz + c0); k <= min(nz - 1, pz + c1); ++k)
+            if (tray[col + k] > 0) {
+                atomicMin(&ls->first, (unsigned long long)(col + k));
+                break;   // the run's first overlap is its smallest index
+            }
     }
 }
 
@@ -209,15 +217,16 @@ __global__ void k_place_write_g(const OrientDesc* __restrict__ od_item, const Lo
     if (!ls->do_place || ls->first != 0xffffffffffffffffULL) return;
     const OrientDesc& od = od_item[ls->orient];
     const int px = ls->px, py = ls->py, pz = ls->pz, id = ls->id;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < od.nvox; v += gridDim.x * blockDim.x) {
-        int4 q = od.vox[v];
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < od.nruns; r += gridDim.x * blockDim.x) {
+        const int4 q = od.runs[r];
         if (q.w <= 0) continue;
-        int oc[3];
-        orient_voxel(od, q.x, q.y, q.z, oc);
-        int i = px + oc[0], j = py + oc[1], k = pz + oc[2];
-        if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) continue;
-        size_t t = ((size_t)i * ny + j) * nz + k;
-        if (tray[t] == 0) tray[t] = id;
+        int a, b, c0, c1;
+        orient_run(od, q, &a, &b, &c0, &c1);
+        const int i = px + a, j = py + b;
+        if (i < 0 || j < 0 || i >= nx || j >= ny) continue;
+        const size_t col = ((size_t)i * ny + j) * nz;
+        for (int k = max(0, pz + c0); k <= min(nz - 1, pz + c1); ++k)
+            if (tray[col + k] == 0) tray[col + k] = id;
     }
 }
 

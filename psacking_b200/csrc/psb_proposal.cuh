@@ -54,6 +54,20 @@ __global__ void k_base_grid(const int4* __restrict__ vox, int nvox, int s, float
     atomicAdd(&out[(i * PSB_PG + j) * PSB_PG + k], 1.0f / (float)(s * s * s));
 }
 
+// the same base grid from the item's z-runs ({x, y, z0 | z1 << 16, value},
+// one per run of equal nonzero values along z): the cells and weights of the
+// voxel form.  grid: (ceil(nruns/256)), block 256; out zeroed
+__global__ void k_base_grid_runs(const int4* __restrict__ runs, int nruns, int s, float* __restrict__ out) {
+    pdl_enter();
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns) return;
+    const int4 q = runs[r];
+    if (q.w <= 0) return;
+    const float w = 1.0f / (float)(s * s * s);
+    const int i = q.x / s, j = q.y / s, z1 = q.z >> 16;
+    for (int z = q.z & 0xffff; z <= z1; ++z) atomicAdd(&out[(i * PSB_PG + j) * PSB_PG + z / s], w);
+}
+
 // oriented grids: out[b*no + o] = the base grid of item b turned by map o
 // (src_axis[3], flip[3]) within its scaled extent G (cells per axis).
 // grid: (PSB_PG3 / 256, no, B), block 256
