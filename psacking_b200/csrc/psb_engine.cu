@@ -21,6 +21,9 @@
 #include <vector>
 #include <atomic>
 #include <thread>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include "../../include/psb200.h"
 #include "psb_kernels2.cuh"
@@ -674,18 +677,15 @@ void build_runs(const int32_t* a, ItemInfo* info, int s) {
     out.clear();
     const int* d = info->dims;
     const int lo = s == 0 ? 1 : 0, hi = s == 2 ? 1 : 2;
-    int idx[3];
+    const size_t stride[3] = {(size_t)d[1] * d[2], (size_t)d[2], 1};
+    const size_t sl = stride[lo], sh = stride[hi], ss = stride[s];
+    const int len = d[s];
     for (int u = 0; u < d[lo]; ++u)
         for (int v = 0; v < d[hi]; ++v) {
+            const int32_t* line = a + u * sl + v * sh;
             int r0 = -1, w = 0;
-            for (int r = 0; r <= d[s]; ++r) {
-                int val = 0;
-                if (r < d[s]) {
-                    idx[lo] = u;
-                    idx[hi] = v;
-                    idx[s] = r;
-                    val = a[((size_t)idx[0] * d[1] + idx[1]) * d[2] + idx[2]];
-                }
+            for (int r = 0; r <= len; ++r) {
+                const int val = r < len ? line[r * ss] : 0;
                 if (r0 >= 0 && val != w) {
                     out.push_back(make_int4(u, v, r0 | ((r - 1) << 16), w));
                     r0 = -1;
@@ -701,11 +701,17 @@ void build_runs(const int32_t* a, ItemInfo* info, int s) {
 // Up to PSB_FSAMP positive voxels spread over the item, for the candidate
 // filter.  Pool: in each cell of a 10x10x10 split of the item's box, the
 // voxel farthest from the box centre (extreme voxels are the ones that stop
-// an item from fitting a gap).  Order: farthest-point (each next sample is
-// the pool voxel farthest from those taken), starting from the voxel farthest
-// from the centre, so the filter's first samples already span the item.  Any
-// subset is exact for the filter; the spread only makes it sharp.
-void pick_samples(const int32_t* a, ItemInfo* info) {
+// an item from fitting a gap; the first such voxel in row-major order).
+// Order: farthest-point (each next sample is the pool voxel farthest from
+// those taken), starting from the voxel farthest from the centre, so the
+// filter's first samples already span the item.  Any subset is exact for the
+// filter; the spread only makes it sharp.  Read from the item's z-runs
+// (build_runs, axis 2), which list the nonzero voxels in row-major order:
+// within the part of a run that falls in one split cell the squared distance
+// to the centre is a convex function of z (and exact in float: sums of
+// squared half-integers below 2^24), so the farthest voxel there is one of
+// the part's two ends, the lower one on a tie.
+void pick_samples(ItemInfo* info) {
     info->samp.clear();
     const int G = 10;
     const int* d = info->dims;
@@ -713,20 +719,32 @@ void pick_samples(const int32_t* a, ItemInfo* info) {
     auto d2 = [](const int4& a, float x, float y, float z) {
         return (a.x - x) * (a.x - x) + (a.y - y) * (a.y - y) + (a.z - z) * (a.z - z);
     };
+    // the split cell of each coordinate, per axis (c * G / extent)
+    std::vector<int> cell_of[3];
+    for (int q = 0; q < 3; ++q) {
+        cell_of[q].resize(d[q]);
+        for (int c = 0; c < d[q]; ++c) cell_of[q][c] = c * G / d[q];
+    }
     std::vector<int4> best(G * G * G, make_int4(0, 0, 0, 0));   // w = 0: cell empty
     std::vector<float> bd(G * G * G, 0.f);
-    // the item's cells in row-major order (the first farthest voxel of a cell wins)
-    for (int i = 0; i < d[0]; ++i)
-        for (int j = 0; j < d[1]; ++j) {
-            const int32_t* line = a + ((size_t)i * d[1] + j) * d[2];
-            for (int k = 0; k < d[2]; ++k) {
-                if (line[k] <= 0) continue;
-                const int4 v = make_int4(i, j, k, line[k]);
-                const int cell = ((i * G / d[0]) * G + j * G / d[1]) * G + k * G / d[2];
-                const float dist = d2(v, cx, cy, cz);
-                if (best[cell].w == 0 || dist > bd[cell]) { best[cell] = v; bd[cell] = dist; }
-            }
+    const std::vector<int4>& zr = info->runs[2];
+    for (const int4& q : zr) {
+        if (q.w <= 0) continue;
+        const int i = q.x, j = q.y, z1 = q.z >> 16;
+        const int cij = (cell_of[0][i] * G + cell_of[1][j]) * G;
+        for (int k = q.z & 0xffff; k <= z1;) {
+            const int c = cell_of[2][k];
+            int e = k;
+            while (e < z1 && cell_of[2][e + 1] == c) ++e;
+            const int4 vk = make_int4(i, j, k, q.w), ve = make_int4(i, j, e, q.w);
+            const float dk = d2(vk, cx, cy, cz), de = d2(ve, cx, cy, cz);
+            const int4 v = de > dk ? ve : vk;
+            const float dist = de > dk ? de : dk;
+            const int cell = cij + c;
+            if (best[cell].w == 0 || dist > bd[cell]) { best[cell] = v; bd[cell] = dist; }
+            k = e + 1;
         }
+    }
     std::vector<int4> pool;
     for (const int4& b : best)
         if (b.w != 0) pool.push_back(b);
@@ -734,22 +752,93 @@ void pick_samples(const int32_t* a, ItemInfo* info) {
     size_t k = 0;
     for (size_t i = 1; i < pool.size(); ++i)
         if (d2(pool[i], cx, cy, cz) > d2(pool[k], cx, cy, cz)) k = i;
-    std::vector<float> dmin(pool.size(), 3.0e38f);
-    std::vector<char> taken(pool.size(), 0);
-    const size_t m = std::min(pool.size(), (size_t)PSB_FSAMP);
+    // farthest-point order over the pool, structure of arrays; a taken entry
+    // holds -1 in dmin, below every distance, so it is never picked again
+    const size_t P = pool.size();
+    std::vector<float> fx(P), fy(P), fz(P), dmin(P, 3.0e38f);
+    for (size_t i = 0; i < P; ++i) {
+        fx[i] = (float)pool[i].x;
+        fy[i] = (float)pool[i].y;
+        fz[i] = (float)pool[i].z;
+    }
+    const size_t m = std::min(P, (size_t)PSB_FSAMP);
     while (info->samp.size() < m) {
-        taken[k] = 1;
+        dmin[k] = -1.f;
         info->samp.push_back(pool[k]);
-        size_t nk = k;
+        const float kx = fx[k], ky = fy[k], kz = fz[k];
         float far = -1.f;
-        for (size_t i = 0; i < pool.size(); ++i) {
-            if (taken[i]) continue;
-            dmin[i] = std::min(dmin[i], d2(pool[i], (float)pool[k].x, (float)pool[k].y, (float)pool[k].z));
-            if (dmin[i] > far) { far = dmin[i]; nk = i; }
+        size_t i = 0;
+#if defined(__SSE2__)
+        // four lanes at a time: the same single-precision products, sums and
+        // min as the scalar form below (minps(a, b) = a < b ? a : b)
+        const __m128 vx = _mm_set1_ps(kx), vy = _mm_set1_ps(ky), vz = _mm_set1_ps(kz);
+        __m128 vfar = _mm_set1_ps(-1.f);
+        for (; i + 4 <= P; i += 4) {
+            const __m128 dx = _mm_sub_ps(_mm_loadu_ps(&fx[i]), vx);
+            const __m128 dy = _mm_sub_ps(_mm_loadu_ps(&fy[i]), vy);
+            const __m128 dz = _mm_sub_ps(_mm_loadu_ps(&fz[i]), vz);
+            const __m128 dd = _mm_add_ps(_mm_add_ps(_mm_mul_ps(dx, dx), _mm_mul_ps(dy, dy)), _mm_mul_ps(dz, dz));
+            const __m128 dm = _mm_min_ps(dd, _mm_loadu_ps(&dmin[i]));
+            _mm_storeu_ps(&dmin[i], dm);
+            vfar = _mm_max_ps(vfar, dm);
         }
-        if (nk == k) break;
+        float lanes[4];
+        _mm_storeu_ps(lanes, vfar);
+        far = std::max(std::max(lanes[0], lanes[1]), std::max(lanes[2], lanes[3]));
+#endif
+        for (; i < P; ++i) {
+            const float dx = fx[i] - kx, dy = fy[i] - ky, dz = fz[i] - kz;
+            dmin[i] = std::min(dmin[i], dx * dx + dy * dy + dz * dz);
+            far = std::max(far, dmin[i]);
+        }
+        if (!(far > -1.f)) break;   // every pool voxel taken
+        size_t nk = 0;
+#if defined(__SSE2__)
+        const __m128 vf = _mm_set1_ps(far);
+        for (; nk + 4 <= P; nk += 4) {
+            const int hit = _mm_movemask_ps(_mm_cmpeq_ps(_mm_loadu_ps(&dmin[nk]), vf));
+            if (hit) { nk += __builtin_ctz(hit); break; }
+        }
+#endif
+        while (dmin[nk] != far) ++nk;   // the first farthest
         k = nk;
     }
+}
+
+// analyse_item's bounds and sums from the item's z-runs (no pass over the
+// dense array).  The sum of squares adds one term per voxel in row-major
+// order, as analyse_item does, unless every partial sum is an integer below
+// 2^53 (then any order gives the same double).
+void analyse_runs(ItemInfo* info) {
+    for (int k = 0; k < 3; ++k) { info->lo[k] = INT32_MAX; info->hi[k] = -1; }
+    info->sum = 0;
+    info->sabs = 0;
+    info->sumsq = 0.0;
+    info->nvox = 0;
+    info->vox.clear();
+    const std::vector<int4>& zr = info->runs[2];
+    long long wmax = 0;
+    for (const int4& q : zr) wmax = std::max(wmax, std::llabs((long long)q.w));
+    long long n = 0;
+    for (const int4& q : zr) n += (q.z >> 16) - (q.z & 0xffff) + 1;
+    const bool exact = wmax <= 32768 && n < (1LL << 22);   // n * wmax^2 < 2^52
+    long long isq = 0;
+    for (const int4& q : zr) {
+        const int z0 = q.z & 0xffff, z1 = q.z >> 16, len = z1 - z0 + 1;
+        const long long w = q.w;
+        info->nvox += len;
+        info->sum += w * len;
+        info->sabs += std::llabs(w) * len;
+        if (exact) isq += w * w * len;
+        else
+            for (int k = 0; k < len; ++k) info->sumsq += (double)w * (double)w;
+        if (w > 0) {
+            info->lo[0] = std::min(info->lo[0], q.x); info->hi[0] = std::max(info->hi[0], q.x);
+            info->lo[1] = std::min(info->lo[1], q.y); info->hi[1] = std::max(info->hi[1], q.y);
+            info->lo[2] = std::min(info->lo[2], z0);  info->hi[2] = std::max(info->hi[2], z1);
+        }
+    }
+    if (exact) info->sumsq = (double)isq;
 }
 
 void analyse_item(const int32_t* a, int ex, int ey, int ez, ItemInfo* info, bool keep_vox = true) {
@@ -2559,10 +2648,13 @@ int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims
                 const int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
                 const size_t m = (size_t)ex * ey * ez;
                 if (has_negative(items[it], m)) { neg[it] = 1; continue; }
-                // the packing loop places items by their runs: no voxel list
-                analyse_item(items[it], ex, ey, ez, &t->staged[it], false);
-                pick_samples(items[it], &t->staged[it]);
-                for (int a = 0; a < 3; ++a) build_runs(items[it], &t->staged[it], a);
+                // the packing loop places items by their runs: no voxel list;
+                // bounds, sums and samples come from the z-runs
+                ItemInfo& inf = t->staged[it];
+                inf.dims[0] = ex; inf.dims[1] = ey; inf.dims[2] = ez;
+                for (int a = 0; a < 3; ++a) build_runs(items[it], &inf, a);
+                analyse_runs(&inf);
+                pick_samples(&inf);
             }
         };
         const int nthr = std::max(1, std::min<int>(n_items / 8, (int)std::thread::hardware_concurrency()));
