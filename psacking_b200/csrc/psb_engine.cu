@@ -209,8 +209,9 @@ bool g_fast_fft = true;  // specialised two-pass kernels where a plan exists
 // taken, so the tray runs the specialised split flow (and its direct
 // decisions) instead of the generic kernels.  The circular correlation stays
 // exact for every translation the search scores (t + x <= n - 1 < F).
-// 0 disables (PSB_PAD_MAX).
-double g_pad_max = 2.0;
+// 0 disables (PSB_PAD_MAX).  Default 3 (config-5 trays, 64 trays of sides
+// 64-160: 0 -> 506, 2 -> 562, 3 -> 578 / 626 items placed/s).
+double g_pad_max = 3.0;
 
 
 using XpassFn = void (*)(const OrientDesc*, SearchBufs, const float2*, const float2*, int, const float2*,
