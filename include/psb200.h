@@ -155,6 +155,12 @@ int psb_tray_set(psb_tray* t, const int32_t* tray, const int32_t* phi);
 /* Copy the device tray / distance field back to the host. */
 int psb_tray_get(psb_tray* t, int32_t* tray, int32_t* phi);
 
+/* Statistics of the device tray for the packing result
+ * (BinPacker._calculate_stats, packer.py:582-601): the number of cells > 0
+ * and their bounding box lo[3]..hi[3] (inclusive; -1 when none), computed
+ * on the device instead of over a host copy. */
+int psb_tray_stats(psb_tray* t, long long* occupied, int32_t* lo, int32_t* hi);
+
 /* fft_search_batch / fft_search_batch_interlocking_free / gpu_tray_search
  * (fft3.cu:1506-1632): search n orientation arrays against the tray.
  * items[o] points at an (dims[3o],dims[3o+1],dims[3o+2]) grid.  Orientations

@@ -14,9 +14,12 @@
 
 #include <cstdint>
 #include <cstring>
+#include <algorithm>
+#include <atomic>
 #include <fstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -324,6 +327,40 @@ py::tuple py_gpu_tray_search(py::handle item) {
 }
 
 // Device-resident greedy loop used by psacking_b200.BinPacker (see psb_pack).
+// cells > 0 of every item (BinPacker's volumes, packer.py: np.sum(item > 0)),
+// items spread over the host cores
+py::list py_positive_counts(py::list items) {
+    auto gs = to_grids(items);
+    std::vector<const int32_t*> ptrs;
+    std::vector<size_t> sizes;
+    for (auto& g : gs) {
+        ptrs.push_back(g.ptr());
+        sizes.push_back((size_t)g.n[0] * g.n[1] * g.n[2]);
+    }
+    std::vector<long long> out(gs.size(), 0);
+    {
+        py::gil_scoped_release nogil;
+        std::atomic<size_t> next(0);
+        auto work = [&]() {
+            for (size_t i = next.fetch_add(1); i < ptrs.size(); i = next.fetch_add(1)) {
+                const int32_t* a = ptrs[i];
+                const size_t m = sizes[i];
+                long long c = 0;
+                for (size_t k = 0; k < m; ++k) c += a[k] > 0;
+                out[i] = c;
+            }
+        };
+        const int nthr = (int)std::min<size_t>(gs.size() / 16 + 1, std::max(1u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (int w = 1; w < nthr; ++w) pool.emplace_back(work);
+        work();
+        for (auto& th : pool) th.join();
+    }
+    py::list r;
+    for (long long c : out) r.append(c);
+    return r;
+}
+
 py::tuple py_pack_native(py::list items, py::handle initial_tray, py::array_t<int32_t> orient_maps, bool interlock,
                          int id_offset) {
     Grid tr = to_grid(initial_tray);
@@ -340,6 +377,8 @@ py::tuple py_pack_native(py::list items, py::handle initial_tray, py::array_t<in
     std::vector<psb_result> res(gs.size());
     auto out = new_grid(tr.n);
     int st;
+    long long occupied = 0;
+    int32_t lo[3] = {-1, -1, -1}, hi[3] = {-1, -1, -1};
     {
         // the packing context (about 90 MB per orientation slot) is kept for
         // the next run with the same tray shape instead of being rebuilt
@@ -358,13 +397,16 @@ py::tuple py_pack_native(py::list items, py::handle initial_tray, py::array_t<in
         if (st == PSB_OK)
             st = psb_pack(pack_ctx, ptrs.data(), dims.data(), (int)gs.size(), maps.data(), n_orient,
                           interlock ? 1 : 0, id_offset, res.data(), out.mutable_data());
+        if (st == PSB_OK) st = psb_tray_stats(pack_ctx, &occupied, lo, hi);
     }
     check(st);
     py::list pl;
     for (auto& r : res)
         pl.append(py::make_tuple(py::make_tuple(r.x, r.y, r.z), (bool)r.found, r.score, r.orientation, r.diag,
                                  r.n_candidates, r.err_ratio));
-    return py::make_tuple(out, pl);
+    // the final tray's occupied cells and bounding box, counted on the device
+    py::tuple stats = py::make_tuple(occupied, py::make_tuple(lo[0], lo[1], lo[2]), py::make_tuple(hi[0], hi[1], hi[2]));
+    return py::make_tuple(out, pl, stats);
 }
 
 // trays: list of (dims, [items in packing order]) -> list of (final tray, placements)
@@ -490,6 +532,8 @@ PYBIND11_MODULE(_core, m) {
           py::arg("tray"), py::arg("tray_distance"), py::arg("generation"));
     m.def("interlocking_free_positions", &py_interlocking_free_positions, py::arg("tray"), py::arg("obj"));
     // engine extensions (not in the reference module)
+    m.def("positive_counts", &py_positive_counts, py::arg("items"),
+          "Number of cells > 0 of each int32 grid (on all host cores).");
     m.def("pack_native", &py_pack_native, py::arg("items"), py::arg("initial_tray"), py::arg("orient_maps"),
           py::arg("interlock"), py::arg("id_offset"));
     m.def("search_detail", &py_search_detail, py::arg("orientations"), py::arg("flags"),

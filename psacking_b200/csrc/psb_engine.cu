@@ -654,6 +654,27 @@ bool has_negative(const int32_t* a, size_t n) {
     return false;
 }
 
+// fn(begin, end) over [0, n) in chunks, on up to all host cores (the calling
+// thread takes part); a single chunk runs inline.
+template <typename F>
+void parallel_chunks(size_t n, size_t chunk, F fn) {
+    const size_t nchunks = (n + chunk - 1) / chunk;
+    const int nthr = (int)std::min<size_t>(nchunks, std::max(1u, std::thread::hardware_concurrency()));
+    if (nthr <= 1) {
+        if (n) fn((size_t)0, n);
+        return;
+    }
+    std::atomic<size_t> next(0);
+    auto work = [&]() {
+        for (size_t c = next.fetch_add(1); c < nchunks; c = next.fetch_add(1))
+            fn(c * chunk, std::min(n, (c + 1) * chunk));
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < nthr; ++w) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+}
+
 // ---------------------------------------------------------------------------
 // host-side item analysis
 // ---------------------------------------------------------------------------
@@ -942,6 +963,7 @@ struct psb_tray {
     // transform descriptors of the occupancy / distance spectra (uploaded once)
     LoopState* d_ls = nullptr;
     PhiStats* d_ps = nullptr;
+    int* d_ostat = nullptr;    // k_occ_stats output: occupied count (8 bytes) + bounding box
     RzDesc* d_rzd = nullptr;    // [0] occ, [1] phi, [2] occ gated, [3] phi gated
     MidDesc* d_midd = nullptr;  // pairs in the same order
     OrientDesc* d_od_all = nullptr;
@@ -1043,6 +1065,7 @@ struct psb_tray {
         if (dev >= 0) cudaSetDevice(dev);
         release_slots();
         dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_wocc, st); dfree(d_pen, st);
+        dfree(d_ostat, st);
         dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st);
         dfree(d_stage_runs, st); dfree(d_runs, st); dfree(d_pphi, st); dfree(d_pocc, st);
         dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_base_all, st); dfree(d_dec, st);
@@ -1296,9 +1319,21 @@ struct psb_tray {
 
     int set(const int32_t* tray, const int32_t* phi) {
         CK(cudaSetDevice(dev));
-        if (has_negative(tray, V)) return fail(PSB_ERR_ARG, "tray holds negative values; item ids must be >= 0");
-        occ = 0;
-        for (size_t i = 0; i < V; ++i) occ += tray[i] != 0;
+        // negative values and occupied cells, one pass over the host cores
+        std::atomic<int> neg(0);
+        std::atomic<size_t> nocc(0);
+        parallel_chunks(V, (size_t)1 << 20, [&](size_t b, size_t e) {
+            size_t c = 0;
+            int ng = 0;
+            for (size_t i = b; i < e; ++i) {
+                c += tray[i] != 0;
+                ng |= tray[i] < 0;
+            }
+            nocc += c;
+            if (ng) neg = 1;
+        });
+        if (neg) return fail(PSB_ERR_ARG, "tray holds negative values; item ids must be >= 0");
+        occ = nocc;
         CK(cudaMemcpyAsync(d_tray, tray, sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
         if (phi) {
             CK(cudaMemcpyAsync(d_phi, phi, sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
@@ -2587,6 +2622,29 @@ int psb_tray_get(psb_tray* t, int32_t* tray, int32_t* phi) {
     if (tray) CK(cudaMemcpyAsync(tray, t->d_tray, sizeof(int32_t) * t->V, cudaMemcpyDeviceToHost, t->st));
     if (phi) CK(cudaMemcpyAsync(phi, t->d_phi, sizeof(int32_t) * t->V, cudaMemcpyDeviceToHost, t->st));
     CK(cudaStreamSynchronize(t->st));
+    return PSB_OK;
+}
+
+int psb_tray_stats(psb_tray* t, long long* occupied, int32_t* lo, int32_t* hi) {
+    if (!t || !occupied || !lo || !hi) return fail(PSB_ERR_ARG, "null pointer");
+    if (!t->ready) return fail(PSB_ERR_STATE, "tray not initialised");
+    CK(cudaSetDevice(t->dev));
+    if (!t->d_ostat) TRY(dalloc(&t->d_ostat, 8, t->st));
+    struct {
+        unsigned long long count;
+        int box[6];
+    } h = {0ULL, {INT_MAX, INT_MAX, INT_MAX, -1, -1, -1}};
+    CK(cudaMemcpyAsync(t->d_ostat, &h, sizeof(h), cudaMemcpyHostToDevice, t->st));
+    pdl(k_occ_stats, 148 * 4, 256, 0, t->st)(t->d_tray, t->nx, t->ny, t->nz, (unsigned long long*)t->d_ostat,
+                                             t->d_ostat + 2);
+    CKL();
+    CK(cudaMemcpyAsync(&h, t->d_ostat, sizeof(h), cudaMemcpyDeviceToHost, t->st));
+    CK(cudaStreamSynchronize(t->st));
+    *occupied = (long long)h.count;
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = h.count ? h.box[a] : -1;
+        hi[a] = h.count ? h.box[3 + a] : -1;
+    }
     return PSB_OK;
 }
 

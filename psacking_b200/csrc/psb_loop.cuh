@@ -8,6 +8,8 @@
 // on "placed".  Gated kernels read a device flag and return at once when it
 // is 0.
 #pragma once
+#include <climits>
+
 #include "psb_kernels2.cuh"
 
 struct PhiStats {
@@ -321,5 +323,37 @@ __global__ void k_box_refresh(const int32_t* __restrict__ tray, int32_t* __restr
             const unsigned int b = __ballot_sync(0xffffffffu, z < nz && t[z] == 0);
             if (lane == 0) out[w] = b;
         }
+    }
+}
+
+// Occupied cells (> 0) of the tray and their bounding box, for the packing
+// result's statistics (packer.py:582-601): count += cells, box[0..2] = min
+// i, j, k, box[3..5] = max (preset to 0, INT_MAX and -1).
+// grid: 148 * 4, block 256
+__global__ void k_occ_stats(const int32_t* __restrict__ tray, int nx, int ny, int nz, unsigned long long* count,
+                            int* box) {
+    pdl_enter();
+    const size_t V = (size_t)nx * ny * nz;
+    unsigned int c = 0;
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {-1, -1, -1};
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < V; t += (size_t)gridDim.x * blockDim.x) {
+        if (tray[t] <= 0) continue;
+        ++c;
+        const int k = (int)(t % nz);
+        const size_t r = t / nz;
+        const int j = (int)(r % ny), i = (int)(r / ny);
+        lo[0] = min(lo[0], i); lo[1] = min(lo[1], j); lo[2] = min(lo[2], k);
+        hi[0] = max(hi[0], i); hi[1] = max(hi[1], j); hi[2] = max(hi[2], k);
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = __reduce_min_sync(0xffffffffu, lo[a]);
+        hi[a] = __reduce_max_sync(0xffffffffu, hi[a]);
+    }
+    if ((threadIdx.x & 31) != 0 || c == 0) return;
+    atomicAdd(count, (unsigned long long)c);
+    for (int a = 0; a < 3; ++a) {
+        atomicMin(&box[a], lo[a]);
+        atomicMax(&box[3 + a], hi[a]);
     }
 }

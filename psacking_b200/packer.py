@@ -108,15 +108,14 @@ class BinPacker:
     def _prepare(self, items, sort_by_volume, initial_tray):
         if len(items) == 0:
             raise ValueError("items list cannot be empty")
-        processed, volumes = [], []
+        processed = []
         for i, item in enumerate(items):
             if not isinstance(item, np.ndarray):
                 raise ValueError(f"Item {i} is not a numpy array")
             if item.ndim != 3:
                 raise ValueError(f"Item {i} must be 3D, got {item.ndim}D")
-            it = np.asarray(item, dtype=np.int32)   # no copy when already int32
-            processed.append(it)
-            volumes.append(int(np.count_nonzero(it > 0)))
+            processed.append(np.ascontiguousarray(item, dtype=np.int32))   # no copy when already int32
+        volumes = [int(v) for v in _core.positive_counts(processed)]   # np.sum(item > 0) per item
         if sort_by_volume:
             order = list(np.argsort(volumes)[::-1])
         else:
@@ -142,7 +141,7 @@ class BinPacker:
     def _pack_native(self, processed, volumes, order, tray, id_offset, n_items):
         maps = orientation_maps(self.num_orientations)
         seq = [np.ascontiguousarray(processed[i]) for i in order]
-        final, res = _core.pack_native(seq, tray, maps, bool(self.interlocking_free), int(id_offset))
+        final, res, stats = _core.pack_native(seq, tray, maps, bool(self.interlocking_free), int(id_offset))
         placements = []
         diag_or, ncand, err = 0, 0, 0.0
         for k, orig in enumerate(order):
@@ -156,7 +155,7 @@ class BinPacker:
             else:
                 placements.append(PlacementInfo(int(orig), None, None, False, volumes[orig], 0))
         return self._finish(final, placements, n_items,
-                            {"diag": diag_or, "candidates": ncand, "max_err_ratio": err})
+                            {"diag": diag_or, "candidates": ncand, "max_err_ratio": err}, stats)
 
     def _pack_calls(self, processed, volumes, order, tray, id_offset, n_items):
         # a fresh run never inherits a cached tray context (the reference's
@@ -204,10 +203,13 @@ class BinPacker:
                 placements.append(PlacementInfo(int(orig), None, None, False, volumes[orig], 0))
         return self._finish(tray, placements, n_items, None)
 
-    def _finish(self, tray, placements, n_items, diag):
+    def _finish(self, tray, placements, n_items, diag, stats=None):
         placements.sort(key=lambda p: p.item_index)
         num_placed = sum(1 for p in placements if p.success)
-        density, total, bbox = self._calculate_stats(tray)
+        if stats is None:
+            density, total, bbox = self._calculate_stats(tray)
+        else:
+            density, total, bbox = self._stats_from_counts(*stats)
         return PackingResult(tray=tray, placements=placements, num_placed=num_placed,
                              num_failed=n_items - num_placed, density=density, total_volume=total,
                              bounding_box=bbox, diagnostics=diag)
@@ -248,6 +250,16 @@ class BinPacker:
         if found:
             return tuple(pos), True, score
         return None, False, 0.0
+
+    @staticmethod
+    def _stats_from_counts(occupied, lo, hi):
+        """_calculate_stats from the occupied-cell count and bounding box
+        the engine computed on the device (psb_tray_stats)."""
+        if occupied == 0:
+            return 0.0, 0, None
+        lo, hi = tuple(int(v) for v in lo), tuple(int(v) for v in hi)
+        vol = int(np.prod([b - a + 1 for a, b in zip(lo, hi)]))
+        return (float(occupied / vol) if vol > 0 else 0.0), int(occupied), (lo, hi)
 
     def _calculate_stats(self, tray: np.ndarray):
         """packer.py:582-601: density = occupied / bounding-box volume."""

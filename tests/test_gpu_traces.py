@@ -45,6 +45,10 @@ def _check(tr, res):
     assert hashlib.sha256(np.ascontiguousarray(res.tray, np.int32).tobytes()).hexdigest() == tr["tray_sha256"]
     assert res.num_placed == tr["num_placed"]
     assert res.density == tr["density"]
+    # the statistics counted on the device equal the host computation
+    from psacking_b200 import BinPacker
+    want = BinPacker(tuple(tr["tray"]))._calculate_stats(res.tray)
+    assert (res.density, res.total_volume, res.bounding_box) == want
 
 
 @pytest.mark.parametrize("name", TRACES)

@@ -64,3 +64,18 @@ def test_workloads_deterministic_and_in_range():
     assert all(20 <= max(i.shape) <= 50 for i in c3)
     c2 = workloads.config2_items(0, n=10)
     assert all(max(i.shape) <= 40 for i in c2)
+
+
+def test_positive_counts_match_numpy():
+    """BinPacker's item volumes (cells > 0) are counted natively on the host
+    cores; they must equal numpy's count for every item, with negative,
+    zero and non-contiguous inputs among them."""
+    from psacking_b200 import _core
+    rng = np.random.default_rng(5)
+    items = [rng.integers(-2, 4, tuple(rng.integers(1, 30, 3))).astype(np.int32) for _ in range(70)]
+    items.append(np.zeros((3, 4, 5), np.int32))
+    items.append(np.asfortranarray(rng.integers(0, 2, (9, 8, 7)).astype(np.int32)))
+    want = [int(np.count_nonzero(a > 0)) for a in items]
+    assert [int(v) for v in _core.positive_counts(items)] == want
+    _, volumes, _, _, _ = BinPacker((40, 40, 40))._prepare(items, True, None)
+    assert volumes == want
