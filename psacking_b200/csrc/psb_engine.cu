@@ -310,7 +310,10 @@ int g_active_grid = 8;
 // orientations' list (PSB_LIST_SELECT=1).  Off: measured slower (same box,
 // items placed/s: off 1243.3, on 1238.2; k_ff_union 9.4 -> 12.4 ms per run):
 // those kernels hold no shared memory, so a CTA row per orientation costs
-// little, and the list serialises orientations within a row.
+// little, and the list serialises orientations within a row.  Also measured
+// with launch overlap on, and only for items the candidate filter ran on:
+// lists there 1380.5 against 1405.3 without; the transform kernels with 2 /
+// 3 / 4 instead of 8 CTA rows on those items 1146.5 / 1258.2 / 1286.8.
 bool g_list_select = false;
 // k_cand_filter variant for trays of at most 128 cells per column (tuning:
 // 0 = 8-sample batches within 64 registers, 1 = 4-sample batches and 12
