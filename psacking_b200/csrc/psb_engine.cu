@@ -14,6 +14,7 @@
 #include <cstddef>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -212,6 +213,11 @@ bool g_fast_fft = true;  // specialised two-pass kernels where a plan exists
 // 0 disables (PSB_PAD_MAX).  Default 3 (config-5 trays, 64 trays of sides
 // 64-160: 0 -> 506, 2 -> 562, 3 -> 578 / 626 items placed/s).
 double g_pad_max = 3.0;
+// psb_pack stages its items in two parts when it has at least 2 x
+// kStreamFirst of them: the first kStreamFirst before the loop, the rest
+// while they are searched (PSB_STREAM_STAGE=0: all before the loop)
+bool g_stream_stage = true;
+constexpr int kStreamFirst = 32;
 
 
 using XpassFn = void (*)(const OrientDesc*, SearchBufs, const float2*, const float2*, int, const float2*,
@@ -409,6 +415,7 @@ int set_smem_attrs() {
         if (atoi(e) > 1) g_filter_groups = atoi(e);
     }
     if (const char* e = getenv("PSB_PDL")) g_pdl = atoi(e) != 0;
+    if (const char* e = getenv("PSB_STREAM_STAGE")) g_stream_stage = atoi(e) != 0;
     if (const char* e = getenv("PSB_LATE_MAX")) g_late_max = std::min(std::max(0, atoi(e)), kCandCap);
     TRY(set_max_dyn_smem(k_rfft_z));
     TRY(set_max_dyn_smem(k_irfft_z_int));
@@ -1025,20 +1032,25 @@ struct psb_tray {
     ResultDev* d_res = nullptr;
     long long sAi = 0, sBi = 0, sP = 0, sD = 0, sBits = 0, sLine = 0, sRun = 0;
 
-    // items of a packing run, staged once (psb_pack_stage)
+    // items of a packing run, staged once (psb_pack_stage) in one part, or
+    // in two by psb_pack (the second part analysed and uploaded while the
+    // first part's items are searched).  A part is one device block (runs,
+    // samples, dense arrays) filled from one pinned host block.
     std::vector<ItemInfo> staged;
-    std::vector<size_t> staged_off;
-    int32_t* d_stage = nullptr;
-    size_t stage_cap = 0;
-    std::vector<size_t> staged_soff;   // the items' filter samples in d_stage_samp
-    int4* d_stage_samp = nullptr;
-    size_t stage_scap = 0;
-    void* h_stage = nullptr;   // pinned host staging buffer of psb_pack_stage
-    size_t h_stage_cap = 0;
-
-    std::vector<std::array<size_t, 3>> staged_roff;   // the items' runs (per source axis) in d_stage_runs
-    int4* d_stage_runs = nullptr;
-    size_t stage_rcap = 0;
+    struct StagedDev {
+        const int32_t* item;    // the item's int32 array
+        const int4* samp;       // its filter samples
+        const int4* runs[3];    // its runs along each source axis
+    };
+    std::vector<StagedDev> sdev;
+    char* d_part[2] = {nullptr, nullptr};
+    size_t part_cap[2] = {0, 0};
+    void* h_part[2] = {nullptr, nullptr};
+    size_t h_part_cap[2] = {0, 0};
+    void* h_desc = nullptr;          // pinned copy of the run's descriptors
+    size_t h_desc_cap = 0;
+    cudaStream_t st_copy = nullptr;  // uploads of the second part
+    cudaEvent_t ev_copy = nullptr;
 
     // item staging
     int32_t* d_items = nullptr;
@@ -1069,20 +1081,36 @@ struct psb_tray {
         release_slots();
         dfree(d_tray, st); dfree(d_phi, st); dfree(d_Socc, st); dfree(d_Sphi, st); dfree(d_w1, st); dfree(d_w2, st); dfree(d_wocc, st); dfree(d_pen, st);
         dfree(d_ostat, st);
-        dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st); dfree(d_stage, st);
-        dfree(d_stage_runs, st); dfree(d_runs, st); dfree(d_pphi, st); dfree(d_pocc, st);
+        dfree(d_rz, st); dfree(d_mid, st); dfree(d_stats, st); dfree(d_err, st); dfree(d_first, st); dfree(d_needff, st); dfree(d_items, st); dfree(d_vox, st);
+        dfree(d_runs, st); dfree(d_pphi, st); dfree(d_pocc, st);
         dfree(d_ls, st); dfree(d_ps, st); dfree(d_rzd, st); dfree(d_midd, st); dfree(d_od_all, st); dfree(d_base_all, st); dfree(d_dec, st);
-        dfree(d_tbits, st); dfree(d_stage_samp, st); dfree(d_work, st); dfree(d_clist, st);
+        dfree(d_tbits, st); dfree(d_work, st); dfree(d_clist, st);
+        for (int p = 0; p < 2; ++p) {
+            dfree(d_part[p], st);
+            part_cap[p] = 0;
+        }
         clist_cap = 0;
         tq = 0;
+        if (st_copy) {
+            cudaStreamSynchronize(st_copy);
+            cudaStreamDestroy(st_copy);
+        }
+        st_copy = nullptr;
+        if (ev_copy) cudaEventDestroy(ev_copy);
+        ev_copy = nullptr;
         if (st) {
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
         }
         st = nullptr;
-        if (h_stage) cudaFreeHost(h_stage);
-        h_stage = nullptr;
-        h_stage_cap = 0;
+        for (int p = 0; p < 2; ++p) {
+            if (h_part[p]) cudaFreeHost(h_part[p]);
+            h_part[p] = nullptr;
+            h_part_cap[p] = 0;
+        }
+        if (h_desc) cudaFreeHost(h_desc);
+        h_desc = nullptr;
+        h_desc_cap = 0;
     }
 
     int init(int x, int y, int z) {
@@ -2689,109 +2717,121 @@ int psb_tray_place(psb_tray* t, const int32_t* item, int ex, int ey, int ez, int
     return PSB_OK;
 }
 
-int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items) {
-    if (!t || (!items && n_items > 0) || !dims || n_items < 0) return fail(PSB_ERR_ARG, "null pointer");
-    CK(cudaSetDevice(t->dev));
-    t->staged.clear();
-    t->staged_off.clear();
-    t->staged_soff.clear();
-    t->staged_roff.clear();
+}  // extern "C"
+
+namespace {
+// Staging of a packing run's items (psb_pack_stage, psb_pack).
+
+// Null arrays, bad dims and negative values, checked for every item before
+// anything is staged (items spread over the host cores).
+int stage_check(const int32_t* const* items, const int32_t* dims, int n_items) {
     for (int it = 0; it < n_items; ++it) {
         const int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
         if (!items[it] || ex <= 0 || ey <= 0 || ez <= 0) return fail(PSB_ERR_ARG, "item %d: bad array", it);
     }
-    // item analysis (bounds, sums, voxel lists) on all host cores
-    t->staged.resize(n_items);
     std::vector<char> neg(n_items, 0);
-    {
-        std::atomic<int> next(0);
-        auto work = [&]() {
-            for (int it = next.fetch_add(1); it < n_items; it = next.fetch_add(1)) {
-                const int ex = dims[3 * it], ey = dims[3 * it + 1], ez = dims[3 * it + 2];
-                const size_t m = (size_t)ex * ey * ez;
-                if (has_negative(items[it], m)) { neg[it] = 1; continue; }
-                // the packing loop places items by their runs: no voxel list;
-                // bounds, sums and samples come from the z-runs
-                ItemInfo& inf = t->staged[it];
-                inf.dims[0] = ex; inf.dims[1] = ey; inf.dims[2] = ez;
-                for (int a = 0; a < 3; ++a) build_runs(items[it], &inf, a);
-                analyse_runs(&inf);
-                pick_samples(&inf);
-            }
-        };
-        const int nthr = std::max(1, std::min<int>(n_items / 8, (int)std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for (int w = 1; w < nthr; ++w) pool.emplace_back(work);
-        work();
-        for (auto& th : pool) th.join();
-    }
+    parallel_chunks((size_t)n_items, 4, [&](size_t b, size_t e) {
+        for (size_t it = b; it < e; ++it) {
+            const size_t m = (size_t)dims[3 * it] * dims[3 * it + 1] * dims[3 * it + 2];
+            neg[it] = has_negative(items[it], m) ? 1 : 0;
+        }
+    });
     for (int it = 0; it < n_items; ++it)
         if (neg[it]) return fail(PSB_ERR_ARG, "item %d holds negative values", it);
-    size_t tot = 0, tots = 0, totr = 0;
-    for (int it = 0; it < n_items; ++it) {
-        const ItemInfo& inf = t->staged[it];
-        t->staged_off.push_back(tot);
-        t->staged_soff.push_back(tots);
-        std::array<size_t, 3> ro;
-        for (int a = 0; a < 3; ++a) {
-            ro[a] = totr;
-            totr += inf.runs[a].size();
+    return PSB_OK;
+}
+
+// Runs, bounds, sums and filter samples of items [i0, i1) into t->staged
+// (host only; the packing loop places items by their runs, so no voxel list
+// is built).
+void stage_analyse(psb_tray* t, const int32_t* const* items, const int32_t* dims, int i0, int i1) {
+    parallel_chunks((size_t)(i1 - i0), 1, [&](size_t b, size_t e) {
+        for (size_t k = b; k < e; ++k) {
+            const int it = i0 + (int)k;
+            ItemInfo& inf = t->staged[it];
+            for (int a = 0; a < 3; ++a) inf.dims[a] = dims[3 * it + a];
+            for (int a = 0; a < 3; ++a) build_runs(items[it], &inf, a);
+            analyse_runs(&inf);
+            pick_samples(&inf);
         }
-        t->staged_roff.push_back(ro);
-        tot += (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
-        tots += inf.samp.size();
+    });
+}
+
+// Items [i0, i1) as one part: the part's device block holds their runs,
+// samples and int32 arrays, filled from the part's pinned host block by one
+// copy on stream s (no synchronisation); t->sdev gets their device pointers.
+int stage_upload(psb_tray* t, const int32_t* const* items, int i0, int i1, int part, cudaStream_t s) {
+    size_t n4 = 0, n1 = 0;   // int4 entries (runs, samples), int32 cells
+    for (int it = i0; it < i1; ++it) {
+        const ItemInfo& inf = t->staged[it];
+        for (int a = 0; a < 3; ++a) n4 += inf.runs[a].size();
+        n4 += inf.samp.size();
+        n1 += (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
     }
-    if (totr > t->stage_rcap) {
-        dfree(t->d_stage_runs, t->st);
-        t->stage_rcap = totr;
-        TRY(dalloc(&t->d_stage_runs, totr, t->st));
+    const size_t bytes = sizeof(int4) * n4 + sizeof(int32_t) * n1;
+    if (bytes > t->part_cap[part]) {
+        dfree(t->d_part[part], t->st);
+        t->part_cap[part] = 0;
+        TRY(dalloc(&t->d_part[part], bytes, s));
+        t->part_cap[part] = bytes;
     }
-    if (tots > t->stage_scap) {
-        dfree(t->d_stage_samp, t->st);
-        t->stage_scap = tots;
-        TRY(dalloc(&t->d_stage_samp, tots, t->st));
+    if (bytes > t->h_part_cap[part]) {
+        if (t->h_part[part]) cudaFreeHost(t->h_part[part]);
+        t->h_part[part] = nullptr;
+        t->h_part_cap[part] = 0;
+        CK(cudaMallocHost(&t->h_part[part], bytes));
+        t->h_part_cap[part] = bytes;
     }
-    if (tot > t->stage_cap) {
-        dfree(t->d_stage, t->st);
-        t->stage_cap = tot;
-        TRY(dalloc(&t->d_stage, tot, t->st));
+    // offsets: every item's runs and samples, then the int32 arrays
+    std::vector<size_t> o4(i1 - i0), o1(i1 - i0);
+    size_t a4 = 0, a1 = 0;
+    for (int it = i0; it < i1; ++it) {
+        const ItemInfo& inf = t->staged[it];
+        o4[it - i0] = a4;
+        o1[it - i0] = a1;
+        for (int a = 0; a < 3; ++a) a4 += inf.runs[a].size();
+        a4 += inf.samp.size();
+        a1 += (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
     }
-    // one pinned staging buffer for the item arrays, samples and runs: three
-    // large copies instead of small pageable ones per item
-    const size_t bytes = sizeof(int32_t) * tot + sizeof(int4) * (tots + totr);
-    if (bytes > t->h_stage_cap) {
-        if (t->h_stage) cudaFreeHost(t->h_stage);
-        t->h_stage = nullptr;
-        t->h_stage_cap = 0;
-        CK(cudaMallocHost(&t->h_stage, bytes));
-        t->h_stage_cap = bytes;
-    }
-    int32_t* hi = (int32_t*)t->h_stage;
-    int4* hs = (int4*)(hi + tot);
-    int4* hr = hs + tots;
-    {
-        // the copies into the pinned buffer, items spread over the host cores
-        std::atomic<int> next(0);
-        auto work = [&]() {
-            for (int it = next.fetch_add(1); it < n_items; it = next.fetch_add(1)) {
-                const ItemInfo& inf = t->staged[it];
-                memcpy(hi + t->staged_off[it], items[it], sizeof(int32_t) * inf.dims[0] * inf.dims[1] * inf.dims[2]);
-                if (!inf.samp.empty())
-                    memcpy(hs + t->staged_soff[it], inf.samp.data(), sizeof(int4) * inf.samp.size());
-                for (int a = 0; a < 3; ++a)
-                    if (!inf.runs[a].empty())
-                        memcpy(hr + t->staged_roff[it][a], inf.runs[a].data(), sizeof(int4) * inf.runs[a].size());
+    int4* h4 = (int4*)t->h_part[part];
+    int32_t* h1 = (int32_t*)(h4 + n4);
+    const int4* d4 = (const int4*)t->d_part[part];
+    const int32_t* d1 = (const int32_t*)(d4 + n4);
+    parallel_chunks((size_t)(i1 - i0), 1, [&](size_t b, size_t e) {
+        for (size_t k = b; k < e; ++k) {
+            const int it = i0 + (int)k;
+            const ItemInfo& inf = t->staged[it];
+            psb_tray::StagedDev& sd = t->sdev[it];
+            size_t q = o4[k];
+            for (int a = 0; a < 3; ++a) {
+                if (!inf.runs[a].empty()) memcpy(h4 + q, inf.runs[a].data(), sizeof(int4) * inf.runs[a].size());
+                sd.runs[a] = d4 + q;
+                q += inf.runs[a].size();
             }
-        };
-        const int nthr = std::max(1, std::min<int>(n_items / 8, (int)std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for (int w = 1; w < nthr; ++w) pool.emplace_back(work);
-        work();
-        for (auto& th : pool) th.join();
-    }
-    if (tot) CK(cudaMemcpyAsync(t->d_stage, hi, sizeof(int32_t) * tot, cudaMemcpyHostToDevice, t->st));
-    if (tots) CK(cudaMemcpyAsync(t->d_stage_samp, hs, sizeof(int4) * tots, cudaMemcpyHostToDevice, t->st));
-    if (totr) CK(cudaMemcpyAsync(t->d_stage_runs, hr, sizeof(int4) * totr, cudaMemcpyHostToDevice, t->st));
+            if (!inf.samp.empty()) memcpy(h4 + q, inf.samp.data(), sizeof(int4) * inf.samp.size());
+            sd.samp = d4 + q;
+            const size_t m = (size_t)inf.dims[0] * inf.dims[1] * inf.dims[2];
+            memcpy(h1 + o1[k], items[it], sizeof(int32_t) * m);
+            sd.item = d1 + o1[k];
+        }
+    });
+    if (bytes) CK(cudaMemcpyAsync(t->d_part[part], t->h_part[part], bytes, cudaMemcpyHostToDevice, s));
+    return PSB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items) {
+    if (!t || (!items && n_items > 0) || !dims || n_items < 0) return fail(PSB_ERR_ARG, "null pointer");
+    CK(cudaSetDevice(t->dev));
+    t->staged.clear();
+    t->sdev.clear();
+    TRY(stage_check(items, dims, n_items));
+    t->staged.resize(n_items);
+    t->sdev.resize(n_items);
+    stage_analyse(t, items, dims, 0, n_items);
+    TRY(stage_upload(t, items, 0, n_items, 0, t->st));
     CK(cudaStreamSynchronize(t->st));
     return PSB_OK;
 }
@@ -2812,6 +2852,10 @@ struct PackOpts {
     // d_local, exchange(ctx) gathers every rank's into d_all, and the merged
     // winner is placed
     int rank = 0, world = 1;
+    // staging in two parts (psb_pack): items from feed_at on are staged by
+    // feed() when the loop reaches them, uploaded on the tray's copy stream
+    std::function<int()> feed;
+    int feed_at = 0;
     void* d_local = nullptr;
     void* d_all = nullptr;
     psb_exchange_fn exchange = nullptr;
@@ -2895,39 +2939,12 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
     TRY(t->ensure_slots(std::max(n_orient, 6)));
     // every orientation of every item, described once (bounds, maps, sizes);
     // the error bounds are filled on the device by k_prep from the current
-    // distance statistics
+    // distance statistics.  Items [i0, i1) at a time: with a feed (psb_pack)
+    // the items from opt.feed_at on are described when the loop reaches them.
     std::vector<OrientDesc> all((size_t)n_items * n_orient);
-    for (int it = 0; it < n_items; ++it)
-        for (int o = 0; o < n_orient; ++o) {
-            const int4* rn[3];
-            for (int a = 0; a < 3; ++a) rn[a] = t->d_stage_runs + t->staged_roff[it][a];
-            t->describe(t->staged[it], orient_maps + 6 * o, orient_maps + 6 * o + 3,
-                        t->d_stage + t->staged_off[it], nullptr, rn,
-                        &all[(size_t)it * n_orient + o]);
-        }
-    // orientation sharding: the other ranks' orientations are not searched here
-    if (opt.world > 1)
-        for (int it = 0; it < n_items; ++it)
-            for (int o = 0; o < n_orient; ++o)
-                if (o % opt.world != opt.rank) all[(size_t)it * n_orient + o].skip = 1;
+    std::vector<OrientDesc> allb((size_t)n_items * 6);   // each item's 6 axis permutations
     // candidate-filter samples (tray columns of at most 256 cells)
     const bool filt = g_cand_filter && t->nzw <= 8;
-    if (filt)
-        for (int it = 0; it < n_items; ++it)
-            for (int o = 0; o < n_orient; ++o) {
-                OrientDesc& od = all[(size_t)it * n_orient + o];
-                od.samp = t->d_stage_samp + t->staged_soff[it];
-                od.nsamp = (int)t->staged[it].samp.size();
-            }
-    // each item's 6 axis permutations (the flips of one share its spectrum)
-    std::vector<OrientDesc> allb((size_t)n_items * 6);
-    for (int it = 0; it < n_items; ++it) {
-        std::vector<OrientDesc> slice(all.begin() + (size_t)it * n_orient, all.begin() + (size_t)(it + 1) * n_orient);
-        std::vector<OrientDesc> b;
-        if (!make_bases(&slice, &b)) return fail(PSB_ERR_STATE, "item %d: orientations of different items", it);
-        std::copy(slice.begin(), slice.end(), all.begin() + (size_t)it * n_orient);
-        std::copy(b.begin(), b.end(), allb.begin() + (size_t)it * 6);
-    }
     if (all.size() > t->od_all_cap) {
         dfree(t->d_od_all, t->st);
         t->od_all_cap = all.size();
@@ -2938,13 +2955,56 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         t->base_all_cap = allb.size();
         TRY(dalloc(&t->d_base_all, t->base_all_cap, t->st));
     }
-    CK(cudaMemcpyAsync(t->d_base_all, allb.data(), sizeof(OrientDesc) * allb.size(), cudaMemcpyHostToDevice, t->st));
     if ((size_t)n_items > t->dec_cap) {
         dfree(t->d_dec, t->st);
         t->dec_cap = n_items;
         TRY(dalloc(&t->d_dec, t->dec_cap, t->st));
     }
-    CK(cudaMemcpyAsync(t->d_od_all, all.data(), sizeof(OrientDesc) * all.size(), cudaMemcpyHostToDevice, t->st));
+    // descriptors go to the device from pinned memory, so an upload queued
+    // while the loop runs does not wait for the stream
+    const size_t dbytes = sizeof(OrientDesc) * (all.size() + allb.size());
+    if (dbytes > t->h_desc_cap) {
+        if (t->h_desc) cudaFreeHost(t->h_desc);
+        t->h_desc = nullptr;
+        t->h_desc_cap = 0;
+        CK(cudaMallocHost(&t->h_desc, dbytes));
+        t->h_desc_cap = dbytes;
+    }
+    OrientDesc* hd_all = (OrientDesc*)t->h_desc;
+    OrientDesc* hd_base = hd_all + all.size();
+    auto describe_range = [&](int i0, int i1, cudaStream_t s) -> int {
+        for (int it = i0; it < i1; ++it) {
+            const psb_tray::StagedDev& sd = t->sdev[it];
+            for (int o = 0; o < n_orient; ++o) {
+                OrientDesc& od = all[(size_t)it * n_orient + o];
+                t->describe(t->staged[it], orient_maps + 6 * o, orient_maps + 6 * o + 3, sd.item, nullptr, sd.runs,
+                            &od);
+                // orientation sharding: the other ranks' orientations are not searched here
+                if (opt.world > 1 && o % opt.world != opt.rank) od.skip = 1;
+                if (filt) {
+                    od.samp = sd.samp;
+                    od.nsamp = (int)t->staged[it].samp.size();
+                }
+            }
+            // the flips of one axis permutation share its spectrum
+            std::vector<OrientDesc> slice(all.begin() + (size_t)it * n_orient,
+                                          all.begin() + (size_t)(it + 1) * n_orient);
+            std::vector<OrientDesc> b;
+            if (!make_bases(&slice, &b)) return fail(PSB_ERR_STATE, "item %d: orientations of different items", it);
+            std::copy(slice.begin(), slice.end(), all.begin() + (size_t)it * n_orient);
+            std::copy(b.begin(), b.end(), allb.begin() + (size_t)it * 6);
+        }
+        const size_t a0 = (size_t)i0 * n_orient, na = (size_t)(i1 - i0) * n_orient;
+        const size_t b0 = (size_t)i0 * 6, nb = (size_t)(i1 - i0) * 6;
+        memcpy(hd_all + a0, all.data() + a0, sizeof(OrientDesc) * na);
+        memcpy(hd_base + b0, allb.data() + b0, sizeof(OrientDesc) * nb);
+        CK(cudaMemcpyAsync(t->d_od_all + a0, hd_all + a0, sizeof(OrientDesc) * na, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(t->d_base_all + b0, hd_base + b0, sizeof(OrientDesc) * nb, cudaMemcpyHostToDevice, s));
+        return PSB_OK;
+    };
+    if (opt.feed && (opt.prop || opt.feed_at <= 0 || opt.feed_at >= n_items))
+        return fail(PSB_ERR_STATE, "a staged feed needs 0 < feed_at < n_items and no proposal");
+    TRY(describe_range(0, opt.feed ? opt.feed_at : n_items, t->st));
     LoopState ls0;
     memset(&ls0, 0, sizeof(ls0));
     ls0.id_offset = id_offset;
@@ -2987,8 +3047,8 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             for (int a = 0; a < 3; ++a) G[3 * it + a] = (inf.dims[a] + sc - 1) / sc;
             const int nr = (int)inf.runs[2].size();
             if (nr > 0)
-                pdl(k_base_grid_runs, (nr + 255) / 256, 256, 0, t->st)(t->d_stage_runs + t->staged_roff[it][2], nr,
-                                                                      sc, d_pgrid + (size_t)it * PSB_PG3);
+                pdl(k_base_grid_runs, (nr + 255) / 256, 256, 0, t->st)(t->sdev[it].runs[2], nr, sc,
+                                                                      d_pgrid + (size_t)it * PSB_PG3);
             CKL();
         }
         CK(cudaMemcpyAsync(d_pG, G.data(), sizeof(int) * G.size(), cudaMemcpyHostToDevice, t->st));
@@ -3024,6 +3084,15 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
     size_t occ_est = t->occ;
     std::vector<OrientDesc> host_ods(n_orient);
     for (int it = 0; it < n_items; ++it) {
+        if (opt.feed && it == opt.feed_at) {
+            // the rest of the items, staged by the caller while the first
+            // part was searched: uploaded on the copy stream, which the
+            // loop's stream then waits for
+            TRY(opt.feed());
+            TRY(describe_range(opt.feed_at, n_items, t->st_copy));
+            CK(cudaEventRecord(t->ev_copy, t->st_copy));
+            CK(cudaStreamWaitEvent(t->st, t->ev_copy, 0));
+        }
         OrientDesc* d_odb = t->d_od_all + (size_t)it * n_orient;
         for (int o = 0; o < n_orient; ++o) host_ods[o] = all[(size_t)it * n_orient + o];
         pdl(k_prep, (n_orient + 63) / 64, 64, 0, t->st)(d_odb, n_orient, t->d_ps);
@@ -3170,8 +3239,39 @@ extern "C" {
 
 int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items, const int32_t* orient_maps,
              int n_orient, int interlock, int32_t id_offset, psb_result* out_placements, int32_t* final_tray) {
-    TRY(psb_pack_stage(t, items, dims, n_items));
-    return psb_pack_staged(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray);
+    const int first = kStreamFirst;
+    if (!g_stream_stage || n_items < 2 * first || !t || !items || !dims || !t->ready) {
+        TRY(psb_pack_stage(t, items, dims, n_items));
+        return psb_pack_staged(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray);
+    }
+    // Staged in two parts: the first items are analysed and uploaded before
+    // the loop starts, the rest is analysed on the host cores while the
+    // first part is searched and uploaded on the copy stream when the loop
+    // reaches it.  Every item is checked before anything is staged.
+    CK(cudaSetDevice(t->dev));
+    t->staged.clear();
+    t->sdev.clear();
+    TRY(stage_check(items, dims, n_items));
+    t->staged.resize(n_items);
+    t->sdev.resize(n_items);
+    if (!t->st_copy) CK(cudaStreamCreateWithFlags(&t->st_copy, cudaStreamNonBlocking));
+    if (!t->ev_copy) CK(cudaEventCreateWithFlags(&t->ev_copy, cudaEventDisableTiming));
+    stage_analyse(t, items, dims, 0, first);
+    TRY(stage_upload(t, items, 0, first, 0, t->st));
+    std::thread rest([=] { stage_analyse(t, items, dims, first, n_items); });
+    struct Join {
+        std::thread& th;
+        ~Join() {
+            if (th.joinable()) th.join();
+        }
+    } join{rest};
+    PackOpts o;
+    o.feed_at = first;
+    o.feed = [&]() -> int {
+        rest.join();
+        return stage_upload(t, items, first, n_items, 1, t->st_copy);
+    };
+    return pack_staged_impl(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray, o);
 }
 
 int psb_pack_many(int n_trays, const int32_t* tray_dims, const int32_t* const* items, const int32_t* item_dims,
