@@ -1465,17 +1465,17 @@ struct psb_tray {
         }
         if (xmax > 0) {
             const dim3 grid(xmax, n);
-            CK(cudaMemsetAsync(d_ccount, 0, sizeof(int) * 3 * cap, st));
+            // (k_cand_prep zeroes the counters d_ccount, d_vcount, d_ncol)
             const size_t smw = sizeof(uint4) * (size_t)emax * ny * tq + (size_t)n;
             if (g_filter_plane && smw <= (size_t)g_smem_optin) {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
-                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound);
+                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap);
                     pdl(k_cand_filter_plane<1>, dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st)(
                         d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
                         d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
                 } else {
-                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound);
+                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap);
                     pdl(k_cand_filter_plane<2>, dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st)(
                         d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
                         d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
@@ -1483,7 +1483,7 @@ struct psb_tray {
             } else {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
-                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound);
+                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap);
                     // the variant (sample batch, CTAs per SM bound) is a tuning switch
                     auto kf = g_filter_variant == 1 ? k_cand_filter<1, 4, 12>
                             : g_filter_variant == 2 ? k_cand_filter<1, 8, 1>
@@ -1492,7 +1492,7 @@ struct psb_tray {
                                                           (long long)nx, d_ccount, d_fsamp, d_fbound, g_filter_cut,
                                                           d_clist, ccap, nz);
                 } else {
-                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound);
+                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap);
                     pdl(k_cand_filter<2>, grid, PSB_FILT_THREADS, 0, st)(d_odb, d_tbits, ny, nzw, d_free, sBits,
                                                                         d_candplane, (long long)nx, d_ccount,
                                                                         d_fsamp, d_fbound, g_filter_cut, d_clist,
@@ -1500,12 +1500,13 @@ struct psb_tray {
                 }
             }
             CKL();
-            pdl(k_cand_apply, (n + 127) / 128, 128, 0, st)(d_odb, n, d_ccount, 0, dmax);
+            // with direct decisions the okplane flags of the free cells
+            // (non-interlocking mode) are set by the verification for direct
+            // orientations, so k_cand_apply clears them first
+            pdl(k_cand_apply, (n + 127) / 128, 128, 0, st)(d_odb, n, d_ccount, 0, dmax, dmax > 0 ? d_okplane : nullptr,
+                                                           (long long)nx, nx);
             CKL();
             if (dmax > 0) {
-                // the okplane flags of the free cells (non-interlocking mode)
-                // are set here for direct orientations, so clear them first
-                CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
                 {
                     PROF("k_cand_verify", st);
                     pdl(k_item_cols, dim3(emax, n), 64, 0, st)(d_odb, d_icols, (long long)nx * ny, d_ncol);
@@ -1515,7 +1516,7 @@ struct psb_tray {
                         (long long)nx * ny, d_ncol, d_vcount, d_okplane, (long long)nx, interlock ? 0 : 1);
                 }
                 CKL();
-                pdl(k_cand_apply, (n + 127) / 128, 128, 0, st)(d_odb, n, d_vcount, 1, dmax);
+                pdl(k_cand_apply, (n + 127) / 128, 128, 0, st)(d_odb, n, d_vcount, 1, dmax, nullptr, 0LL, 0);
                 CKL();
             }
         }
@@ -1536,6 +1537,17 @@ struct psb_tray {
         return sp;
     }
 
+    // Reset of the search state before a search's kernels (k_search_reset);
+    // split: the split flow, whose plane flags are cleared here unless the
+    // candidate filter has done so for its direct orientations
+    int search_reset(int n, bool split) {
+        SearchReset a{d_smin, d_best, d_bestkey, d_diag, d_errmax, d_ncand, d_total, d_err,
+                      split && !direct_active ? d_okplane : nullptr, (long long)nx * n, n};
+        pdl(k_search_reset, 4, 256, 0, st)(a);
+        CKL();
+        return PSB_OK;
+    }
+
     // Flood fill (Algorithm 3) of every orientation's free bits into its
     // reach bits.  okplane, when set, receives the planes that hold a
     // reachable cell; gate, when set, makes every launch conditional.
@@ -1549,7 +1561,7 @@ struct psb_tray {
         const int lines = nx * ny;
         const int nblk = (lines + 255) / 256;
         const dim3 gl(nblk, rows);
-        CK(cudaMemsetAsync(d_total, 0, sizeof(int) * n, st));
+        // (the run counters d_total were zeroed by search_reset)
         {
             PROF("k_ff_runs", st);
             pdl(k_ff_runs, gl, 256, 0, st)(d_odb, fb, sp);
@@ -1582,9 +1594,9 @@ struct psb_tray {
                      PlaneFn p1, size_t smem, ResultDev* d_out, bool spec) {
         SearchBufs sb{d_Bi, d_Pc, d_Pd, sBi, sP, d_work, act_ready ? d_act : nullptr, act_ready ? d_nact : nullptr};
         const int rows = act_ready ? std::min(n, g_active_grid) : n;
-        // (with direct orientations the candidate filter cleared the flags and
-        // set those of its verified planes already)
-        if (!direct_active) CK(cudaMemsetAsync(d_okplane, 0, (size_t)nx * n, st));
+        // (the plane flags were cleared by search_reset, or, with direct
+        // orientations, by the candidate filter, which set those of its
+        // verified planes already)
         const int ncols = g.F[1] * g.H;
         XpassFn xf1 = xf ? xpass2_for(g.F[0], 1, spec) : nullptr, xf2 = xf ? xpass2_for(g.F[0], 2, spec) : nullptr;
         const BaseMap bm{g.F[1], g.H, g.F[2], g.p[1].tw, g.p[2].tw};
@@ -1726,13 +1738,7 @@ struct psb_tray {
                     pdl(ffb, dim3(bx, 6), 256, smf, st)(src, d_bases_in, g.p[1].tw, g.p[2].tw);
                 }
                 CKL();
-                CK(cudaMemsetAsync(d_smin, 0xff, sizeof(unsigned long long) * n, st));
-                CK(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long) * n, st));
-                CK(cudaMemsetAsync(d_bestkey, 0xff, sizeof(unsigned long long) * n, st));
-                CK(cudaMemsetAsync(d_diag, 0, sizeof(unsigned int) * n, st));
-                CK(cudaMemsetAsync(d_errmax, 0, sizeof(unsigned int) * n, st));
-                CK(cudaMemsetAsync(d_ncand, 0, sizeof(int) * n, st));
-                CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
+                TRY(search_reset(n, true));
                 return search_split(d_odb, n, score_params(mode), interlock, xf, p0, p1, sm3, d_out, true);
             }
         }
@@ -1775,13 +1781,7 @@ struct psb_tray {
             }
         }
         CKL();
-        CK(cudaMemsetAsync(d_smin, 0xff, sizeof(unsigned long long) * n, st));
-        CK(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long) * n, st));
-        CK(cudaMemsetAsync(d_bestkey, 0xff, sizeof(unsigned long long) * n, st));
-        CK(cudaMemsetAsync(d_diag, 0, sizeof(unsigned int) * n, st));
-        CK(cudaMemsetAsync(d_errmax, 0, sizeof(unsigned int) * n, st));
-        CK(cudaMemsetAsync(d_ncand, 0, sizeof(int) * n, st));
-        CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned int), st));
+        TRY(search_reset(n, p0 != nullptr));
         ScoreParams sp = score_params(mode);
         if (p0) return search_split(d_odb, n, sp, interlock, xf, p0, p1, sm3, d_out, false);
         PlaneFn pf = nullptr;

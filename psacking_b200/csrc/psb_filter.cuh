@@ -50,11 +50,15 @@ __global__ void k_tray_bits(const int32_t* __restrict__ tray, int nx, int ny, in
 // s.z / 32 (bucket k holds fs[o][bound[o][k] .. bound[o][k+1])), once per
 // item, so the filter's CTAs only load them.  One warp per orientation.
 // grid: n, block 32
+// It also zeroes the orientation's filter counters (candidates, verified
+// cells, item columns: counts[o], counts[cap + o], counts[2 cap + o]).
 template <int NQ>
-__global__ void k_cand_prep(const OrientDesc* __restrict__ orients, int4* __restrict__ fs, int* __restrict__ fbound) {
+__global__ void k_cand_prep(const OrientDesc* __restrict__ orients, int4* __restrict__ fs, int* __restrict__ fbound,
+                            int* __restrict__ counts, int cap) {
     pdl_enter();
     constexpr int NW = 4 * NQ;
     const int o = blockIdx.x, lane = threadIdx.x;
+    if (lane < 3) counts[(size_t)lane * cap + o] = 0;
     const OrientDesc& od = orients[o];
     if (od.skip || od.nsamp <= 0) return;
     const int ns = min(od.nsamp, PSB_FSAMP);
@@ -341,12 +345,16 @@ k_cand_filter_plane(const OrientDesc* __restrict__ orients, int n, const uint4* 
 // a candidate is skipped; one with at most direct_max candidates and an item
 // at most 64 cells high (two mask words per column) becomes direct.
 // Stage 1 (after k_cand_verify_list, count = verified free cells): a direct
-// orientation without a free cell is skipped.  grid: ceil(n / 128), block 128
+// orientation without a free cell is skipped.  okclear, when given, has the
+// orientation's nclear plane flags (stride okstride) cleared first, for the
+// verification to set.  grid: ceil(n / 128), block 128
 __global__ void k_cand_apply(OrientDesc* __restrict__ orients, int n, const int* __restrict__ count, int stage,
-                             int direct_max) {
+                             int direct_max, unsigned char* __restrict__ okclear, long long okstride, int nclear) {
     pdl_enter();
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
+    if (okclear)
+        for (int x = 0; x < nclear; ++x) okclear[(size_t)o * okstride + x] = 0;
     OrientDesc& od = orients[o];
     if (od.skip || od.nsamp <= 0) return;
     if (stage == 0) {

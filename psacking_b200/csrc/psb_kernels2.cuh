@@ -959,3 +959,39 @@ __global__ void k_bits_to_mask(const uint32_t* __restrict__ bits, int32_t* __res
         out[t] = (bits[line * nzw + (z >> 5)] >> (z & 31)) & 1u;
     }
 }
+
+// The per-search reset of the selection and flood-fill state, one launch in
+// place of a memset per array (a memset between two kernels also ends their
+// launch overlap): the plane minima, best cells and tie keys to all ones,
+// the diagnostics, error maxima, candidate and run counters to zero, the
+// union-find error word to zero and, when given, the plane flags of the n
+// orientations (okbytes bytes) to zero.  grid: 4, block 256
+struct SearchReset {
+    unsigned long long* smin;
+    unsigned long long* best;
+    unsigned long long* bestkey;
+    unsigned int* diag;
+    unsigned int* errmax;
+    int* ncand;
+    int* total;
+    unsigned int* err;
+    unsigned char* okplane;
+    long long okbytes;
+    int n;
+};
+__global__ void k_search_reset(SearchReset a) {
+    pdl_enter();
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    for (int o = tid; o < a.n; o += nth) {
+        a.smin[o] = ~0ULL;
+        a.best[o] = ~0ULL;
+        a.bestkey[o] = ~0ULL;
+        a.diag[o] = 0u;
+        a.errmax[o] = 0u;
+        a.ncand[o] = 0;
+        a.total[o] = 0;
+    }
+    if (tid == 0) *a.err = 0u;
+    if (a.okplane)
+        for (long long i = tid; i < a.okbytes; i += nth) a.okplane[i] = 0;
+}
