@@ -1002,6 +1002,9 @@ struct psb_tray {
     unsigned char* d_okplane = nullptr;     // per (orientation, x plane): holds an ok cell
     unsigned char* d_candplane = nullptr;   // per (orientation, x plane): holds a filter candidate
     bool cand_active = false;               // the current search's candidate words and planes are valid
+    const PhiStats* prep_ps = nullptr;      // when set, k_cand_prep also does k_prep's work
+    bool pending_apply = false;             // stage 1 of k_cand_apply still to run on the current item
+    int apply_dmax = 0;
     bool direct_active = false;             // ... and direct orientations may exist
     bool late_active = false;               // the current search may hold late-direct orientations
     DecideArgs decide{nullptr, nullptr, nullptr, nullptr};   // the loop's decision, fused into the
@@ -1470,12 +1473,12 @@ struct psb_tray {
             if (g_filter_plane && smw <= (size_t)g_smem_optin) {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
-                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap);
+                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap, prep_ps);
                     pdl(k_cand_filter_plane<1>, dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st)(
                         d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
                         d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
                 } else {
-                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap);
+                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap, prep_ps);
                     pdl(k_cand_filter_plane<2>, dim3(xmax, g_filter_groups), PSB_FILT_PLANE_THREADS, smw, st)(
                         d_odb, n, d_tbits, nx, ny, nzw, emax, d_free, sBits, d_candplane, (long long)nx, d_ccount,
                         d_fsamp, d_fbound, g_filter_cut, d_clist, ccap, nz);
@@ -1483,7 +1486,7 @@ struct psb_tray {
             } else {
                 PROF("k_cand_filter", st);
                 if (tq == 1) {
-                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap);
+                    pdl(k_cand_prep<1>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap, prep_ps);
                     // the variant (sample batch, CTAs per SM bound) is a tuning switch
                     auto kf = g_filter_variant == 1 ? k_cand_filter<1, 4, 12>
                             : g_filter_variant == 2 ? k_cand_filter<1, 8, 1>
@@ -1492,7 +1495,7 @@ struct psb_tray {
                                                           (long long)nx, d_ccount, d_fsamp, d_fbound, g_filter_cut,
                                                           d_clist, ccap, nz);
                 } else {
-                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap);
+                    pdl(k_cand_prep<2>, n, 32, 0, st)(d_odb, d_fsamp, d_fbound, d_ccount, (int)cap, prep_ps);
                     pdl(k_cand_filter<2>, grid, PSB_FILT_THREADS, 0, st)(d_odb, d_tbits, ny, nzw, d_free, sBits,
                                                                         d_candplane, (long long)nx, d_ccount,
                                                                         d_fsamp, d_fbound, g_filter_cut, d_clist,
@@ -1516,12 +1519,29 @@ struct psb_tray {
                         (long long)nx * ny, d_ncol, d_vcount, d_okplane, (long long)nx, interlock ? 0 : 1);
                 }
                 CKL();
-                pdl(k_cand_apply, (n + 127) / 128, 128, 0, st)(d_odb, n, d_vcount, 1, dmax, nullptr, 0LL, 0);
-                CKL();
+                // stage 1 of k_cand_apply: done by the search's k_active_list
+                // when it launches one, else by flush_apply
+                pending_apply = true;
+                apply_dmax = dmax;
             }
+        }
+        if (xmax <= 0 && prep_ps) {
+            // no filter kernels ran: the error bounds the caller left to k_cand_prep
+            pdl(k_prep, (n + 63) / 64, 64, 0, st)(d_odb, n, prep_ps);
+            CKL();
         }
         cand_active = true;
         direct_active = dmax > 0 && xmax > 0;   // the okplane flags were cleared above
+        return PSB_OK;
+    }
+
+    // the candidate filter's verification outcome (stage 1 of k_cand_apply),
+    // when no k_active_list has taken it over
+    int flush_apply(OrientDesc* d_odb, int n) {
+        if (!pending_apply) return PSB_OK;
+        pending_apply = false;
+        pdl(k_cand_apply, (n + 127) / 128, 128, 0, st)(d_odb, n, d_vcount, 1, apply_dmax, nullptr, 0LL, 0);
+        CKL();
         return PSB_OK;
     }
 
@@ -1726,6 +1746,7 @@ struct psb_tray {
         FwdPlaneFn ffb = g_fast_fft ? fwd_plane_for(g.F[1], g.F[2]) : nullptr;
         const bool spec = g_share_flips && d_bases_in && hbases && p0 && xf && ffb;
         if (spec) {
+            TRY(flush_apply(const_cast<OrientDesc*>(d_odb), n));
             // the bases' z,y forward into slab slots 0..5; the x passes read them
             int bx = 1, by = 1;
             for (auto& b : *hbases)
@@ -1754,13 +1775,17 @@ struct psb_tray {
         FwdPlaneFn ff = g_fast_fft ? fwd_plane_for(g.F[1], g.F[2]) : nullptr;
         const size_t smf = fwd_plane_smem(g.F[1], g.F[2], eymax) + 64;
         act_ready = false;
+        if (!(ff && smf <= (size_t)g_smem_optin && g_active_grid > 0))
+            TRY(flush_apply(const_cast<OrientDesc*>(d_odb), n));
         if (ff && smf <= (size_t)g_smem_optin) {
             // the transforms take the active orientations from a list: a few
             // CTA rows loop over them instead of a row per orientation
             const int rows = g_active_grid > 0 ? std::min(n, g_active_grid) : n;
             if (g_active_grid > 0) {
-                pdl(k_active_list, 1, 32, 0, st)(d_odb, n, d_act, d_nact, d_srch, d_nsrch);
+                pdl(k_active_list, 1, 32, 0, st)(const_cast<OrientDesc*>(d_odb), n, d_act, d_nact, d_srch, d_nsrch,
+                                                 pending_apply ? d_vcount : nullptr);
                 CKL();
+                pending_apply = false;
                 act_ready = true;
             }
             FwdSrc src{SRC_ITEM, nullptr, 0, 0, 0, nullptr, nullptr, d_Bi, sBi, nullptr,
@@ -3095,8 +3120,13 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         }
         OrientDesc* d_odb = t->d_od_all + (size_t)it * n_orient;
         for (int o = 0; o < n_orient; ++o) host_ods[o] = all[(size_t)it * n_orient + o];
-        pdl(k_prep, (n_orient + 63) / 64, 64, 0, t->st)(d_odb, n_orient, t->d_ps);
-        CKL();
+        // with the filter, k_cand_prep fills the error bounds (k_prep's work)
+        const bool filter_now = filt && occ_est * 4 >= t->V;
+        const bool fold_prep = filter_now && !opt.prop && !d_hm;
+        if (!fold_prep) {
+            pdl(k_prep, (n_orient + 63) / 64, 64, 0, t->st)(d_odb, n_orient, t->d_ps);
+            CKL();
+        }
         if (d_hm) {
             pdl(k_height_map, PSB_PH * PSB_PH, 256, 0, t->st)(t->d_tray, t->nx, t->ny, t->nz,
                                                              d_hm + (size_t)it * PSB_PH * PSB_PH);
@@ -3121,7 +3151,12 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             CKL();
         }
         std::vector<OrientDesc> hb(allb.begin() + (size_t)it * 6, allb.begin() + (size_t)(it + 1) * 6);
-        if (filt && occ_est * 4 >= t->V) TRY(t->cand_filter(d_odb, host_ods, interlock != 0));
+        if (filter_now) {
+            t->prep_ps = fold_prep ? t->d_ps : nullptr;
+            const int fst = t->cand_filter(d_odb, host_ods, interlock != 0);
+            t->prep_ps = nullptr;
+            TRY(fst);
+        }
         occ_est += (size_t)t->staged[it].nvox;
         ShardRecord* rec = opt.world > 1 || opt.d_local ? (ShardRecord*)opt.d_local : nullptr;
         // the decision below may be fused into the search's last launch
@@ -3129,7 +3164,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         t->fused = false;
         const int sst = t->search_async(d_odb, host_ods, mode, interlock != 0, t->d_res, true,
                                         t->d_base_all + (size_t)it * 6, &hb);
-        t->cand_active = t->direct_active = t->late_active = false;
+        t->cand_active = t->direct_active = t->late_active = t->pending_apply = false;
         t->decide = DecideArgs{nullptr, nullptr, nullptr, nullptr};
         TRY(sst);
         if (d_per)
@@ -3152,16 +3187,9 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
             CKL();
         }
         {
-            PROF("k_place_check", t->st);
-            pdl(k_place_check_g, 64, 256, 0, t->st)(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
+            PROF("k_place", t->st);
+            pdl(k_place_item, 1, 1024, 0, t->st)(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz, t->d_dec + it);
         }
-        CKL();
-        {
-            PROF("k_place_write", t->st);
-            pdl(k_place_write_g, 64, 256, 0, t->st)(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz);
-        }
-        CKL();
-        pdl(k_place_done, 1, 32, 0, t->st)(d_odb, t->d_ls, t->d_dec + it);
         CKL();
         {
             // the placed item's columns: occupancy prefix sums and the

@@ -51,14 +51,17 @@ __global__ void k_tray_bits(const int32_t* __restrict__ tray, int nx, int ny, in
 // item, so the filter's CTAs only load them.  One warp per orientation.
 // grid: n, block 32
 // It also zeroes the orientation's filter counters (candidates, verified
-// cells, item columns: counts[o], counts[cap + o], counts[2 cap + o]).
+// cells, item columns: counts[o], counts[cap + o], counts[2 cap + o]) and,
+// when ps is given, fills its error bound (k_prep's work, one launch less).
 template <int NQ>
-__global__ void k_cand_prep(const OrientDesc* __restrict__ orients, int4* __restrict__ fs, int* __restrict__ fbound,
-                            int* __restrict__ counts, int cap) {
+__global__ void k_cand_prep(OrientDesc* __restrict__ orients, int4* __restrict__ fs, int* __restrict__ fbound,
+                            int* __restrict__ counts, int cap, const PhiStats* __restrict__ ps) {
     pdl_enter();
     constexpr int NW = 4 * NQ;
     const int o = blockIdx.x, lane = threadIdx.x;
     if (lane < 3) counts[(size_t)lane * cap + o] = 0;
+    if (ps && lane == 0) prep_orient(orients[o], ps);
+    __syncwarp();
     const OrientDesc& od = orients[o];
     if (od.skip || od.nsamp <= 0) return;
     const int ns = min(od.nsamp, PSB_FSAMP);

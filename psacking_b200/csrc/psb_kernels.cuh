@@ -337,14 +337,18 @@ struct SearchBufs {
 // decided directly) and the ones it searches at all (srch: not skipped; the
 // flood fill and the selection), compacted, so those kernels launch a few
 // CTA rows that loop over them instead of one row per orientation, most of
-// which would only read their descriptor and exit.  grid 1, block 32
-__global__ void k_active_list(const OrientDesc* __restrict__ od, int n, int* __restrict__ act, int* __restrict__ nact,
-                              int* __restrict__ srch, int* __restrict__ nsrch) {
+// which would only read their descriptor and exit.  vcount, when given,
+// first applies the candidate filter's verification (stage 1 of
+// k_cand_apply, one launch less): a direct orientation without a verified
+// free cell is skipped.  grid 1, block 32
+__global__ void k_active_list(OrientDesc* __restrict__ od, int n, int* __restrict__ act, int* __restrict__ nact,
+                              int* __restrict__ srch, int* __restrict__ nsrch, const int* __restrict__ vcount) {
     pdl_enter();
     int base = 0, sbase = 0;
     const unsigned int below = (1u << threadIdx.x) - 1u;
     for (int o0 = 0; o0 < n; o0 += 32) {
         const int o = o0 + threadIdx.x;
+        if (vcount && o < n && !od[o].skip && od[o].direct && vcount[o] == 0) od[o].skip = 1;
         const bool s = o < n && !od[o].skip;
         const bool on = s && !od[o].direct;
         const unsigned int b = __ballot_sync(0xffffffffu, on);

@@ -3,8 +3,8 @@
 //
 // Per item the stream runs: k_prep (error bounds from the current distance
 // statistics) -> the search -> k_decide (best orientation, strict <, first
-// wins: fft3.cu:1625 / packer.py:500) -> k_place_check / k_place_write /
-// k_place_done (packing.cpp:773-788) -> the occupancy spectrum rebuild, gated
+// wins: fft3.cu:1625 / packer.py:500) -> k_place_item (check, write and
+// commit, packing.cpp:773-788) -> the occupancy spectrum rebuild, gated
 // on "placed".  Gated kernels read a device flag and return at once when it
 // is 0.
 #pragma once
@@ -32,12 +32,9 @@ struct LoopState {
     unsigned long long first;  // first overlapping tray cell of the current item
 };
 
-// error bound and base of every orientation of one item (psb_tray::describe)
-__global__ void k_prep(OrientDesc* __restrict__ od, int n, const PhiStats* __restrict__ ps) {
-    pdl_enter();
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n) return;
-    OrientDesc& d = od[o];
+// error bound and base of one orientation from the current distance
+// statistics (psb_tray::describe)
+__device__ __forceinline__ void prep_orient(OrientDesc& d, const PhiStats* __restrict__ ps) {
     const double maxD = (double)d.sabs * (double)ps->maxabs;
     double ulp = 1.1920928955078125e-07;
     if (maxD >= 1.0) {
@@ -49,6 +46,14 @@ __global__ void k_prep(OrientDesc* __restrict__ od, int n, const PhiStats* __res
     d.delta = 2.0 * eps * sqrt(d.sumsq) * ps->norm + 0.5 * ulp + 1e-3;
     d.exact = (d.delta >= 0.4 || maxD >= 8388608.0) ? 1 : 0;
     d.base = (double)ps->mean * (double)d.sumI;
+}
+
+// prep_orient for every orientation of one item.  grid: ceil(n / 64), block 64
+__global__ void k_prep(OrientDesc* __restrict__ od, int n, const PhiStats* __restrict__ ps) {
+    pdl_enter();
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    prep_orient(od[o], ps);
 }
 
 struct DecisionDev {
@@ -187,17 +192,23 @@ __global__ void k_decide_merge(const ShardRecord* __restrict__ all, int world, L
     }
 }
 
-// The decided placement, walked by the item's z-runs (each run a contiguous
-// stretch of one tray column): the check records the smallest tray index an
-// item cell would overwrite, the write then fills the free cells with the id.
-// grid: 64, block 256
-__global__ void k_place_check_g(const OrientDesc* __restrict__ od_item, LoopState* ls, const int32_t* __restrict__ tray,
-                                int nx, int ny, int nz) {
+// The decided placement in one block: the item's z-runs (each a contiguous
+// stretch of one tray column) are checked against the tray (the smallest
+// overlapped index), then, without an overlap, written with the id and the
+// placement is committed (packing.cpp:773-788); an overlap (an FP32 "free"
+// cell that the exact check rejects) marks the item unplaced and raises the
+// run's error word.  grid: 1, block 1024
+__global__ void __launch_bounds__(1024)
+k_place_item(const OrientDesc* __restrict__ od_item, LoopState* ls, int32_t* __restrict__ tray, int nx, int ny,
+             int nz, DecisionDev* out) {
     pdl_enter();
     if (!ls->do_place) return;
+    __shared__ unsigned long long s_first;
+    if (threadIdx.x == 0) s_first = 0xffffffffffffffffULL;
+    __syncthreads();
     const OrientDesc& od = od_item[ls->orient];
-    const int px = ls->px, py = ls->py, pz = ls->pz;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < od.nruns; r += gridDim.x * blockDim.x) {
+    const int px = ls->px, py = ls->py, pz = ls->pz, id = ls->id;
+    for (int r = threadIdx.x; r < od.nruns; r += blockDim.x) {
         const int4 q = od.runs[r];
         if (q.w <= 0) continue;
         int a, b, c0, c1;
@@ -207,39 +218,28 @@ __global__ void k_place_check_g(const OrientDesc* __restrict__ od_item, LoopStat
         const size_t col = ((size_t)i * ny + j) * nz;
         for (int k = max(0, pz + c0); k <= min(nz - 1, pz + c1); ++k)
             if (tray[col + k] > 0) {
-                atomicMin(&ls->first, (unsigned long long)(col + k));
+                atomicMin(&s_first, (unsigned long long)(col + k));
                 break;   // the run's first overlap is its smallest index
             }
     }
-}
-
-__global__ void k_place_write_g(const OrientDesc* __restrict__ od_item, const LoopState* ls, int32_t* __restrict__ tray,
-                                int nx, int ny, int nz) {
-    pdl_enter();
-    if (!ls->do_place || ls->first != 0xffffffffffffffffULL) return;
-    const OrientDesc& od = od_item[ls->orient];
-    const int px = ls->px, py = ls->py, pz = ls->pz, id = ls->id;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < od.nruns; r += gridDim.x * blockDim.x) {
-        const int4 q = od.runs[r];
-        if (q.w <= 0) continue;
-        int a, b, c0, c1;
-        orient_run(od, q, &a, &b, &c0, &c1);
-        const int i = px + a, j = py + b;
-        if (i < 0 || j < 0 || i >= nx || j >= ny) continue;
-        const size_t col = ((size_t)i * ny + j) * nz;
-        for (int k = max(0, pz + c0); k <= min(nz - 1, pz + c1); ++k)
-            if (tray[col + k] == 0) tray[col + k] = id;
+    __syncthreads();
+    const unsigned long long first = s_first;
+    if (first == 0xffffffffffffffffULL) {
+        for (int r = threadIdx.x; r < od.nruns; r += blockDim.x) {
+            const int4 q = od.runs[r];
+            if (q.w <= 0) continue;
+            int a, b, c0, c1;
+            orient_run(od, q, &a, &b, &c0, &c1);
+            const int i = px + a, j = py + b;
+            if (i < 0 || j < 0 || i >= nx || j >= ny) continue;
+            const size_t col = ((size_t)i * ny + j) * nz;
+            for (int k = max(0, pz + c0); k <= min(nz - 1, pz + c1); ++k)
+                if (tray[col + k] == 0) tray[col + k] = id;
+        }
     }
-}
-
-// commit: count the placement, set the rebuild gates; an overlap (an FP32
-// "free" cell that the exact check rejects) marks the item unplaced and
-// raises the run's error word
-__global__ void k_place_done(const OrientDesc* __restrict__ od_item, LoopState* ls, DecisionDev* out) {
-    pdl_enter();
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (!ls->do_place) return;
-    if (ls->first != 0xffffffffffffffffULL) {
+    if (threadIdx.x != 0) return;
+    ls->first = first;
+    if (first != 0xffffffffffffffffULL) {
         ls->err |= 4u;
         out->found = 0;
         out->x = out->y = out->z = -1;
@@ -249,8 +249,8 @@ __global__ void k_place_done(const OrientDesc* __restrict__ od_item, LoopState* 
         return;
     }
     ls->placed += 1;
-    ls->placed_now = od_item[ls->orient].nvox > 0 ? 1 : 0;
-    ls->need_phi = (ls->id == 1 && od_item[ls->orient].nvox > 0) ? 1 : 0;
+    ls->placed_now = od.nvox > 0 ? 1 : 0;
+    ls->need_phi = (id == 1 && od.nvox > 0) ? 1 : 0;
 }
 
 // distance statistics on the device: mean after the first k_stats pass,
