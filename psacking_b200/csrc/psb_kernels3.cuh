@@ -7,6 +7,11 @@
 #include "psb_kernels2.cuh"
 
 #define PSB_XCOLS 16   // spectrum columns (ky*Hz + kz) per CTA in k_xpass2
+// (Measured and not taken: the one-product modes with the item's x transform
+// kept in the work buffer, its second pass and the product pass in place, to
+// halve the tile's shared memory for a fourth CTA per SM.  Holding a radix-16
+// butterfly across the in-place barrier takes 126 registers, and capped at 64
+// it spills 224 bytes: 1393.8 against 1451.8 items placed/s.)
 
 // ---------------------------------------------------------------------------
 // z,y transforms shared by the flips of one axis permutation
