@@ -1055,6 +1055,22 @@ struct psb_tray {
     size_t h_part_cap[2] = {0, 0};
     void* h_desc = nullptr;          // pinned copy of the run's descriptors
     size_t h_desc_cap = 0;
+    // item column masks of every orientation of the staged items
+    // (k_item_cols_all), per part: item it at d_icp[part] + icol_off[it],
+    // icol_stride[it] entries per orientation, counts in d_icn[it * n + o]
+    uint4* d_icp[2] = {nullptr, nullptr};
+    size_t icp_cap[2] = {0, 0};
+    long long* d_icoff = nullptr;    // icol_off and icol_stride on the device
+    int* d_icstr = nullptr;
+    int* d_icn = nullptr;
+    size_t icmeta_cap = 0, icn_cap = 0;
+    void* h_icmeta = nullptr;        // pinned staging of the two tables
+    std::vector<long long> icol_off;
+    std::vector<int> icol_stride;
+    // the current item's precomputed columns for cand_filter (null: compute)
+    const uint4* cur_icols = nullptr;
+    long long cur_cstride = 0;
+    const int* cur_ncol = nullptr;
     cudaStream_t st_copy = nullptr;  // uploads of the second part
     cudaEvent_t ev_copy = nullptr;
 
@@ -1094,7 +1110,11 @@ struct psb_tray {
         for (int p = 0; p < 2; ++p) {
             dfree(d_part[p], st);
             part_cap[p] = 0;
+            dfree(d_icp[p], st);
+            icp_cap[p] = 0;
         }
+        dfree(d_icoff, st); dfree(d_icstr, st); dfree(d_icn, st);
+        icmeta_cap = icn_cap = 0;
         clist_cap = 0;
         tq = 0;
         if (st_copy) {
@@ -1117,6 +1137,8 @@ struct psb_tray {
         if (h_desc) cudaFreeHost(h_desc);
         h_desc = nullptr;
         h_desc_cap = 0;
+        if (h_icmeta) cudaFreeHost(h_icmeta);
+        h_icmeta = nullptr;
     }
 
     int init(int x, int y, int z) {
@@ -1515,11 +1537,19 @@ struct psb_tray {
             if (dmax > 0) {
                 {
                     PROF("k_cand_verify", st);
-                    pdl(k_item_cols, dim3(emax, n), 64, 0, st)(d_odb, d_icols, (long long)nx * ny, d_ncol);
-                    CKL();
+                    const uint4* cols = cur_icols;
+                    long long cstride = cur_cstride;
+                    const int* ncol = cur_ncol;
+                    if (!cols) {
+                        pdl(k_item_cols, dim3(emax, n), 64, 0, st)(d_odb, d_icols, (long long)nx * ny, d_ncol);
+                        CKL();
+                        cols = d_icols;
+                        cstride = (long long)nx * ny;
+                        ncol = d_ncol;
+                    }
                     pdl(k_cand_verify_list, 148 * 4, 256, sizeof(int) * (n + 1), st)(
-                        d_odb, n, d_tbits, ny, nz, nzw, tq, d_free, sBits, d_clist, ccap, d_ccount, d_icols,
-                        (long long)nx * ny, d_ncol, d_vcount, d_okplane, (long long)nx, interlock ? 0 : 1);
+                        d_odb, n, d_tbits, ny, nz, nzw, tq, d_free, sBits, d_clist, ccap, d_ccount, cols,
+                        cstride, ncol, d_vcount, d_okplane, (long long)nx, interlock ? 0 : 1);
                 }
                 CKL();
                 // stage 1 of k_cand_apply: done by the search's k_active_list
@@ -3000,6 +3030,60 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
     }
     OrientDesc* hd_all = (OrientDesc*)t->h_desc;
     OrientDesc* hd_base = hd_all + all.size();
+    // item columns of the direct checks, for every item up front (they do not
+    // depend on the tray): one k_item_cols_all per described range
+    const bool icols_pre = filt && t->split_flow() && g_direct_max > 0;
+    if (icols_pre) {
+        t->icol_off.assign(n_items, 0);
+        t->icol_stride.assign(n_items, 0);
+        if ((size_t)n_items > t->icmeta_cap) {
+            dfree(t->d_icoff, t->st);
+            dfree(t->d_icstr, t->st);
+            t->icmeta_cap = 0;
+            TRY(dalloc(&t->d_icoff, (size_t)n_items, t->st));
+            TRY(dalloc(&t->d_icstr, (size_t)n_items, t->st));
+            if (t->h_icmeta) cudaFreeHost(t->h_icmeta);
+            t->h_icmeta = nullptr;
+            CK(cudaMallocHost(&t->h_icmeta, (size_t)n_items * (sizeof(long long) + sizeof(int))));
+            t->icmeta_cap = n_items;
+        }
+        if ((size_t)n_items * n_orient > t->icn_cap) {
+            dfree(t->d_icn, t->st);
+            t->icn_cap = 0;
+            TRY(dalloc(&t->d_icn, (size_t)n_items * n_orient, t->st));
+            t->icn_cap = (size_t)n_items * n_orient;
+        }
+    }
+    auto item_cols_range = [&](int i0, int i1, cudaStream_t s) -> int {
+        const int part = i0 == 0 ? 0 : 1;
+        long long acc = 0;
+        int emax = 1;
+        for (int it = i0; it < i1; ++it) {
+            const int* d = t->staged[it].dims;
+            const int str = std::max(std::max(d[0] * d[1], d[0] * d[2]), d[1] * d[2]);
+            t->icol_off[it] = acc;
+            t->icol_stride[it] = str;
+            acc += (long long)n_orient * str;
+            emax = std::max(emax, std::max(d[0], std::max(d[1], d[2])));
+        }
+        if ((size_t)acc > t->icp_cap[part]) {
+            dfree(t->d_icp[part], t->st);
+            t->icp_cap[part] = 0;
+            TRY(dalloc(&t->d_icp[part], (size_t)acc, s));
+            t->icp_cap[part] = (size_t)acc;
+        }
+        long long* hoff = (long long*)t->h_icmeta;
+        int* hstr = (int*)(hoff + t->icmeta_cap);
+        memcpy(hoff + i0, t->icol_off.data() + i0, sizeof(long long) * (i1 - i0));
+        memcpy(hstr + i0, t->icol_stride.data() + i0, sizeof(int) * (i1 - i0));
+        CK(cudaMemcpyAsync(t->d_icoff + i0, hoff + i0, sizeof(long long) * (i1 - i0), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(t->d_icstr + i0, hstr + i0, sizeof(int) * (i1 - i0), cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(t->d_icn + (size_t)i0 * n_orient, 0, sizeof(int) * (size_t)(i1 - i0) * n_orient, s));
+        pdl(k_item_cols_all, dim3(emax, n_orient, i1 - i0), 64, 0, s)(t->d_od_all, n_orient, i0, t->d_icp[part],
+                                                                     t->d_icoff, t->d_icstr, t->d_icn);
+        CKL();
+        return PSB_OK;
+    };
     auto describe_range = [&](int i0, int i1, cudaStream_t s) -> int {
         for (int it = i0; it < i1; ++it) {
             const psb_tray::StagedDev& sd = t->sdev[it];
@@ -3028,6 +3112,7 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         memcpy(hd_base + b0, allb.data() + b0, sizeof(OrientDesc) * nb);
         CK(cudaMemcpyAsync(t->d_od_all + a0, hd_all + a0, sizeof(OrientDesc) * na, cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(t->d_base_all + b0, hd_base + b0, sizeof(OrientDesc) * nb, cudaMemcpyHostToDevice, s));
+        if (icols_pre) TRY(item_cols_range(i0, i1, s));
         return PSB_OK;
     };
     if (opt.feed && (opt.prop || opt.feed_at <= 0 || opt.feed_at >= n_items))
@@ -3156,8 +3241,16 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         std::vector<OrientDesc> hb(allb.begin() + (size_t)it * 6, allb.begin() + (size_t)(it + 1) * 6);
         if (filter_now) {
             t->prep_ps = fold_prep ? t->d_ps : nullptr;
+            if (icols_pre) {
+                const int part = (opt.feed && it >= opt.feed_at) ? 1 : 0;
+                t->cur_icols = t->d_icp[part] + t->icol_off[it];
+                t->cur_cstride = t->icol_stride[it];
+                t->cur_ncol = t->d_icn + (size_t)it * n_orient;
+            }
             const int fst = t->cand_filter(d_odb, host_ods, interlock != 0);
             t->prep_ps = nullptr;
+            t->cur_icols = nullptr;
+            t->cur_ncol = nullptr;
             TRY(fst);
         }
         occ_est += (size_t)t->staged[it].nvox;

@@ -398,6 +398,41 @@ __global__ void k_item_cols(const OrientDesc* __restrict__ orients, uint4* __res
     }
 }
 
+// k_item_cols for every orientation of a range of staged items at once
+// (they depend on the item only, not on the tray), ahead of the packing
+// loop: item i's columns go to cols + off[i] with stride[i] entries per
+// orientation, counts to ncol[i * n + o] (zeroed first).  Orientations that
+// do not fit the tray (skip) are left out; which ones become direct is known
+// only per item, and the verification reads the direct ones only.
+// grid: (max e[0], n, items), block 64
+__global__ void k_item_cols_all(const OrientDesc* __restrict__ od_all, int n, int i0, uint4* __restrict__ cols,
+                                const long long* __restrict__ off, const int* __restrict__ stride,
+                                int* __restrict__ ncol) {
+    pdl_enter();
+    const int it = i0 + blockIdx.z, o = blockIdx.y, a = blockIdx.x;
+    const OrientDesc& od = od_all[(size_t)it * n + o];
+    if (od.skip || a >= od.e[0]) return;
+    const int lane = threadIdx.x & 31;
+    uint4* out = cols + off[it] + (size_t)o * stride[it];
+    int* cnt = ncol + (size_t)it * n + o;
+    for (int b0 = 0; b0 < od.e[1]; b0 += blockDim.x) {
+        const int b = b0 + threadIdx.x;
+        uint32_t m0 = 0u, m1 = 0u;
+        if (b < od.e[1])
+            for (int c = 0; c < od.e[2] && c < 64; ++c)
+                if (__ldg(&od.item[orient_src_index(od, a, b, c)]) > 0) {
+                    if (c < 32) m0 |= 1u << c;
+                    else m1 |= 1u << (c - 32);
+                }
+        const bool has = (m0 | m1) != 0u;
+        const unsigned int bal = __ballot_sync(0xffffffffu, has);
+        int slot = 0;
+        if (lane == 0 && bal) slot = atomicAdd(cnt, __popc(bal));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (has) out[slot + __popc(bal & ((1u << lane) - 1u))] = make_uint4((uint32_t)a | ((uint32_t)b << 16), m0, m1, 0u);
+    }
+}
+
 // Exact collision check of every candidate of the direct orientations, from
 // the candidate lists k_cand_filter wrote: the translation (x, y, z) is free
 // when no item column (a, b) meets an occupied cell of tray column
