@@ -3284,7 +3284,8 @@ int pack_staged_impl(psb_tray* t, const int32_t* orient_maps, int n_orient, int 
         }
         {
             PROF("k_place", t->st);
-            pdl(k_place_item, 1, 1024, 0, t->st)(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz, t->d_dec + it);
+            pdl(k_place_item, 1, 1024, 0, t->st)(d_odb, t->d_ls, t->d_tray, t->nx, t->ny, t->nz, t->d_dec + it,
+                                                 t->d_pocc);
         }
         CKL();
         {

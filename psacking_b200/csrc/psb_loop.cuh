@@ -198,9 +198,13 @@ __global__ void k_decide_merge(const ShardRecord* __restrict__ all, int world, L
 // placement is committed (packing.cpp:773-788); an overlap (an FP32 "free"
 // cell that the exact check rejects) marks the item unplaced and raises the
 // run's error word.  grid: 1, block 1024
+// The check reads the occupancy prefix sums of the tray columns (pocc,
+// k_col_prefix<1>, current up to the previous placement): a run meets an
+// occupied cell iff its column's count over the run's z range is nonzero,
+// two loads per run; only then are the run's cells scanned for the index.
 __global__ void __launch_bounds__(1024)
 k_place_item(const OrientDesc* __restrict__ od_item, LoopState* ls, int32_t* __restrict__ tray, int nx, int ny,
-             int nz, DecisionDev* out) {
+             int nz, DecisionDev* out, const int32_t* __restrict__ pocc) {
     pdl_enter();
     if (!ls->do_place) return;
     __shared__ unsigned long long s_first;
@@ -216,7 +220,11 @@ k_place_item(const OrientDesc* __restrict__ od_item, LoopState* ls, int32_t* __r
         const int i = px + a, j = py + b;
         if (i < 0 || j < 0 || i >= nx || j >= ny) continue;
         const size_t col = ((size_t)i * ny + j) * nz;
-        for (int k = max(0, pz + c0); k <= min(nz - 1, pz + c1); ++k)
+        const int k0 = max(0, pz + c0), k1 = min(nz - 1, pz + c1);
+        if (k0 > k1) continue;
+        const int32_t* P = pocc + ((size_t)i * ny + j) * (nz + 1);
+        if (P[k1 + 1] - P[k0] == 0) continue;
+        for (int k = k0; k <= k1; ++k)
             if (tray[col + k] > 0) {
                 atomicMin(&s_first, (unsigned long long)(col + k));
                 break;   // the run's first overlap is its smallest index
