@@ -198,6 +198,8 @@ __global__ void k_decide_merge(const ShardRecord* __restrict__ all, int world, L
 // placement is committed (packing.cpp:773-788); an overlap (an FP32 "free"
 // cell that the exact check rejects) marks the item unplaced and raises the
 // run's error word.  grid: 1, block 1024
+// (An 8-CTA thread-block cluster version, the overlap minimum combined in
+// CTA 0's distributed shared memory, measured the same: 1488.2 items/s.)
 // The check reads the occupancy prefix sums of the tray columns (pocc,
 // k_col_prefix<1>, current up to the previous placement): a run meets an
 // occupied cell iff its column's count over the run's z range is nonzero,
