@@ -194,3 +194,68 @@ def test_injected_allocation_failures_are_clean():
     assert failures >= 3
     want_tray, want = O.pack_voxels(items, tray0.shape, 4, True, sort_by_volume=False)
     np.testing.assert_array_equal(out, want_tray)
+
+
+def test_injected_allocation_failures_streamed_staging_are_clean():
+    """psb_pack with 64 items or more stages them in two parts, the second
+    one uploaded (and its item columns computed) while the first part is
+    searched: an allocation failure anywhere, including mid-run, returns
+    PSB_ERR_CUDA, and destroying the tray frees everything."""
+    abi = _Abi()
+    lib = abi.lib
+    base = abi.live()
+    from psacking_b200 import workloads
+    from psacking_b200.rotations import orientation_maps
+    items = [np.ascontiguousarray(i) for s in range(4) for i in workloads.config1_items(s)][:70]
+    ptrs = (ctypes.POINTER(ctypes.c_int32) * len(items))(
+        *[i.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) for i in items])
+    dims = np.array([i.shape for i in items], np.int32).ravel()
+    maps = np.ascontiguousarray(orientation_maps(4), np.int32)
+    shape = (64, 64, 40)
+    tray0 = np.zeros(shape, np.int32)
+
+    class Res(ctypes.Structure):
+        _fields_ = [("x", ctypes.c_int32), ("y", ctypes.c_int32), ("z", ctypes.c_int32),
+                    ("found", ctypes.c_int32), ("score", ctypes.c_double), ("orientation", ctypes.c_int32),
+                    ("diag", ctypes.c_uint32), ("n_candidates", ctypes.c_int32), ("err_ratio", ctypes.c_float)]
+
+    def pack(k):
+        t = ctypes.c_void_p()
+        assert lib.psb_tray_create(*shape, ctypes.byref(t)) == 0, abi.err()
+        assert lib.psb_tray_set(t, tray0.ctypes.data, None) == 0, abi.err()
+        res = (Res * len(items))()
+        out = np.zeros_like(tray0)
+        lib.psb_debug_fail_alloc(k)
+        st = lib.psb_pack(t, ptrs, dims.ctypes.data, len(items), maps.ctypes.data, 4, 1, 0, res, out.ctypes.data)
+        lib.psb_debug_fail_alloc(0)
+        msg = abi.err()
+        assert lib.psb_tray_destroy(t) == 0
+        return st, msg, res, out
+
+    failures = 0
+    for k in range(1, 160):
+        st, msg, res, out = pack(k)
+        assert abi.live() == base, k
+        if st == 0:
+            break
+        assert st == PSB_ERR_CUDA and "injected" in msg, (k, st, msg)
+        failures += 1
+    assert failures >= 3
+    st, _, res, out = pack(0)
+    assert st == 0
+    # the same placements as staging everything first (the oracle for this
+    # 70-item run is minutes of CPU; the staged path is oracle-checked elsewhere)
+    t = ctypes.c_void_p()
+    assert lib.psb_tray_create(*shape, ctypes.byref(t)) == 0
+    assert lib.psb_tray_set(t, tray0.ctypes.data, None) == 0
+    lib.psb_pack_stage.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    assert lib.psb_pack_stage(t, ptrs, dims.ctypes.data, len(items)) == 0, abi.err()
+    res2 = (Res * len(items))()
+    out2 = np.zeros_like(tray0)
+    lib.psb_pack_staged.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int32,
+                                    ctypes.c_void_p, ctypes.c_void_p]
+    assert lib.psb_pack_staged(t, maps.ctypes.data, 4, 1, 0, res2, out2.ctypes.data) == 0, abi.err()
+    assert lib.psb_tray_destroy(t) == 0
+    np.testing.assert_array_equal(out, out2)
+    assert [(r.found, r.x, r.y, r.z, r.orientation, r.score) for r in res] == \
+           [(r.found, r.x, r.y, r.z, r.orientation, r.score) for r in res2]
