@@ -193,8 +193,10 @@ int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int 
              psb_result* out_placements, int32_t* final_tray);
 
 /* psb_pack split in two: stage the items of a run on the device once (their
- * voxel lists and bounds are computed here), then run the greedy loop over the
- * staged items.  psb_pack == psb_pack_stage + psb_pack_staged. */
+ * runs, bounds and filter samples are computed here), then run the greedy
+ * loop over the staged items.  psb_pack gives the same results as
+ * psb_pack_stage + psb_pack_staged; with 64 items or more it stages the
+ * items after the first 32 while those are searched. */
 int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items);
 int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                     psb_result* out_placements, int32_t* final_tray);

@@ -32,7 +32,9 @@ struct OrientDesc {
     double delta;             // bound on |D~ - D|
     double base;              // m * sumI (integer, exact in double)
     const int32_t* item;      // device base item
-    const int4* vox;          // device voxel list of the base item (x,y,z,value)
+    const int4* vox;          // device voxel list of the base item (x,y,z,value); the
+                              // synchronous calls only (null in the packing loop, which
+                              // places items by their runs)
     int nvox;
     int perm;                 // index of its axis permutation among the item's 6 bases
     double sumsq;             // sum of squared item values

@@ -42,7 +42,8 @@ __device__ __forceinline__ float bf16_val(uint16_t h) { return __uint_as_float((
 // ---------------------------------------------------------------------------
 // inputs
 // ---------------------------------------------------------------------------
-// base grid of one item from its voxel list: cell floor(v / s) gains 1/s^3,
+// base grid of one item from its voxel list (the synchronous item-grid call;
+// the packing loop uses k_base_grid_runs): cell floor(v / s) gains 1/s^3,
 // s = ceil(max extent / 32).  grid: (ceil(nvox/256)), block 256; out zeroed
 __global__ void k_base_grid(const int4* __restrict__ vox, int nvox, int s, float* __restrict__ out) {
     pdl_enter();
