@@ -394,6 +394,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "256 MiB buffer written before every step", "parallelism": f"replicas x{world} (independent trays)",
                    "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag,
                    "parity_vs_oracle_trace": parity,
+                   "density": round(float(r.density), 5) if r is not None else None,
                    "tie_guard": {"candidates_per_item_mean": round(statistics.mean(cands), 1),
                                  "candidates_per_item_max": max(cands),
                                  "max_fp32_error_over_bound": round(err_ratio, 4)}},
@@ -530,6 +531,22 @@ def run_learned(args, rank, world, local_rank):
                        "density_gap_pp": round(100 * (tot["plain"][2] - tot["learned"][2]), 3),
                        "fallback_rate": round(tot["learned"][3], 4),
                        "parallelism": "one tray, one GPU"}}
+
+
+def learned_leg(args, local_rank):
+    """The learned-proposal form beside the headline line (the metric's
+    "density vs plain GPU path"): one untimed and one timed pass of
+    run_learned over the 10 held-out config-4 seeds, plain and learned."""
+    import argparse
+    try:
+        doc = run_learned(argparse.Namespace(steps=1, warmup=1), 0, 1, local_rank)
+    except Exception as e:  # reported, never fatal for the headline line
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    c = doc["config"]
+    return {"workload": c["workload"] + " (128^3 tray, config-2 items)", "items_per_s": doc["value"],
+            "plain_items_per_s": c["plain_items_per_s"], "speedup_vs_plain": c["speedup_vs_plain"],
+            "density_learned": c["density_learned"], "density_plain": c["density_plain"],
+            "density_gap_pp": c["density_gap_pp"], "fallback_rate": c["fallback_rate"], "steps": 1, "warmup": 1}
 
 
 def _density(tray):
@@ -672,6 +689,7 @@ def main():
     ap.add_argument("--items", type=int, default=N_ITEMS, help="profiling only: shorter item stream")
     ap.add_argument("--value-only", action="store_true", help="profiling only: skip the e2e leg")
     ap.add_argument("--workload", default="config3", choices=["config3", "config4", "config5"])
+    ap.add_argument("--no-learned", action="store_true", help="config3: skip the learned-proposal leg")
     ap.add_argument("--trays", type=int, default=64, help="config5: number of trays")
     ap.add_argument("--concurrency", type=int, default=8, help="config5: trays packed at once per GPU")
     args = ap.parse_args()
@@ -699,6 +717,8 @@ def main():
     if rank == 0 and out is not None:
         if world == 1 and not args.no_cpu_baseline and args.workload == "config3":
             out["cpu_baseline"] = cpu_baseline()
+        if world == 1 and not args.no_learned and args.workload == "config3":
+            out["learned_proposal"] = learned_leg(args, local_rank)
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch

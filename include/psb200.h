@@ -282,7 +282,9 @@ int psb_pack_staged_prop(psb_tray* t, psb_proposal* prop, const int32_t* orient_
  * surface voxels only (the reference compiles the inside fill out), tight
  * bounding box.  tris: ntri x 3 vertices x (x, y, z) floats, as read from an
  * STL file.  out must hold resolution^3 int32; it receives the tight grid
- * (C order, values 0/1) and dims_out its shape ({0,0,0} when empty).       */
+ * (C order, values 0/1) and dims_out its shape ({0,0,0} when empty).  The
+ * triangle degeneracy test is evaluated modulo 2^32, as the reference's
+ * 32-bit int products wrap (packing.cpp rasterize).                        */
 int psb_voxelize_mesh(const float* tris, int ntri, int resolution, int32_t* out, int32_t* dims_out);
 
 /* Kernel variant switch (default on): FFT lengths 64, 100, 128, 240 use

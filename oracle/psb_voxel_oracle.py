@@ -15,9 +15,11 @@ A restatement of the reference's voxelize_stl path for triangle meshes:
                                           of the position in lexicographic order
   LibSL Matrix4x4.h:245-294               float32 matrix product and mulPoint,
                                           accumulated from zero in index order
-The reference itself is not built here (LibSL and a generated header), so
-this restatement is "parity unpinned": it is checked against hand-derived
-voxelizations of simple meshes in the tests.  Only tests import it.
+Pinned against the reference's own voxelize_stl (its module compiled from
+its sources by oracle/Makefile): tests/golden/make_voxel_golden.py records
+its outputs on seeded meshes in tests/golden/ref_voxels.npz, which this
+restatement reproduces bit for bit (tests/test_voxel_oracle.py).  Only tests
+import it.
 """
 from __future__ import annotations
 
@@ -146,7 +148,10 @@ def rasterize(tri, pts, vox):
         e02 = (tp[0][0] - tp[2][0], tp[0][1] - tp[2][1])
         if e10 == (0, 0) or e21 == (0, 0) or e02 == (0, 0):
             continue
-        if e02[0] * e10[1] - e02[1] * e10[0] == 0:
+        # the reference forms this determinant from int products (v2i), which
+        # wrap modulo 2^32 at these fixed-point magnitudes: a triangle whose
+        # determinant is a nonzero multiple of 2^32 is skipped as degenerate
+        if (e02[0] * e10[1] - e02[1] * e10[0]) % (1 << 32) == 0:
             continue
         xs = [p[0] // FP_SCALE for p in tp]
         ys = [p[1] // FP_SCALE for p in tp]
@@ -164,9 +169,11 @@ def rasterize(tri, pts, vox):
 
 
 def make_tight(g: np.ndarray) -> np.ndarray:
+    """voxelGrid.cpp:166-178: the bounding box of the occupied cells; an
+    empty grid raises, as the reference does."""
     idx = np.argwhere(g > 0)
     if len(idx) == 0:
-        return g
+        raise RuntimeError("(make_voxel_grid_tight) Voxel grid doesn't have any occupied cells")
     lo, hi = idx.min(axis=0), idx.max(axis=0) + 1
     return g[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
 

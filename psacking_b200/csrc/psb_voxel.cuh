@@ -68,7 +68,11 @@ __global__ void k_voxel_raster(const int* __restrict__ pts, const int* __restric
     const long long e21x = tp[2][0] - tp[1][0], e21y = tp[2][1] - tp[1][1];
     const long long e02x = tp[0][0] - tp[2][0], e02y = tp[0][1] - tp[2][1];
     if ((e10x == 0 && e10y == 0) || (e21x == 0 && e21y == 0) || (e02x == 0 && e02y == 0)) return;
-    if (e02x * e10y - e02y * e10x == 0) return;
+    // the reference forms this determinant from 32-bit int products (v2i),
+    // which wrap at these fixed-point magnitudes: a nonzero multiple of 2^32
+    // counts as degenerate there, so it is evaluated modulo 2^32 here too
+    // (a unit cube at a resolution where 0.95 * res is an integer loses every face)
+    if ((unsigned int)e02x * (unsigned int)e10y - (unsigned int)e02y * (unsigned int)e10x == 0u) return;
     const int x0 = min(tp[0][0], min(tp[1][0], tp[2][0])) / PSB_FP_SCALE;
     const int x1 = max(tp[0][0], max(tp[1][0], tp[2][0])) / PSB_FP_SCALE;
     const int y0 = min(tp[0][1], min(tp[1][1], tp[2][1])) / PSB_FP_SCALE;

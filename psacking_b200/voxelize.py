@@ -51,6 +51,8 @@ def voxelize_mesh(tris: np.ndarray, resolution: int = 128) -> np.ndarray:
     L.psb_voxelize_mesh.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     check(L.psb_voxelize_mesh(tris.ctypes.data, len(tris), int(resolution), out.ctypes.data, dims.ctypes.data))
     n = int(np.prod(dims))
+    if n == 0:  # make_voxel_grid_tight raises on a grid without occupied cells (voxelGrid.cpp:166-170)
+        raise RuntimeError("(make_voxel_grid_tight) Voxel grid doesn't have any occupied cells")
     return out[:n].reshape(tuple(int(d) for d in dims)).copy()
 
 

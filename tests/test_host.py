@@ -55,6 +55,20 @@ def test_vox_layout():
     assert len(b) == 12 + 6 + 768
 
 
+def test_vox_bytes_match_reference_save_vox():
+    """encode_vox equals, byte for byte, the files the reference's own
+    save_vox wrote for seeded grids (values 0, 8, above 255 and negative;
+    tests/golden/ref_voxels.npz)."""
+    import hashlib
+
+    from tests import golden_vox
+    cases = golden_vox.load_save_vox()
+    assert len(cases) == 12
+    for g, sha, n in cases:
+        b = encode_vox(g)
+        assert len(b) == n and hashlib.sha256(b).hexdigest() == sha
+
+
 def test_workloads_deterministic_and_in_range():
     a = workloads.config1_items(3)
     b = workloads.config1_items(3)
