@@ -38,8 +38,11 @@ from ._core import (  # noqa: E402
 )
 from .packer import BinPacker, PackingResult, PlacementInfo  # noqa: E402
 from .rotations import (  # noqa: E402
+    ROTATION_MATRICES_3x3,
     get_24_orientations,
     get_orientations,
+    get_rotation_matrix_3x3,
+    get_rotation_matrix_4x4,
     orientation_maps,
     rotate_90_x,
     rotate_90_y,
@@ -64,5 +67,5 @@ __all__ = [
     "get_bounds", "gpu_tray_cleanup", "gpu_tray_init", "gpu_tray_is_initialized", "gpu_tray_search",
     "interlocking_free_positions", "make_tight", "place_in_tray", "save_vox", "voxelize_stl",
     "get_orientations", "get_24_orientations", "orientation_maps", "rotate_90_x", "rotate_90_y",
-    "rotate_90_z",
+    "rotate_90_z", "get_rotation_matrix_3x3", "get_rotation_matrix_4x4", "ROTATION_MATRICES_3x3",
 ]

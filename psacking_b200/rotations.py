@@ -102,3 +102,39 @@ def apply_map(item: np.ndarray, row) -> np.ndarray:
     g = np.transpose(item, axes)
     sl = tuple(slice(None, None, -1) if flips[a] else slice(None) for a in range(3))
     return np.ascontiguousarray(g[sl])
+
+
+def _rotation_matrices() -> List[np.ndarray]:
+    """The 24 orientations as rotation matrices on voxel-centre coordinates
+    measured from the grid centre: a voxel at x in the item lands at R @ x
+    in the oriented grid.  Row a of R holds one entry, at the source axis of
+    output axis a (orientation_maps), -1 where that axis is reversed.  These
+    equal the reference's ROTATION_MATRICES_3x3 (rotations.py:41-89), which
+    blender export uses to turn a placement's orientation_index into a mesh
+    transform."""
+    out = []
+    for row in orientation_maps(24):
+        r = np.zeros((3, 3), dtype=np.float64)
+        for a in range(3):
+            r[a, int(row[a])] = -1.0 if row[3 + a] else 1.0
+        out.append(r)
+    return out
+
+
+ROTATION_MATRICES_3x3: List[np.ndarray] = _rotation_matrices()
+
+
+def get_rotation_matrix_3x3(orientation_index: int) -> np.ndarray:
+    """3x3 rotation of orientation `orientation_index` (0..23, the order of
+    get_24_orientations); IndexError outside that range (rotations.py:92-112)."""
+    if not 0 <= orientation_index < 24:
+        raise IndexError(f"orientation_index must be 0-23, got {orientation_index}")
+    return ROTATION_MATRICES_3x3[orientation_index].copy()
+
+
+def get_rotation_matrix_4x4(orientation_index: int) -> np.ndarray:
+    """The same rotation as a 4x4 homogeneous matrix, no translation
+    (rotations.py:115-138)."""
+    m = np.eye(4, dtype=np.float64)
+    m[:3, :3] = get_rotation_matrix_3x3(orientation_index)
+    return m

@@ -13,7 +13,9 @@ module, so this needs no GPU:
       first overlapping cell in row-major order);
   make_tight / get_bounds (bindings.cpp, voxelGrid.cpp:166-178, 279-299):
       sparse grids with negative values, single voxels, full grids, and
-      empty grids (make_tight raises).
+      empty grids (make_tight raises);
+and from its Python package, the 24 rotation matrices of the orientation
+order (spectral_packer/rotations.py:41-89).
 """
 from __future__ import annotations
 
@@ -80,6 +82,8 @@ def main(ref_dir: str) -> None:
         except ValueError:
             rec[f"grid/{k}/tight_error"] = np.int8(1)
     rec["grid_count"] = np.int32(k + 1)
+    from spectral_packer import rotations as RR  # the reference's unmodified package next to the module
+    rec["rotation_matrices_3x3"] = np.asarray(RR.ROTATION_MATRICES_3x3, np.float64)
     np.savez_compressed(ROOT / "tests" / "golden" / "ref_host.npz", **rec)
     n_err = sum(1 for key in rec if key.endswith("/error"))
     print(f"{int(rec['place_count'])} place_in_tray cases ({n_err} raise), {int(rec['grid_count'])} grids")

@@ -93,3 +93,31 @@ def test_positive_counts_match_numpy():
     assert [int(v) for v in _core.positive_counts(items)] == want
     _, volumes, _, _, _ = BinPacker((40, 40, 40))._prepare(items, True, None)
     assert volumes == want
+
+
+def test_rotation_matrices_match_reference_and_grids():
+    """ROTATION_MATRICES_3x3 equals the reference's own list
+    (tests/golden/ref_host.npz), and each matrix moves a voxel's centre
+    (measured from the grid centre) to where get_24_orientations puts it."""
+    from pathlib import Path
+
+    from psacking_b200 import rotations as R
+    want = np.load(Path(__file__).resolve().parent / "golden" / "ref_host.npz")["rotation_matrices_3x3"]
+    assert len(R.ROTATION_MATRICES_3x3) == 24
+    assert all(m.dtype == np.float64 and np.array_equal(m, w) for m, w in zip(R.ROTATION_MATRICES_3x3, want))
+    g = np.zeros((2, 3, 5), np.int32)
+    marks = [(0, 0, 0), (1, 2, 4), (1, 0, 3), (0, 2, 1)]
+    for v, p in enumerate(marks, start=1):
+        g[p] = v
+    for o, og in enumerate(R.get_24_orientations(g)):
+        m = R.get_rotation_matrix_3x3(o)
+        assert np.allclose(m @ m.T, np.eye(3)) and np.isclose(np.linalg.det(m), 1.0)
+        for v, p in enumerate(marks, start=1):
+            src = np.asarray(p, float) - (np.asarray(g.shape) - 1) / 2
+            dst = np.argwhere(og == v)[0] - (np.asarray(og.shape) - 1) / 2
+            assert np.allclose(m @ src, dst), (o, v)
+        m4 = R.get_rotation_matrix_4x4(o)
+        assert np.array_equal(m4[:3, :3], m) and np.array_equal(m4[3], [0, 0, 0, 1]) and not m4[:3, 3].any()
+    for bad in (-1, 24):
+        with pytest.raises(IndexError):
+            R.get_rotation_matrix_3x3(bad)
