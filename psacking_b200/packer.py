@@ -101,8 +101,28 @@ class BinPacker:
     # ------------------------------------------------------------------ files
     def pack_files(self, paths: Sequence[Union[str, Path]], sort_by_volume: bool = True,
                    validate_meshes: bool = True, repair_meshes: bool = True) -> PackingResult:
-        raise NotImplementedError(
-            "mesh voxelization is outside this engine; voxelize items first and call pack_voxels")
+        """Pack STL meshes (packer.py:253-295 of the reference): each file is
+        voxelized at `voxel_resolution` by voxelize_stl (the path the
+        reference's Voxelizer.voxelize_file takes for .stl files), then the
+        grids are packed by pack_voxels.  Other mesh formats, and STL files
+        voxelize_stl rejects, go through trimesh in the reference, which is
+        not part of this engine: they raise NotImplementedError.  The
+        validate/repair flags only concern that loader and are accepted for
+        interface compatibility."""
+        from .voxelize import voxelize_stl
+        voxels = []
+        for path in paths:
+            path = Path(path)
+            if not path.exists():
+                raise FileNotFoundError(f"Mesh file not found: {path}")
+            if path.suffix.lower() != ".stl":
+                raise NotImplementedError(f"{path}: only STL meshes are voxelized by this engine")
+            try:
+                voxels.append(voxelize_stl(path, self.voxel_resolution))
+            except RuntimeError as e:
+                raise NotImplementedError(f"{path}: voxelize_stl failed ({e}); the reference would fall back "
+                                          "to its trimesh voxelizer, which this engine does not include") from e
+        return self.pack_voxels(voxels, sort_by_volume=sort_by_volume)
 
     # ------------------------------------------------------------------ voxels
     def _prepare(self, items, sort_by_volume, initial_tray):

@@ -121,3 +121,35 @@ def test_rotation_matrices_match_reference_and_grids():
     for bad in (-1, 24):
         with pytest.raises(IndexError):
             R.get_rotation_matrix_3x3(bad)
+
+
+def test_pack_files_voxelizes_stl_then_packs(tmp_path, monkeypatch):
+    """pack_files voxelizes every STL at the packer's voxel_resolution with
+    voxelize_stl, in the order given, and hands the grids to pack_voxels
+    (here the GPU voxelizer is replaced by its oracle and pack_voxels by a
+    recorder: host logic only)."""
+    from oracle import psb_voxel_oracle as V
+    from psacking_b200 import voxelize as VZ
+    from tests import meshes
+    shapes = [meshes.box(), meshes.tetra(), meshes.icosphere(1)]
+    paths = []
+    for k, tris in enumerate(shapes):
+        paths.append(tmp_path / f"m{k}.STL")
+        VZ.write_stl(paths[-1], tris)
+    monkeypatch.setattr(VZ, "voxelize_stl", lambda p, res: V.voxelize(VZ.read_stl(p), res))
+    seen = {}
+
+    def record(self, items, sort_by_volume=True, initial_tray=None):
+        seen["items"], seen["sort"] = items, sort_by_volume
+        return "packed"
+    monkeypatch.setattr(BinPacker, "pack_voxels", record)
+    bp = BinPacker((40, 40, 40), voxel_resolution=12)
+    assert bp.pack_files([str(p) for p in paths], sort_by_volume=False) == "packed"
+    assert seen["sort"] is False and len(seen["items"]) == 3
+    for got, tris in zip(seen["items"], shapes):
+        assert np.array_equal(got, V.voxelize(tris, 12))
+    with pytest.raises(FileNotFoundError):
+        bp.pack_files([tmp_path / "missing.stl"])
+    (tmp_path / "x.obj").write_text("v 0 0 0\n")
+    with pytest.raises(NotImplementedError):
+        bp.pack_files([tmp_path / "x.obj"])
