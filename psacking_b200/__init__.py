@@ -61,7 +61,7 @@ def voxelize_stl(path, resolution: int = VOXEL_RESOLUTION):
 
 
 __all__ = [
-    "BinPacker", "PackingResult", "PlacementInfo", "HEIGHT_PENALTY", "VOXEL_RESOLUTION",
+    "__version__", "BinPacker", "PackingResult", "PlacementInfo", "HEIGHT_PENALTY", "VOXEL_RESOLUTION",
     "calculate_distance", "collision_grid", "dft_conv3", "dft_corr3", "fft_search_batch",
     "fft_search_batch_interlocking_free", "fft_search_placement", "fft_search_placement_with_cache",
     "get_bounds", "gpu_tray_cleanup", "gpu_tray_init", "gpu_tray_is_initialized", "gpu_tray_search",

@@ -262,8 +262,9 @@ class BinPacker:
             results.append(sub._finish(final, placements, n_items, None))
         return results
 
-    def pack_single(self, item: np.ndarray, tray: Optional[np.ndarray] = None):
-        """packer.py:546-580."""
+    def pack_single(self, item: np.ndarray,
+                    tray: Optional[np.ndarray] = None) -> Tuple[Optional[Tuple[int, int, int]], bool, float]:
+        """packer.py:546-580: (position or None, found, score)."""
         if tray is None:
             tray = np.zeros(self.tray_size, dtype=np.int32)
         pos, found, score = _core.fft_search_placement(item.astype(np.int32), tray)
