@@ -84,6 +84,28 @@ def main(ref_dir: str) -> None:
     rec["grid_count"] = np.int32(k + 1)
     from spectral_packer import rotations as RR  # the reference's unmodified package next to the module
     rec["rotation_matrices_3x3"] = np.asarray(RR.ROTATION_MATRICES_3x3, np.float64)
+    # packing statistics and the result summary (packer.py:145-162, 582-601)
+    from spectral_packer.packer import BinPacker, PackingResult
+    for k in range(8):
+        shape = tuple(int(v) for v in rng.integers(2, 30, 3))
+        tray = np.zeros(shape, np.int32)
+        if k:
+            m = rng.random(shape) < [0.0005, 0.01, 0.2, 0.6, 0.9, 1.0, 0.05][k - 1]
+            tray[m] = rng.integers(1, 40, int(m.sum()))
+            tray[rng.random(shape) < 0.02] *= -1
+        bp = BinPacker(shape, voxel_resolution=int(rng.integers(16, 200)), num_orientations=[1, 4, 6, 24][k % 4])
+        dens, total, bbox = bp._calculate_stats(tray)
+        placed, failed = int(rng.integers(0, 50)), int(rng.integers(0, 50))
+        res = PackingResult(tray=tray, num_placed=placed, num_failed=failed, density=dens, total_volume=total,
+                            bounding_box=bbox)
+        rec[f"stats/{k}/tray"] = tray
+        rec[f"stats/{k}/args"] = np.asarray([bp.voxel_resolution, bp.num_orientations, placed, failed], np.int64)
+        rec[f"stats/{k}/density"] = np.float64(dens)
+        rec[f"stats/{k}/total"] = np.int64(total)
+        rec[f"stats/{k}/bbox"] = np.asarray(bbox if bbox else [[-1, -1, -1], [-1, -1, -1]], np.int64)
+        rec[f"stats/{k}/summary"] = np.asarray(res.summary())
+        rec[f"stats/{k}/repr"] = np.asarray(repr(bp))
+    rec["stats_count"] = np.int32(8)
     np.savez_compressed(ROOT / "tests" / "golden" / "ref_host.npz", **rec)
     n_err = sum(1 for key in rec if key.endswith("/error"))
     print(f"{int(rec['place_count'])} place_in_tray cases ({n_err} raise), {int(rec['grid_count'])} grids")

@@ -45,3 +45,26 @@ def test_bounds_and_tight_match_reference(k):
     t = O.make_tight(g)
     want = Z[f"grid/{k}/tight"]
     assert t.shape == want.shape and np.array_equal(t, want)
+
+
+@pytest.mark.parametrize("k", range(int(Z["stats_count"])))
+def test_packing_stats_and_summary_match_reference(k):
+    """BinPacker's density / volume / bounding box, from the tray on the
+    host (_calculate_stats) and from the device's counts (_stats_from_counts,
+    fed here with numpy's), PackingResult.summary() and BinPacker's repr equal
+    the reference's on the same trays (packer.py:145-162, 582-608)."""
+    from psacking_b200 import BinPacker, PackingResult
+    tray = Z[f"stats/{k}/tray"]
+    res, n_or, placed, failed = (int(v) for v in Z[f"stats/{k}/args"])
+    bp = BinPacker(tray.shape, voxel_resolution=res, num_orientations=n_or)
+    bbox = Z[f"stats/{k}/bbox"].tolist()
+    want = (float(Z[f"stats/{k}/density"]), int(Z[f"stats/{k}/total"]),
+            None if bbox[0][0] < 0 else (tuple(bbox[0]), tuple(bbox[1])))
+    assert bp._calculate_stats(tray) == want
+    occ = np.argwhere(tray > 0)
+    lo, hi = (occ.min(axis=0), occ.max(axis=0)) if len(occ) else ((0, 0, 0), (-1, -1, -1))
+    assert BinPacker._stats_from_counts(len(occ), lo, hi) == want
+    r = PackingResult(tray=tray, num_placed=placed, num_failed=failed, density=want[0], total_volume=want[1],
+                      bounding_box=want[2])
+    assert r.summary() == str(Z[f"stats/{k}/summary"])
+    assert repr(bp) == str(Z[f"stats/{k}/repr"])
