@@ -35,3 +35,28 @@ def test_reference_arm_loads_no_repository_native_code():
     done, total = (int(v) for v in line["config"]["sample_parity_vs_trace"].split("/"))
     assert total > 0 and done == total
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+
+
+def test_learned_leg_reports_and_never_fails_the_line(monkeypatch):
+    """The learned-proposal object of the headline line copies the config-4
+    run's figures, and any exception there becomes an `unavailable` entry
+    instead of ending the bench (host logic; run_learned is stubbed)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    doc = {"value": 2000.0, "config": {"workload": "config4: w", "plain_items_per_s": 1250.0,
+                                       "speedup_vs_plain": 1.6, "density_learned": 0.44,
+                                       "density_plain": 0.45, "density_gap_pp": 0.8, "fallback_rate": 0.03}}
+    seen = {}
+
+    def fake(args, rank, world, local_rank):
+        seen.update(steps=args.steps, warmup=args.warmup, rank=rank, world=world, local_rank=local_rank)
+        return doc
+    monkeypatch.setattr(bench, "run_learned", fake)
+    out = bench.learned_leg(None, 0)
+    assert seen == {"steps": 1, "warmup": 1, "rank": 0, "world": 1, "local_rank": 0}
+    assert out["items_per_s"] == 2000.0 and out["speedup_vs_plain"] == 1.6 and out["density_gap_pp"] == 0.8
+
+    def boom(*a):
+        raise RuntimeError("no device")
+    monkeypatch.setattr(bench, "run_learned", boom)
+    assert bench.learned_leg(None, 0) == {"unavailable": "RuntimeError: no device"}
