@@ -7,7 +7,11 @@
 //   * CUDA failures raise RuntimeError (the reference only prints them,
 //     fft3.cu:59-91) and there is no CPU fallback;
 //   * negative voxel values are rejected with RuntimeError;
-//   * the GIL is released while the device works.
+//   * the GIL is released while the device works.  The module's two
+//     process-wide device contexts (the search context behind the
+//     generation cache, and the packing context of pack_native) are each
+//     guarded by a mutex instead, so calls from several Python threads are
+//     serialised per context as the GIL serialises them in the reference.
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -17,6 +21,7 @@
 #include <algorithm>
 #include <atomic>
 #include <fstream>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <thread>
@@ -71,6 +76,25 @@ py::tuple result_tuple(const psb_result& r) {
 // ---------------------------------------------------------------------------
 psb_tray* g_ctx = nullptr;
 uint64_t g_cached_generation = 0;
+
+// Holds g_ctx_mu for the whole call of a function that reads or changes
+// g_ctx, g_ctx_initialized or g_cached_generation, so a tray set up for one
+// generation is searched by the same call.  The mutex is only waited for
+// with the GIL released (the GIL is taken back once it is held), so a thread
+// holding the GIL never waits for it and no two threads can wait on each
+// other.  Recursive: the search functions call gpu_tray_is_initialized.
+std::recursive_mutex g_ctx_mu;
+
+class CtxLock {
+  public:
+    CtxLock() : lk_(g_ctx_mu, std::defer_lock) {
+        py::gil_scoped_release nogil;
+        lk_.lock();
+    }
+
+  private:
+    std::unique_lock<std::recursive_mutex> lk_;
+};
 
 void ctx_init(const Grid& tray, const Grid& phi) {
     if (phi.n[0] != tray.n[0] || phi.n[1] != tray.n[1] || phi.n[2] != tray.n[2])
@@ -142,6 +166,7 @@ py::tuple py_fft_search_placement(py::handle item, py::handle tray) {
 py::tuple py_fft_search_placement_with_cache(py::handle item, py::handle tray, py::handle tray_distance,
                                              uint64_t generation) {
     Grid it = to_grid(item), tr = to_grid(tray), ph = to_grid(tray_distance);
+    CtxLock lock;
     if (it.n[0] > tr.n[0] || it.n[1] > tr.n[1] || it.n[2] > tr.n[2])  // bindings.cpp:230-234
         return py::make_tuple(py::make_tuple(-1, -1, -1), false, 0.0);
     if (!g_ctx_initialized || generation != g_cached_generation) {
@@ -155,6 +180,7 @@ py::tuple py_fft_search_placement_with_cache(py::handle item, py::handle tray, p
 
 py::tuple py_fft_search_batch(py::list orientations, py::handle tray, py::handle tray_distance, uint64_t generation) {
     Grid tr = to_grid(tray), ph = to_grid(tray_distance);
+    CtxLock lock;
     if (!g_ctx_initialized || generation != g_cached_generation) {
         ctx_init(tr, ph);
         g_ctx_initialized = true;
@@ -170,6 +196,7 @@ py::tuple py_fft_search_batch(py::list orientations, py::handle tray, py::handle
 py::tuple py_fft_search_batch_interlocking_free(py::list orientations, py::handle tray, py::handle tray_distance,
                                                 uint64_t generation) {
     Grid tr = to_grid(tray), ph = to_grid(tray_distance);
+    CtxLock lock;
     if (!g_ctx_initialized || generation != g_cached_generation) {
         ctx_init(tr, ph);
         g_ctx_initialized = true;
@@ -306,19 +333,25 @@ py::array_t<int32_t> py_make_tight(py::handle grid) {
 
 void py_gpu_tray_init(py::handle tray, py::handle tray_distance) {
     Grid tr = to_grid(tray), ph = to_grid(tray_distance);
+    CtxLock lock;
     ctx_init(tr, ph);
     g_ctx_initialized = true;
 }
 
 void py_gpu_tray_cleanup() {
+    CtxLock lock;
     if (g_ctx) psb_tray_destroy(g_ctx);
     g_ctx = nullptr;
     g_ctx_initialized = false;
 }
 
-bool py_gpu_tray_is_initialized() { return g_ctx_initialized && ctx_ready(); }
+bool py_gpu_tray_is_initialized() {
+    CtxLock lock;
+    return g_ctx_initialized && ctx_ready();
+}
 
 py::tuple py_gpu_tray_search(py::handle item) {
+    CtxLock lock;
     if (!py_gpu_tray_is_initialized())
         throw std::runtime_error("GPU tray context not initialized. Call gpu_tray_init() first.");
     Grid it = to_grid(item);
@@ -384,6 +417,8 @@ py::tuple py_pack_native(py::list items, py::handle initial_tray, py::array_t<in
         // the next run with the same tray shape instead of being rebuilt
         py::gil_scoped_release nogil;
         static psb_tray* pack_ctx = nullptr;
+        static std::mutex pack_mu;  // one run at a time on the shared context (GIL released here)
+        std::lock_guard<std::mutex> lk(pack_mu);
         if (pack_ctx) {
             int dx, dy, dz;
             psb_tray_dims(pack_ctx, &dx, &dy, &dz);
@@ -459,6 +494,7 @@ py::list py_pack_many(py::list trays, py::array_t<int32_t> orient_maps, bool int
 }
 
 py::dict py_search_detail(py::list orientations, int flags, bool per_orientation) {
+    CtxLock lock;
     if (!py_gpu_tray_is_initialized()) throw std::runtime_error("GPU tray context not initialized");
     auto gs = to_grids(orientations);
     std::vector<const int32_t*> ptrs;

@@ -85,3 +85,39 @@ def test_no_gpu_fails_loudly(core):
         core.calculate_distance(np.zeros((4, 4, 4), np.int32))
     with pytest.raises(RuntimeError):
         core.fft_search_placement(np.ones((2, 2, 2), np.int32), np.zeros((6, 6, 6), np.int32))
+
+
+def test_context_calls_from_threads_are_serialised(core):
+    """The module's process-wide search context is guarded by a mutex that
+    is only waited for with the GIL released: calls that use it from several
+    Python threads at once neither deadlock nor crash.  Without a GPU every
+    such call raises, which exercises the lock on the error path too."""
+    import threading
+    if core.device_count() > 0:
+        pytest.skip("a GPU is visible (the GPU tests cover the context itself)")
+    tray = np.zeros((6, 6, 6), np.int32)
+    phi = np.zeros_like(tray)
+    item = np.ones((2, 2, 2), np.int32)
+    errors, done = [], []
+
+    def worker(k):
+        for g in range(20):
+            for call in (lambda: core.gpu_tray_init(tray, phi),
+                         lambda: core.fft_search_batch([item], tray, phi, 1000 * k + g),
+                         lambda: core.fft_search_placement_with_cache(item, tray, phi, 1000 * k + g),
+                         lambda: core.gpu_tray_search(item)):
+                try:
+                    call()
+                except RuntimeError as e:
+                    errors.append(str(e))
+            core.gpu_tray_is_initialized()
+            core.gpu_tray_cleanup()
+        done.append(k)
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=120)
+    assert sorted(done) == [0, 1, 2, 3]
+    assert len(errors) == 4 * 20 * 4
+    assert not core.gpu_tray_is_initialized()
