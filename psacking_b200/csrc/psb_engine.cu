@@ -2042,9 +2042,13 @@ int stage_arrays(psb_tray* t, const int32_t* const* items, const int32_t* dims, 
     return PSB_OK;
 }
 
-// cached contexts for the stateless entry points, keyed by dims
+// cached contexts for the stateless entry points, keyed by dims.  A caller
+// holds g_util_call_mu for its whole call (UtilCall), so a cached context is
+// used by one call at a time and is never dropped while another call uses it.
 std::mutex g_util_mu;
 std::map<std::tuple<int, int, int, int>, std::unique_ptr<psb_tray>> g_util;
+std::recursive_mutex g_util_call_mu;
+typedef std::lock_guard<std::recursive_mutex> UtilCall;
 
 int util_tray(int nx, int ny, int nz, psb_tray** out) {
     TRY(ensure_device());
@@ -2543,6 +2547,7 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
     size_t V = (size_t)nx * ny * nz;
     std::vector<int32_t> coll(V);
     TRY(psb_collision_grid(tray, nx, ny, nz, obj, ex, ey, ez, coll.data()));
+    UtilCall serial(g_util_call_mu);
     psb_tray* t = nullptr;
     TRY(util_tray(nx, ny, nz, &t));
     TRY(t->ensure_slots(1));
@@ -2602,6 +2607,7 @@ int psb_fft_search_placement(const int32_t* item, int ex, int ey, int ez, const 
     psb_result none{-1, -1, -1, 0, 0.0, -1, 0, 0, 0.f};
     *out = none;
     if (ex > nx || ey > ny || ez > nz) return PSB_OK;  // bindings.cpp:189-194
+    UtilCall serial(g_util_call_mu);
     psb_tray* t = nullptr;
     TRY(util_tray(nx, ny, nz, &t));
     TRY(t->set(tray, nullptr));

@@ -89,9 +89,11 @@ def test_no_gpu_fails_loudly(core):
 
 def test_context_calls_from_threads_are_serialised(core):
     """The module's process-wide search context is guarded by a mutex that
-    is only waited for with the GIL released: calls that use it from several
-    Python threads at once neither deadlock nor crash.  Without a GPU every
-    such call raises, which exercises the lock on the error path too."""
+    is only waited for with the GIL released, and the engine's cached
+    contexts of the stateless searches by a call lock: calls that use them
+    from several Python threads at once neither deadlock nor crash.  Without
+    a GPU every such call raises, which exercises the locks on the error
+    path too."""
     import threading
     if core.device_count() > 0:
         pytest.skip("a GPU is visible (the GPU tests cover the context itself)")
@@ -105,7 +107,8 @@ def test_context_calls_from_threads_are_serialised(core):
             for call in (lambda: core.gpu_tray_init(tray, phi),
                          lambda: core.fft_search_batch([item], tray, phi, 1000 * k + g),
                          lambda: core.fft_search_placement_with_cache(item, tray, phi, 1000 * k + g),
-                         lambda: core.gpu_tray_search(item)):
+                         lambda: core.gpu_tray_search(item),
+                         lambda: core.fft_search_placement(item, tray)):
                 try:
                     call()
                 except RuntimeError as e:
@@ -119,5 +122,5 @@ def test_context_calls_from_threads_are_serialised(core):
     for t in threads:
         t.join(timeout=120)
     assert sorted(done) == [0, 1, 2, 3]
-    assert len(errors) == 4 * 20 * 4
+    assert len(errors) == 4 * 20 * 5
     assert not core.gpu_tray_is_initialized()
