@@ -395,6 +395,8 @@ def run_ours(args, rank, world, local_rank):
                    "fft_dims": F, "deterministic_across_steps": same, "diag_bits": diag,
                    "parity_vs_oracle_trace": parity,
                    "density": round(float(r.density), 5) if r is not None else None,
+                   "density_definition": "occupied cells / their bounding box (PackingResult.density)",
+                   "occupied_of_tray": round(float(r.total_volume) / float(np.prod(TRAY)), 5) if r is not None else None,
                    "tie_guard": {"candidates_per_item_mean": round(statistics.mean(cands), 1),
                                  "candidates_per_item_max": max(cands),
                                  "max_fp32_error_over_bound": round(err_ratio, 4)}},
