@@ -14,6 +14,8 @@ Two engines produce identical results:
 """
 from __future__ import annotations
 
+import hashlib
+import os
 from dataclasses import dataclass, field
 from pathlib import Path
 from typing import List, Optional, Sequence, Tuple, Union
@@ -235,11 +237,20 @@ class BinPacker:
                              bounding_box=bbox, diagnostics=diag)
 
     def pack_many(self, trays: Sequence[Tuple[Tuple[int, int, int], Sequence[np.ndarray]]],
-                  sort_by_volume: bool = True, concurrency: int = 8) -> List[PackingResult]:
+                  sort_by_volume: bool = True, concurrency: int = 8,
+                  checkpoint: Optional[Union[str, Path]] = None) -> List[PackingResult]:
         """Pack independent trays (each (dims, items), starting empty) with
         this packer's orientation and interlocking settings.  Equivalent to one
         BinPacker(dims, ...).pack_voxels(items) per tray; up to `concurrency`
-        trays run at once on separate CUDA streams."""
+        trays run at once on separate CUDA streams.
+
+        checkpoint: an .npz path.  The trays are then packed `concurrency` at
+        a time, and after each group the final tray and the per-item results
+        of every finished tray are written there (to a temporary file, then
+        renamed over it).  A call given an existing checkpoint reads the
+        finished trays back and packs only the others; the file records a
+        digest of every tray's dimensions, items and the packer's settings,
+        and a checkpoint written for other inputs raises ValueError."""
         jobs, metas = [], []
         for dims, items in trays:
             sub = BinPacker(dims, self.voxel_resolution, self.height_penalty, self.num_orientations,
@@ -247,8 +258,11 @@ class BinPacker:
             processed, volumes, order, _, _ = sub._prepare(items, sort_by_volume, None)
             jobs.append((tuple(int(d) for d in dims), [np.ascontiguousarray(processed[i]) for i in order]))
             metas.append((sub, volumes, order, len(items)))
-        outs = _core.pack_many(jobs, orientation_maps(self.num_orientations), bool(self.interlocking_free),
-                               int(concurrency))
+        if checkpoint is None:
+            outs = _core.pack_many(jobs, orientation_maps(self.num_orientations), bool(self.interlocking_free),
+                                   int(concurrency))
+        else:
+            outs = self._pack_many_checkpointed(jobs, int(concurrency), Path(checkpoint))
         results = []
         for (sub, volumes, order, n_items), (final, res) in zip(metas, outs):
             placements = []
@@ -261,6 +275,49 @@ class BinPacker:
                     placements.append(PlacementInfo(int(orig), None, None, False, volumes[orig], 0))
             results.append(sub._finish(final, placements, n_items, None))
         return results
+
+    def _job_digest(self, dims, items) -> str:
+        h = hashlib.sha256()
+        h.update(repr((tuple(dims), int(self.num_orientations), bool(self.interlocking_free))).encode())
+        for it in items:
+            h.update(repr(it.shape).encode())
+            h.update(np.ascontiguousarray(it, dtype=np.int32).tobytes())
+        return h.hexdigest()
+
+    def _pack_many_checkpointed(self, jobs, concurrency: int, path: Path):
+        """_core.pack_many's (final tray, results) per job, `concurrency` jobs
+        per call, with the finished ones kept in the checkpoint file."""
+        keys = [self._job_digest(dims, items) for dims, items in jobs]
+        done = {}
+        if path.exists():
+            with np.load(path) as z:
+                if [str(k) for k in z["keys"]] != keys:
+                    raise ValueError(f"checkpoint {path} was written for other trays, items or settings")
+                for i in z["done"].tolist():
+                    done[int(i)] = (np.array(z[f"final_{i}"]), np.array(z[f"rec_{i}"]))
+        todo = [i for i in range(len(jobs)) if i not in done]
+        maps = orientation_maps(self.num_orientations)
+        step = max(1, concurrency)
+        for c in range(0, len(todo), step):
+            part = todo[c:c + step]
+            outs = _core.pack_many([jobs[i] for i in part], maps, bool(self.interlocking_free), concurrency)
+            for i, (final, res) in zip(part, outs):
+                # per item: found, x, y, z, score, orientation (float64 holds them exactly)
+                rec = np.asarray([[float(bool(r[1])), *(float(v) for v in r[0]), float(r[2]), float(r[3])]
+                                  for r in res], dtype=np.float64).reshape(-1, 6)
+                done[i] = (np.asarray(final, dtype=np.int32), rec)
+            arrays = {"keys": np.asarray(keys), "done": np.asarray(sorted(done), dtype=np.int64)}
+            for i, (final, rec) in done.items():
+                arrays[f"final_{i}"], arrays[f"rec_{i}"] = final, rec
+            tmp = path.with_name(path.name + ".tmp")
+            with open(tmp, "wb") as f:
+                np.savez(f, **arrays)
+            os.replace(tmp, path)
+        outs = []
+        for i in range(len(jobs)):
+            final, rec = done[i]
+            outs.append((final, [((int(r[1]), int(r[2]), int(r[3])), bool(r[0]), float(r[4]), int(r[5])) for r in rec]))
+        return outs
 
     def pack_single(self, item: np.ndarray,
                     tray: Optional[np.ndarray] = None) -> Tuple[Optional[Tuple[int, int, int]], bool, float]:

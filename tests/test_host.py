@@ -153,3 +153,57 @@ def test_pack_files_voxelizes_stl_then_packs(tmp_path, monkeypatch):
     (tmp_path / "x.obj").write_text("v 0 0 0\n")
     with pytest.raises(NotImplementedError):
         bp.pack_files([tmp_path / "x.obj"])
+
+
+def test_pack_many_checkpoint_resumes_where_it_stopped(tmp_path, monkeypatch):
+    """pack_many with a checkpoint: an interrupted call keeps the finished
+    groups of trays, a resumed call packs only the rest, and the results
+    equal an uninterrupted run; a checkpoint of other inputs is refused.
+    _core.pack_many is replaced by the oracle's packing loop (host logic)."""
+    from psacking_b200 import packer as PK
+    calls = []
+
+    def fake_pack_many(jobs, maps, interlock, concurrency):
+        calls.append(len(jobs))
+        outs = []
+        for dims, items in jobs:
+            tray, pl = O.pack_voxels(items, dims, 1, interlock, sort_by_volume=False)
+            res = [((tuple(p["position"]) if p["success"] else (-1, -1, -1)), p["success"],
+                    float(p["score"]) if p["success"] else 0.0, p["orientation_index"], 0, 0, 0.0) for p in pl]
+            outs.append((tray, res))
+        return outs
+    monkeypatch.setattr(PK._core, "pack_many", fake_pack_many)
+    rng = np.random.default_rng(5)
+    trays = []
+    for k in range(5):
+        items = [np.ones(tuple(int(v) for v in rng.integers(2, 6, 3)), np.int32) for _ in range(4)]
+        trays.append(((8, 9, 7), items))
+    bp = BinPacker((8, 8, 8), num_orientations=1)
+    full = bp.pack_many(trays, concurrency=2)
+    ck = tmp_path / "run.npz"
+    calls.clear()
+    real = fake_pack_many
+
+    def failing(jobs, *a):
+        if len(calls) == 1:
+            calls.append("fail")
+            raise RuntimeError("interrupted")
+        return real(jobs, *a)
+    monkeypatch.setattr(PK._core, "pack_many", failing)
+    with pytest.raises(RuntimeError, match="interrupted"):
+        bp.pack_many(trays, concurrency=2, checkpoint=ck)
+    with np.load(ck) as z:
+        assert z["done"].tolist() == [0, 1]
+    monkeypatch.setattr(PK._core, "pack_many", fake_pack_many)
+    calls.clear()
+    resumed = bp.pack_many(trays, concurrency=2, checkpoint=ck)
+    assert calls == [2, 1]  # trays 2-4 only
+    calls.clear()
+    again = bp.pack_many(trays, concurrency=2, checkpoint=ck)
+    assert calls == []
+    for a, b, c in zip(full, resumed, again):
+        assert np.array_equal(a.tray, b.tray) and np.array_equal(a.tray, c.tray)
+        assert a.placements == b.placements == c.placements
+        assert (a.num_placed, a.density) == (b.num_placed, b.density)
+    with pytest.raises(ValueError, match="other trays"):
+        bp.pack_many(trays[:4], concurrency=2, checkpoint=ck)
