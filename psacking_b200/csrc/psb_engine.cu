@@ -34,6 +34,17 @@
 #include "psb_filter.cuh"
 #include "psb_proposal.cuh"
 #include "psb_voxel.cuh"
+#include <nvtx3/nvToolsExt.h>
+
+// NVTX range around a C-ABI call, so the engine's calls show on an Nsight
+// Systems timeline next to their kernels; with no tool attached the range
+// calls return at once.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 namespace {
 
@@ -2351,6 +2362,7 @@ int psb_device_count(int* n) {
 }
 
 int psb_dft_conv3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, int32_t* out) {
+    NvtxRange nvtx_range("psb_dft_conv3");
     TRY(check_grid_args(a, nx, ny, nz, "dft_conv3"));
     TRY(check_grid_args(b, nx, ny, nz, "dft_conv3"));
     if (!out) return fail(PSB_ERR_ARG, "dft_conv3: null output");
@@ -2358,6 +2370,7 @@ int psb_dft_conv3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, in
 }
 
 int psb_dft_corr3(const int32_t* a, const int32_t* b, int nx, int ny, int nz, int32_t* out) {
+    NvtxRange nvtx_range("psb_dft_corr3");
     TRY(check_grid_args(a, nx, ny, nz, "dft_corr3"));
     TRY(check_grid_args(b, nx, ny, nz, "dft_corr3"));
     if (!out) return fail(PSB_ERR_ARG, "dft_corr3: null output");
@@ -2488,6 +2501,7 @@ int psb_dft_corr3_noalloc(const int32_t* d_a, const int32_t* d_b, int nx, int ny
 
 int psb_collision_grid(const int32_t* tray, int nx, int ny, int nz, const int32_t* item, int ex, int ey, int ez,
                        int32_t* out) {
+    NvtxRange nvtx_range("psb_collision_grid");
     TRY(check_grid_args(tray, nx, ny, nz, "collision_grid"));
     TRY(check_grid_args(item, ex, ey, ez, "collision_grid"));
     if (ex > nx || ey > ny || ez > nz)
@@ -2515,6 +2529,7 @@ int psb_collision_grid(const int32_t* tray, int nx, int ny, int nz, const int32_
 }
 
 int psb_calculate_distance(const int32_t* grid, int nx, int ny, int nz, int32_t* out) {
+    NvtxRange nvtx_range("psb_calculate_distance");
     TRY(check_grid_args(grid, nx, ny, nz, "calculate_distance"));
     if (!out) return fail(PSB_ERR_ARG, "calculate_distance: null output");
     TRY(ensure_device());
@@ -2532,6 +2547,7 @@ int psb_calculate_distance(const int32_t* grid, int nx, int ny, int nz, int32_t*
 
 int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz, const int32_t* obj, int ex, int ey,
                                     int ez, int32_t* out) {
+    NvtxRange nvtx_range("psb_interlocking_free_positions");
     TRY(check_grid_args(tray, nx, ny, nz, "interlocking_free_positions"));
     TRY(check_grid_args(obj, ex, ey, ez, "interlocking_free_positions"));
     if (ex > nx || ey > ny || ez > nz)
@@ -2601,6 +2617,7 @@ int psb_interlocking_free_positions(const int32_t* tray, int nx, int ny, int nz,
 
 int psb_fft_search_placement(const int32_t* item, int ex, int ey, int ez, const int32_t* tray, int nx, int ny, int nz,
                              psb_result* out) {
+    NvtxRange nvtx_range("psb_fft_search_placement");
     TRY(check_grid_args(item, ex, ey, ez, "fft_search_placement"));
     TRY(check_grid_args(tray, nx, ny, nz, "fft_search_placement"));
     if (!out) return fail(PSB_ERR_ARG, "fft_search_placement: null result");
@@ -2618,6 +2635,7 @@ int psb_fft_search_placement(const int32_t* item, int ex, int ey, int ez, const 
 
 int psb_place_in_tray(const int32_t* item, int ex, int ey, int ez, const int32_t* tray, int nx, int ny, int nz, int px,
                       int py, int pz, int32_t item_id, int32_t* out_tray, int32_t* overlap_ijk) {
+    NvtxRange nvtx_range("psb_place_in_tray");
     TRY(check_grid_args(item, ex, ey, ez, "place_in_tray"));
     TRY(check_grid_args(tray, nx, ny, nz, "place_in_tray"));
     if (!out_tray) return fail(PSB_ERR_ARG, "place_in_tray: null output");
@@ -2707,6 +2725,7 @@ int psb_tray_dims(const psb_tray* t, int* nx, int* ny, int* nz) {
 }
 
 int psb_tray_set(psb_tray* t, const int32_t* tray, const int32_t* phi) {
+    NvtxRange nvtx_range("psb_tray_set");
     if (!t || !tray) return fail(PSB_ERR_ARG, "null pointer");
     return t->set(tray, phi);
 }
@@ -2745,6 +2764,7 @@ int psb_tray_stats(psb_tray* t, long long* occupied, int32_t* lo, int32_t* hi) {
 
 int psb_tray_search(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n, int mode_flags,
                     psb_result* out, psb_result* per_orient) {
+    NvtxRange nvtx_range("psb_tray_search");
     if (!t || !items || !dims || !out || n < 0) return fail(PSB_ERR_ARG, "null pointer");
     if (!t->ready) return fail(PSB_ERR_STATE, "GPU tray context not initialized. Call gpu_tray_init() first.");
     CK(cudaSetDevice(t->dev));
@@ -2769,6 +2789,7 @@ int psb_tray_search(psb_tray* t, const int32_t* const* items, const int32_t* dim
 }
 
 int psb_tray_place(psb_tray* t, const int32_t* item, int ex, int ey, int ez, int px, int py, int pz, int32_t item_id) {
+    NvtxRange nvtx_range("psb_tray_place");
     if (!t || !item) return fail(PSB_ERR_ARG, "null pointer");
     if (!t->ready) return fail(PSB_ERR_STATE, "tray not initialised");
     CK(cudaSetDevice(t->dev));
@@ -2887,6 +2908,7 @@ int stage_upload(psb_tray* t, const int32_t* const* items, int i0, int i1, int p
 extern "C" {
 
 int psb_pack_stage(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items) {
+    NvtxRange nvtx_range("psb_pack_stage");
     if (!t || (!items && n_items > 0) || !dims || n_items < 0) return fail(PSB_ERR_ARG, "null pointer");
     CK(cudaSetDevice(t->dev));
     t->staged.clear();
@@ -2933,11 +2955,13 @@ extern "C" {
 
 int psb_pack_staged(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                     psb_result* out_placements, int32_t* final_tray) {
+    NvtxRange nvtx_range("psb_pack_staged");
     return pack_staged_impl(t, orient_maps, n_orient, interlock, id_offset, out_placements, final_tray, PackOpts());
 }
 
 int psb_pack_staged_detail(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                            psb_result* out_placements, int32_t* final_tray, psb_result* per_orient, float* hmaps) {
+    NvtxRange nvtx_range("psb_pack_staged_detail");
     PackOpts o;
     o.per_orient = per_orient;
     o.hmaps = hmaps;
@@ -2947,6 +2971,7 @@ int psb_pack_staged_detail(psb_tray* t, const int32_t* orient_maps, int n_orient
 int psb_pack_staged_sharded(psb_tray* t, const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
                             int rank, int world, void* d_local, void* d_all, psb_exchange_fn exchange, void* ctx,
                             psb_result* out_placements, int32_t* final_tray) {
+    NvtxRange nvtx_range("psb_pack_staged_sharded");
     if (world < 1 || rank < 0 || rank >= world) return fail(PSB_ERR_ARG, "bad rank %d of world %d", rank, world);
     if (!d_local || !d_all) return fail(PSB_ERR_ARG, "sharded packing needs the decision buffers");
     if (world > 1 && !exchange) return fail(PSB_ERR_ARG, "sharded packing over %d ranks needs an exchange", world);
@@ -2963,6 +2988,7 @@ int psb_pack_staged_sharded(psb_tray* t, const int32_t* orient_maps, int n_orien
 int psb_pack_staged_prop(psb_tray* t, psb_proposal* prop, const int32_t* orient_maps, int n_orient, int interlock,
                          int32_t id_offset, int topk, float margin, psb_result* out_placements, int32_t* final_tray,
                          int32_t* gate_stats) {
+    NvtxRange nvtx_range("psb_pack_staged_prop");
     if (!prop) return fail(PSB_ERR_ARG, "pack_staged_prop: null proposal");
     if (n_orient != PSB_PNO) return fail(PSB_ERR_ARG, "the proposal network ranks exactly %d orientations", PSB_PNO);
     if (topk < 1) return fail(PSB_ERR_ARG, "topk must be >= 1");
@@ -3370,6 +3396,7 @@ extern "C" {
 
 int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int n_items, const int32_t* orient_maps,
              int n_orient, int interlock, int32_t id_offset, psb_result* out_placements, int32_t* final_tray) {
+    NvtxRange nvtx_range("psb_pack");
     const int first = kStreamFirst;
     if (!g_stream_stage || n_items < 2 * first || !t || !items || !dims || !t->ready) {
         TRY(psb_pack_stage(t, items, dims, n_items));
@@ -3408,6 +3435,7 @@ int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int 
 int psb_pack_many(int n_trays, const int32_t* tray_dims, const int32_t* const* items, const int32_t* item_dims,
                   const int32_t* items_per_tray, const int32_t* orient_maps, int n_orient, int interlock,
                   int concurrency, psb_result* out_placements, int32_t* const* final_trays) {
+    NvtxRange nvtx_range("psb_pack_many");
     if (n_trays < 0 || !tray_dims || !items_per_tray || !orient_maps || !out_placements)
         return fail(PSB_ERR_ARG, "pack_many: null pointer");
     TRY(ensure_device());
@@ -3602,6 +3630,7 @@ int psb_height_map(const int32_t* d_tray, int nx, int ny, int nz, float* d_out) 
 // mesh voxelizer (voxelize_stl: bindings.cpp:285-302, packing.cpp:540-588)
 // ---------------------------------------------------------------------------
 int psb_voxelize_mesh(const float* tris, int ntri, int resolution, int32_t* out, int32_t* dims_out) {
+    NvtxRange nvtx_range("psb_voxelize_mesh");
     if (!tris || !out || !dims_out || ntri <= 0 || resolution <= 0)
         return fail(PSB_ERR_ARG, "voxelize: null pointer, no triangles or bad resolution");
     TRY(ensure_device());
