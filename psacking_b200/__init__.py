@@ -53,6 +53,15 @@ from .vox import save_vox  # noqa: E402
 __version__ = _core.__version__
 
 
+def is_cuda_available() -> bool:
+    """spectral_packer.is_cuda_available (__init__.py:163-172 of the
+    reference), which is always True there because its module imports only
+    with CUDA support.  Here the extension also imports on a machine without
+    a GPU (its calls then raise), so this reports whether a CUDA device is
+    visible to the engine."""
+    return _core.device_count() > 0
+
+
 def voxelize_stl(path, resolution: int = VOXEL_RESOLUTION):
     """The reference's mesh voxelizer (bindings.cpp:285-302): surface voxels
     of a binary or ASCII STL mesh, tight int32 grid (psacking_b200.voxelize)."""
@@ -61,7 +70,7 @@ def voxelize_stl(path, resolution: int = VOXEL_RESOLUTION):
 
 
 __all__ = [
-    "__version__", "BinPacker", "PackingResult", "PlacementInfo", "HEIGHT_PENALTY", "VOXEL_RESOLUTION",
+    "__version__", "is_cuda_available", "BinPacker", "PackingResult", "PlacementInfo", "HEIGHT_PENALTY", "VOXEL_RESOLUTION",
     "calculate_distance", "collision_grid", "dft_conv3", "dft_corr3", "fft_search_batch",
     "fft_search_batch_interlocking_free", "fft_search_placement", "fft_search_placement_with_cache",
     "get_bounds", "gpu_tray_cleanup", "gpu_tray_init", "gpu_tray_is_initialized", "gpu_tray_search",

@@ -124,3 +124,8 @@ def test_context_calls_from_threads_are_serialised(core):
     assert sorted(done) == [0, 1, 2, 3]
     assert len(errors) == 4 * 20 * 5
     assert not core.gpu_tray_is_initialized()
+
+
+def test_is_cuda_available_reports_the_device(core):
+    import psacking_b200 as p
+    assert p.is_cuda_available() == (core.device_count() > 0)
