@@ -129,3 +129,33 @@ def test_context_calls_from_threads_are_serialised(core):
 def test_is_cuda_available_reports_the_device(core):
     import psacking_b200 as p
     assert p.is_cuda_available() == (core.device_count() > 0)
+
+
+def test_product_never_reaches_the_oracle():
+    """The oracle is test infrastructure only: no module of the package
+    imports it, no native source includes or links anything under oracle/,
+    and importing the whole package (every module) leaves it unloaded."""
+    import ast
+    import subprocess
+    import sys
+    pkg = ROOT / "psacking_b200"
+    for py in pkg.rglob("*.py"):
+        tree = ast.parse(py.read_text())
+        for node in ast.walk(tree):
+            names = []
+            if isinstance(node, ast.Import):
+                names = [a.name for a in node.names]
+            elif isinstance(node, ast.ImportFrom) and node.level == 0:
+                names = [node.module or ""]
+            assert not any(n.split(".")[0] == "oracle" for n in names), (py, names)
+    for src in list((pkg / "csrc").iterdir()) + [pkg / "build.py"]:
+        text = src.read_text()
+        assert "oracle/" not in text and '"oracle' not in text, src
+    mods = sorted(p.stem for p in pkg.glob("*.py") if p.stem != "__init__")
+    code = ("import importlib, sys, psacking_b200\n"
+            f"for m in {mods!r}:\n"
+            "    importlib.import_module('psacking_b200.' + m)\n"
+            "print(sorted(k for k in sys.modules if k.split('.')[0] == 'oracle'))\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "[]"
