@@ -69,7 +69,8 @@ typedef struct psb_result {
 
 typedef struct psb_tray psb_tray;   /* a device-resident tray (GPUTrayContext) */
 
-/* ---- library ------------------------------------------------------------ */
+/* ---- library (no counterpart in the reference: its pybind11 module prints
+ *      CUDA errors, fft3.cu:59-91, and raises Python exceptions) --------- */
 const char* psb_version(void);
 /* Copies the calling thread's last error message into buf (NUL-terminated). */
 int psb_last_error(char* buf, size_t len);
@@ -192,7 +193,8 @@ int psb_pack(psb_tray* t, const int32_t* const* items, const int32_t* dims, int 
              const int32_t* orient_maps, int n_orient, int interlock, int32_t id_offset,
              psb_result* out_placements, int32_t* final_tray);
 
-/* psb_pack split in two: stage the items of a run on the device once (their
+/* psb_pack split in two (the same loop, packer.py:447-528): stage the items
+ * of a run on the device once (their
  * runs, bounds and filter samples are computed here), then run the greedy
  * loop over the staged items.  psb_pack gives the same results as
  * psb_pack_stage + psb_pack_staged; with 64 items or more it stages the
@@ -237,6 +239,7 @@ int psb_pack_staged_detail(psb_tray* t, const int32_t* orient_maps, int n_orient
                            int32_t id_offset, psb_result* out_placements, int32_t* final_tray,
                            psb_result* per_orient, float* hmaps);
 
+/* ---- learned orientation proposal (no counterpart in the reference) ---- */
 typedef struct psb_proposal psb_proposal;   /* network weights and work buffers on one GPU */
 int psb_prop_create(psb_proposal** out);
 int psb_prop_destroy(psb_proposal* p);
@@ -287,7 +290,8 @@ int psb_pack_staged_prop(psb_tray* t, psb_proposal* prop, const int32_t* orient_
  * 32-bit int products wrap (packing.cpp rasterize).                        */
 int psb_voxelize_mesh(const float* tris, int ntri, int resolution, int32_t* out, int32_t* dims_out);
 
-/* Kernel variant switch (default on): FFT lengths 64, 100, 128, 240 use
+/* ---- engine settings (no counterpart in the reference) ------------------
+ * Kernel variant switch (default on): FFT lengths 64, 100, 128, 240 use
  * the specialised two-pass kernels; off forces the generic mixed-radix path
  * (used by the tests to check both). */
 int psb_set_fast_fft(int on);
@@ -345,7 +349,8 @@ int psb_debug_live_allocs(long long* n);
  * reference. */
 int psb_set_share_flips(int on);
 
-/* Many independent trays (the many-tray form of the benchmark set): tray i
+/* Many independent trays (the many-tray form of the benchmark set; no
+ * counterpart in the reference, which packs one tray per call): tray i
  * has dims tray_dims[3i..3i+2] and items_per_tray[i] items, which follow the
  * previous trays' items in `items` / `item_dims` and are already in packing
  * order.  Each tray starts empty and is packed exactly as psb_pack would;
@@ -364,7 +369,8 @@ int psb_profile_enable(int on);          /* clears previous records            *
  * names, e.g. "k_plane,k_xpass"); NULL or "" records every kernel. */
 int psb_profile_filter(const char* names);
 int psb_profile_report(char* buf, size_t len);
-/* FFT grid of a tray (F[0..2] >= nx, ny, nz; 2^a 3^b 5^c 7^d). */
+/* ---- tray introspection for the benchmark (no counterpart in the reference)
+ * FFT grid of a tray (F[0..2] >= nx, ny, nz; 2^a 3^b 5^c 7^d). */
 int psb_tray_fft_dims(const psb_tray* t, int* F);
 /* The CUDA stream (cudaStream_t) a tray's kernels run on. */
 int psb_tray_stream(psb_tray* t, void** stream);

@@ -159,3 +159,21 @@ def test_product_never_reaches_the_oracle():
     r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip().splitlines()[-1] == "[]"
+
+
+def test_header_cites_each_entry_point():
+    """Every declaration in include/psb200.h sits under a comment that
+    cites the reference interface it replaces (file:line) or says that it
+    has no counterpart in the reference."""
+    text = HEADER.read_text()
+    decls = list(re.finditer(r"^(?:int|void|const char\*)\s+(psb_[a-z0-9_]+)\(", text, re.M))
+    assert len(decls) >= 50
+    prev, section, missing = 0, "", []
+    for m in decls:
+        chunk = text[prev:m.start()]
+        prev = m.end()
+        if "/* ----" in chunk:
+            section = chunk[chunk.rfind("/* ----"):]
+        if not re.search(r"\.(cpp|cu|py|h):\d|counterpart|[Rr]eplaces", chunk + section):
+            missing.append(m.group(1))
+    assert not missing, missing
